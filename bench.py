@@ -1,0 +1,472 @@
+"""Benchmark of the B200 voxel-editing path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the primitives sweep): exclusive scan of 2^28 u32 values in
+[0, 255]; stable radix sort of 2^28 u32 keys (uniform) with a u32 payload =
+index; stable radix sort of 2^28 u64 Morton keys (20 bits per axis, 64
+Gaussian blobs with sigma 2^14 in a 2^20 cube) with payload = index.  One
+step runs all three on a fresh copy of the inputs (every step has its own
+input buffers, each larger than the 126 MB L2, so no step reads another's data
+from cache).  The value is algorithmic bytes moved (scan 8 B/elem, u32 sort
+68 B/elem, u64 sort 200 B/elem) per second of device time.
+
+Multi-GPU: every rank runs the same sweep on its own inputs (independent
+replicas, weak scaling); the timed region is bracketed by barriers and the
+maximum over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("Hash DAG voxels edited/s batched vs plain (bit-exact); "
+          "sort/scan GB/s; p99 ms")
+N_SCAN = 1 << 28
+N_SORT = 1 << 28
+BYTES_SCAN = 8          # read 4 + write 4 per element
+BYTES_SORT_U32 = 68     # 4 passes x (read 8 + write 8) + 4 histogram read
+BYTES_SORT_U64 = 200    # 8 passes x (read 12 + write 12) + 8 histogram read
+# Per-launch algorithmic bytes of the dominant kernel (one u64 partition
+# pass: read key 8 + value 4, write key 8 + value 4 per element).
+PART_U64_BYTES = N_SORT * 24
+# DRAM bytes per sort_partition_u64 launch from ncu (profiles/), scaled to
+# 2^28 elements; None until a capture is committed.
+PART_U64_TRAFFIC = None
+
+
+# --------------------------------------------------------------- helpers --
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}",
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------ workloads --
+
+def make_inputs(torch, device, seed_base=0):
+    """Device-resident inputs of one step (generated on the GPU)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(2 + seed_base)
+    scan = torch.randint(0, 256, (N_SCAN,), dtype=torch.int32, device=device,
+                         generator=g)
+    g.manual_seed(3 + seed_base)
+    k32 = torch.randint(-2**31, 2**31, (N_SORT,), dtype=torch.int32,
+                        device=device, generator=g)
+    k64 = morton_keys(torch, device, N_SORT, 4 + seed_base)
+    return scan, k32, k64
+
+
+def morton_keys(torch, device, n, seed):
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    centers = torch.randint(0, 1 << 20, (64, 3), dtype=torch.int64,
+                            device=device, generator=g)
+    key = torch.zeros(n, dtype=torch.int64, device=device)
+    chunk = 1 << 25
+    for s in range(0, n, chunk):
+        m = min(chunk, n - s)
+        idx = torch.randint(0, 64, (m,), device=device, generator=g)
+        pts = centers[idx] + (torch.randn(m, 3, device=device, generator=g)
+                              * float(1 << 14)).round().to(torch.int64)
+        pts = pts.clamp_(0, (1 << 20) - 1)
+        k = torch.zeros(m, dtype=torch.int64, device=device)
+        for b in range(20):
+            for a in range(3):
+                k |= ((pts[:, a] >> b) & 1) << (3 * b + a)
+        key[s:s + m] = k
+    return key
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import voxel_b200 as vx
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = vx.lib()
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    steps, warm = args.steps, args.warmup
+    base_scan, base_k32, base_k64 = make_inputs(torch, device, seed_base=rank * 10)
+    vals = torch.arange(N_SORT, dtype=torch.int32, device=device)
+    bufs = []
+    for _ in range(steps + warm):
+        bufs.append((base_scan.clone(), base_k32.clone(), vals.clone(),
+                     base_k64.clone(), vals.clone()))
+    ws_scan = torch.empty(lib.vx_scan_workspace_size(N_SCAN), dtype=torch.uint8, device=device)
+    ws_sort = torch.empty(lib.vx_sort_workspace_size(N_SORT, 8), dtype=torch.uint8, device=device)
+    torch.cuda.synchronize()
+
+    def step(b):
+        scan, k32, v32, k64, v64 = b
+        vx.exclusive_sum(scan, ws_scan)
+        vx.sort_pairs(k32, v32, 32, ws_sort)
+        vx.sort_pairs(k64, v64, 60, ws_sort)
+
+    for i in range(warm):
+        step(bufs[i])
+    torch.cuda.synchronize()
+
+    # Per-component times (events around each op) and the whole step.
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    lib.vx_profile_reset()
+    lib.vx_profile_enable(1)
+    launches0 = lib.vx_profile_launches()
+    stream = torch.cuda.current_stream()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+          for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(steps):
+            scan, k32, v32, k64, v64 = bufs[warm + i]
+            ev[i][0].record(stream)
+            vx.exclusive_sum(scan, ws_scan)
+            ev[i][1].record(stream)
+            vx.sort_pairs(k32, v32, 32, ws_sort)
+            ev[i][2].record(stream)
+            vx.sort_pairs(k64, v64, 60, ws_sort)
+            ev[i][3].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = lib.vx_profile_launches() - launches0
+    lib.vx_profile_enable(0)
+    total_ms = t0.elapsed_time(t1)
+    scan_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    s32_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    s64_ms = sum(e[2].elapsed_time(e[3]) for e in ev)
+    part_ms = _prof(lib, "sort_partition_u64")
+
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # correctness spot check of the timed outputs (cheap, device-side)
+    scan, k32, v32, k64, v64 = bufs[warm]
+    ok = bool(((k64[1:] >= k64[:-1]) | (k64[1:] < 0) | (k64[:-1] < 0)).all()) and \
+        bool((k32[1:].to(torch.int64) & 0xFFFFFFFF >= k32[:-1].to(torch.int64) & 0xFFFFFFFF).all())
+
+    bytes_step = N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+    value = ws * bytes_step * steps / (total_ms / 1e3) / 1e9
+    del bufs
+    torch.cuda.empty_cache()
+
+    e2e = run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals,
+                  ws_scan, ws_sort, max(1, min(steps, 3)), ws)
+    hbm, kind = peaks()
+    part_n, part_total = part_ms
+    achieved = PART_U64_BYTES / (part_total / part_n / 1e3) / 1e9 if part_n else None
+    result = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": ws,
+        "steps": steps,
+        "warmup": warm,
+        "ms_per_step": round(total_ms / steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32/u64",
+        "data": "synthetic (seeded on device: uniform u32, clustered Morton u64)",
+        "config": {
+            "workload": "primitives sweep: exclusive scan 2^28 u32 in [0,255]; "
+                        "stable sort 2^28 u32 keys + u32 index payload; "
+                        "stable sort 2^28 u64 60-bit Morton keys (64 Gaussian "
+                        "blobs, sigma 2^14, 2^20 cube) + u32 index payload",
+            "elements": N_SORT,
+            "l2_policy": "inputs larger than L2 (fresh 1-3 GB buffers per step)",
+            "parallelism": f"replicas x{ws}",
+        },
+        "components": {
+            "scan_u32_GBps": round(N_SCAN * BYTES_SCAN * steps / scan_ms / 1e6, 1),
+            "sort_u32_GBps": round(N_SORT * BYTES_SORT_U32 * steps / s32_ms / 1e6, 1),
+            "sort_u64_GBps": round(N_SORT * BYTES_SORT_U64 * steps / s64_ms / 1e6, 1),
+            "scan_u32_ms": round(scan_ms / steps, 3),
+            "sort_u32_ms": round(s32_ms / steps, 3),
+            "sort_u64_ms": round(s64_ms / steps, 3),
+            "sort_u32_Gkeys_per_s": round(N_SORT * steps / s32_ms / 1e6, 3),
+            "sort_u64_Gkeys_per_s": round(N_SORT * steps / s64_ms / 1e6, 3),
+        },
+        "roofline": {
+            "kernel": "sort_partition_u64",
+            "bound": "hbm",
+            "achieved": round(achieved, 1) if achieved else None,
+            "peak": hbm,
+            "peak_kind": kind,
+            "unit": "GB/s",
+            "frac": round(achieved / hbm, 3) if achieved else None,
+            "traffic": PART_U64_TRAFFIC,
+            "algorithmic_bytes_per_launch": PART_U64_BYTES,
+            "launches": part_n,
+        },
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "outputs_sorted": ok,
+    }
+    if rank == 0:
+        result["cpu_baseline"] = cpu_baseline()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return result
+
+
+def _prof(lib, name):
+    import ctypes as C
+    ms = C.c_double(0)
+    n = C.c_uint64(0)
+    lib.vx_profile_query(name.encode(), C.byref(ms), C.byref(n))
+    return n.value, ms.value
+
+
+def run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals, ws_scan,
+            ws_sort, steps, world):
+    """Same sweep through the public API with host inputs: every step copies
+    its inputs from pinned host memory and reads every result back."""
+    h_scan = base_scan.cpu().pin_memory()
+    h_k32 = base_k32.cpu().pin_memory()
+    h_k64 = base_k64.cpu().pin_memory()
+    h_vals = vals.cpu().pin_memory()
+    outs = [torch.empty_like(t).pin_memory() for t in (h_scan, h_k32, h_vals, h_k64, h_vals)]
+    d = [torch.empty_like(t, device=device) for t in (h_scan, h_k32, h_vals, h_k64, h_vals)]
+    stream = torch.cuda.current_stream()
+    h2d = sum(t.numel() * t.element_size() for t in (h_scan, h_k32, h_vals, h_k64, h_vals))
+
+    def one():
+        for dst, src in zip(d, (h_scan, h_k32, h_vals, h_k64, h_vals)):
+            dst.copy_(src, non_blocking=True)
+        vx.exclusive_sum(d[0], ws_scan)
+        vx.sort_pairs(d[1], d[2], 32, ws_sort)
+        vx.sort_pairs(d[3], d[4], 60, ws_sort)
+        for o, s in zip(outs, d):
+            o.copy_(s, non_blocking=True)
+
+    one()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        one()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    bytes_step = N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+    return {"value": round(world * bytes_step * steps / (ms / 1e3) / 1e9, 2),
+            "unit": "GB/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": h2d, "ms_per_step": round(ms / steps, 2)}
+
+
+def cpu_baseline(sample_log2=24):
+    """Oracle port on all host threads over a 2^24-element sample of each
+    component, reported in the same algorithmic GB/s."""
+    import oracle
+    threads = os.cpu_count() or 1
+    n = 1 << sample_log2
+    rng = np.random.default_rng(2)
+    x = rng.integers(0, 256, n, dtype=np.uint32)
+    out = np.empty_like(x)
+    k32 = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    k64 = rng.integers(0, 2**60, n, dtype=np.uint64)
+    v = np.arange(n, dtype=np.uint32)
+    L = oracle.lib()
+    t = time.perf_counter()
+    L.orc_exclusive_scan_u32_mt(x.ctypes.data, out.ctypes.data, n, threads)
+    t_scan = time.perf_counter() - t
+    kk, vv = k32.copy(), v.copy()
+    t = time.perf_counter()
+    L.orc_radix_sort_pairs_u32_mt(kk.ctypes.data, vv.ctypes.data, n, 32, threads)
+    t_s32 = time.perf_counter() - t
+    kk, vv = k64.copy(), v.copy()
+    t = time.perf_counter()
+    L.orc_radix_sort_pairs_u64_mt(kk.ctypes.data, vv.ctypes.data, n, 60, threads)
+    t_s64 = time.perf_counter() - t
+    total_b = n * (BYTES_SCAN + BYTES_SORT_U32 + BYTES_SORT_U64)
+    return {"value": round(total_b / (t_scan + t_s32 + t_s64) / 1e9, 3),
+            "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"2^{sample_log2} elements per component (scan u32, "
+                      f"sort u32, sort u64 60-bit) on {threads} host threads",
+            "seconds": round(t_scan + t_s32 + t_s64, 3)}
+
+
+def run_reference(args, ws, rank):
+    """The reference has no CPU scan or sort (its benches compare GPU kernels
+    with CUB), so the reference arm times this project's oracle port of the
+    same operations on all host threads: each step is a 2^24-element sample."""
+    if rank != 0:
+        return None
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline())
+    v = statistics.median(x["value"] for x in vals)
+    base = vals[0]
+    return {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(statistics.median(x["seconds"] for x in vals) * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/u64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "primitives sweep (CPU sample)",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": base["cores"],
+                             "kind": "port", "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_case(args):
+    """One operation on a small input, for profiler captures:
+    --case scan|sort_u32|sort_u64 --elements N (runs --steps launches)."""
+    import torch
+    import voxel_b200 as vx
+    dev = torch.device("cuda:0")
+    n = args.elements
+    ms = []
+    for _ in range(args.steps):
+        if args.case == "scan":
+            x = torch.randint(0, 256, (n,), dtype=torch.int32, device=dev)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            vx.exclusive_sum(x)
+        elif args.case == "sort_u32":
+            k = torch.randint(-2**31, 2**31, (n,), dtype=torch.int32, device=dev)
+            v = torch.arange(n, dtype=torch.int32, device=dev)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            vx.sort_pairs(k, v, 32)
+        else:
+            k = morton_keys(torch, dev, n, 4)
+            v = torch.arange(n, dtype=torch.int32, device=dev)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            vx.sort_pairs(k, v, 60)
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t) * 1e3)
+    print(json.dumps({"case": args.case, "elements": n, "ms": ms}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64"], default=None)
+    ap.add_argument("--elements", type=int, default=1 << 24)
+    args = ap.parse_args()
+    if args.case is not None:
+        run_case(args)
+        return
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        res = run_reference(args, ws, rank)
+    else:
+        if args.warmup < 3:
+            args.warmup = 3
+        res = run_ours(args, ws, rank, local)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,106 @@
+/*
+ * voxel_b200.h - C ABI of the B200-native voxel-editing library.
+ *
+ * The reference (yamaatsu1112/voxel, algorithm/lib/include/algo) is a
+ * header-only C++/CUDA template library whose entry points all have the shape
+ *
+ *     cudaError_t f(View, const T* in, uint32_t count,
+ *                   void* workspace, size_t workspace_size, cudaStream_t)
+ *     size_t      f_workspace_size(uint32_t count)
+ *
+ * This header exposes the same contract as plain C: device pointers, counts,
+ * a caller-owned workspace whose size depends only on the count, a stream, and
+ * a status code.  Status values 0..999 are cudaError_t values (0 = success,
+ * 1 = cudaErrorInvalidValue, 2 = cudaErrorMemoryAllocation, ...); values from
+ * 1000 up are this library's own.  No C++ exception crosses this boundary.
+ * Every pointer is a device pointer unless its name starts with host_.
+ * Every call is stream-ordered and asynchronous unless documented otherwise.
+ *
+ * Each declaration names the reference interface it replaces (file:line,
+ * relative to algorithm/lib/include/algo/).
+ */
+#ifndef VOXEL_B200_H
+#define VOXEL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "vx_workload.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t vx_status;
+typedef void *vx_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+#define VX_OK 0
+#define VX_ERR_INVALID_VALUE 1      /* == cudaErrorInvalidValue */
+#define VX_ERR_MEMORY_ALLOCATION 2  /* == cudaErrorMemoryAllocation */
+#define VX_ERR_TIMEOUT 1001         /* a bounded device wait gave up */
+#define VX_ERR_CAPACITY 1002        /* a node pool / table / arena is full */
+#define VX_ERR_NO_DEVICE 1003       /* no CUDA device is visible */
+
+/* Library version and a human-readable name for a status code. */
+uint32_t vx_version(void);
+const char *vx_status_string(vx_status status);
+
+/* Scan and sort calls are fully asynchronous; a bounded device wait that gave
+ * up is recorded in their workspace.  This synchronises the stream and returns
+ * VX_OK or VX_ERR_TIMEOUT for the last call that used the workspace. */
+vx_status vx_workspace_status(const void *workspace, vx_stream stream);
+
+/* Built-in per-kernel timing (off by default): when enabled, every kernel
+ * launch of the library is bracketed by a CUDA event pair on its stream;
+ * vx_profile_query sums the elapsed milliseconds and launches per kernel name
+ * since the last reset (it synchronises on those events). */
+void vx_profile_enable(uint32_t on);
+void vx_profile_reset(void);
+/* Number of kernels the library has launched in this process. */
+uint64_t vx_profile_launches(void);
+vx_status vx_profile_query(const char *name, double *host_total_ms,
+                           uint64_t *host_launches);
+
+/* ------------------------------------------------------------------ scan --
+ * In-place prefix sums over uint32 / uint64 with modular (wrapping)
+ * arithmetic.  Replaces algo::cuda::scan::{exclusive,inclusive}_sum<T> and
+ * required_workspace_size<T> (cuda/scan/scan.cuh:107-161, defaults at
+ * cuda/scan/scan.cuh:18-19) with a single-pass decoupled look-back scan.
+ * count == 0 is a no-op; data == NULL with count > 0, or a NULL/short
+ * workspace, returns VX_ERR_INVALID_VALUE (docs/cuda/scan.md).
+ * A look-back wait that exceeds its iteration bound returns VX_ERR_TIMEOUT. */
+size_t vx_scan_workspace_size(uint32_t count);
+vx_status vx_scan_exclusive_sum_u32(uint32_t *data, uint32_t count,
+                                    void *workspace, size_t workspace_bytes,
+                                    vx_stream stream);
+vx_status vx_scan_inclusive_sum_u32(uint32_t *data, uint32_t count,
+                                    void *workspace, size_t workspace_bytes,
+                                    vx_stream stream);
+vx_status vx_scan_exclusive_sum_u64(uint64_t *data, uint32_t count,
+                                    void *workspace, size_t workspace_bytes,
+                                    vx_stream stream);
+
+/* ------------------------------------------------------------------ sort --
+ * Stable LSD radix sort ("onesweep": one all-pass digit histogram, then one
+ * partition kernel per 8-bit digit with decoupled look-back), in place.
+ * Only the low key_bits bits of each key order the output (key_bits in
+ * [1, 32] for u32 keys, [1, 64] for u64 keys), matching the KeyBits contract
+ * of algo::cuda::sort::RadixSort (docs/cuda/sort.md "Configuration").
+ * Replaces sort::sort_keys / sort::sort_by_key with one value array and
+ * required_sort_by_key_workspace_size (cuda/sort/sort.cuh:100-167,
+ * cuda/sort/radix/onesweep/host.cuh:135-204).  values may be NULL for a
+ * key-only sort.  count <= 1 needs no workspace; count must be < 2^30
+ * (the reference's onesweep bound, cuda/sort/radix/onesweep/host.cuh:85-86). */
+size_t vx_sort_workspace_size(uint32_t count, uint32_t key_bytes);
+vx_status vx_sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t count,
+                            uint32_t key_bits, void *workspace,
+                            size_t workspace_bytes, vx_stream stream);
+vx_status vx_sort_pairs_u64(uint64_t *keys, uint32_t *values, uint32_t count,
+                            uint32_t key_bits, void *workspace,
+                            size_t workspace_bytes, vx_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOXEL_B200_H */

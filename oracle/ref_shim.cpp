@@ -1,0 +1,229 @@
+// ORACLE - test infrastructure only.  A thin C shim over the reference's own
+// CPU implementations, compiled from the reference headers where they lie
+// (algorithm/lib/include/algo/svt/hash_dag.hpp and svo.hpp); see build.py.
+// It exists to pin this project's oracle and to time the reference's CPU path
+// as a baseline.  Nothing here is part of the product.
+//
+// The canonical dumps below read the reference objects' internal node stores,
+// so the shim opens their private members to this translation unit only.
+#include <cstdint>
+#include <unordered_map>
+#include <vector>
+
+#define private public
+#include <algo/svt/hash_dag.hpp>
+#include <algo/svt/svo.hpp>
+#undef private
+
+using u32 = std::uint32_t;
+using u64 = std::uint64_t;
+using algo::svt::HashDAG;
+using algo::svt::SVO;
+
+namespace {
+
+// DFS first-visit canonical form of a HashDAG (children 0..7): per inner level
+// 10 words per node [child_mask, fill_mask, id x 8] where id 0 = empty,
+// 1 = full, k + 2 = node k of the next level; leaves as u64 masks.  Full
+// subtrees (HashDAG::full_node_ptrs_, full_leaf_ptr_, hash_dag.hpp:329-341)
+// become id 1.
+struct DagDump {
+  const HashDAG &dag;
+  std::vector<std::unordered_map<u32, u32>> ids;
+  std::vector<std::vector<u32>> nodes;
+  std::vector<u64> leaves;
+
+  explicit DagDump(const HashDAG &d)
+      : dag(d), ids(d.depth_ + 1), nodes(d.depth_) {}
+
+  bool is_full(u32 level, u32 ptr) const {
+    if (level == dag.depth_) return ptr == dag.full_leaf_ptr_;
+    return ptr == dag.full_node_ptrs_[level];
+  }
+
+  u32 visit(u32 level, u32 ptr) {
+    if (ptr == 0) return 0;
+    if (is_full(level, ptr)) return 1;
+    auto it = ids[level].find(ptr);
+    if (it != ids[level].end()) return it->second + 2;
+    if (level == dag.depth_) {
+      const u32 id = static_cast<u32>(leaves.size());
+      ids[level][ptr] = id;
+      leaves.push_back(dag.read_leaf(ptr));
+      return id + 2;
+    }
+    const u32 id = static_cast<u32>(nodes[level].size() / 10);
+    ids[level][ptr] = id;
+    nodes[level].resize(nodes[level].size() + 10, 0);
+    const auto node = dag.read_node(ptr);
+    u32 rec[10] = {0};
+    for (u32 c = 0; c < 8; ++c) {
+      u32 child = 0;
+      if (node.child_mask & (1u << c)) child = visit(level + 1, node.child_ptrs[c]);
+      rec[2 + c] = child;
+      if (child == 1) rec[1] |= 1u << c;
+      if (child >= 2) rec[0] |= 1u << c;
+    }
+    for (u32 w = 0; w < 10; ++w) nodes[level][id * 10 + w] = rec[w];
+    return id + 2;
+  }
+};
+
+// DFS pre-order canonical form of an SVO: node ids in first-visit order (root
+// = 0), leaf ids in first-visit order, child words keep bits 30/31 and carry
+// the canonical index (svo.hpp:19-91, CHILD_* constants at svo.hpp:11-16).
+struct SvoDump {
+  const SVO &svo;
+  std::vector<u32> nodes;
+  std::vector<u64> leaves;
+
+  explicit SvoDump(const SVO &s) : svo(s) {}
+
+  u32 visit(u32 index, u32 depth) {
+    const u32 id = static_cast<u32>(nodes.size() / 8);
+    nodes.resize(nodes.size() + 8, 0);
+    const auto &node = svo.nodes_[index];
+    u32 rec[8];
+    for (u32 c = 0; c < 8; ++c) {
+      const u32 info = node.child_info[c].info;
+      if (info & algo::svt::CHILD_MASK_BIT) {
+        const u32 child = info & algo::svt::CHILD_INDEX_MASK;
+        u32 cid;
+        if (depth + 1 < svo.max_depth_) {
+          cid = visit(child, depth + 1);
+        } else {
+          cid = static_cast<u32>(leaves.size());
+          leaves.push_back(svo.leaves_[child].voxel_data);
+        }
+        rec[c] = (info & ~algo::svt::CHILD_INDEX_MASK) | cid;
+      } else {
+        rec[c] = info;
+      }
+    }
+    for (u32 c = 0; c < 8; ++c) nodes[id * 8 + c] = rec[c];
+    return id;
+  }
+};
+
+} // namespace
+
+extern "C" {
+
+void *ref_dag_new(u32 depth) {
+  try {
+    return new HashDAG(depth);
+  } catch (...) {
+    return nullptr;
+  }
+}
+void ref_dag_free(void *h) { delete static_cast<HashDAG *>(h); }
+
+// Boxes are half-open [min, max) like HashDAG::Box (hash_dag.hpp:22-29).
+int ref_dag_edit_box(void *h, u32 x0, u32 y0, u32 z0, u32 x1, u32 y1, u32 z1,
+                     int fill) {
+  try {
+    HashDAG::Box b{x0, y0, z0, x1, y1, z1};
+    auto *d = static_cast<HashDAG *>(h);
+    if (fill) d->fill_box(b);
+    else d->clear_box(b);
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int ref_dag_set_voxel(void *h, u32 x, u32 y, u32 z, int value) {
+  try {
+    static_cast<HashDAG *>(h)->set_voxel(x, y, z, value != 0);
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int ref_dag_get_voxel(void *h, u32 x, u32 y, u32 z) {
+  try {
+    return static_cast<HashDAG *>(h)->get_voxel(x, y, z) ? 1 : 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
+u64 ref_dag_node_count(void *h) { return static_cast<HashDAG *>(h)->node_count(); }
+
+// Canonical dump; arrays may be NULL to query sizes.  counts has depth + 1
+// entries (nodes per inner level, then leaves).
+int ref_dag_export(void *h, u32 *root, u64 *counts, u32 *nodes, u64 cap_words,
+                   u64 *leaves, u64 cap_leaves) {
+  const HashDAG &d = *static_cast<HashDAG *>(h);
+  DagDump dump(d);
+  const u32 r = dump.visit(0, d.root_);
+  if (root) *root = r;
+  u64 words = 0;
+  for (u32 l = 0; l < d.depth_; ++l) {
+    if (counts) counts[l] = dump.nodes[l].size() / 10;
+    words += dump.nodes[l].size();
+  }
+  if (counts) counts[d.depth_] = dump.leaves.size();
+  if (nodes) {
+    if (words > cap_words) return 2;
+    u64 o = 0;
+    for (u32 l = 0; l < d.depth_; ++l)
+      for (u32 w : dump.nodes[l]) nodes[o++] = w;
+  }
+  if (leaves) {
+    if (dump.leaves.size() > cap_leaves) return 2;
+    for (u64 i = 0; i < dump.leaves.size(); ++i) leaves[i] = dump.leaves[i];
+  }
+  return 0;
+}
+
+void *ref_svo_new(u32 depth) {
+  try {
+    return new SVO(depth);
+  } catch (...) {
+    return nullptr;
+  }
+}
+void ref_svo_free(void *h) { delete static_cast<SVO *>(h); }
+
+int ref_svo_set_voxel(void *h, u32 x, u32 y, u32 z, int value) {
+  try {
+    static_cast<SVO *>(h)->set_voxel(x, y, z, value != 0);
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int ref_svo_get_voxel(void *h, u32 x, u32 y, u32 z) {
+  try {
+    return static_cast<SVO *>(h)->get_voxel(x, y, z) ? 1 : 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
+u64 ref_svo_node_count(void *h) { return static_cast<SVO *>(h)->node_count(); }
+u64 ref_svo_leaf_count(void *h) { return static_cast<SVO *>(h)->leaf_count(); }
+
+int ref_svo_export(void *h, u32 *node_count, u32 *leaf_count, u32 *nodes,
+                   u32 cap_nodes, u64 *leaves, u32 cap_leaves) {
+  SvoDump dump(*static_cast<SVO *>(h));
+  dump.visit(0, 0);
+  const u32 nn = static_cast<u32>(dump.nodes.size() / 8);
+  const u32 nl = static_cast<u32>(dump.leaves.size());
+  if (node_count) *node_count = nn;
+  if (leaf_count) *leaf_count = nl;
+  if (nodes) {
+    if (nn > cap_nodes) return 2;
+    for (u64 i = 0; i < dump.nodes.size(); ++i) nodes[i] = dump.nodes[i];
+  }
+  if (leaves) {
+    if (nl > cap_leaves) return 2;
+    for (u32 i = 0; i < nl; ++i) leaves[i] = dump.leaves[i];
+  }
+  return 0;
+}
+
+} // extern "C"

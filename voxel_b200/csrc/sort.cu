@@ -1,0 +1,371 @@
+// Stable LSD radix sort, onesweep form (Adinets & Merrill 2022, "Onesweep: A
+// Faster Least Significant Digit Radix Sort for GPUs"), for u32 / u64 keys
+// with an optional u32 payload, on sm_100a:
+//
+//   1. one read of the keys builds every pass's 256-bin digit histogram
+//      (shared-memory counters per block, then one global atomicAdd per bin);
+//   2. one partition kernel per 8-bit digit:
+//        - dynamic tile id, so a tile only waits on tiles already running;
+//        - each warp loads 32 x kItems keys with coalesced row loads and ranks
+//          them by digit with __match_any_sync (stable: rank follows the
+//          original order inside the warp);
+//        - warp counts are combined per digit, the tile publishes its digit
+//          counts and looks back over predecessor tiles per digit (bounded
+//          by the GPU timer);
+//        - keys and payloads are first sorted inside the tile in shared
+//          memory, then written out in that order so consecutive threads write
+//          consecutive addresses of each digit's run.
+//
+// Replaces algo::cuda::sort::sort_by_key with OneSweepPass
+// (cuda/sort/radix/onesweep/host.cuh:135-204, partition.cuh:117-200,
+// lookback.cuh:7-79, global_offsets.cuh:52-146), whose scatter is direct and
+// uncoalesced and whose look-back spin is unbounded.
+#include "common.cuh"
+#include "profile.cuh"
+
+namespace vx::sort {
+
+constexpr uint32_t kRadixBits = 8;
+constexpr uint32_t kBins = 1u << kRadixBits;
+constexpr uint32_t kBlock = 256;
+constexpr uint32_t kWarps = kBlock / kWarp;
+constexpr uint32_t kMaxPasses = 8;
+constexpr uint32_t kMaxCount = (1u << 30) - 1u;
+
+// Look-back record: state in bits 30-31, count in bits 0-29.
+constexpr uint32_t kRecAgg = 1u << 30, kRecInc = 2u << 30;
+constexpr uint32_t kRecValue = (1u << 30) - 1u;
+
+template <class K> struct Shape;
+template <> struct Shape<uint32_t> { static constexpr uint32_t kItems = 16; };
+template <> struct Shape<uint64_t> { static constexpr uint32_t kItems = 12; };
+
+template <class K> __host__ __device__ constexpr uint32_t tile_keys() {
+  return kBlock * Shape<K>::kItems;
+}
+
+inline uint32_t pass_count(uint32_t key_bits) {
+  return (key_bits + kRadixBits - 1) / kRadixBits;
+}
+
+template <class K>
+__device__ __forceinline__ uint32_t digit_of(K key, uint32_t shift,
+                                             uint32_t mask) {
+  return static_cast<uint32_t>(key >> shift) & mask;
+}
+
+struct PassInfo {
+  uint32_t shift[kMaxPasses];
+  uint32_t mask[kMaxPasses];
+};
+
+struct Layout {
+  uint32_t *counters;  // [1] device status, [2 + p] tile counter of pass p
+  uint32_t *hist;      // passes x 256 digit counts
+  uint32_t *records;   // passes x tiles x 256
+  void *tmp_keys;
+  uint32_t *tmp_vals;
+  size_t clear_bytes;
+};
+
+template <class K> Layout carve(void *ws, uint32_t count, uint32_t passes) {
+  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  Carver c(ws);
+  Layout l;
+  l.counters = c.take<uint32_t>(kMaxPasses + 2);
+  l.hist = c.take<uint32_t>(kMaxPasses * kBins);
+  l.records = c.take<uint32_t>(static_cast<size_t>(passes) * tiles * kBins);
+  l.clear_bytes = c.offset;
+  l.tmp_keys = c.take<K>(count);
+  l.tmp_vals = c.take<uint32_t>(count);
+  return l;
+}
+
+template <class K> size_t workspace_bytes(uint32_t count, uint32_t passes) {
+  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  Sizer s;
+  s.take<uint32_t>(kMaxPasses + 2);
+  s.take<uint32_t>(kMaxPasses * kBins);
+  s.take<uint32_t>(static_cast<size_t>(passes) * tiles * kBins);
+  s.take<K>(count);
+  s.take<uint32_t>(count);
+  return s.offset;
+}
+
+// ------------------------------------------------------------ histogram --
+
+template <class K>
+__global__ void __launch_bounds__(kBlock)
+    histogram_kernel(const K *__restrict__ keys, uint32_t count,
+                     uint32_t passes, PassInfo info, uint32_t *hist) {
+  // Two copies of the per-pass counters (even / odd warps) halve contention
+  // on skewed digits.
+  __shared__ uint32_t s_hist[2][kMaxPasses][kBins];
+  for (uint32_t i = threadIdx.x; i < 2 * kMaxPasses * kBins; i += kBlock)
+    (&s_hist[0][0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t copy = (threadIdx.x / kWarp) & 1u;
+  constexpr uint32_t kPerVec = 16 / sizeof(K);
+  const uint32_t vecs = count / kPerVec;
+  const uint4 *vkeys = reinterpret_cast<const uint4 *>(keys);
+  const bool aligned = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+  const uint32_t stride = gridDim.x * kBlock;
+  if (aligned) {
+    for (uint32_t v = blockIdx.x * kBlock + threadIdx.x; v < vecs; v += stride) {
+      const uint4 q = ld_stream_u4(vkeys + v);
+      const K *kq = reinterpret_cast<const K *>(&q);
+#pragma unroll
+      for (uint32_t e = 0; e < kPerVec; ++e)
+        for (uint32_t p = 0; p < passes; ++p)
+          atomicAdd(&s_hist[copy][p][digit_of(kq[e], info.shift[p], info.mask[p])], 1u);
+    }
+  }
+  const uint32_t tail_begin = aligned ? vecs * kPerVec : 0;
+  for (uint32_t i = tail_begin + blockIdx.x * kBlock + threadIdx.x; i < count;
+       i += stride) {
+    const K k = keys[i];
+    for (uint32_t p = 0; p < passes; ++p)
+      atomicAdd(&s_hist[copy][p][digit_of(k, info.shift[p], info.mask[p])], 1u);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < passes * kBins; i += kBlock) {
+    const uint32_t c = (&s_hist[0][0][0])[i] + (&s_hist[1][0][0])[i];
+    if (c != 0) atomicAdd(hist + i, c);
+  }
+}
+
+// ------------------------------------------------------------ partition --
+
+// Exclusive scan of one value per thread across the 256-thread block.
+__device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
+                                                        uint32_t *s_tmp) {
+  const uint32_t lane = lane_id(), warp = threadIdx.x / kWarp;
+  const uint32_t inc = warp_inclusive_sum<uint32_t>(v);
+  if (lane == kWarp - 1) s_tmp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < kWarps ? s_tmp[lane] : 0u;
+    const uint32_t wi = warp_inclusive_sum<uint32_t>(w);
+    if (lane < kWarps) s_tmp[lane] = wi - w;
+  }
+  __syncthreads();
+  const uint32_t r = s_tmp[warp] + inc - v;
+  __syncthreads();
+  return r;
+}
+
+template <class K, bool HasValues>
+__global__ void __launch_bounds__(kBlock)
+    partition_kernel(const K *__restrict__ in_keys,
+                     const uint32_t *__restrict__ in_vals,
+                     K *__restrict__ out_keys, uint32_t *__restrict__ out_vals,
+                     uint32_t count, uint32_t shift, uint32_t mask,
+                     const uint32_t *__restrict__ pass_hist,
+                     uint32_t *records, uint32_t *tile_counter,
+                     uint32_t *status) {
+  constexpr uint32_t kItems = Shape<K>::kItems;
+  constexpr uint32_t kTile = tile_keys<K>();
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp_hist[kWarps][kBins];
+  __shared__ uint32_t s_digit_off[kBins];
+  __shared__ uint32_t s_global[kBins];
+  __shared__ uint32_t s_tmp[kWarps];
+  __shared__ K s_keys[kTile];
+  __shared__ uint32_t s_vals[HasValues ? kTile : 1];
+
+  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
+  if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+#pragma unroll
+  for (uint32_t w = 0; w < kWarps; ++w) s_warp_hist[w][t] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t tile_base = static_cast<uint64_t>(tile) * kTile;
+  const uint64_t warp_base = tile_base + warp * kWarp * kItems;
+
+  K key[kItems];
+  uint32_t val[kItems];
+  uint32_t rank[kItems];
+#pragma unroll
+  for (uint32_t i = 0; i < kItems; ++i) {
+    const uint64_t idx = warp_base + i * kWarp + lane;
+    if (idx < count) {
+      key[i] = in_keys[idx];
+      if (HasValues) val[i] = in_vals[idx];
+    } else {
+      key[i] = K(0);
+      val[i] = 0;
+    }
+  }
+
+  // Warp-level multi-split: rank each key among the warp's keys of its digit.
+#pragma unroll
+  for (uint32_t i = 0; i < kItems; ++i) {
+    const uint64_t idx = warp_base + i * kWarp + lane;
+    const bool valid = idx < count;
+    const uint32_t d = valid ? digit_of(key[i], shift, mask) : kBins;
+    const uint32_t peers = __match_any_sync(kFullMask, d);
+    const uint32_t below = __popc(peers & lanemask_lt());
+    const uint32_t leader = 31u - __clz(peers);
+    uint32_t pre = 0;
+    if (valid) pre = s_warp_hist[warp][d];
+    rank[i] = pre + below;
+    __syncwarp();
+    if (valid && lane == leader) s_warp_hist[warp][d] = pre + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Thread t owns digit t: warp offsets, tile count, tile-local digit offset.
+  uint32_t tile_count = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kWarps; ++w) {
+    const uint32_t c = s_warp_hist[w][t];
+    s_warp_hist[w][t] = tile_count;
+    tile_count += c;
+  }
+  const uint32_t digit_off = block_exclusive_256(tile_count, s_tmp);
+  const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
+  s_digit_off[t] = digit_off;
+
+  // Per-digit decoupled look-back over predecessor tiles.
+  uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
+  uint32_t exclusive = 0;
+  if (tile == 0) {
+    st_relaxed_u32(rec, kRecInc | tile_count);
+  } else {
+    st_relaxed_u32(rec, kRecAgg | tile_count);
+    const uint64_t t0 = global_ns();
+    int64_t pred = static_cast<int64_t>(tile) - 1;
+    while (pred >= 0) {
+      const uint32_t r = ld_relaxed_u32(records + static_cast<size_t>(pred) * kBins + t);
+      if ((r & ~kRecValue) == 0) {
+        if (global_ns() - t0 > kWaitLimitNs) {
+          set_status(status, kDevTimeout);
+          break;
+        }
+        __nanosleep(20);
+        continue;
+      }
+      exclusive += r & kRecValue;
+      if ((r & ~kRecValue) == kRecInc) break;
+      --pred;
+    }
+    st_relaxed_u32(rec, kRecInc | (exclusive + tile_count));
+  }
+  s_global[t] = global_start + exclusive - digit_off;
+  __syncthreads();
+
+  // Sort the tile in shared memory.
+#pragma unroll
+  for (uint32_t i = 0; i < kItems; ++i) {
+    const uint64_t idx = warp_base + i * kWarp + lane;
+    if (idx < count) {
+      const uint32_t d = digit_of(key[i], shift, mask);
+      const uint32_t pos = s_digit_off[d] + s_warp_hist[warp][d] + rank[i];
+      s_keys[pos] = key[i];
+      if (HasValues) s_vals[pos] = val[i];
+    }
+  }
+  __syncthreads();
+
+  // Write the tile's runs out in order.
+  const uint32_t valid_in_tile =
+      count - tile_base < kTile ? static_cast<uint32_t>(count - tile_base) : kTile;
+#pragma unroll 4
+  for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
+    const K k = s_keys[j];
+    const uint32_t dst = s_global[digit_of(k, shift, mask)] + j;
+    if (dst >= count) continue; // only reachable after a look-back timeout
+    out_keys[dst] = k;
+    if (HasValues) out_vals[dst] = s_vals[j];
+  }
+}
+
+template <class K>
+vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
+                     uint32_t key_bits, void *workspace, size_t ws_bytes,
+                     cudaStream_t stream) {
+  constexpr uint32_t kMaxBits = sizeof(K) * 8;
+  if (key_bits == 0 || key_bits > kMaxBits) return VX_ERR_INVALID_VALUE;
+  if (keys == nullptr && count != 0) return VX_ERR_INVALID_VALUE;
+  if (count > kMaxCount) return VX_ERR_INVALID_VALUE;
+  if (count <= 1) return VX_OK;
+  const uint32_t passes = pass_count(key_bits);
+  if (workspace == nullptr || ws_bytes < workspace_bytes<K>(count, passes))
+    return VX_ERR_INVALID_VALUE;
+  const Layout l = carve<K>(workspace, count, passes);
+  VX_TRY_CUDA(cudaMemsetAsync(workspace, 0, l.clear_bytes, stream));
+
+  PassInfo info{};
+  for (uint32_t p = 0; p < passes; ++p) {
+    info.shift[p] = p * kRadixBits;
+    const uint32_t bits = key_bits - p * kRadixBits < kRadixBits
+                              ? key_bits - p * kRadixBits
+                              : kRadixBits;
+    info.mask[p] = (1u << bits) - 1u;
+  }
+  const uint32_t hist_blocks =
+      std::min<uint32_t>(ceil_div(count, kBlock * 16), sm_count() * 4);
+  {
+    prof::Scope scope(sizeof(K) == 4 ? "sort_histogram_u32" : "sort_histogram_u64", stream);
+    histogram_kernel<K><<<hist_blocks, kBlock, 0, stream>>>(keys, count, passes,
+                                                            info, l.hist);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+
+  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
+  uint32_t *src_v = values, *dst_v = l.tmp_vals;
+  for (uint32_t p = 0; p < passes; ++p) {
+    uint32_t *rec = l.records + static_cast<size_t>(p) * tiles * kBins;
+    prof::Scope scope(sizeof(K) == 4 ? "sort_partition_u32" : "sort_partition_u64", stream);
+    if (values != nullptr)
+      partition_kernel<K, true><<<tiles, kBlock, 0, stream>>>(
+          src_k, src_v, dst_k, dst_v, count, info.shift[p], info.mask[p],
+          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1);
+    else
+      partition_kernel<K, false><<<tiles, kBlock, 0, stream>>>(
+          src_k, nullptr, dst_k, nullptr, count, info.shift[p], info.mask[p],
+          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1);
+    VX_TRY_CUDA(cudaGetLastError());
+    std::swap(src_k, dst_k);
+    std::swap(src_v, dst_v);
+  }
+  if (src_k != keys) {
+    VX_TRY_CUDA(cudaMemcpyAsync(keys, src_k, sizeof(K) * count,
+                                cudaMemcpyDeviceToDevice, stream));
+    if (values != nullptr)
+      VX_TRY_CUDA(cudaMemcpyAsync(values, src_v, sizeof(uint32_t) * count,
+                                  cudaMemcpyDeviceToDevice, stream));
+  }
+  return VX_OK;
+}
+
+} // namespace vx::sort
+
+extern "C" {
+
+size_t vx_sort_workspace_size(uint32_t count, uint32_t key_bytes) {
+  if (count <= 1) return 0;
+  if (key_bytes == 8)
+    return vx::sort::workspace_bytes<uint64_t>(count, vx::sort::kMaxPasses);
+  return vx::sort::workspace_bytes<uint32_t>(count, 4);
+}
+
+vx_status vx_sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t count,
+                            uint32_t key_bits, void *workspace,
+                            size_t workspace_bytes, vx_stream stream) {
+  return vx::sort::sort_pairs<uint32_t>(keys, values, count, key_bits,
+                                        workspace, workspace_bytes,
+                                        static_cast<cudaStream_t>(stream));
+}
+
+vx_status vx_sort_pairs_u64(uint64_t *keys, uint32_t *values, uint32_t count,
+                            uint32_t key_bits, void *workspace,
+                            size_t workspace_bytes, vx_stream stream) {
+  return vx::sort::sort_pairs<uint64_t>(keys, values, count, key_bits,
+                                        workspace, workspace_bytes,
+                                        static_cast<cudaStream_t>(stream));
+}
+
+} // extern "C"
