@@ -69,6 +69,7 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.rows = []
+        self.marks = {}
         self.proc = None
         self.thread = None
 
@@ -78,18 +79,25 @@ class ClockSampler:
                 ["nvidia-smi", f"--id={self.gpu}",
                  f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL, text=True)
+                stderr=subprocess.PIPE, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi needs a moment before its first sample.
+            deadline = time.time() + 10
+            while not self.rows and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.05)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
+
+    def mark(self, name):
+        self.marks[name] = time.time()
 
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.rows.append(parts)
+                self.rows.append((time.time(), parts))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -102,20 +110,28 @@ class ClockSampler:
             self.thread.join(timeout=5)
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        """Median SM clock and active throttle reasons of the samples taken
+        between mark('start') and mark('end') (all samples if none fell in
+        that window)."""
+        t0 = self.marks.get("start", 0.0) - 0.25
+        t1 = self.marks.get("end", float("inf")) + 0.25
+        rows = [r for t, r in self.rows if t0 <= t <= t1] or [r for _, r in self.rows]
+        if not rows:
+            err = self.proc.stderr.read() if self.proc is not None else "not started"
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": ["unsampled"], "error": str(err)[:200]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             for name, v in zip(names, r[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def dist_setup():
@@ -211,6 +227,7 @@ def run_ours(args, ws, rank, local):
     with ClockSampler(local) as clk:
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
+        clk.mark("start")
         t0.record(stream)
         for i in range(steps):
             scan, k32, v32, k64, v64 = bufs[warm + i]
@@ -223,6 +240,7 @@ def run_ours(args, ws, rank, local):
             ev[i][3].record(stream)
         t1.record(stream)
         torch.cuda.synchronize()
+        clk.mark("end")
     barrier()
     launches = lib.vx_profile_launches() - launches0
     lib.vx_profile_enable(0)
@@ -448,7 +466,7 @@ def run_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64"], default=None)
