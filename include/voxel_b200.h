@@ -99,6 +99,69 @@ vx_status vx_sort_pairs_u64(uint64_t *keys, uint32_t *values, uint32_t count,
                             uint32_t key_bits, void *workspace,
                             size_t workspace_bytes, vx_stream stream);
 
+/* ----------------------------------------------------------- hash tables --
+ * Per-key status codes, identical in value to the reference's
+ * kSlabHashStatus* (cuda/hash_table/slab_hash/common.cuh:18-25). */
+#define VX_HASH_NOT_FOUND 0u
+#define VX_HASH_INSERTED 1u
+#define VX_HASH_REPLACED 2u
+#define VX_HASH_ERASED 3u
+#define VX_HASH_OVERFLOW 4u
+#define VX_HASH_INVALID_KEY 5u
+#define VX_HASH_FOUND 6u
+#define VX_HASH_ALREADY_PRESENT 7u
+
+/* Reserved u64 keys (the u64 widening of kSlabHashEmptyKey / DeletedKey). */
+#define VX_HASH_EMPTY_KEY 0xFFFFFFFFFFFFFFFFull
+#define VX_HASH_DELETED_KEY 0xFFFFFFFFFFFFFFFEull
+#define VX_HASH_NOT_FOUND_VALUE 0xFFFFFFFFu
+
+/* Slab hash set of u64 keys: buckets of 128-byte slabs (15 keys + link),
+ * chained through a pool of slab_capacity overflow slabs.  The u64 widening
+ * of BasicSlabHashSetU32 (cuda/hash_table/slab_hash/set/host.cuh:13-121,
+ * device ops cuda/hash_table/slab_hash/set/device.cuh:31-315).  statuses may
+ * be NULL.  A full slab pool reports VX_HASH_OVERFLOW for that key. */
+typedef struct vx_slab_set vx_slab_set;
+vx_status vx_slab_set_create(uint32_t bucket_count, uint32_t slab_capacity,
+                             vx_slab_set **out);
+vx_status vx_slab_set_destroy(vx_slab_set *set);
+vx_status vx_slab_set_clear(vx_slab_set *set, vx_stream stream);
+vx_status vx_slab_set_insert(vx_slab_set *set, const uint64_t *keys,
+                             uint32_t count, uint32_t *statuses,
+                             vx_stream stream);
+vx_status vx_slab_set_contains(const vx_slab_set *set, const uint64_t *keys,
+                               uint32_t count, uint32_t *contains,
+                               uint32_t *statuses, vx_stream stream);
+vx_status vx_slab_set_erase(vx_slab_set *set, const uint64_t *keys,
+                            uint32_t count, uint32_t *statuses,
+                            vx_stream stream);
+/* Bytes of device memory the table holds (buckets + overflow pool). */
+size_t vx_slab_set_bytes(const vx_slab_set *set);
+
+/* Cuckoo hash map u64 -> u32 with 4 hash functions over one slot array and a
+ * bounded eviction chain (max_evictions).  The u64-keyed, inline-key
+ * widening of cuckoo_insert / cuckoo_find / initialize_cuckoo_table
+ * (cuda/cuckoo_hash.cuh:54-120), which store an index into triple-u32 key
+ * arrays instead.  insert reports VX_HASH_INSERTED, VX_HASH_REPLACED (key
+ * already present: value overwritten) or VX_HASH_OVERFLOW (eviction chain
+ * exhausted: the key that was in hand at the end is dropped and reported).
+ * find writes the value or VX_HASH_NOT_FOUND_VALUE. */
+typedef struct vx_cuckoo vx_cuckoo;
+vx_status vx_cuckoo_create(uint32_t slot_count, uint32_t max_evictions,
+                           vx_cuckoo **out);
+vx_status vx_cuckoo_destroy(vx_cuckoo *table);
+vx_status vx_cuckoo_clear(vx_cuckoo *table, vx_stream stream);
+vx_status vx_cuckoo_insert(vx_cuckoo *table, const uint64_t *keys,
+                           const uint32_t *values, uint32_t count,
+                           uint32_t *statuses, vx_stream stream);
+vx_status vx_cuckoo_find(const vx_cuckoo *table, const uint64_t *keys,
+                         uint32_t count, uint32_t *values, vx_stream stream);
+size_t vx_cuckoo_bytes(const vx_cuckoo *table);
+/* Keys lost to exhausted eviction chains since the last clear (host read,
+ * synchronises the stream). */
+vx_status vx_cuckoo_dropped(const vx_cuckoo *table, uint64_t *host_count,
+                            vx_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

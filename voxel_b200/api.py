@@ -14,7 +14,7 @@ from . import check, lib
 
 __all__ = [
     "stream_handle", "ptr", "exclusive_sum", "inclusive_sum", "sort_pairs",
-    "workspace_status",
+    "workspace_status", "SlabHashSet", "CuckooMap",
 ]
 
 
@@ -91,3 +91,95 @@ def workspace_status(workspace: torch.Tensor) -> int:
     """Synchronise and return the device status a scan/sort left in its
     workspace (0 = ok, VX_ERR_TIMEOUT if a bounded wait gave up)."""
     return lib().vx_workspace_status(ptr(workspace), stream_handle())
+
+
+class SlabHashSet:
+    """u64 slab hash set (BasicSlabHashSetU32 widened to u64 keys,
+    cuda/hash_table/slab_hash/set/host.cuh:13-121)."""
+
+    def __init__(self, bucket_count: int, slab_capacity: int):
+        h = C.c_void_p()
+        check(lib().vx_slab_set_create(bucket_count, slab_capacity, C.byref(h)),
+              "vx_slab_set_create")
+        self._h = h
+        self.bucket_count = bucket_count
+        self.slab_capacity = slab_capacity
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_slab_set_destroy(h)
+            self._h = None
+
+    @property
+    def nbytes(self) -> int:
+        return lib().vx_slab_set_bytes(self._h)
+
+    def clear(self):
+        check(lib().vx_slab_set_clear(self._h, stream_handle()), "slab clear")
+
+    def insert(self, keys: torch.Tensor, statuses: torch.Tensor | None = None):
+        check(lib().vx_slab_set_insert(self._h, ptr(keys), keys.numel(),
+                                       ptr(statuses), stream_handle()),
+              "slab insert")
+        return statuses
+
+    def contains(self, keys: torch.Tensor, out: torch.Tensor | None = None,
+                 statuses: torch.Tensor | None = None):
+        if out is None:
+            out = torch.empty(keys.numel(), dtype=torch.int32, device=keys.device)
+        check(lib().vx_slab_set_contains(self._h, ptr(keys), keys.numel(),
+                                         ptr(out), ptr(statuses),
+                                         stream_handle()), "slab contains")
+        return out
+
+    def erase(self, keys: torch.Tensor, statuses: torch.Tensor | None = None):
+        check(lib().vx_slab_set_erase(self._h, ptr(keys), keys.numel(),
+                                      ptr(statuses), stream_handle()),
+              "slab erase")
+        return statuses
+
+
+class CuckooMap:
+    """u64 -> u32 cuckoo map with 4 hash functions and bounded eviction
+    (cuda/cuckoo_hash.cuh:54-120 widened to inline u64 keys)."""
+
+    def __init__(self, slot_count: int, max_evictions: int = 1000):
+        h = C.c_void_p()
+        check(lib().vx_cuckoo_create(slot_count, max_evictions, C.byref(h)),
+              "vx_cuckoo_create")
+        self._h = h
+        self.slot_count = slot_count
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_cuckoo_destroy(h)
+            self._h = None
+
+    @property
+    def nbytes(self) -> int:
+        return lib().vx_cuckoo_bytes(self._h)
+
+    def clear(self):
+        check(lib().vx_cuckoo_clear(self._h, stream_handle()), "cuckoo clear")
+
+    def insert(self, keys: torch.Tensor, values: torch.Tensor | None = None,
+               statuses: torch.Tensor | None = None):
+        check(lib().vx_cuckoo_insert(self._h, ptr(keys), ptr(values),
+                                     keys.numel(), ptr(statuses),
+                                     stream_handle()), "cuckoo insert")
+        return statuses
+
+    def find(self, keys: torch.Tensor, out: torch.Tensor | None = None):
+        if out is None:
+            out = torch.empty(keys.numel(), dtype=torch.int32, device=keys.device)
+        check(lib().vx_cuckoo_find(self._h, ptr(keys), keys.numel(), ptr(out),
+                                   stream_handle()), "cuckoo find")
+        return out
+
+    def dropped(self) -> int:
+        v = C.c_uint64(0)
+        check(lib().vx_cuckoo_dropped(self._h, C.byref(v), stream_handle()),
+              "cuckoo dropped")
+        return v.value

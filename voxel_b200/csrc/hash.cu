@@ -1,0 +1,505 @@
+// u64-keyed hash tables for sm_100a.
+//
+// Slab hash set: the u64 widening of the reference's BasicSlabHashSetU32
+// (cuda/hash_table/slab_hash/set/host.cuh:13-121, device.cuh:31-315).  A slab
+// is one 128-byte line: 15 u64 key slots and a u64 link to the next slab of
+// the bucket's chain.  Sixteen lanes read a slab with one coalesced request,
+// so each warp works on two keys at once (one per half-warp), where the
+// reference's u32 slab needs the whole warp per key.  Inserts CAS an empty or
+// deleted slot; full chains grow from a pool of overflow slabs taken with a
+// bump counter.  Statuses are the reference's kSlabHashStatus* values.  Every
+// retry loop is bounded (the reference's kSlabHashMaxContentionRetries).
+//
+// Cuckoo map: the u64-keyed widening of cuckoo_insert / cuckoo_find
+// (cuda/cuckoo_hash.cuh:54-120).  Four hash functions address one array of
+// 16-byte slots {key, value | hash id << 32}; an eviction moves a whole slot
+// with one 128-bit atomic exchange (atom.exch.b128, sm_90+), so key and value
+// never separate.  Eviction chains are bounded by max_evictions (the
+// reference's insertion_attempts); a chain that runs out drops the key in
+// hand, reports VX_HASH_OVERFLOW and counts it.
+#include "common.cuh"
+#include "profile.cuh"
+
+#include <new>
+
+namespace vx::hash {
+
+constexpr uint64_t kEmpty = VX_HASH_EMPTY_KEY;
+constexpr uint64_t kDeleted = VX_HASH_DELETED_KEY;
+constexpr uint64_t kNullLink = ~0ull;
+constexpr uint32_t kSlotsPerSlab = 15;
+constexpr uint32_t kMaxContentionRetries = 65536;
+constexpr uint32_t kBlock = 256;
+
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
+  // splitmix64 finaliser (Steele, Lea & Flood 2014)
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+
+// Map a 64-bit hash onto [0, n) without a division (multiply-high).
+__device__ __forceinline__ uint32_t reduce(uint64_t h, uint32_t n) {
+  return static_cast<uint32_t>(__umul64hi(h, n));
+}
+
+struct Slab {
+  uint64_t w[16]; // w[0..14] keys, w[15] link
+};
+static_assert(sizeof(Slab) == 128, "slab must be one 128-byte line");
+
+} // namespace vx::hash
+
+struct vx_slab_set {
+  vx::hash::Slab *slabs = nullptr; // buckets, then the overflow pool
+  uint32_t *alloc = nullptr;       // overflow slabs handed out
+  uint32_t bucket_count = 0;
+  uint32_t capacity = 0;
+};
+
+struct vx_cuckoo {
+  ulonglong2 *slots = nullptr;
+  unsigned long long *dropped = nullptr;
+  uint32_t slot_count = 0;
+  uint32_t max_evictions = 0;
+};
+
+namespace vx::hash {
+
+struct SetView {
+  Slab *slabs;
+  uint32_t *alloc;
+  uint32_t bucket_count;
+  uint32_t capacity;
+};
+
+__global__ void slab_init_kernel(SetView t, uint64_t words) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < words; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    reinterpret_cast<uint64_t *>(t.slabs)[i] = (i & 15u) == 15u ? kNullLink : kEmpty;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *t.alloc = 0;
+}
+
+enum class SetOp { Insert, Contains, Erase };
+
+// One key per half-warp at a time.  All 32 lanes call this; each half-warp
+// drains its own queue of active lanes.
+template <SetOp Op>
+__global__ void __launch_bounds__(kBlock)
+    slab_set_kernel(SetView t, const uint64_t *__restrict__ keys,
+                    uint32_t count, uint32_t *contains, uint32_t *statuses) {
+  const uint32_t lane = lane_id();
+  const uint32_t sub = lane & 15u;
+  const uint32_t half = lane >> 4;
+  const uint32_t hmask = half ? 0xffff0000u : 0x0000ffffu;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  // Every lane of a warp iterates the same number of rounds.
+  const uint64_t warp_first = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) - lane;
+  for (uint64_t base = warp_first; base < count; base += stride) {
+    const uint64_t idx = base + lane;
+    bool active = idx < count;
+    uint64_t key = active ? keys[idx] : 0;
+    uint32_t status = VX_HASH_NOT_FOUND, found = 0;
+    if (active && (key == kEmpty || key == kDeleted)) {
+      status = VX_HASH_INVALID_KEY;
+      active = false;
+    }
+    uint32_t queue = __ballot_sync(hmask, active) & hmask;
+    while (queue) {
+      const uint32_t src = __ffs(queue) - 1u;
+      const uint64_t k = __shfl_sync(hmask, key, src);
+      Slab *slab = &t.slabs[reduce(mix64(k), t.bucket_count)];
+      uint32_t result = VX_HASH_OVERFLOW;
+      const uint64_t max_steps =
+          Op == SetOp::Contains
+              ? t.capacity + 1ull
+              : (t.capacity + 1ull) * static_cast<uint64_t>(kMaxContentionRetries);
+      for (uint64_t step = 0; step < max_steps; ++step) {
+        const uint64_t w = ld_relaxed_u64(&slab->w[sub]);
+        const bool key_slot = sub < kSlotsPerSlab;
+        const uint32_t hit = __ballot_sync(hmask, key_slot && w == k) & hmask;
+        if (hit) {
+          if (Op == SetOp::Erase) {
+            const uint32_t dst = __ffs(hit) - 1u;
+            unsigned long long old = 0;
+            if (lane == dst)
+              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]),
+                              k, kDeleted);
+            old = __shfl_sync(hmask, old, dst);
+            if (old != k) continue; // lost a race: re-read this slab
+            result = VX_HASH_ERASED;
+          } else {
+            result = Op == SetOp::Insert ? VX_HASH_ALREADY_PRESENT : VX_HASH_FOUND;
+          }
+          break;
+        }
+        if (Op == SetOp::Insert) {
+          const uint32_t free_mask =
+              __ballot_sync(hmask, key_slot && (w == kEmpty || w == kDeleted)) & hmask;
+          if (free_mask) {
+            const uint32_t dst = __ffs(free_mask) - 1u;
+            const uint64_t expect = __shfl_sync(hmask, w, dst);
+            unsigned long long old = 0;
+            if (lane == dst)
+              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]),
+                              expect, k);
+            old = __shfl_sync(hmask, old, dst);
+            if (old == expect) {
+              result = VX_HASH_INSERTED;
+              break;
+            }
+            continue; // slot taken meanwhile: re-read this slab
+          }
+        }
+        const uint64_t link = __shfl_sync(hmask, w, (half << 4) + 15u);
+        if (link != kNullLink) {
+          slab = &t.slabs[link];
+          continue;
+        }
+        if (Op != SetOp::Insert) {
+          result = VX_HASH_NOT_FOUND;
+          break;
+        }
+        // Grow the chain: take a pool slab, initialise it, link it with CAS.
+        uint32_t ord = 0;
+        if (sub == 0) ord = atomicAdd(t.alloc, 1u);
+        ord = __shfl_sync(hmask, ord, half << 4);
+        if (ord >= t.capacity) {
+          // Pool exhausted; another half-warp may have linked a slab since.
+          uint64_t again = 0;
+          if (sub == 15u) again = ld_relaxed_u64(&slab->w[15]);
+          again = __shfl_sync(hmask, again, (half << 4) + 15u);
+          if (again != kNullLink) {
+            slab = &t.slabs[again];
+            continue;
+          }
+          result = VX_HASH_OVERFLOW;
+          break;
+        }
+        Slab *fresh = &t.slabs[t.bucket_count + ord];
+        fresh->w[sub] = sub == 15u ? kNullLink : kEmpty;
+        __threadfence();
+        __syncwarp(hmask);
+        unsigned long long observed = 0;
+        if (sub == 15u)
+          observed = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[15]),
+                               kNullLink, t.bucket_count + ord);
+        observed = __shfl_sync(hmask, observed, (half << 4) + 15u);
+        // Either our slab was linked or another warp's was; follow the link.
+        // (A pool slab that lost the race stays unused.)
+        slab = &t.slabs[observed == kNullLink ? t.bucket_count + ord : observed];
+      }
+      if (lane == src) {
+        status = result;
+        found = (result == VX_HASH_FOUND) ? 1u : 0u;
+        active = false;
+      }
+      queue = __ballot_sync(hmask, active) & hmask;
+    }
+    if (idx < count) {
+      if (statuses) statuses[idx] = status;
+      if (Op == SetOp::Contains && contains) contains[idx] = found;
+    }
+  }
+}
+
+// ------------------------------------------------------------ cuckoo --
+
+constexpr uint32_t kCuckooHashes = 4;
+
+__device__ __forceinline__ uint32_t cuckoo_slot(uint64_t key, uint32_t hid,
+                                                uint32_t n) {
+  constexpr uint64_t salts[kCuckooHashes] = {
+      0x9e3779b97f4a7c15ull, 0xc2b2ae3d27d4eb4full, 0x165667b19e3779f9ull,
+      0x27d4eb2f165667c5ull};
+  return reduce(mix64(key ^ salts[hid]), n);
+}
+
+__device__ __forceinline__ ulonglong2 exch128(ulonglong2 *p, ulonglong2 v) {
+  ulonglong2 old;
+  asm volatile(
+      "{\n\t.reg .b128 d, b;\n\t"
+      "mov.b128 b, {%2, %3};\n\t"
+      "atom.global.exch.b128 d, [%4], b;\n\t"
+      "mov.b128 {%0, %1}, d;\n\t}"
+      : "=l"(old.x), "=l"(old.y)
+      : "l"(v.x), "l"(v.y), "l"(p)
+      : "memory");
+  return old;
+}
+
+__device__ __forceinline__ ulonglong2 ld_slot(const ulonglong2 *p) {
+  ulonglong2 v;
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+               : "=l"(v.x), "=l"(v.y)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+
+__global__ void cuckoo_init_kernel(ulonglong2 *slots, uint32_t n,
+                                   unsigned long long *dropped) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    slots[i] = make_ulonglong2(kEmpty, 0);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dropped = 0;
+}
+
+__device__ __forceinline__ bool cuckoo_lookup(const ulonglong2 *slots,
+                                              uint32_t n, uint64_t key,
+                                              uint32_t &value, uint32_t &where) {
+#pragma unroll
+  for (uint32_t h = 0; h < kCuckooHashes; ++h) {
+    const uint32_t s = cuckoo_slot(key, h, n);
+    const ulonglong2 v = ld_slot(slots + s);
+    if (v.x == key) {
+      value = static_cast<uint32_t>(v.y);
+      where = s;
+      return true;
+    }
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    cuckoo_insert_kernel(ulonglong2 *slots, uint32_t n, uint32_t max_evictions,
+                         unsigned long long *dropped,
+                         const uint64_t *__restrict__ keys,
+                         const uint32_t *__restrict__ values, uint32_t count,
+                         uint32_t *statuses) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= count) return;
+  const uint64_t key = keys[i];
+  const uint32_t value = values ? values[i] : static_cast<uint32_t>(i);
+  uint32_t status;
+  uint32_t old_value, where;
+  if (key == kEmpty || key == kDeleted) {
+    status = VX_HASH_INVALID_KEY;
+  } else if (cuckoo_lookup(slots, n, key, old_value, where)) {
+    // Replace in place (a concurrent eviction may move the slot meanwhile;
+    // duplicate keys inside one batch are not supported, as in the reference).
+    atomicExch(reinterpret_cast<unsigned long long *>(&slots[where].y),
+               static_cast<unsigned long long>(value));
+    status = VX_HASH_REPLACED;
+  } else {
+    ulonglong2 cur = make_ulonglong2(key, value);
+    uint32_t hid = 0;
+    status = VX_HASH_OVERFLOW;
+    for (uint32_t a = 0; a <= max_evictions; ++a) {
+      cur.y = (cur.y & 0xffffffffull) | (static_cast<uint64_t>(hid) << 32);
+      const ulonglong2 prev = exch128(slots + cuckoo_slot(cur.x, hid, n), cur);
+      if (prev.x == kEmpty) {
+        status = VX_HASH_INSERTED;
+        break;
+      }
+      if (prev.x == cur.x) { // same key displaced: keep the newer value
+        status = VX_HASH_INSERTED;
+        break;
+      }
+      cur = prev;
+      hid = (static_cast<uint32_t>(prev.y >> 32) + 1u) % kCuckooHashes;
+    }
+    if (status == VX_HASH_OVERFLOW) atomicAdd(dropped, 1ull);
+  }
+  if (statuses) statuses[i] = status;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    cuckoo_find_kernel(const ulonglong2 *slots, uint32_t n,
+                       const uint64_t *__restrict__ keys, uint32_t count,
+                       uint32_t *values) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= count) return;
+  uint32_t v = VX_HASH_NOT_FOUND_VALUE, where;
+  const uint64_t key = keys[i];
+  if (key != kEmpty && key != kDeleted) cuckoo_lookup(slots, n, key, v, where);
+  values[i] = v;
+}
+
+inline uint32_t grid_for(uint64_t items, uint32_t per_block = kBlock) {
+  const uint64_t g = (items + per_block - 1) / per_block;
+  const uint64_t cap = static_cast<uint64_t>(sm_count()) * 16u;
+  return static_cast<uint32_t>(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+} // namespace vx::hash
+
+using namespace vx::hash;
+
+static SetView view_of(const vx_slab_set *s) {
+  return SetView{s->slabs, s->alloc, s->bucket_count, s->capacity};
+}
+
+template <SetOp Op>
+static vx_status slab_launch(const vx_slab_set *s, const uint64_t *keys,
+                             uint32_t count, uint32_t *contains,
+                             uint32_t *statuses, vx_stream stream,
+                             const char *name) {
+  if (s == nullptr || (keys == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
+  if (Op == SetOp::Contains && contains == nullptr && count != 0)
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope(name, st);
+  slab_set_kernel<Op><<<grid_for(count), kBlock, 0, st>>>(view_of(s), keys, count,
+                                                          contains, statuses);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+
+extern "C" {
+
+vx_status vx_slab_set_clear(vx_slab_set *s, vx_stream stream) {
+  if (s == nullptr) return VX_ERR_INVALID_VALUE;
+  const uint64_t words = (static_cast<uint64_t>(s->bucket_count) + s->capacity) * 16u;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope("slab_init", st);
+  slab_init_kernel<<<grid_for(words), kBlock, 0, st>>>(view_of(s), words);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+
+
+vx_status vx_slab_set_create(uint32_t bucket_count, uint32_t slab_capacity,
+                             vx_slab_set **out) {
+  if (out == nullptr || bucket_count == 0) return VX_ERR_INVALID_VALUE;
+  auto *s = new (std::nothrow) vx_slab_set;
+  if (s == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  s->bucket_count = bucket_count;
+  s->capacity = slab_capacity;
+  const size_t slabs = static_cast<size_t>(bucket_count) + slab_capacity;
+  cudaError_t e = cudaMalloc(&s->slabs, slabs * sizeof(Slab));
+  if (e == cudaSuccess) e = cudaMalloc(&s->alloc, sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    vx_slab_set_destroy(s);
+    return vx::from_cuda(e);
+  }
+  const vx_status st = vx_slab_set_clear(s, nullptr);
+  if (st != VX_OK) {
+    vx_slab_set_destroy(s);
+    return st;
+  }
+  VX_TRY_CUDA(cudaStreamSynchronize(nullptr));
+  *out = s;
+  return VX_OK;
+}
+
+vx_status vx_slab_set_destroy(vx_slab_set *s) {
+  if (s == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaFree(s->slabs);
+  cudaFree(s->alloc);
+  delete s;
+  return VX_OK;
+}
+
+vx_status vx_slab_set_insert(vx_slab_set *s, const uint64_t *keys,
+                             uint32_t count, uint32_t *statuses,
+                             vx_stream stream) {
+  return slab_launch<SetOp::Insert>(s, keys, count, nullptr, statuses, stream,
+                                    "slab_insert");
+}
+
+vx_status vx_slab_set_contains(const vx_slab_set *s, const uint64_t *keys,
+                               uint32_t count, uint32_t *contains,
+                               uint32_t *statuses, vx_stream stream) {
+  return slab_launch<SetOp::Contains>(s, keys, count, contains, statuses,
+                                      stream, "slab_contains");
+}
+
+vx_status vx_slab_set_erase(vx_slab_set *s, const uint64_t *keys,
+                            uint32_t count, uint32_t *statuses,
+                            vx_stream stream) {
+  return slab_launch<SetOp::Erase>(s, keys, count, nullptr, statuses, stream,
+                                   "slab_erase");
+}
+
+size_t vx_slab_set_bytes(const vx_slab_set *s) {
+  if (s == nullptr) return 0;
+  return (static_cast<size_t>(s->bucket_count) + s->capacity) * sizeof(Slab);
+}
+
+vx_status vx_cuckoo_create(uint32_t slot_count, uint32_t max_evictions,
+                           vx_cuckoo **out) {
+  if (out == nullptr || slot_count == 0) return VX_ERR_INVALID_VALUE;
+  auto *c = new (std::nothrow) vx_cuckoo;
+  if (c == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  c->slot_count = slot_count;
+  c->max_evictions = max_evictions;
+  cudaError_t e = cudaMalloc(&c->slots, sizeof(ulonglong2) * slot_count);
+  if (e == cudaSuccess) e = cudaMalloc(&c->dropped, sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    vx_cuckoo_destroy(c);
+    return vx::from_cuda(e);
+  }
+  const vx_status st = vx_cuckoo_clear(c, nullptr);
+  if (st != VX_OK) {
+    vx_cuckoo_destroy(c);
+    return st;
+  }
+  VX_TRY_CUDA(cudaStreamSynchronize(nullptr));
+  *out = c;
+  return VX_OK;
+}
+
+vx_status vx_cuckoo_destroy(vx_cuckoo *c) {
+  if (c == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaFree(c->slots);
+  cudaFree(c->dropped);
+  delete c;
+  return VX_OK;
+}
+
+vx_status vx_cuckoo_clear(vx_cuckoo *c, vx_stream stream) {
+  if (c == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope("cuckoo_init", st);
+  cuckoo_init_kernel<<<grid_for(c->slot_count), kBlock, 0, st>>>(
+      c->slots, c->slot_count, c->dropped);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_cuckoo_insert(vx_cuckoo *c, const uint64_t *keys,
+                           const uint32_t *values, uint32_t count,
+                           uint32_t *statuses, vx_stream stream) {
+  if (c == nullptr || (keys == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope("cuckoo_insert", st);
+  cuckoo_insert_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, st>>>(
+      c->slots, c->slot_count, c->max_evictions, c->dropped, keys, values,
+      count, statuses);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_cuckoo_find(const vx_cuckoo *c, const uint64_t *keys,
+                         uint32_t count, uint32_t *values, vx_stream stream) {
+  if (c == nullptr || ((keys == nullptr || values == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope("cuckoo_find", st);
+  cuckoo_find_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, st>>>(
+      c->slots, c->slot_count, keys, count, values);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+size_t vx_cuckoo_bytes(const vx_cuckoo *c) {
+  return c == nullptr ? 0 : sizeof(ulonglong2) * static_cast<size_t>(c->slot_count);
+}
+
+vx_status vx_cuckoo_dropped(const vx_cuckoo *c, uint64_t *host_count,
+                            vx_stream stream) {
+  if (c == nullptr || host_count == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned long long v = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(&v, c->dropped, sizeof(v), cudaMemcpyDeviceToHost, st));
+  VX_TRY_CUDA(cudaStreamSynchronize(st));
+  *host_count = v;
+  return VX_OK;
+}
+
+} // extern "C"
