@@ -45,6 +45,10 @@ PART_U64_BYTES = N_SORT * 24
 # DRAM bytes per sort_partition_u64 launch from ncu (profiles/), scaled to
 # 2^28 elements; None until a capture is committed.
 PART_U64_TRAFFIC = None
+N_HASH = 1 << 26
+HASH_LOAD = 0.8
+BYTES_HASH_INSERT = 40  # read key 8 + one 32-B sector read-modify-write
+BYTES_HASH_LOOKUP = 44  # read key 8 + one 32-B sector + 4-B result
 
 
 # --------------------------------------------------------------- helpers --
@@ -196,6 +200,18 @@ def run_ours(args, ws, rank, local):
     for _ in range(steps + warm):
         bufs.append((base_scan.clone(), base_k32.clone(), vals.clone(),
                      base_k64.clone(), vals.clone()))
+    gh = torch.Generator(device=device)
+    gh.manual_seed(5 + rank * 10)
+    hkeys = torch.randint(-2**63, 2**63 - 2, (N_HASH,), dtype=torch.int64,
+                          device=device, generator=gh)
+    fresh = torch.randint(-2**63, 2**63 - 2, (N_HASH // 2,), dtype=torch.int64,
+                          device=device, generator=gh)
+    hq = torch.cat([hkeys[torch.randperm(N_HASH, device=device, generator=gh)[:N_HASH // 2]], fresh])
+    hq = hq[torch.randperm(N_HASH, device=device, generator=gh)].contiguous()
+    del fresh
+    slab = vx.SlabHashSet(int(N_HASH / (HASH_LOAD * 15)) + 1, N_HASH // 30)
+    cuckoo = vx.CuckooMap(int(N_HASH / HASH_LOAD) + 1, 2000)
+    hfound = torch.empty(N_HASH, dtype=torch.int32, device=device)
     ws_scan = torch.empty(lib.vx_scan_workspace_size(N_SCAN), dtype=torch.uint8, device=device)
     ws_sort = torch.empty(lib.vx_sort_workspace_size(N_SORT, 8), dtype=torch.uint8, device=device)
     torch.cuda.synchronize()
@@ -205,6 +221,12 @@ def run_ours(args, ws, rank, local):
         vx.exclusive_sum(scan, ws_scan)
         vx.sort_pairs(k32, v32, 32, ws_sort)
         vx.sort_pairs(k64, v64, 60, ws_sort)
+        slab.clear()
+        slab.insert(hkeys)
+        slab.contains(hq, hfound)
+        cuckoo.clear()
+        cuckoo.insert(hkeys)
+        cuckoo.find(hq, hfound)
 
     for i in range(warm):
         step(bufs[i])
@@ -220,7 +242,7 @@ def run_ours(args, ws, rank, local):
     lib.vx_profile_enable(1)
     launches0 = lib.vx_profile_launches()
     stream = torch.cuda.current_stream()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(10)]
           for _ in range(steps)]
     barrier()
     torch.cuda.synchronize()
@@ -238,6 +260,18 @@ def run_ours(args, ws, rank, local):
             ev[i][2].record(stream)
             vx.sort_pairs(k64, v64, 60, ws_sort)
             ev[i][3].record(stream)
+            slab.clear()
+            ev[i][4].record(stream)
+            slab.insert(hkeys)
+            ev[i][5].record(stream)
+            slab.contains(hq, hfound)
+            ev[i][6].record(stream)
+            cuckoo.clear()
+            ev[i][7].record(stream)
+            cuckoo.insert(hkeys)
+            ev[i][8].record(stream)
+            cuckoo.find(hq, hfound)
+            ev[i][9].record(stream)
         t1.record(stream)
         torch.cuda.synchronize()
         clk.mark("end")
@@ -248,6 +282,12 @@ def run_ours(args, ws, rank, local):
     scan_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     s32_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
     s64_ms = sum(e[2].elapsed_time(e[3]) for e in ev)
+    slab_ins_ms = sum(e[4].elapsed_time(e[5]) for e in ev)
+    slab_q_ms = sum(e[5].elapsed_time(e[6]) for e in ev)
+    ck_ins_ms = sum(e[7].elapsed_time(e[8]) for e in ev)
+    ck_q_ms = sum(e[8].elapsed_time(e[9]) for e in ev)
+    hits = int(hfound.ne(-1).sum().item())
+    dropped = cuckoo.dropped()
     part_ms = _prof(lib, "sort_partition_u64")
 
     if ws > 1:
@@ -261,13 +301,15 @@ def run_ours(args, ws, rank, local):
     ok = bool(((k64[1:] >= k64[:-1]) | (k64[1:] < 0) | (k64[:-1] < 0)).all()) and \
         bool((k32[1:].to(torch.int64) & 0xFFFFFFFF >= k32[:-1].to(torch.int64) & 0xFFFFFFFF).all())
 
-    bytes_step = N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+    bytes_step = (N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+                  + 2 * N_HASH * (BYTES_HASH_INSERT + BYTES_HASH_LOOKUP))
     value = ws * bytes_step * steps / (total_ms / 1e3) / 1e9
     del bufs
     torch.cuda.empty_cache()
 
     e2e = run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals,
-                  ws_scan, ws_sort, max(1, min(steps, 3)), ws)
+                  ws_scan, ws_sort, max(1, min(steps, 3)), ws,
+                  (slab, cuckoo, hkeys, hq))
     hbm, kind = peaks()
     part_n, part_total = part_ms
     achieved = PART_U64_BYTES / (part_total / part_n / 1e3) / 1e9 if part_n else None
@@ -288,7 +330,9 @@ def run_ours(args, ws, rank, local):
             "workload": "primitives sweep: exclusive scan 2^28 u32 in [0,255]; "
                         "stable sort 2^28 u32 keys + u32 index payload; "
                         "stable sort 2^28 u64 60-bit Morton keys (64 Gaussian "
-                        "blobs, sigma 2^14, 2^20 cube) + u32 index payload",
+                        "blobs, sigma 2^14, 2^20 cube) + u32 index payload; "
+                        "slab set and cuckoo map: 2^26 uniform u64 keys at "
+                        "load factor 0.8, then 2^26 lookups at 50% hits",
             "elements": N_SORT,
             "l2_policy": "inputs larger than L2 (fresh 1-3 GB buffers per step)",
             "parallelism": f"replicas x{ws}",
@@ -302,6 +346,16 @@ def run_ours(args, ws, rank, local):
             "sort_u64_ms": round(s64_ms / steps, 3),
             "sort_u32_Gkeys_per_s": round(N_SORT * steps / s32_ms / 1e6, 3),
             "sort_u64_Gkeys_per_s": round(N_SORT * steps / s64_ms / 1e6, 3),
+            "slab_insert_GBps": round(N_HASH * BYTES_HASH_INSERT * steps / slab_ins_ms / 1e6, 1),
+            "slab_lookup_GBps": round(N_HASH * BYTES_HASH_LOOKUP * steps / slab_q_ms / 1e6, 1),
+            "cuckoo_insert_GBps": round(N_HASH * BYTES_HASH_INSERT * steps / ck_ins_ms / 1e6, 1),
+            "cuckoo_lookup_GBps": round(N_HASH * BYTES_HASH_LOOKUP * steps / ck_q_ms / 1e6, 1),
+            "slab_insert_Mops": round(N_HASH * steps / slab_ins_ms / 1e3, 1),
+            "slab_lookup_Mops": round(N_HASH * steps / slab_q_ms / 1e3, 1),
+            "cuckoo_insert_Mops": round(N_HASH * steps / ck_ins_ms / 1e3, 1),
+            "cuckoo_lookup_Mops": round(N_HASH * steps / ck_q_ms / 1e3, 1),
+            "cuckoo_lookup_hit_fraction": round(hits / N_HASH, 4),
+            "cuckoo_dropped": dropped,
         },
         "roofline": {
             "kernel": "sort_partition_u64",
@@ -337,26 +391,36 @@ def _prof(lib, name):
 
 
 def run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals, ws_scan,
-            ws_sort, steps, world):
+            ws_sort, steps, world, hash_parts):
     """Same sweep through the public API with host inputs: every step copies
     its inputs from pinned host memory and reads every result back."""
-    h_scan = base_scan.cpu().pin_memory()
-    h_k32 = base_k32.cpu().pin_memory()
-    h_k64 = base_k64.cpu().pin_memory()
-    h_vals = vals.cpu().pin_memory()
-    outs = [torch.empty_like(t).pin_memory() for t in (h_scan, h_k32, h_vals, h_k64, h_vals)]
-    d = [torch.empty_like(t, device=device) for t in (h_scan, h_k32, h_vals, h_k64, h_vals)]
+    slab, cuckoo, hkeys, hq = hash_parts
+    srcs = [t.cpu().pin_memory() for t in (base_scan, base_k32, vals, base_k64,
+                                            vals, hkeys, hq)]
+    d = [torch.empty_like(t, device=device) for t in srcs]
+    found = torch.empty(N_HASH, dtype=torch.int32, device=device)
+    outs = [torch.empty_like(t).pin_memory() for t in srcs[:5]]
+    h_found = [torch.empty(N_HASH, dtype=torch.int32).pin_memory() for _ in range(2)]
     stream = torch.cuda.current_stream()
-    h2d = sum(t.numel() * t.element_size() for t in (h_scan, h_k32, h_vals, h_k64, h_vals))
+    h2d = sum(t.numel() * t.element_size() for t in srcs)
+    d2h = sum(t.numel() * t.element_size() for t in outs) + 2 * N_HASH * 4
 
     def one():
-        for dst, src in zip(d, (h_scan, h_k32, h_vals, h_k64, h_vals)):
+        for dst, src in zip(d, srcs):
             dst.copy_(src, non_blocking=True)
         vx.exclusive_sum(d[0], ws_scan)
         vx.sort_pairs(d[1], d[2], 32, ws_sort)
         vx.sort_pairs(d[3], d[4], 60, ws_sort)
         for o, s in zip(outs, d):
             o.copy_(s, non_blocking=True)
+        slab.clear()
+        slab.insert(d[5])
+        slab.contains(d[6], found)
+        h_found[0].copy_(found, non_blocking=True)
+        cuckoo.clear()
+        cuckoo.insert(d[5])
+        cuckoo.find(d[6], found)
+        h_found[1].copy_(found, non_blocking=True)
 
     one()
     torch.cuda.synchronize()
@@ -368,10 +432,11 @@ def run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals, ws_scan,
     t1.record(stream)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
-    bytes_step = N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+    bytes_step = (N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
+                  + 2 * N_HASH * (BYTES_HASH_INSERT + BYTES_HASH_LOOKUP))
     return {"value": round(world * bytes_step * steps / (ms / 1e3) / 1e9, 2),
             "unit": "GB/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": h2d, "ms_per_step": round(ms / steps, 2)}
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms / steps, 2)}
 
 
 def cpu_baseline(sample_log2=24):
@@ -398,12 +463,23 @@ def cpu_baseline(sample_log2=24):
     t = time.perf_counter()
     L.orc_radix_sort_pairs_u64_mt(kk.ctypes.data, vv.ctypes.data, n, 60, threads)
     t_s64 = time.perf_counter() - t
-    total_b = n * (BYTES_SCAN + BYTES_SORT_U32 + BYTES_SORT_U64)
-    return {"value": round(total_b / (t_scan + t_s32 + t_s64) / 1e9, 3),
+    nh = n >> 2
+    hk = rng.integers(0, 2**64 - 2, nh, dtype=np.uint64)
+    hq = np.concatenate([hk[: nh // 2], rng.integers(0, 2**64 - 2, nh // 2, dtype=np.uint64)])
+    t = time.perf_counter()
+    oracle.hash_set(hk, hq)
+    t_hash = time.perf_counter() - t
+    total_b = (n * (BYTES_SCAN + BYTES_SORT_U32 + BYTES_SORT_U64)
+               + 2 * nh * (BYTES_HASH_INSERT + BYTES_HASH_LOOKUP))
+    # std::unordered_set is single-threaded: one set stands for both tables.
+    secs = t_scan + t_s32 + t_s64 + 2 * t_hash
+    return {"value": round(total_b / secs / 1e9, 3),
             "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"2^{sample_log2} elements per component (scan u32, "
-                      f"sort u32, sort u64 60-bit) on {threads} host threads",
-            "seconds": round(t_scan + t_s32 + t_s64, 3)}
+            "sample": f"2^{sample_log2} elements per scan/sort component on "
+                      f"{threads} host threads; 2^{sample_log2 - 2} u64 keys "
+                      "inserted + looked up in std::unordered_set (1 thread), "
+                      "counted for both hash tables",
+            "seconds": round(secs, 3)}
 
 
 def run_reference(args, ws, rank):
