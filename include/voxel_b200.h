@@ -61,6 +61,12 @@ uint64_t vx_profile_launches(void);
 vx_status vx_profile_query(const char *name, double *host_total_ms,
                            uint64_t *host_launches);
 
+/* Seeded edit primitives of a benchmark mix, into host memory (the generator
+ * defined in vx_workload.h: PCG32 stream `stream` seeded with `seed`). */
+vx_status vx_generate_primitives(const vx_edit_mix *mix, uint64_t seed,
+                                 uint64_t stream, uint64_t count,
+                                 vx_primitive *host_out);
+
 /* ------------------------------------------------------------------ scan --
  * In-place prefix sums over uint32 / uint64 with modular (wrapping)
  * arithmetic.  Replaces algo::cuda::scan::{exclusive,inclusive}_sum<T> and
@@ -161,6 +167,103 @@ size_t vx_cuckoo_bytes(const vx_cuckoo *table);
  * synchronises the stream). */
 vx_status vx_cuckoo_dropped(const vx_cuckoo *table, uint64_t *host_count,
                             vx_stream stream);
+
+/* ------------------------------------------------------- common records -- */
+
+/* Voxel coordinate; coordinates outside the world are ignored by edits and
+ * read as empty by queries (hash_dag_gpu/types.cuh:11-15,
+ * svt/cuda/voxel/types.cuh:11-15). */
+typedef struct vx_voxel {
+    uint32_t x, y, z;
+} vx_voxel;
+
+#define VX_EDIT_DESTROY 0u /* EditOp::Destroy (hash_dag_gpu/types.cuh:30-33) */
+#define VX_EDIT_PLACE 1u   /* EditOp::Place */
+
+/* ------------------------------------------------------------- Hash DAG --
+ * A hash-consed sparse voxel DAG resident on one GPU.  World side is
+ * 4 << depth voxels (depth = inner levels above the 4^3 leaves, the
+ * reference's HashDAG(depth), svt/hash_dag.hpp:32-36); the reference GPU DAG
+ * is fixed at depth 8 (hash_dag_gpu/config.cuh:14-24), this one takes
+ * 1 <= depth <= 14.  Refs are 32-bit: 0 = empty subtree, 1 = full subtree,
+ * otherwise a node of that level's pool.  One content-addressed table per
+ * level; inner items are [child_mask | fill_mask << 8, child refs...]
+ * (hash_dag_gpu/detail/node.cuh:266-289); leaves are 64-bit occupancy masks,
+ * bit = x + 4y + 16z.  Replaces HashDagGpu / DeviceHashDagGpu
+ * (hash_dag_gpu/storage.cuh:16-105). */
+typedef struct vx_dag vx_dag;
+
+typedef struct vx_dag_config {
+    uint32_t depth;            /* inner levels, 1..14 */
+    uint32_t reserved0;
+    uint64_t max_nodes;        /* capacity per level (inner and leaf) */
+    uint64_t arena_bytes;      /* scratch for batched / terrain builds (0 = default) */
+} vx_dag_config;
+
+vx_status vx_dag_create(const vx_dag_config *config, vx_dag **out);
+vx_status vx_dag_destroy(vx_dag *dag);
+/* Clear every table and publish the empty root (HashDagGpu::reset,
+ * hash_dag_gpu/storage.cuh:57-69). */
+vx_status vx_dag_reset(vx_dag *dag, vx_stream stream);
+uint32_t vx_dag_depth(const vx_dag *dag);
+
+/* Plain per-call path: one op applied to a list of voxels.  Replaces
+ * hash_dag_gpu::{place,destroy,apply}_voxel_edits and
+ * apply_voxel_edits_workspace_size (hash_dag_gpu/edit.cuh:16-61).
+ * Errors: VX_ERR_INVALID_VALUE for NULL edits with count > 0 or a NULL/short
+ * workspace; VX_ERR_CAPACITY (reported as cudaErrorMemoryAllocation's
+ * meaning: a node table is full) leaves the previous root published
+ * (hash_dag_gpu/detail/edit/root.cuh:13-48).  Synchronises the stream once to
+ * read the status, as the reference does. */
+size_t vx_dag_voxel_workspace_size(uint32_t count);
+vx_status vx_dag_apply_voxels(vx_dag *dag, const vx_voxel *edits,
+                              uint32_t count, uint32_t op, void *workspace,
+                              size_t workspace_bytes, vx_stream stream);
+
+/* Batched path: a list of sphere / box primitives of mixed add/remove,
+ * applied as if sequentially in array order, in one stream-ordered
+ * submission with no host synchronisation (capturable in a CUDA graph).
+ * Uses the DAG's own arena; the status is left on the device and read with
+ * vx_dag_status.  No counterpart in the reference API (which applies one op
+ * per call to voxel lists); its result equals applying each primitive's voxel
+ * list with apply_voxel_edits in order. */
+vx_status vx_dag_apply_primitives(vx_dag *dag, const vx_primitive *prims,
+                                  uint32_t count, vx_stream stream);
+/* Read and clear the device status of the last submissions (synchronises). */
+vx_status vx_dag_status(vx_dag *dag, vx_stream stream);
+
+/* Build the terrain of the given generator into an empty DAG (replaces the
+ * DAG with the terrain; stream-ordered, status via vx_dag_status). */
+vx_status vx_dag_build_terrain(vx_dag *dag, const vx_terrain *terrain,
+                               vx_stream stream);
+
+/* Point queries: out[i] = 1 if voxel pts[i] is solid (hash_dag_gpu::get_voxel,
+ * hash_dag_gpu/query.cuh:12-39). */
+vx_status vx_dag_query(const vx_dag *dag, const vx_voxel *pts, uint32_t count,
+                       uint8_t *out, vx_stream stream);
+
+/* Canonical dump (host memory, synchronises): DFS from the root, children
+ * 0..7, first visit numbers the nodes of each level.  Each inner node is
+ * written as 10 words [child_mask, fill_mask, child ids x 8] (id 0 = empty,
+ * 1 = full, k + 2 = k-th node of the next level); each leaf as its u64 mask.
+ * host_counts[depth + 1] receives the number of nodes per level.  Call with
+ * NULL arrays to query the sizes first.  The root is reported in *host_root
+ * (0 empty, 1 full, 2 = node 0 of level 0). */
+vx_status vx_dag_export_canonical(const vx_dag *dag, uint32_t *host_root,
+                                  uint64_t *host_counts, uint32_t *host_nodes,
+                                  uint64_t nodes_capacity_words,
+                                  uint64_t *host_leaves,
+                                  uint64_t leaves_capacity, vx_stream stream);
+
+typedef struct vx_dag_stats {
+    uint64_t nodes_per_level[16]; /* items stored (live and superseded) */
+    uint64_t words_per_level[16];
+    uint64_t bytes_reserved;
+    uint32_t root;
+    uint32_t status;
+} vx_dag_stats;
+vx_status vx_dag_get_stats(const vx_dag *dag, vx_dag_stats *host_stats,
+                           vx_stream stream);
 
 #ifdef __cplusplus
 }

@@ -364,6 +364,70 @@ VX_HD uint64_t vx_terrain_leaf_mask(const vx_terrain *t, uint32_t x0,
     return m;
 }
 
+/* ------------------------------------------------- edit-stream generator --
+ * Host-only: seeded primitive lists for the benchmark configurations.  Per
+ * primitive, in this order: centre x, y, z uniform in [0, world); shape
+ * (sphere with probability sphere_permille / 1000, else box); op (add with
+ * probability add_permille / 1000); radius (spheres) or three half-extents
+ * (boxes), each uniform in [r_min, r_max] or, with log_uniform, floor of
+ * exp(u * ln(r_max + 1)) clamped to [r_min, r_max]; material uniform in
+ * [material_min, material_max] for adds, 0 for removes. */
+typedef struct vx_edit_mix {
+    uint32_t world_exp;
+    uint32_t sphere_permille;
+    uint32_t add_permille;
+    uint32_t r_min;
+    uint32_t r_max;
+    uint32_t log_uniform;
+    uint32_t material_min;
+    uint32_t material_max;
+} vx_edit_mix;
+
+#include <math.h>
+
+static inline double vx_pcg32_unit(vx_pcg32 *rng) {
+    return (double)vx_pcg32_next(rng) * (1.0 / 4294967296.0);
+}
+
+static inline uint32_t vx_draw_radius(vx_pcg32 *rng, const vx_edit_mix *m) {
+    if (!m->log_uniform)
+        return m->r_min + vx_pcg32_bounded(rng, m->r_max - m->r_min + 1u);
+    double r = floor(exp(vx_pcg32_unit(rng) * log((double)m->r_max + 1.0)));
+    if (r < (double)m->r_min) r = (double)m->r_min;
+    if (r > (double)m->r_max) r = (double)m->r_max;
+    return (uint32_t)r;
+}
+
+static inline void vx_generate_primitives_host(const vx_edit_mix *m, uint64_t seed,
+                                               uint64_t stream, uint64_t count,
+                                               vx_primitive *out) {
+    vx_pcg32 rng;
+    vx_pcg32_seed(&rng, seed, stream);
+    const uint32_t world = 4u << (m->world_exp - 2u);
+    for (uint64_t i = 0; i < count; ++i) {
+        vx_primitive p;
+        p.c[0] = (int32_t)vx_pcg32_bounded(&rng, world);
+        p.c[1] = (int32_t)vx_pcg32_bounded(&rng, world);
+        p.c[2] = (int32_t)vx_pcg32_bounded(&rng, world);
+        const uint32_t shape =
+            vx_pcg32_bounded(&rng, 1000u) < m->sphere_permille ? VX_SHAPE_SPHERE : VX_SHAPE_BOX;
+        const uint32_t op = vx_pcg32_bounded(&rng, 1000u) < m->add_permille ? VX_OP_ADD : VX_OP_REMOVE;
+        p.r[0] = vx_draw_radius(&rng, m);
+        if (shape == VX_SHAPE_BOX) {
+            p.r[1] = vx_draw_radius(&rng, m);
+            p.r[2] = vx_draw_radius(&rng, m);
+        } else {
+            p.r[1] = p.r[2] = 0u;
+        }
+        uint32_t mat = m->material_min +
+                       vx_pcg32_bounded(&rng, m->material_max - m->material_min + 1u);
+        if (op == VX_OP_REMOVE) mat = 0u;
+        p.flags = vx_make_flags(shape, op, mat);
+        p.reserved = 0u;
+        out[i] = p;
+    }
+}
+
 #ifdef __cplusplus
 }
 #endif

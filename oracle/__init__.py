@@ -127,3 +127,227 @@ def hash_set(inserts: np.ndarray, queries: np.ndarray):
     found = np.empty(q.size, np.uint32)
     lib().orc_hash_set_u64(_p(ins), ins.size, _p(st), _p(q), q.size, _p(found))
     return st, found
+
+
+# --------------------------------------------------------------- voxels --
+
+_VOXEL_SIGS = [
+    ("orc_grid_new", _P, [_U32, _I]),
+    ("orc_grid_free", None, [_P]),
+    ("orc_grid_terrain", None, [_P, _P]),
+    ("orc_grid_apply_prims", None, [_P, _P, _U64]),
+    ("orc_grid_apply_voxels", None, [_P, _P, _U64, _I, _U32]),
+    ("orc_grid_count", _U64, [_P]),
+    ("orc_grid_get", _I, [_P, _U32, _U32, _U32]),
+    ("orc_grid_export_dag", _I, [_P, C.POINTER(_U32), _P, _P, _U64, _P, _U64]),
+    ("orc_grid_export_svo", _I, [_P, C.POINTER(_U32), C.POINTER(_U32), _P, _U32,
+                                 _P, _P, _U32]),
+    ("orc_eval_voxels", None, [_P, _U32, _P, _U64, _P, _U64, _P, _I]),
+]
+_SIGS.extend(_VOXEL_SIGS)
+
+PRIM_DTYPE = np.dtype([("c", "<i4", 3), ("r", "<u4", 3), ("flags", "<u4"),
+                       ("reserved", "<u4")])
+TERRAIN_DTYPE = np.dtype([("seed", "<u4"), ("scale", "<u4"), ("caves", "<u4"),
+                          ("world_exp", "<u4")])
+
+
+def terrain(seed: int, scale: int, caves: bool, world_exp: int = 0) -> np.ndarray:
+    t = np.zeros(1, TERRAIN_DTYPE)
+    t[0] = (seed, scale, int(caves), world_exp)
+    return t
+
+
+class DagCanon:
+    """A canonical Hash DAG dump: root id, per-level node records
+    (10 words: child_mask, fill_mask, 8 child ids) and leaf masks."""
+
+    def __init__(self, root, counts, nodes, leaves):
+        self.root = int(root)
+        self.counts = [int(c) for c in counts]
+        self.nodes = np.asarray(nodes, np.uint32)
+        self.leaves = np.asarray(leaves, np.uint64)
+
+    def __eq__(self, other):
+        return (self.root == other.root and self.counts == other.counts
+                and np.array_equal(self.nodes, other.nodes)
+                and np.array_equal(self.leaves, other.leaves))
+
+    def __repr__(self):
+        return f"DagCanon(root={self.root}, counts={self.counts})"
+
+
+class SvoCanon:
+    def __init__(self, nodes, leaves, mats=None):
+        self.nodes = np.asarray(nodes, np.uint32)
+        self.leaves = np.asarray(leaves, np.uint64)
+        self.mats = None if mats is None else np.asarray(mats, np.uint8)
+
+    def __eq__(self, other):
+        if not (np.array_equal(self.nodes, other.nodes)
+                and np.array_equal(self.leaves, other.leaves)):
+            return False
+        if self.mats is None or other.mats is None:
+            return True
+        return np.array_equal(self.mats, other.mats)
+
+    def __repr__(self):
+        return f"SvoCanon(nodes={self.nodes.size // 8}, leaves={self.leaves.size})"
+
+
+def _dump_dag(fn, h, depth):
+    root = C.c_uint32(0)
+    counts = np.zeros(depth + 1, np.uint64)
+    fn(h, C.byref(root), counts.ctypes.data, None, 0, None, 0)
+    words = int(counts[:depth].sum()) * 10
+    nodes = np.zeros(max(words, 1), np.uint32)
+    leaves = np.zeros(max(int(counts[depth]), 1), np.uint64)
+    rc = fn(h, C.byref(root), counts.ctypes.data, nodes.ctypes.data, words,
+            leaves.ctypes.data, int(counts[depth]))
+    assert rc == 0
+    return DagCanon(root.value, counts, nodes[:words], leaves[:int(counts[depth])])
+
+
+class Grid:
+    """Dense voxel grid of a 4 << depth world with sequential edit semantics."""
+
+    def __init__(self, depth: int, materials: bool = False):
+        self.depth = depth
+        self.materials = materials
+        self._h = lib().orc_grid_new(depth, int(materials))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_grid_free(self._h)
+            self._h = None
+
+    def terrain(self, t: np.ndarray):
+        lib().orc_grid_terrain(self._h, t.ctypes.data)
+        return self
+
+    def apply_prims(self, prims: np.ndarray):
+        p = np.ascontiguousarray(prims, PRIM_DTYPE)
+        lib().orc_grid_apply_prims(self._h, p.ctypes.data, p.size)
+        return self
+
+    def apply_voxels(self, xyz: np.ndarray, op: int, material: int = 1):
+        v = np.ascontiguousarray(xyz, np.uint32).reshape(-1, 3)
+        lib().orc_grid_apply_voxels(self._h, v.ctypes.data, v.shape[0], op, material)
+        return self
+
+    def count(self) -> int:
+        return lib().orc_grid_count(self._h)
+
+    def get(self, x, y, z) -> int:
+        return lib().orc_grid_get(self._h, x, y, z)
+
+    def dag(self) -> DagCanon:
+        return _dump_dag(lib().orc_grid_export_dag, self._h, self.depth)
+
+    def svo(self) -> SvoCanon:
+        nn, nl = C.c_uint32(0), C.c_uint32(0)
+        f = lib().orc_grid_export_svo
+        f(self._h, C.byref(nn), C.byref(nl), None, 0, None, None, 0)
+        nodes = np.zeros(max(nn.value * 8, 1), np.uint32)
+        leaves = np.zeros(max(nl.value, 1), np.uint64)
+        mats = np.zeros(max(nl.value * 64, 1), np.uint8) if self.materials else None
+        rc = f(self._h, C.byref(nn), C.byref(nl), nodes.ctypes.data, nn.value,
+               leaves.ctypes.data, None if mats is None else mats.ctypes.data, nl.value)
+        assert rc == 0
+        return SvoCanon(nodes[:nn.value * 8], leaves[:nl.value],
+                        None if mats is None else mats[:nl.value * 64])
+
+
+def eval_voxels(t, world_exp, prims, xyz, materials=False) -> np.ndarray:
+    p = np.ascontiguousarray(prims, PRIM_DTYPE)
+    v = np.ascontiguousarray(xyz, np.uint32).reshape(-1, 3)
+    out = np.zeros(v.shape[0], np.uint8)
+    lib().orc_eval_voxels(None if t is None else t.ctypes.data, world_exp,
+                          p.ctypes.data, p.size, v.ctypes.data, v.shape[0],
+                          out.ctypes.data, int(materials))
+    return out
+
+
+class RefDag:
+    """The reference's own CPU HashDAG (algorithm/lib/include/algo/svt/hash_dag.hpp)."""
+
+    def __init__(self, depth: int):
+        self.depth = depth
+        self._h = ref().ref_dag_new(depth)
+        assert self._h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref().ref_dag_free(self._h)
+            self._h = None
+
+    def box(self, lo, hi, fill: bool):
+        """Half-open box [lo, hi) like HashDAG::Box."""
+        rc = ref().ref_dag_edit_box(self._h, *map(int, lo), *map(int, hi), int(fill))
+        assert rc == 0
+
+    def set_voxel(self, x, y, z, v: bool):
+        assert ref().ref_dag_set_voxel(self._h, x, y, z, int(v)) == 0
+
+    def get_voxel(self, x, y, z) -> int:
+        return ref().ref_dag_get_voxel(self._h, x, y, z)
+
+    def apply_prim_runs(self, p):
+        """Apply one sphere / box primitive as x-runs of boxes."""
+        world = 4 << self.depth
+        add = ((int(p["flags"]) >> 8) & 0xFF) == 1
+        c = [int(v) for v in p["c"]]
+        r = [int(v) for v in p["r"]]
+        if (int(p["flags"]) & 0xFF) == 1:  # box
+            lo = [max(0, c[a] - r[a]) for a in range(3)]
+            hi = [min(world, c[a] + r[a] + 1) for a in range(3)]
+            if all(hi[a] > lo[a] for a in range(3)):
+                self.box(lo, hi, add)
+            return
+        rad = r[0]
+        for z in range(max(0, c[2] - rad), min(world, c[2] + rad + 1)):
+            for y in range(max(0, c[1] - rad), min(world, c[1] + rad + 1)):
+                rem = rad * rad - (z - c[2]) ** 2 - (y - c[1]) ** 2
+                if rem < 0:
+                    continue
+                dx = int(np.floor(np.sqrt(rem)))
+                while dx * dx > rem:
+                    dx -= 1
+                while (dx + 1) * (dx + 1) <= rem:
+                    dx += 1
+                x0, x1 = max(0, c[0] - dx), min(world, c[0] + dx + 1)
+                if x1 > x0:
+                    self.box((x0, y, z), (x1, y + 1, z + 1), add)
+
+    def canon(self) -> DagCanon:
+        return _dump_dag(ref().ref_dag_export, self._h, self.depth)
+
+
+class RefSvo:
+    """The reference's own CPU SVO (algorithm/lib/include/algo/svt/svo.hpp)."""
+
+    def __init__(self, depth: int):
+        self.depth = depth
+        self._h = ref().ref_svo_new(depth)
+        assert self._h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref().ref_svo_free(self._h)
+            self._h = None
+
+    def set_voxel(self, x, y, z, v: bool):
+        assert ref().ref_svo_set_voxel(self._h, x, y, z, int(v)) == 0
+
+    def get_voxel(self, x, y, z) -> int:
+        return ref().ref_svo_get_voxel(self._h, x, y, z)
+
+    def canon(self) -> SvoCanon:
+        nn, nl = C.c_uint32(0), C.c_uint32(0)
+        f = ref().ref_svo_export
+        f(self._h, C.byref(nn), C.byref(nl), None, 0, None, 0)
+        nodes = np.zeros(max(nn.value * 8, 1), np.uint32)
+        leaves = np.zeros(max(nl.value, 1), np.uint64)
+        assert f(self._h, C.byref(nn), C.byref(nl), nodes.ctypes.data, nn.value,
+                 leaves.ctypes.data, nl.value) == 0
+        return SvoCanon(nodes[:nn.value * 8], leaves[:nl.value])

@@ -68,6 +68,13 @@ class vx_terrain(C.Structure):
                 ("caves", C.c_uint32), ("world_exp", C.c_uint32)]
 
 
+class vx_edit_mix(C.Structure):
+    _fields_ = [("world_exp", C.c_uint32), ("sphere_permille", C.c_uint32),
+                ("add_permille", C.c_uint32), ("r_min", C.c_uint32),
+                ("r_max", C.c_uint32), ("log_uniform", C.c_uint32),
+                ("material_min", C.c_uint32), ("material_max", C.c_uint32)]
+
+
 class vx_dag_config(C.Structure):
     _fields_ = [("depth", C.c_uint32), ("reserved0", C.c_uint32),
                 ("max_nodes", C.c_uint64), ("arena_bytes", C.c_uint64)]
@@ -110,6 +117,7 @@ _SIGS = {
     "vx_profile_launches": (_U64, []),
     "vx_profile_query": (_ST, [C.c_char_p, C.POINTER(C.c_double),
                                C.POINTER(_U64)]),
+    "vx_generate_primitives": (_ST, [C.POINTER(vx_edit_mix), _U64, _U64, _U64, _P]),
     "vx_scan_workspace_size": (_SZ, [_U32]),
     "vx_scan_exclusive_sum_u32": (_ST, [_P, _U32, _P, _SZ, _P]),
     "vx_scan_inclusive_sum_u32": (_ST, [_P, _U32, _P, _SZ, _P]),

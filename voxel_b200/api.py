@@ -8,13 +8,17 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import check, lib
 
 __all__ = [
     "stream_handle", "ptr", "exclusive_sum", "inclusive_sum", "sort_pairs",
-    "workspace_status", "SlabHashSet", "CuckooMap",
+    "workspace_status", "SlabHashSet", "CuckooMap", "PRIM_DTYPE",
+    "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
+    "generate_primitives", "config_c1_edits", "config_c3_edits",
+    "config_c4_edits",
 ]
 
 
@@ -183,3 +187,145 @@ class CuckooMap:
         check(lib().vx_cuckoo_dropped(self._h, C.byref(v), stream_handle()),
               "cuckoo dropped")
         return v.value
+
+
+PRIM_DTYPE = np.dtype([("c", "<i4", 3), ("r", "<u4", 3), ("flags", "<u4"),
+                       ("reserved", "<u4")])
+
+
+def make_flags(shape: int, op: int, material: int = 0) -> int:
+    return shape | (op << 8) | (material << 16)
+
+
+def prims_to_device(prims: np.ndarray, device) -> torch.Tensor:
+    """vx_primitive records (PRIM_DTYPE) -> int32 [n, 8] CUDA tensor."""
+    a = np.ascontiguousarray(prims, PRIM_DTYPE)
+    return torch.from_numpy(a.view(np.int32).reshape(-1, 8).copy()).to(device)
+
+
+def voxels_to_device(xyz: np.ndarray, device) -> torch.Tensor:
+    a = np.ascontiguousarray(xyz, np.uint32).reshape(-1, 3)
+    return torch.from_numpy(a.view(np.int32)).to(device)
+
+
+class HashDag:
+    """Hash DAG resident on the GPU (HashDagGpu / DeviceHashDagGpu,
+    hash_dag_gpu/storage.cuh:16-105, widened to depth 1..14)."""
+
+    def __init__(self, depth: int, max_nodes: int = 1 << 20, arena_bytes: int = 0):
+        from . import vx_dag_config
+        cfg = vx_dag_config(depth, 0, max_nodes, arena_bytes)
+        h = C.c_void_p()
+        check(lib().vx_dag_create(C.byref(cfg), C.byref(h)), "vx_dag_create")
+        self._h = h
+        self.depth = depth
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_dag_destroy(h)
+            self._h = None
+
+    @property
+    def world(self) -> int:
+        return 4 << self.depth
+
+    def reset(self):
+        check(lib().vx_dag_reset(self._h, stream_handle()), "vx_dag_reset")
+
+    def workspace_size(self, count: int) -> int:
+        return lib().vx_dag_voxel_workspace_size(count)
+
+    def apply_voxels(self, voxels: torch.Tensor, op: int,
+                     workspace: torch.Tensor | None = None) -> int:
+        """Plain path: place (op=1) or destroy (op=0) a voxel list
+        (hash_dag_gpu::apply_voxel_edits, hash_dag_gpu/edit.cuh:21-41).
+        Returns the status (0 or an error code) like the reference."""
+        n = voxels.numel() // 3
+        ws = workspace
+        if ws is None and n:
+            ws = torch.empty(self.workspace_size(n), dtype=torch.uint8,
+                             device=voxels.device)
+        return lib().vx_dag_apply_voxels(self._h, ptr(voxels) if n else None, n,
+                                         op, ptr(ws) if n else None,
+                                         ws.numel() if n else 0, stream_handle())
+
+    def apply_primitives(self, prims: torch.Tensor) -> None:
+        """Batched path: primitives applied as if in order; asynchronous
+        (check with status())."""
+        n = prims.numel() // 8
+        check(lib().vx_dag_apply_primitives(self._h, ptr(prims) if n else None,
+                                            n, stream_handle()),
+              "vx_dag_apply_primitives")
+
+    def status(self) -> int:
+        return lib().vx_dag_status(self._h, stream_handle())
+
+    def build_terrain(self, seed: int, scale: int, caves: bool) -> None:
+        from . import vx_terrain
+        t = vx_terrain(seed, scale, int(caves), self.depth + 2)
+        check(lib().vx_dag_build_terrain(self._h, C.byref(t), stream_handle()),
+              "vx_dag_build_terrain")
+
+    def query(self, voxels: torch.Tensor) -> torch.Tensor:
+        n = voxels.numel() // 3
+        out = torch.empty(n, dtype=torch.uint8, device=voxels.device)
+        check(lib().vx_dag_query(self._h, ptr(voxels), n, ptr(out), stream_handle()),
+              "vx_dag_query")
+        return out
+
+    def stats(self):
+        from . import vx_dag_stats
+        st = vx_dag_stats()
+        check(lib().vx_dag_get_stats(self._h, C.byref(st), stream_handle()),
+              "vx_dag_get_stats")
+        return st
+
+    def canonical(self):
+        """(root, counts, nodes, leaves): DFS first-visit canonical dump."""
+        root = C.c_uint32(0)
+        counts = np.zeros(self.depth + 1, np.uint64)
+        f = lib().vx_dag_export_canonical
+        check(f(self._h, C.byref(root), counts.ctypes.data, None, 0, None, 0,
+                stream_handle()), "export sizes")
+        words = int(counts[:self.depth].sum()) * 10
+        nodes = np.zeros(max(words, 1), np.uint32)
+        nl = int(counts[self.depth])
+        leaves = np.zeros(max(nl, 1), np.uint64)
+        check(f(self._h, C.byref(root), counts.ctypes.data, nodes.ctypes.data,
+                words, leaves.ctypes.data, nl, stream_handle()), "export")
+        return root.value, counts, nodes[:words], leaves[:nl]
+
+
+def generate_primitives(world_exp: int, count: int, seed: int, *,
+                        sphere_permille: int = 1000, add_permille: int = 500,
+                        r_min: int = 1, r_max: int = 16, log_uniform: bool = False,
+                        material_min: int = 1, material_max: int = 255,
+                        stream: int = 0) -> np.ndarray:
+    """Seeded primitive list (PRIM_DTYPE) from the library's generator."""
+    from . import vx_edit_mix
+    mix = vx_edit_mix(world_exp, sphere_permille, add_permille, r_min, r_max,
+                      int(log_uniform), material_min, material_max)
+    out = np.zeros(count, PRIM_DTYPE)
+    check(lib().vx_generate_primitives(C.byref(mix), seed, stream, count,
+                                       out.ctypes.data if count else None),
+          "vx_generate_primitives")
+    return out
+
+
+# The benchmark configurations' edit mixes.
+def config_c1_edits(count: int = 1000, seed: int = 1) -> np.ndarray:
+    """Plain SVO: 256^3, spheres r in U{2..16}, 50/50, materials U{1..255}."""
+    return generate_primitives(8, count, seed, r_min=2, r_max=16)
+
+
+def config_c3_edits(count: int = 65536, seed: int = 6, world_exp: int = 12) -> np.ndarray:
+    """Batched SVO: 70% spheres / 30% boxes, r log-uniform [1, 64], 50/50."""
+    return generate_primitives(world_exp, count, seed, sphere_permille=700,
+                               r_min=1, r_max=64, log_uniform=True)
+
+
+def config_c4_edits(count: int = 16384, seed: int = 7, world_exp: int = 14) -> np.ndarray:
+    """Batched Hash DAG: spheres r log-uniform [1, 256], 60% add."""
+    return generate_primitives(world_exp, count, seed, add_permille=600,
+                               r_min=1, r_max=256, log_uniform=True)

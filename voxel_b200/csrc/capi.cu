@@ -134,3 +134,19 @@ vx_status vx_profile_query(const char *name, double *host_total_ms,
 }
 
 } // extern "C"
+
+extern "C" {
+
+// Seeded primitive list for a benchmark configuration, written to host memory
+// (the generator of vx_workload.h; no device work).
+vx_status vx_generate_primitives(const vx_edit_mix *mix, uint64_t seed,
+                                 uint64_t stream, uint64_t count,
+                                 vx_primitive *host_out) {
+  if (mix == nullptr || (host_out == nullptr && count != 0) || mix->world_exp < 3 ||
+      mix->r_max < mix->r_min || mix->material_max < mix->material_min)
+    return VX_ERR_INVALID_VALUE;
+  vx_generate_primitives_host(mix, seed, stream, count, host_out);
+  return VX_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,980 @@
+// Hash DAG resident on one B200: hash-consed per-level tables, batched
+// primitive edits, the plain per-call voxel-list path, terrain builds,
+// queries and a canonical dump.
+//
+// Storage (one table per level):
+//   inner level l < depth: a word pool holding items
+//       [child_mask | fill_mask << 8, child refs of child_mask in order]
+//     (the reference's canonical item, hash_dag_gpu/detail/node.cuh:266-289)
+//     and an open-addressing index of 64-bit slots {tag, ref}; ref = word
+//     offset + 2.  An insert reserves an empty slot with the busy marker,
+//     appends the item to the pool and publishes {tag, ref} with a release
+//     store; readers that meet a busy slot with their tag wait (bounded).
+//   leaf level: an open-addressing set of the 64-bit masks themselves;
+//     ref = slot + 2.  Masks 0 and ~0 are never stored: refs 0 and 1 are the
+//     empty / full subtree of any level (hash_dag_gpu/config.cuh:30-37).
+// Structural sharing is by content: two equal subtrees of a level always
+// have the same ref, so an edit copies only the paths it changes.
+#include "edit_common.cuh"
+#include "profile.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+namespace vx::dag {
+
+using namespace vx::edit;
+
+constexpr uint32_t kEmptyRef = 0, kFullRef = 1;
+constexpr uint32_t kBusy = 0xffffffffu;
+constexpr uint32_t kMaxDepth = 14;
+constexpr uint32_t kMaxProbes = 1u << 16;
+
+struct Tables {
+  uint32_t depth;
+  uint32_t *pool[kMaxDepth];
+  uint64_t *index[kMaxDepth];
+  uint64_t pool_cap[kMaxDepth];
+  uint64_t index_mask[kMaxDepth];
+  uint64_t *leaves;
+  uint64_t leaf_mask;
+  Header *hdr;
+};
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+
+__device__ __forceinline__ uint64_t hash_words(const uint32_t *w, uint32_t n) {
+  uint64_t h = 0x243f6a8885a308d3ull ^ n;
+  for (uint32_t i = 0; i < n; ++i) h = mix64(h ^ (static_cast<uint64_t>(w[i]) + (static_cast<uint64_t>(i) << 32)));
+  return h;
+}
+
+// ------------------------------------------------------------- reading --
+
+__device__ __forceinline__ uint64_t read_leaf(const Tables &t, uint32_t ref) {
+  if (ref == kEmptyRef) return 0ull;
+  if (ref == kFullRef) return ~0ull;
+  return t.leaves[ref - 2];
+}
+
+// Child c of the node `ref` at inner level l (refs 0/1 are uniform subtrees).
+__device__ __forceinline__ uint32_t child_ref(const Tables &t, uint32_t l,
+                                              uint32_t ref, uint32_t c) {
+  if (ref <= kFullRef) return ref;
+  const uint32_t *item = t.pool[l] + (ref - 2);
+  const uint32_t header = item[0];
+  const uint32_t cm = header & 0xffu, fm = (header >> 8) & 0xffu;
+  const uint32_t bit = 1u << c;
+  if (cm & bit) return item[1 + __popc(cm & (bit - 1u))];
+  return (fm & bit) ? kFullRef : kEmptyRef;
+}
+
+// ---------------------------------------------------------- hash-consing --
+
+__device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
+  uint64_t pos = mix64(mask) & t.leaf_mask;
+  for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+    const uint64_t v = ld_relaxed_u64(t.leaves + pos);
+    if (v == mask) return static_cast<uint32_t>(pos + 2);
+    if (v == 0) {
+      const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(t.leaves + pos),
+                                     0ull, static_cast<unsigned long long>(mask));
+      if (old == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[t.depth]), 1ull);
+        return static_cast<uint32_t>(pos + 2);
+      }
+      if (old == mask) return static_cast<uint32_t>(pos + 2);
+    }
+    pos = (pos + 1) & t.leaf_mask;
+  }
+  set_status(&t.hdr->status, kDevCapacity);
+  return kEmptyRef;
+}
+
+__device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
+                                        const uint32_t *w, uint32_t n) {
+  const uint64_t h = hash_words(w, n);
+  const uint32_t tag = static_cast<uint32_t>(h >> 32) | 1u;
+  uint64_t *idx = t.index[l];
+  uint32_t *pool = t.pool[l];
+  uint64_t pos = h & t.index_mask[l];
+  for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+    uint64_t v = ld_acquire_u64(idx + pos);
+    if (v == 0) {
+      const uint64_t claim = (static_cast<uint64_t>(tag) << 32) | kBusy;
+      const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos),
+                                     0ull, static_cast<unsigned long long>(claim));
+      if (old == 0) {
+        const uint32_t off = atomicAdd(&t.hdr->pool_used[l], n);
+        if (static_cast<uint64_t>(off) + n > t.pool_cap[l]) {
+          set_status(&t.hdr->status, kDevCapacity);
+          // Leave a dead entry (ref 1 never matches an item) so waiters move on.
+          st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | kFullRef);
+          return kEmptyRef;
+        }
+        for (uint32_t i = 0; i < n; ++i) pool[off + i] = w[i];
+        st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | (off + 2u));
+        atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]), 1ull);
+        return off + 2u;
+      }
+      v = old;
+    }
+    if (static_cast<uint32_t>(v >> 32) == tag) {
+      uint32_t r = static_cast<uint32_t>(v);
+      if (r == kBusy) {
+        const uint64_t t0 = global_ns();
+        while (r == kBusy) {
+          if (global_ns() - t0 > kWaitLimitNs) {
+            set_status(&t.hdr->status, kDevTimeout);
+            return kEmptyRef;
+          }
+          __nanosleep(64);
+          r = static_cast<uint32_t>(ld_acquire_u64(idx + pos));
+        }
+      }
+      if (r >= 2u) {
+        const uint32_t *item = pool + (r - 2u);
+        bool eq = true;
+        for (uint32_t i = 0; i < n && eq; ++i) eq = item[i] == w[i];
+        if (eq) return r;
+      }
+    }
+    pos = (pos + 1) & t.index_mask[l];
+  }
+  set_status(&t.hdr->status, kDevCapacity);
+  return kEmptyRef;
+}
+
+// Canonical ref of a node given its 8 child refs: uniform nodes collapse to
+// the sentinels, everything else is hash-consed into level l's table.
+__device__ uint32_t canon_node(const Tables &t, uint32_t l,
+                               const uint32_t (&child)[8]) {
+  uint32_t w[9];
+  uint32_t cm = 0, fm = 0, n = 1;
+#pragma unroll
+  for (uint32_t c = 0; c < 8; ++c) {
+    const uint32_t r = child[c];
+    if (r == kFullRef) fm |= 1u << c;
+    else if (r >= 2u) {
+      cm |= 1u << c;
+      w[n++] = r;
+    }
+  }
+  if (cm == 0) {
+    if (fm == 0) return kEmptyRef;
+    if (fm == 0xffu) return kFullRef;
+  }
+  w[0] = cm | (fm << 8);
+  return node_find_or_insert(t, l, w, n);
+}
+
+__device__ __forceinline__ uint32_t canon_leaf(const Tables &t, uint64_t mask) {
+  if (mask == 0) return kEmptyRef;
+  if (mask == ~0ull) return kFullRef;
+  return leaf_find_or_insert(t, mask);
+}
+
+// ------------------------------------------------------------ pipeline --
+
+struct Ctx {
+  Tables t;
+  Arena a;
+  const vx_primitive *prims;
+  const uint32_t *d_prim_count; // device count (NULL: use host_prim_count)
+  uint32_t host_prim_count;
+};
+
+__global__ void init_kernel(Ctx x) {
+  Header *h = x.t.hdr;
+  const uint32_t n = x.d_prim_count ? *x.d_prim_count : x.host_prim_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (uint32_t l = 0; l < 16; ++l) {
+      h->item_off[l] = 0;
+      h->item_count[l] = 0;
+      h->pair_count[l] = 0;
+    }
+    h->prim_count = n;
+    const uint32_t ok = h->status == kDevOk && n <= x.a.pair_cap;
+    if (h->status == kDevOk && n > x.a.pair_cap) h->status = kDevCapacity;
+    if (ok) {
+      h->item_count[0] = 1;
+      h->pair_count[0] = n;
+      Item it{};
+      it.cell = 0;
+      it.old = h->root;
+      it.pstart = 0;
+      it.pcount = n;
+      x.a.items[0] = it;
+    }
+  }
+  if (n > x.a.pair_cap) return;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    x.a.pairs[0][i] = static_cast<uint32_t>(i);
+}
+
+// Top-down expansion of level l into level l + 1 (l + 1 < depth).  One warp
+// per work item; lanes walk the item's primitive list 32 at a time.
+template <class Tree>
+__global__ void __launch_bounds__(kBlock)
+    expand_kernel(Ctx x, Tree tree, uint32_t l) {
+  Header *h = x.t.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t depth = x.t.depth;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  const uint32_t next_base = base + W;
+  if (blockIdx.x == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
+  const uint32_t *in_pairs = x.a.pairs[l & 1u];
+  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
+  const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
+  const uint32_t world_exp = depth + 2;
+
+  __shared__ uint32_t s_items[kBlock / kWarp], s_pairs[kBlock / kWarp];
+  __shared__ uint32_t s_item_base, s_pair_base;
+  const uint32_t warp = threadIdx.x / kWarp, lane = lane_id();
+  constexpr uint32_t kWarpsPerBlock = kBlock / kWarp;
+
+  for (uint64_t tile = blockIdx.x; tile * kWarpsPerBlock < W; tile += gridDim.x) {
+    const uint32_t wi = static_cast<uint32_t>(tile * kWarpsPerBlock) + warp;
+    const bool have = wi < W;
+    Item it{};
+    if (have) it = x.a.items[base + wi];
+    const Cell cell = unpack_cell(it.cell);
+    int32_t full_max[8];
+    uint32_t cnt[8];
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      full_max[c] = -1;
+      cnt[c] = 0;
+    }
+    const uint32_t pc = have ? it.pcount : 0;
+    // Pass 1: last fully-covering primitive per child.
+    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
+      const uint32_t k = k0 + lane;
+      int32_t p = -1;
+      uint32_t code = 0;
+      if (k < pc) {
+        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
+        const vx_primitive pr = x.prims[p];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
+          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
+          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
+          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
+        }
+      }
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        const int32_t f = ((code >> (2 * c)) & 3u) == VX_CELL_FULL ? p : -1;
+        full_max[c] = max(full_max[c], __reduce_max_sync(kFullMask, f));
+      }
+    }
+    // Pass 2: partially-covering primitives after that.
+    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
+      const uint32_t k = k0 + lane;
+      int32_t p = -1;
+      uint32_t code = 0;
+      if (k < pc) {
+        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
+        const vx_primitive pr = x.prims[p];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
+          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
+          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
+          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
+        }
+      }
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c)
+        cnt[c] += __popc(__ballot_sync(
+            kFullMask, ((code >> (2 * c)) & 3u) == VX_CELL_MIXED && p > full_max[c]));
+    }
+    uint32_t child_mask = 0, const_mask = 0, const_full = 0, n_items = 0, n_pairs = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      if (cnt[c]) {
+        child_mask |= 1u << c;
+        ++n_items;
+        n_pairs += cnt[c];
+      }
+      if (full_max[c] >= 0) {
+        const_mask |= 1u << c;
+        if (vx_prim_op(&x.prims[full_max[c]]) == VX_OP_ADD) const_full |= 1u << c;
+      }
+    }
+    if (lane == 0) {
+      s_items[warp] = n_items;
+      s_pairs[warp] = n_pairs;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t ti = 0, tp = 0;
+      for (uint32_t w = 0; w < kWarpsPerBlock; ++w) {
+        const uint32_t a = s_items[w], b = s_pairs[w];
+        s_items[w] = ti;
+        s_pairs[w] = tp;
+        ti += a;
+        tp += b;
+      }
+      s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
+      s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
+      if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
+        set_status(&h->status, kDevCapacity);
+      if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
+        set_status(&h->status, kDevCapacity);
+    }
+    __syncthreads();
+    const bool room = ld_relaxed_u32(&h->status) == kDevOk;
+    const uint32_t item_off = s_item_base + s_items[warp];
+    uint32_t pair_off = s_pair_base + s_pairs[warp];
+    __syncthreads(); // s_* reused by the next tile
+    if (!have || !room) continue;
+
+    // Emit child items (in child order) and their primitive lists.
+    uint32_t child_pstart[8];
+    {
+      uint32_t k = 0, po = pair_off;
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        child_pstart[c] = po;
+        if (cnt[c] && lane == 0) {
+          Item ci{};
+          ci.cell = child_cell(it.cell, c);
+          ci.old = (const_mask >> c) & 1u ? (((const_full >> c) & 1u) ? kFullRef : kEmptyRef)
+                                          : tree.child(l, it.old, c);
+          ci.pstart = po;
+          ci.pcount = cnt[c];
+          x.a.items[next_base + item_off + k] = ci;
+        }
+        if (cnt[c]) ++k;
+        po += cnt[c];
+      }
+    }
+    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
+      const uint32_t k = k0 + lane;
+      int32_t p = -1;
+      uint32_t code = 0;
+      if (k < pc) {
+        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
+        const vx_primitive pr = x.prims[p];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
+          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
+          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
+          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
+        }
+      }
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        const bool take = ((code >> (2 * c)) & 3u) == VX_CELL_MIXED && p > full_max[c];
+        const uint32_t b = __ballot_sync(kFullMask, take);
+        if (take) out_pairs[child_pstart[c] + __popc(b & lanemask_lt())] = static_cast<uint32_t>(p);
+        child_pstart[c] += __popc(b);
+      }
+    }
+    if (lane == 0) {
+      x.a.items[base + wi].child_base = next_base + item_off;
+      x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
+    }
+  }
+}
+
+struct DagTree {
+  Tables t;
+  __device__ uint32_t child(uint32_t l, uint32_t ref, uint32_t c) const {
+    return child_ref(t, l, ref, c);
+  }
+};
+
+// Level depth - 1: evaluate the 8 leaves of every item (8 threads per item)
+// and hash-cons the item.
+__global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
+  Header *h = x.t.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t l = x.t.depth - 1;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  const uint32_t *pairs = x.a.pairs[l & 1u];
+  const uint32_t world_exp = x.t.depth + 2;
+  const uint32_t lane = lane_id();
+  const uint64_t total = static_cast<uint64_t>(W) * 8u;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
+       g0 < total; g0 += stride) {
+    const uint64_t g = g0 + lane;
+    const bool have = g < total;
+    const uint32_t wi = static_cast<uint32_t>(g >> 3), c = lane & 7u;
+    uint32_t result = kEmptyRef;
+    Item it{};
+    if (have) {
+      it = x.a.items[base + wi];
+      const Cell cell = unpack_cell(it.cell);
+      const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * 4;
+      const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
+      const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
+      const uint32_t old_child = child_ref(x.t, l, it.old, c);
+      uint64_t mask = 0;
+      bool loaded = false, touched = false;
+      for (uint32_t k = 0; k < it.pcount; ++k) {
+        const vx_primitive pr = x.prims[pairs[it.pstart + k]];
+        const uint32_t cls = classify(pr, world_exp, ox, oy, oz, 4);
+        if (cls == VX_CELL_EMPTY) continue;
+        const bool add = vx_prim_op(&pr) == VX_OP_ADD;
+        touched = true;
+        if (cls == VX_CELL_FULL) {
+          mask = add ? ~0ull : 0ull;
+          loaded = true;
+          continue;
+        }
+        if (!loaded) {
+          mask = read_leaf(x.t, old_child);
+          loaded = true;
+        }
+        const uint64_t m = leaf_mask(pr, world_exp, ox, oy, oz);
+        mask = add ? (mask | m) : (mask & ~m);
+      }
+      result = touched ? canon_leaf(x.t, mask) : old_child;
+    }
+    uint32_t child[8];
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k)
+      child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
+    if (have && c == 0) x.a.items[base + wi].result = canon_node(x.t, l, child);
+  }
+}
+
+// Bottom-up rebuild of level l from its children's results.
+__global__ void __launch_bounds__(kBlock) build_kernel(Ctx x, uint32_t l) {
+  Header *h = x.t.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < W; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const Item it = x.a.items[base + i];
+    const uint32_t cm = it.masks & 0xffu, km = (it.masks >> 8) & 0xffu,
+                   kf = (it.masks >> 16) & 0xffu;
+    uint32_t child[8];
+    uint32_t k = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const uint32_t bit = 1u << c;
+      if (cm & bit) child[c] = x.a.items[it.child_base + k++].result;
+      else if (km & bit) child[c] = (kf & bit) ? kFullRef : kEmptyRef;
+      else child[c] = child_ref(x.t, l, it.old, c);
+    }
+    x.a.items[base + i].result = canon_node(x.t, l, child);
+  }
+}
+
+__global__ void publish_kernel(Ctx x) {
+  Header *h = x.t.hdr;
+  if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;
+}
+
+__global__ void query_kernel(Tables t, const vx_voxel *pts, uint32_t n,
+                             uint8_t *out) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const vx_voxel p = pts[i];
+  const uint32_t side_exp = t.depth + 2;
+  if ((p.x >> side_exp) | (p.y >> side_exp) | (p.z >> side_exp)) {
+    out[i] = 0;
+    return;
+  }
+  uint32_t ref = t.hdr->root;
+  for (uint32_t l = 0; l < t.depth && ref >= 2u; ++l) {
+    const uint32_t s = side_exp - 1 - l;
+    const uint32_t c = ((p.x >> s) & 1u) | (((p.y >> s) & 1u) << 1) | (((p.z >> s) & 1u) << 2);
+    ref = child_ref(t, l, ref, c);
+  }
+  if (ref <= kFullRef) {
+    out[i] = static_cast<uint8_t>(ref);
+    return;
+  }
+  const uint32_t bit = (p.x & 3u) + 4u * (p.y & 3u) + 16u * (p.z & 3u);
+  out[i] = static_cast<uint8_t>((t.leaves[ref - 2] >> bit) & 1ull);
+}
+
+// ------------------------------------------------------- plain path prep --
+
+// Voxel -> (leaf key, bit).  The key is the leaf's Morton path, 3 bits per
+// inner level with the root's child in the top bits (the reference's
+// make_leaf_key, hash_dag_gpu/detail/node.cuh:67-85, widened to 64 bits);
+// voxels outside the world get key 1 << (3 * depth) and are dropped.
+__global__ void pack_voxels_kernel(const vx_voxel *v, uint32_t n, uint32_t depth,
+                                   uint64_t *keys, uint32_t *bits) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const vx_voxel p = v[i];
+  const uint32_t side_exp = depth + 2;
+  if ((p.x >> side_exp) | (p.y >> side_exp) | (p.z >> side_exp)) {
+    keys[i] = 1ull << (3 * depth);
+    bits[i] = 0;
+    return;
+  }
+  uint64_t key = 0;
+  for (uint32_t l = 0; l < depth; ++l) {
+    const uint32_t s = side_exp - 1 - l;
+    key = (key << 3) | (((p.x >> s) & 1u) | (((p.y >> s) & 1u) << 1) | (((p.z >> s) & 1u) << 2));
+  }
+  keys[i] = key;
+  bits[i] = (p.x & 3u) + 4u * (p.y & 3u) + 16u * (p.z & 3u);
+}
+
+__global__ void run_flags_kernel(const uint64_t *keys, uint32_t n, uint32_t depth,
+                                 uint32_t *flags) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const bool valid = keys[i] < (1ull << (3 * depth));
+  flags[i] = (valid && (i == 0 || keys[i - 1] != keys[i])) ? 1u : 0u;
+}
+
+// Each run start ORs its run's bits into one leaf-mask primitive.
+__global__ void reduce_runs_kernel(const uint64_t *keys, const uint32_t *bits,
+                                   const uint32_t *offsets, uint32_t n,
+                                   uint32_t depth, uint32_t op,
+                                   vx_primitive *out, uint32_t *out_count) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t key = keys[i];
+  const bool valid = key < (1ull << (3 * depth));
+  const bool start = valid && (i == 0 || keys[i - 1] != key);
+  if (start) {
+    uint64_t mask = 0;
+    for (uint64_t j = i; j < n && keys[j] == key; ++j) mask |= 1ull << bits[j];
+    uint32_t lx = 0, ly = 0, lz = 0;
+    for (uint32_t l = 0; l < depth; ++l) {
+      const uint32_t c = static_cast<uint32_t>(key >> (3 * (depth - 1 - l))) & 7u;
+      lx = (lx << 1) | (c & 1u);
+      ly = (ly << 1) | ((c >> 1) & 1u);
+      lz = (lz << 1) | ((c >> 2) & 1u);
+    }
+    vx_primitive p{};
+    p.c[0] = static_cast<int32_t>(lx * 4);
+    p.c[1] = static_cast<int32_t>(ly * 4);
+    p.c[2] = static_cast<int32_t>(lz * 4);
+    p.r[0] = static_cast<uint32_t>(mask);
+    p.r[1] = static_cast<uint32_t>(mask >> 32);
+    p.flags = vx_make_flags(kShapeLeafMask, op, 0);
+    out[offsets[i]] = p;
+  }
+  if (i == n - 1) *out_count = offsets[i] + (start ? 1u : 0u);
+}
+
+} // namespace vx::dag
+
+// ================================================================ handle ==
+
+struct vx_dag {
+  vx::dag::Tables t{};
+  vx::edit::Arena a{};
+  uint64_t index_slots[vx::dag::kMaxDepth] = {};
+  uint64_t leaf_slots = 0;
+  void *arena_mem = nullptr;
+  size_t bytes = 0;
+  vx_primitive *tmp_prim = nullptr; // one terrain primitive
+};
+
+namespace vx::dag {
+
+inline uint64_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
+                       const uint32_t *d_count, uint32_t host_count,
+                       cudaStream_t s) {
+  Ctx x{d->t, d->a, prims, d_count, host_count};
+  const uint32_t depth = d->t.depth;
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
+  {
+    prof::Scope sc("dag_init", s);
+    init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),
+                  kBlock, 0, s>>>(x);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  DagTree tree{d->t};
+  for (uint32_t l = 0; l + 1 < depth; ++l) {
+    prof::Scope sc("dag_expand", s);
+    expand_kernel<DagTree><<<grid, kBlock, 0, s>>>(x, tree, l);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  {
+    prof::Scope sc("dag_leafparent", s);
+    leafparent_kernel<<<grid, kBlock, 0, s>>>(x);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  for (uint32_t r = depth - 1; r > 0; --r) {
+    prof::Scope sc("dag_build", s);
+    build_kernel<<<grid, kBlock, 0, s>>>(x, r - 1);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  {
+    prof::Scope sc("dag_publish", s);
+    publish_kernel<<<1, 1, 0, s>>>(x);
+  }
+  return from_cuda(cudaGetLastError());
+}
+
+vx_status read_status(vx_dag *d, cudaStream_t s, bool clear) {
+  uint32_t code = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(&code, &d->t.hdr->status, sizeof(code),
+                              cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  if (clear && code != kDevOk)
+    VX_TRY_CUDA(cudaMemsetAsync(&d->t.hdr->status, 0, sizeof(uint32_t), s));
+  if (clear) VX_TRY_CUDA(cudaStreamSynchronize(s));
+  return status_from_device(code);
+}
+
+struct PlainLayout {
+  uint64_t *keys;
+  uint32_t *bits;
+  uint32_t *offsets;
+  vx_primitive *prims;
+  uint32_t *count;
+  void *sort_ws;
+  size_t sort_ws_bytes;
+  void *scan_ws;
+  size_t scan_ws_bytes;
+};
+
+template <class C> PlainLayout plain_layout(C &c, uint32_t n) {
+  PlainLayout p{};
+  p.keys = c.template take<uint64_t>(n);
+  p.bits = c.template take<uint32_t>(n);
+  p.offsets = c.template take<uint32_t>(n);
+  p.prims = c.template take<vx_primitive>(n);
+  p.count = c.template take<uint32_t>(1);
+  p.sort_ws_bytes = vx_sort_workspace_size(n, 8);
+  p.sort_ws = c.template take<char>(p.sort_ws_bytes);
+  p.scan_ws_bytes = vx_scan_workspace_size(n);
+  p.scan_ws = c.template take<char>(p.scan_ws_bytes);
+  return p;
+}
+
+struct NullCarver {
+  size_t offset = 0;
+  template <class T> T *take(size_t count) {
+    offset = align_up(offset, 256);
+    offset += count * sizeof(T);
+    return nullptr;
+  }
+};
+
+} // namespace vx::dag
+
+using namespace vx::dag;
+
+extern "C" {
+
+vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
+  if (cfg == nullptr || out == nullptr || cfg->depth < 1 || cfg->depth > kMaxDepth ||
+      cfg->max_nodes < 16)
+    return VX_ERR_INVALID_VALUE;
+  int devs = 0;
+  if (cudaGetDeviceCount(&devs) != cudaSuccess || devs == 0) return VX_ERR_NO_DEVICE;
+  auto *d = new (std::nothrow) vx_dag;
+  if (d == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  d->t.depth = cfg->depth;
+  auto fail = [&](cudaError_t e) {
+    vx_dag_destroy(d);
+    return vx::from_cuda(e);
+  };
+  cudaError_t e;
+  for (uint32_t l = 0; l < cfg->depth; ++l) {
+    // Level l holds at most 8^l live nodes, plus superseded ones from earlier
+    // edits; small levels keep room for 2^20 items.
+    const double live = l < 21 ? std::pow(8.0, static_cast<double>(l)) : 1e30;
+    const uint64_t cap = std::min<uint64_t>(
+        cfg->max_nodes, std::max<uint64_t>(1u << 20, static_cast<uint64_t>(std::min(live * 4, 1e18))));
+    d->index_slots[l] = next_pow2(cap * 2);
+    d->t.index_mask[l] = d->index_slots[l] - 1;
+    d->t.pool_cap[l] = std::min<uint64_t>(cap * 6, 0xfffffff0ull);
+    if ((e = cudaMalloc(&d->t.index[l], d->index_slots[l] * 8)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&d->t.pool[l], d->t.pool_cap[l] * 4)) != cudaSuccess) return fail(e);
+    d->bytes += d->index_slots[l] * 8 + d->t.pool_cap[l] * 4;
+  }
+  d->leaf_slots = next_pow2(cfg->max_nodes * 2);
+  d->t.leaf_mask = d->leaf_slots - 1;
+  if ((e = cudaMalloc(&d->t.leaves, d->leaf_slots * 8)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&d->t.hdr, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&d->tmp_prim, sizeof(vx_primitive))) != cudaSuccess) return fail(e);
+  d->bytes += d->leaf_slots * 8;
+  const uint64_t arena = cfg->arena_bytes ? cfg->arena_bytes : (512ull << 20);
+  if ((e = cudaMalloc(&d->arena_mem, arena)) != cudaSuccess) return fail(e);
+  d->bytes += arena;
+  const uint64_t item_bytes = arena / 10 * 6;
+  d->a.items = static_cast<vx::edit::Item *>(d->arena_mem);
+  d->a.item_cap = static_cast<uint32_t>(std::min<uint64_t>(item_bytes / sizeof(vx::edit::Item), 0xffffffffull));
+  const uint64_t pair_bytes = (arena - item_bytes) / 2 / 256 * 256;
+  d->a.pairs[0] = reinterpret_cast<uint32_t *>(static_cast<char *>(d->arena_mem) + item_bytes);
+  d->a.pairs[1] = reinterpret_cast<uint32_t *>(static_cast<char *>(d->arena_mem) + item_bytes + pair_bytes);
+  d->a.pair_cap = static_cast<uint32_t>(std::min<uint64_t>(pair_bytes / 4, 0xffffffffull));
+  const vx_status st = vx_dag_reset(d, nullptr);
+  if (st != VX_OK) {
+    vx_dag_destroy(d);
+    return st;
+  }
+  if ((e = cudaStreamSynchronize(nullptr)) != cudaSuccess) return fail(e);
+  *out = d;
+  return VX_OK;
+}
+
+vx_status vx_dag_destroy(vx_dag *d) {
+  if (d == nullptr) return VX_ERR_INVALID_VALUE;
+  for (uint32_t l = 0; l < kMaxDepth; ++l) {
+    cudaFree(d->t.index[l]);
+    cudaFree(d->t.pool[l]);
+  }
+  cudaFree(d->t.leaves);
+  cudaFree(d->t.hdr);
+  cudaFree(d->arena_mem);
+  cudaFree(d->tmp_prim);
+  delete d;
+  return VX_OK;
+}
+
+vx_status vx_dag_reset(vx_dag *d, vx_stream stream) {
+  if (d == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (uint32_t l = 0; l < d->t.depth; ++l)
+    VX_TRY_CUDA(cudaMemsetAsync(d->t.index[l], 0, d->index_slots[l] * 8, s));
+  VX_TRY_CUDA(cudaMemsetAsync(d->t.leaves, 0, d->leaf_slots * 8, s));
+  VX_TRY_CUDA(cudaMemsetAsync(d->t.hdr, 0, sizeof(vx::edit::Header), s));
+  return VX_OK;
+}
+
+uint32_t vx_dag_depth(const vx_dag *d) { return d ? d->t.depth : 0; }
+
+size_t vx_dag_voxel_workspace_size(uint32_t count) {
+  if (count == 0) return 0;
+  NullCarver c;
+  plain_layout(c, count);
+  return c.offset;
+}
+
+vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
+                              uint32_t op, void *workspace,
+                              size_t workspace_bytes, vx_stream stream) {
+  if (d == nullptr || (edits == nullptr && count != 0) || op > 1)
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  if (workspace == nullptr || workspace_bytes < vx_dag_voxel_workspace_size(count))
+    return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::Carver c(workspace);
+  const PlainLayout p = plain_layout(c, count);
+  const uint32_t blocks = vx::ceil_div(count, kBlock);
+  {
+    vx::prof::Scope sc("dag_pack_voxels", s);
+    pack_voxels_kernel<<<blocks, kBlock, 0, s>>>(edits, count, d->t.depth, p.keys, p.bits);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_sort_pairs_u64(p.keys, p.bits, count, 3 * d->t.depth + 1, p.sort_ws,
+                           p.sort_ws_bytes, s));
+  {
+    vx::prof::Scope sc("dag_run_flags", s);
+    run_flags_kernel<<<blocks, kBlock, 0, s>>>(p.keys, count, d->t.depth, p.offsets);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_scan_exclusive_sum_u32(p.offsets, count, p.scan_ws, p.scan_ws_bytes, s));
+  {
+    vx::prof::Scope sc("dag_reduce_runs", s);
+    reduce_runs_kernel<<<blocks, kBlock, 0, s>>>(p.keys, p.bits, p.offsets, count,
+                                                 d->t.depth, op, p.prims, p.count);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(run_pipeline(d, p.prims, p.count, count, s));
+  return read_status(d, s, true);
+}
+
+vx_status vx_dag_apply_primitives(vx_dag *d, const vx_primitive *prims,
+                                  uint32_t count, vx_stream stream) {
+  if (d == nullptr || (prims == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  return run_pipeline(d, prims, nullptr, count, static_cast<cudaStream_t>(stream));
+}
+
+vx_status vx_dag_status(vx_dag *d, vx_stream stream) {
+  if (d == nullptr) return VX_ERR_INVALID_VALUE;
+  return read_status(d, static_cast<cudaStream_t>(stream), true);
+}
+
+vx_status vx_dag_build_terrain(vx_dag *d, const vx_terrain *terrain,
+                               vx_stream stream) {
+  if (d == nullptr || terrain == nullptr || terrain->scale == 0) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx_primitive p{};
+  p.c[0] = static_cast<int32_t>(terrain->seed);
+  p.c[1] = static_cast<int32_t>(terrain->scale);
+  p.c[2] = static_cast<int32_t>(terrain->caves);
+  p.flags = vx_make_flags(vx::edit::kShapeTerrain, VX_OP_ADD, 0);
+  VX_TRY(vx_dag_reset(d, stream));
+  VX_TRY_CUDA(cudaMemcpyAsync(d->tmp_prim, &p, sizeof(p), cudaMemcpyHostToDevice, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  return run_pipeline(d, d->tmp_prim, nullptr, 1, s);
+}
+
+vx_status vx_dag_query(const vx_dag *d, const vx_voxel *pts, uint32_t count,
+                       uint8_t *out, vx_stream stream) {
+  if (d == nullptr || ((pts == nullptr || out == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope sc("dag_query", s);
+  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(d->t, pts, count, out);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_dag_get_stats(const vx_dag *d, vx_dag_stats *st, vx_stream stream) {
+  if (d == nullptr || st == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::edit::Header h;
+  VX_TRY_CUDA(cudaMemcpyAsync(&h, d->t.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  *st = vx_dag_stats{};
+  for (uint32_t l = 0; l <= d->t.depth && l < 16; ++l) {
+    st->nodes_per_level[l] = h.node_count[l];
+    st->words_per_level[l] = l < d->t.depth ? h.pool_used[l] : 2 * h.node_count[l];
+  }
+  st->bytes_reserved = d->bytes;
+  st->root = h.root;
+  st->status = h.status;
+  return VX_OK;
+}
+
+vx_status vx_dag_export_canonical(const vx_dag *d, uint32_t *host_root,
+                                  uint64_t *host_counts, uint32_t *host_nodes,
+                                  uint64_t nodes_capacity_words,
+                                  uint64_t *host_leaves,
+                                  uint64_t leaves_capacity, vx_stream stream) {
+  if (d == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t D = d->t.depth;
+  vx::edit::Header h;
+  VX_TRY_CUDA(cudaMemcpyAsync(&h, d->t.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  std::vector<std::vector<uint32_t>> pools(D);
+  for (uint32_t l = 0; l < D; ++l) {
+    const uint64_t used = std::min<uint64_t>(h.pool_used[l], d->t.pool_cap[l]);
+    pools[l].resize(used);
+    if (used)
+      VX_TRY_CUDA(cudaMemcpyAsync(pools[l].data(), d->t.pool[l], used * 4,
+                                  cudaMemcpyDeviceToHost, s));
+  }
+  std::vector<uint64_t> leaves(d->leaf_slots);
+  VX_TRY_CUDA(cudaMemcpyAsync(leaves.data(), d->t.leaves, d->leaf_slots * 8,
+                              cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  // DFS first-visit numbering per level (children 0..7).
+  std::vector<std::vector<uint32_t>> out_nodes(D);
+  std::vector<uint64_t> out_leaves;
+  std::vector<std::vector<int64_t>> ids(D + 1);
+  for (uint32_t l = 0; l < D; ++l) ids[l].assign(pools[l].size() + 2, -1);
+  std::vector<int64_t> leaf_ids(d->leaf_slots + 2, -1);
+  // iterative DFS with an explicit stack of (level, ref, next child)
+  struct Frame {
+    uint32_t l, ref, c, id;
+    uint32_t rec[10];
+  };
+  auto visit_leaf = [&](uint32_t ref) -> uint32_t {
+    if (leaf_ids[ref] < 0) {
+      leaf_ids[ref] = static_cast<int64_t>(out_leaves.size());
+      out_leaves.push_back(leaves[ref - 2]);
+    }
+    return static_cast<uint32_t>(leaf_ids[ref]) + 2;
+  };
+  uint32_t root_id = h.root;
+  if (h.root >= 2) {
+    if (D == 0) return VX_ERR_INVALID_VALUE;
+    std::vector<Frame> st;
+    auto open = [&](uint32_t l, uint32_t ref) {
+      Frame f{};
+      f.l = l;
+      f.ref = ref;
+      f.c = 0;
+      f.id = static_cast<uint32_t>(out_nodes[l].size() / 10);
+      ids[l][ref] = f.id;
+      out_nodes[l].resize(out_nodes[l].size() + 10, 0);
+      st.push_back(f);
+    };
+    open(0, h.root);
+    root_id = 2;
+    while (!st.empty()) {
+      Frame &f = st.back();
+      if (f.c == 8) {
+        for (uint32_t w = 0; w < 10; ++w) out_nodes[f.l][f.id * 10 + w] = f.rec[w];
+        const uint32_t id = f.id, l = f.l;
+        st.pop_back();
+        if (!st.empty()) {
+          Frame &p = st.back();
+          p.rec[2 + p.c] = id + 2;
+          p.rec[0] |= 1u << p.c;
+          ++p.c;
+        }
+        (void)l;
+        continue;
+      }
+      const uint32_t *item = pools[f.l].data() + (f.ref - 2);
+      const uint32_t cm = item[0] & 0xffu, fm = (item[0] >> 8) & 0xffu;
+      const uint32_t bit = 1u << f.c;
+      if (cm & bit) {
+        const uint32_t child = item[1 + __builtin_popcount(cm & (bit - 1u))];
+        if (f.l + 1 == D) {
+          f.rec[2 + f.c] = visit_leaf(child);
+          f.rec[0] |= bit;
+          ++f.c;
+        } else if (ids[f.l + 1][child] >= 0) {
+          f.rec[2 + f.c] = static_cast<uint32_t>(ids[f.l + 1][child]) + 2;
+          f.rec[0] |= bit;
+          ++f.c;
+        } else {
+          open(f.l + 1, child); // completes when popped
+        }
+      } else {
+        if (fm & bit) {
+          f.rec[2 + f.c] = 1;
+          f.rec[1] |= bit;
+        }
+        ++f.c;
+      }
+    }
+  }
+  if (host_root) *host_root = root_id;
+  uint64_t words = 0;
+  for (uint32_t l = 0; l < D; ++l) {
+    if (host_counts) host_counts[l] = out_nodes[l].size() / 10;
+    words += out_nodes[l].size();
+  }
+  if (host_counts) host_counts[D] = out_leaves.size();
+  if (host_nodes) {
+    if (words > nodes_capacity_words) return VX_ERR_INVALID_VALUE;
+    uint64_t o = 0;
+    for (uint32_t l = 0; l < D; ++l)
+      for (uint32_t w : out_nodes[l]) host_nodes[o++] = w;
+  }
+  if (host_leaves) {
+    if (out_leaves.size() > leaves_capacity) return VX_ERR_INVALID_VALUE;
+    std::copy(out_leaves.begin(), out_leaves.end(), host_leaves);
+  }
+  return VX_OK;
+}
+
+} // extern "C"
