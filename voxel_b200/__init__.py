@@ -149,7 +149,7 @@ _SIGS = {
     "vx_dag_status": (_ST, [_P, _P]),
     "vx_dag_build_terrain": (_ST, [_P, C.POINTER(vx_terrain), _P]),
     "vx_dag_query": (_ST, [_P, _P, _U32, _P, _P]),
-    "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), C.POINTER(_U64),
+    "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), _P,
                                       _P, _U64, _P, _U64, _P]),
     "vx_dag_get_stats": (_ST, [_P, C.POINTER(vx_dag_stats), _P]),
     "vx_svo_create": (_ST, [C.POINTER(vx_svo_config), C.POINTER(_P)]),

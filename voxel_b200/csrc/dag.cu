@@ -720,7 +720,9 @@ vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
   const uint64_t arena = cfg->arena_bytes ? cfg->arena_bytes : (512ull << 20);
   if ((e = cudaMalloc(&d->arena_mem, arena)) != cudaSuccess) return fail(e);
   d->bytes += arena;
-  const uint64_t item_bytes = arena / 10 * 6;
+  // Items take 60 % of the arena, the two pair buffers the rest; every
+  // sub-buffer starts on a 256-byte boundary.
+  const uint64_t item_bytes = arena / 10 * 6 / 256 * 256;
   d->a.items = static_cast<vx::edit::Item *>(d->arena_mem);
   d->a.item_cap = static_cast<uint32_t>(std::min<uint64_t>(item_bytes / sizeof(vx::edit::Item), 0xffffffffull));
   const uint64_t pair_bytes = (arena - item_bytes) / 2 / 256 * 256;
