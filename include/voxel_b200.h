@@ -255,15 +255,34 @@ vx_status vx_dag_export_canonical(const vx_dag *dag, uint32_t *host_root,
                                   uint64_t *host_leaves,
                                   uint64_t leaves_capacity, vx_stream stream);
 
+/* Copy the complete table state of src into dst (same configuration): a
+ * device-side snapshot / restore of a resident DAG.  No counterpart in the
+ * reference (its GPU DAG is not copyable, hash_dag_gpu/storage.cuh:40-43). */
+vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream);
+
 typedef struct vx_dag_stats {
     uint64_t nodes_per_level[16]; /* items stored (live and superseded) */
     uint64_t words_per_level[16];
+    uint32_t items_per_level[16]; /* work items of the last edit submission */
+    uint32_t pairs_per_level[16]; /* (cell, primitive) pairs of the last submission */
     uint64_t bytes_reserved;
     uint32_t root;
     uint32_t status;
 } vx_dag_stats;
 vx_status vx_dag_get_stats(const vx_dag *dag, vx_dag_stats *host_stats,
                            vx_stream stream);
+
+/* ---------------------------------------------------------- rasterising --
+ * Expand primitives into voxel lists (the plain path's input shape).
+ * out_offsets[i] = first voxel of primitive i (exclusive scan of counts);
+ * voxels are clipped to [0, world)^3.  Returns VX_ERR_CAPACITY if the total
+ * exceeds capacity (out_total still receives it). */
+vx_status vx_rasterize_count(const vx_primitive *prims, uint32_t count,
+                             uint32_t world_exp, uint64_t *out_counts,
+                             vx_stream stream);
+vx_status vx_rasterize(const vx_primitive *prims, uint32_t count,
+                       uint32_t world_exp, const uint64_t *offsets,
+                       vx_voxel *out, vx_stream stream);
 
 #ifdef __cplusplus
 }

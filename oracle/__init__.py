@@ -76,6 +76,7 @@ _REF_SIGS = [
     ("ref_dag_free", None, [_P]),
     ("ref_dag_edit_box", _I, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _I]),
     ("ref_dag_set_voxel", _I, [_P, _U32, _U32, _U32, _I]),
+    ("ref_dag_apply_prim", C.c_longlong, [_P, _I] + [C.c_longlong] * 6 + [_I]),
     ("ref_dag_get_voxel", _I, [_P, _U32, _U32, _U32]),
     ("ref_dag_node_count", _U64, [_P]),
     ("ref_dag_export", _I, [_P, C.POINTER(_U32), _P, _P, _U64, _P, _U64]),

@@ -6,6 +6,8 @@
 //
 // The canonical dumps below read the reference objects' internal node stores,
 // so the shim opens their private members to this translation unit only.
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <unordered_map>
 #include <vector>
@@ -130,6 +132,45 @@ int ref_dag_edit_box(void *h, u32 x0, u32 y0, u32 z0, u32 x1, u32 y1, u32 z1,
   } catch (...) {
     return 1;
   }
+}
+
+// Apply one sphere (|p - c|^2 <= r^2) or box as x-runs of fill_box / clear_box
+// calls, clipped to the world; returns the number of voxels covered (the CPU
+// baseline's unit of work), or -1 on error.
+long long ref_dag_apply_prim(void *h, int shape, long long cx, long long cy,
+                             long long cz, long long r0, long long r1,
+                             long long r2, int fill) {
+  auto *d = static_cast<HashDAG *>(h);
+  const long long world = d->world_voxel_count();
+  long long voxels = 0;
+  try {
+    if (shape == 1) {
+      const long long x0 = std::max(0ll, cx - r0), x1 = std::min(world, cx + r0 + 1);
+      const long long y0 = std::max(0ll, cy - r1), y1 = std::min(world, cy + r1 + 1);
+      const long long z0 = std::max(0ll, cz - r2), z1 = std::min(world, cz + r2 + 1);
+      if (x1 <= x0 || y1 <= y0 || z1 <= z0) return 0;
+      HashDAG::Box b{u32(x0), u32(y0), u32(z0), u32(x1), u32(y1), u32(z1)};
+      fill ? d->fill_box(b) : d->clear_box(b);
+      return (x1 - x0) * (y1 - y0) * (z1 - z0);
+    }
+    const long long r = r0;
+    for (long long z = std::max(0ll, cz - r); z < std::min(world, cz + r + 1); ++z)
+      for (long long y = std::max(0ll, cy - r); y < std::min(world, cy + r + 1); ++y) {
+        const long long rem = r * r - (z - cz) * (z - cz) - (y - cy) * (y - cy);
+        if (rem < 0) continue;
+        long long dx = static_cast<long long>(std::sqrt(static_cast<double>(rem)));
+        while (dx * dx > rem) --dx;
+        while ((dx + 1) * (dx + 1) <= rem) ++dx;
+        const long long x0 = std::max(0ll, cx - dx), x1 = std::min(world, cx + dx + 1);
+        if (x1 <= x0) continue;
+        HashDAG::Box b{u32(x0), u32(y), u32(z), u32(x1), u32(y + 1), u32(z + 1)};
+        fill ? d->fill_box(b) : d->clear_box(b);
+        voxels += x1 - x0;
+      }
+  } catch (...) {
+    return -1;
+  }
+  return voxels;
 }
 
 int ref_dag_set_voxel(void *h, u32 x, u32 y, u32 z, int value) {

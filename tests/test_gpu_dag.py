@@ -178,3 +178,39 @@ def test_capacity_overflow_keeps_previous_root(cuda):
     st = dag.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE)
     assert st == vx.VX_ERR_CAPACITY
     assert canon(dag) == before
+
+
+def test_rasterize_matches_voxel_definition(cuda):
+    rng = np.random.default_rng(21)
+    depth = 5
+    world = 4 << depth
+    prims = rand_prims(rng, 40, world, 20)
+    vox, off = vx.rasterize(vx.prims_to_device(prims, cuda), depth + 2)
+    vox = vox.cpu().numpy().view(np.uint32)
+    off = off.cpu().numpy()
+    for i, p in enumerate(prims):
+        got = {tuple(v) for v in vox[off[i]:off[i + 1]].tolist()}
+        assert len(got) == off[i + 1] - off[i]
+        single = np.zeros(1, oracle.PRIM_DTYPE)
+        single[0] = p
+        single[0]["flags"] = int(p["flags"]) | (1 << 8)
+        g = oracle.Grid(depth).apply_prims(single)
+        assert g.count() == len(got)
+        assert all(g.get(*v) for v in list(got)[:200])
+
+
+def test_copy_restores_snapshot(cuda):
+    depth = 6
+    rng = np.random.default_rng(5)
+    a = vx.HashDag(depth, max_nodes=1 << 18, arena_bytes=32 << 20)
+    a.build_terrain(2, 1, True)
+    b = vx.HashDag(depth, max_nodes=1 << 18, arena_bytes=32 << 20)
+    b.copy_from(a)
+    assert canon(b) == canon(a)
+    prims = rand_prims(rng, 80, 4 << depth, 20)
+    b.apply_primitives(vx.prims_to_device(prims, cuda))
+    assert b.status() == 0
+    t = oracle.terrain(2, 1, True)
+    assert canon(b) == oracle.Grid(depth).terrain(t).apply_prims(prims).dag()
+    b.copy_from(a)
+    assert canon(b) == canon(a)

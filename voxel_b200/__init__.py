@@ -83,6 +83,8 @@ class vx_dag_config(C.Structure):
 class vx_dag_stats(C.Structure):
     _fields_ = [("nodes_per_level", C.c_uint64 * 16),
                 ("words_per_level", C.c_uint64 * 16),
+                ("items_per_level", C.c_uint32 * 16),
+                ("pairs_per_level", C.c_uint32 * 16),
                 ("bytes_reserved", C.c_uint64), ("root", C.c_uint32),
                 ("status", C.c_uint32)]
 
@@ -152,6 +154,7 @@ _SIGS = {
     "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), _P,
                                       _P, _U64, _P, _U64, _P]),
     "vx_dag_get_stats": (_ST, [_P, C.POINTER(vx_dag_stats), _P]),
+    "vx_dag_copy": (_ST, [_P, _P, _P]),
     "vx_svo_create": (_ST, [C.POINTER(vx_svo_config), C.POINTER(_P)]),
     "vx_svo_destroy": (_ST, [_P]),
     "vx_svo_reset": (_ST, [_P, _P]),

@@ -18,7 +18,7 @@ __all__ = [
     "workspace_status", "SlabHashSet", "CuckooMap", "PRIM_DTYPE",
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
-    "config_c4_edits",
+    "config_c4_edits", "rasterize",
 ]
 
 
@@ -274,6 +274,10 @@ class HashDag:
               "vx_dag_query")
         return out
 
+    def copy_from(self, other: "HashDag") -> None:
+        """Device-side snapshot restore: take other's complete table state."""
+        check(lib().vx_dag_copy(self._h, other._h, stream_handle()), "vx_dag_copy")
+
     def stats(self):
         from . import vx_dag_stats
         st = vx_dag_stats()
@@ -329,3 +333,22 @@ def config_c4_edits(count: int = 16384, seed: int = 7, world_exp: int = 14) -> n
     """Batched Hash DAG: spheres r log-uniform [1, 256], 60% add."""
     return generate_primitives(world_exp, count, seed, add_permille=600,
                                r_min=1, r_max=256, log_uniform=True)
+
+
+def rasterize(prims: torch.Tensor, world_exp: int):
+    """Voxel lists of primitives (clipped to the world): returns
+    (voxels int32 [total, 3], offsets int64 [n + 1])."""
+    n = prims.numel() // 8
+    dev = prims.device
+    counts = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    if n == 0:
+        return torch.zeros((0, 3), dtype=torch.int32, device=dev), counts
+    check(lib().vx_rasterize_count(ptr(prims), n, world_exp, ptr(counts),
+                                   stream_handle()), "vx_rasterize_count")
+    offsets = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    offsets[1:] = torch.cumsum(counts[:n], 0)
+    total = int(offsets[-1].item())
+    out = torch.empty((max(total, 1), 3), dtype=torch.int32, device=dev)
+    check(lib().vx_rasterize(ptr(prims), n, world_exp, ptr(offsets), ptr(out),
+                             stream_handle()), "vx_rasterize")
+    return out[:total], offsets

@@ -856,6 +856,10 @@ vx_status vx_dag_get_stats(const vx_dag *d, vx_dag_stats *st, vx_stream stream) 
     st->nodes_per_level[l] = h.node_count[l];
     st->words_per_level[l] = l < d->t.depth ? h.pool_used[l] : 2 * h.node_count[l];
   }
+  for (uint32_t l = 0; l < 16; ++l) {
+    st->items_per_level[l] = h.item_count[l];
+    st->pairs_per_level[l] = h.pair_count[l];
+  }
   st->bytes_reserved = d->bytes;
   st->root = h.root;
   st->status = h.status;
@@ -976,6 +980,41 @@ vx_status vx_dag_export_canonical(const vx_dag *d, uint32_t *host_root,
     if (out_leaves.size() > leaves_capacity) return VX_ERR_INVALID_VALUE;
     std::copy(out_leaves.begin(), out_leaves.end(), host_leaves);
   }
+  return VX_OK;
+}
+
+} // extern "C"
+
+// ============================================================ snapshots ==
+
+extern "C" {
+
+// Copy the whole table state (roots, counters, indexes, pools, leaves) of src
+// into dst; both must have been created with the same configuration.
+vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream) {
+  if (dst == nullptr || src == nullptr || dst->t.depth != src->t.depth ||
+      dst->leaf_slots != src->leaf_slots)
+    return VX_ERR_INVALID_VALUE;
+  for (uint32_t l = 0; l < src->t.depth; ++l)
+    if (dst->index_slots[l] != src->index_slots[l] ||
+        dst->t.pool_cap[l] != src->t.pool_cap[l])
+      return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::edit::Header h;
+  VX_TRY_CUDA(cudaMemcpyAsync(&h, src->t.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t l = 0; l < src->t.depth; ++l) {
+    VX_TRY_CUDA(cudaMemcpyAsync(dst->t.index[l], src->t.index[l],
+                                src->index_slots[l] * 8, cudaMemcpyDeviceToDevice, s));
+    const uint64_t used = std::min<uint64_t>(h.pool_used[l], src->t.pool_cap[l]);
+    if (used)
+      VX_TRY_CUDA(cudaMemcpyAsync(dst->t.pool[l], src->t.pool[l], used * 4,
+                                  cudaMemcpyDeviceToDevice, s));
+  }
+  VX_TRY_CUDA(cudaMemcpyAsync(dst->t.leaves, src->t.leaves, src->leaf_slots * 8,
+                              cudaMemcpyDeviceToDevice, s));
+  VX_TRY_CUDA(cudaMemcpyAsync(dst->t.hdr, src->t.hdr, sizeof(vx::edit::Header),
+                              cudaMemcpyDeviceToDevice, s));
   return VX_OK;
 }
 
