@@ -377,9 +377,13 @@ def run_dag(args, ws, rank, local, torch, vx, device):
     tb1.record()
     st = pristine.status()
     terrain_ms = tb0.elapsed_time(tb1)
-    if st != 0:
-        raise RuntimeError(f"terrain build failed: status {st}")
     ts = pristine.stats()
+    if st != 0:
+        raise RuntimeError(
+            f"terrain build failed: status {st}; items/level "
+            f"{list(ts.items_per_level)[:DAG_DEPTH]} pairs/level "
+            f"{list(ts.pairs_per_level)[:DAG_DEPTH]} nodes/level "
+            f"{list(ts.nodes_per_level)[:DAG_DEPTH + 1]}")
     terrain_nodes = [int(ts.nodes_per_level[l]) for l in range(DAG_DEPTH + 1)]
 
     work = vx.HashDag(DAG_DEPTH, DAG_MAX_NODES, DAG_ARENA)
@@ -803,7 +807,12 @@ def run_case(args):
             depth = 10
             dag = vx.HashDag(depth, 1 << 25, 4 << 30)
             dag.build_terrain(7, 16, True)
-            assert dag.status() == 0
+            st = dag.status()
+            ts = dag.stats()
+            print(json.dumps({"terrain_status": st,
+                              "items": list(ts.items_per_level)[:depth],
+                              "nodes": list(ts.nodes_per_level)[:depth + 1]}))
+            assert st == 0
             prims = vx.prims_to_device(vx.config_c4_edits(n, seed=7, world_exp=depth + 2), dev)
             torch.cuda.synchronize()
             t = time.perf_counter()

@@ -199,41 +199,78 @@ VX_HD void vx_lattice_bounds(uint32_t seed, uint32_t stream, int64_t i0,
     *hi = mx;
 }
 
+/* Bounds of one height octave (spacing sp, stream) over the footprint
+ * [x0, x1] x [y0, y1] of integer columns, in numerator units (sp^2 * value).
+ * Inside one lattice cell the bilinear interpolant is multilinear, so its
+ * extrema are at the footprint's corner columns (exact bound); larger
+ * footprints use the range of the lattice values they span. */
+VX_HD void vx_octave_bounds(uint32_t seed, uint32_t stream, int64_t sp,
+                            uint32_t x0, uint32_t x1, uint32_t y0, uint32_t y1,
+                            int64_t *lo, int64_t *hi) {
+    if (x0 / sp == x1 / sp && y0 / sp == y1 / sp) {
+        const uint32_t xs[2] = {x0, x1}, ys[2] = {y0, y1};
+        int64_t mn = 0, mx = 0;
+        for (int k = 0; k < 4; ++k) {
+            const int64_t v = vx_noise2_num(seed, stream, (uint32_t)sp, xs[k & 1], ys[k >> 1]);
+            mn = (k == 0 || v < mn) ? v : mn;
+            mx = (k == 0 || v > mx) ? v : mx;
+        }
+        *lo = mn;
+        *hi = mx;
+        return;
+    }
+    int64_t l, h;
+    vx_lattice_bounds(seed, stream, x0 / sp, x1 / sp + 1, y0 / sp, y1 / sp + 1, 0, 0,
+                      &l, &h);
+    *lo = l * sp * sp;
+    *hi = h * sp * sp;
+}
+
 /* Classify the terrain occupancy of the cube [x0, x0+n)x[y0, y0+n)x[z0, z0+n).
- * Interpolated noise never leaves the range of the lattice values around it,
- * so the bounds are exact enough to prune whole subtrees and never wrong. */
+ * The bounds never exclude a value the noise takes inside the cube, so FULL /
+ * EMPTY answers are exact; MIXED means "subdivide". */
 VX_HD uint32_t vx_terrain_classify(const vx_terrain *t, uint32_t x0,
                                    uint32_t y0, uint32_t z0, uint32_t n) {
     const int64_t s = t->scale;
     const int64_t den = vx_terrain_hden(t);
+    const uint32_t x1 = x0 + n - 1, y1 = y0 + n - 1, z1 = z0 + n - 1;
     int64_t hlo = 0, hhi = 0;
     for (uint32_t o = 0; o < 3u; ++o) {
         const int64_t sp = (64 * s) >> o;
         int64_t lo, hi;
-        vx_lattice_bounds(t->seed, 1u + o, x0 / sp, (x0 + n - 1) / sp + 1,
-                          y0 / sp, (y0 + n - 1) / sp + 1, 0, 0, &lo, &hi);
+        vx_octave_bounds(t->seed, 1u + o, sp, x0, x1, y0, y1, &lo, &hi);
         const int64_t w = (int64_t)1 << o; /* octave weight 1, 2, 4 */
-        /* numerator bound: weight * s_o^2 * value, s_o^2 = s0^2 / 4^o */
-        const int64_t sq = sp * sp;
-        hlo += w * sq * lo;
-        hhi += w * sq * hi;
+        hlo += w * lo;
+        hhi += w * hi;
     }
-    /* all voxels below: (z0+n-1) * den < 128 s den + 40 s hlo */
-    const int all_below =
-        (int64_t)(z0 + n - 1) * den < 128 * s * den + 40 * s * hlo;
+    /* all voxels below: z1 * den < 128 s den + 40 s hlo */
+    const int all_below = (int64_t)z1 * den < 128 * s * den + 40 * s * hlo;
     /* no voxel below: z0 * den >= 128 s den + 40 s hhi */
     const int none_below = (int64_t)z0 * den >= 128 * s * den + 40 * s * hhi;
     if (none_below) return VX_CELL_EMPTY;
     if (!t->caves) return all_below ? VX_CELL_FULL : VX_CELL_MIXED;
     const int64_t c = 8 * s;
-    int64_t clo, chi;
-    vx_lattice_bounds(t->seed, 4u, x0 / c, (x0 + n - 1) / c + 1, y0 / c,
-                      (y0 + n - 1) / c + 1, z0 / c, (z0 + n - 1) / c + 1, &clo,
-                      &chi);
-    const int64_t thr = 55 * c * c * c * VX_NOISE_ONE;
     const int64_t c3 = c * c * c;
-    if (100 * c3 * clo > thr) return VX_CELL_EMPTY;          /* all carved */
-    const int none_carved = 100 * c3 * chi <= thr;
+    int64_t clo, chi;
+    if (x0 / c == x1 / c && y0 / c == y1 / c && z0 / c == z1 / c) {
+        /* one lattice cell: the trilinear extrema are at the 8 cube corners */
+        const uint32_t xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
+        for (int k = 0; k < 8; ++k) {
+            const int64_t v = vx_noise3_num(t->seed, 4u, (uint32_t)c, xs[k & 1],
+                                            ys[(k >> 1) & 1], zs[k >> 2]);
+            clo = (k == 0 || v < clo) ? v : clo;
+            chi = (k == 0 || v > chi) ? v : chi;
+        }
+    } else {
+        int64_t l, h;
+        vx_lattice_bounds(t->seed, 4u, x0 / c, x1 / c + 1, y0 / c, y1 / c + 1,
+                          z0 / c, z1 / c + 1, &l, &h);
+        clo = l * c3;
+        chi = h * c3;
+    }
+    const int64_t thr = 55 * c3 * VX_NOISE_ONE;
+    if (100 * clo > thr) return VX_CELL_EMPTY;          /* all carved */
+    const int none_carved = 100 * chi <= thr;
     return (all_below && none_carved) ? VX_CELL_FULL : VX_CELL_MIXED;
 }
 
