@@ -222,9 +222,13 @@ __global__ void init_kernel(Ctx x) {
     x.a.pairs[0][i] = static_cast<uint32_t>(i);
 }
 
-// Top-down expansion of level l into level l + 1 (l + 1 < depth).  One warp
-// per work item; lanes walk the item's primitive list 32 at a time.
-template <class Tree>
+// Top-down expansion of level l into level l + 1 (l + 1 < depth).  Eight
+// lanes per work item, one per child cell: lane c walks the item's ordered
+// primitive list once, remembering the last primitive that covers child c
+// entirely (which resets the count of partial ones before it) and counting the
+// partial ones after it; a second walk writes those to the child's list.
+// Output space for a block's 32 items is taken with one atomicAdd per counter.
+template <class Tree, bool Terrain>
 __global__ void __launch_bounds__(kBlock)
     expand_kernel(Ctx x, Tree tree, uint32_t l) {
   Header *h = x.t.hdr;
@@ -238,93 +242,63 @@ __global__ void __launch_bounds__(kBlock)
   uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
   const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
   const uint32_t world_exp = depth + 2;
+  constexpr uint32_t kGroups = kBlock / 8;
 
-  __shared__ uint32_t s_items[kBlock / kWarp], s_pairs[kBlock / kWarp];
+  __shared__ uint32_t s_items[kGroups], s_pairs[kGroups];
   __shared__ uint32_t s_item_base, s_pair_base;
-  const uint32_t warp = threadIdx.x / kWarp, lane = lane_id();
-  constexpr uint32_t kWarpsPerBlock = kBlock / kWarp;
+  const uint32_t group = threadIdx.x >> 3, c = threadIdx.x & 7u;
+  const uint32_t gshift = (lane_id() >> 3) * 8u; // this group's byte in a ballot
 
-  for (uint64_t tile = blockIdx.x; tile * kWarpsPerBlock < W; tile += gridDim.x) {
-    const uint32_t wi = static_cast<uint32_t>(tile * kWarpsPerBlock) + warp;
+  for (uint64_t tile = blockIdx.x; tile * kGroups < W; tile += gridDim.x) {
+    const uint32_t wi = static_cast<uint32_t>(tile * kGroups) + group;
     const bool have = wi < W;
     Item it{};
     if (have) it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
-    int32_t full_max[8];
-    uint32_t cnt[8];
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      full_max[c] = -1;
-      cnt[c] = 0;
-    }
-    const uint32_t pc = have ? it.pcount : 0;
-    // Pass 1: last fully-covering primitive per child.
-    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
-      const uint32_t k = k0 + lane;
-      int32_t p = -1;
-      uint32_t code = 0;
-      if (k < pc) {
-        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
-        const vx_primitive pr = x.prims[p];
-#pragma unroll
-        for (uint32_t c = 0; c < 8; ++c) {
-          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
-          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
-          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
-          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
-        }
-      }
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        const int32_t f = ((code >> (2 * c)) & 3u) == VX_CELL_FULL ? p : -1;
-        full_max[c] = max(full_max[c], __reduce_max_sync(kFullMask, f));
+    const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+    const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+    const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+    int32_t last_full = -1;
+    uint32_t cnt = 0;
+    for (uint32_t k = 0; k < it.pcount; ++k) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const uint32_t cls = classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize);
+      if (cls == VX_CELL_FULL) {
+        last_full = static_cast<int32_t>(p);
+        cnt = 0;
+      } else if (cls == VX_CELL_MIXED) {
+        ++cnt;
       }
     }
-    // Pass 2: partially-covering primitives after that.
-    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
-      const uint32_t k = k0 + lane;
-      int32_t p = -1;
-      uint32_t code = 0;
-      if (k < pc) {
-        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
-        const vx_primitive pr = x.prims[p];
+    // Prefix sums over the 8 lanes of the group.
+    uint32_t inc_items = cnt ? 1u : 0u, inc_pairs = cnt;
 #pragma unroll
-        for (uint32_t c = 0; c < 8; ++c) {
-          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
-          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
-          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
-          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
-        }
-      }
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c)
-        cnt[c] += __popc(__ballot_sync(
-            kFullMask, ((code >> (2 * c)) & 3u) == VX_CELL_MIXED && p > full_max[c]));
-    }
-    uint32_t child_mask = 0, const_mask = 0, const_full = 0, n_items = 0, n_pairs = 0;
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      if (cnt[c]) {
-        child_mask |= 1u << c;
-        ++n_items;
-        n_pairs += cnt[c];
-      }
-      if (full_max[c] >= 0) {
-        const_mask |= 1u << c;
-        if (vx_prim_op(&x.prims[full_max[c]]) == VX_OP_ADD) const_full |= 1u << c;
+    for (uint32_t d = 1; d < 8; d <<= 1) {
+      const uint32_t a = __shfl_up_sync(kFullMask, inc_items, d, 8);
+      const uint32_t b = __shfl_up_sync(kFullMask, inc_pairs, d, 8);
+      if (c >= d) {
+        inc_items += a;
+        inc_pairs += b;
       }
     }
-    if (lane == 0) {
-      s_items[warp] = n_items;
-      s_pairs[warp] = n_pairs;
+    const uint32_t group_items = __shfl_sync(kFullMask, inc_items, 7, 8);
+    const uint32_t group_pairs = __shfl_sync(kFullMask, inc_pairs, 7, 8);
+    const bool full_add =
+        last_full >= 0 && vx_prim_op(&x.prims[last_full]) == VX_OP_ADD;
+    const uint32_t child_mask = (__ballot_sync(kFullMask, cnt != 0) >> gshift) & 0xffu;
+    const uint32_t const_mask = (__ballot_sync(kFullMask, last_full >= 0) >> gshift) & 0xffu;
+    const uint32_t const_full = (__ballot_sync(kFullMask, full_add) >> gshift) & 0xffu;
+    if (c == 0) {
+      s_items[group] = have ? group_items : 0u;
+      s_pairs[group] = have ? group_pairs : 0u;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t ti = 0, tp = 0;
-      for (uint32_t w = 0; w < kWarpsPerBlock; ++w) {
-        const uint32_t a = s_items[w], b = s_pairs[w];
-        s_items[w] = ti;
-        s_pairs[w] = tp;
+      for (uint32_t g = 0; g < kGroups; ++g) {
+        const uint32_t a = s_items[g], b = s_pairs[g];
+        s_items[g] = ti;
+        s_pairs[g] = tp;
         ti += a;
         tp += b;
       }
@@ -337,55 +311,29 @@ __global__ void __launch_bounds__(kBlock)
     }
     __syncthreads();
     const bool room = ld_relaxed_u32(&h->status) == kDevOk;
-    const uint32_t item_off = s_item_base + s_items[warp];
-    uint32_t pair_off = s_pair_base + s_pairs[warp];
-    __syncthreads(); // s_* reused by the next tile
+    const uint32_t item_off = s_item_base + s_items[group];
+    const uint32_t pair_off = s_pair_base + s_pairs[group];
+    __syncthreads(); // s_* are reused by the next tile
     if (!have || !room) continue;
 
-    // Emit child items (in child order) and their primitive lists.
-    uint32_t child_pstart[8];
-    {
-      uint32_t k = 0, po = pair_off;
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        child_pstart[c] = po;
-        if (cnt[c] && lane == 0) {
-          Item ci{};
-          ci.cell = child_cell(it.cell, c);
-          ci.old = (const_mask >> c) & 1u ? (((const_full >> c) & 1u) ? kFullRef : kEmptyRef)
-                                          : tree.child(l, it.old, c);
-          ci.pstart = po;
-          ci.pcount = cnt[c];
-          x.a.items[next_base + item_off + k] = ci;
-        }
-        if (cnt[c]) ++k;
-        po += cnt[c];
+    if (cnt) {
+      const uint32_t my_pairs = pair_off + inc_pairs - cnt;
+      Item ci{};
+      ci.cell = child_cell(it.cell, c);
+      ci.old = last_full >= 0 ? (full_add ? kFullRef : kEmptyRef)
+                              : tree.child(l, it.old, c);
+      ci.pstart = my_pairs;
+      ci.pcount = cnt;
+      x.a.items[next_base + item_off + inc_items - 1] = ci;
+      uint32_t j = 0;
+      for (uint32_t k = 0; k < it.pcount && j < cnt; ++k) {
+        const uint32_t p = in_pairs[it.pstart + k];
+        if (static_cast<int32_t>(p) <= last_full) continue;
+        if (classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
+          out_pairs[my_pairs + j++] = p;
       }
     }
-    for (uint32_t k0 = 0; k0 < pc; k0 += kWarp) {
-      const uint32_t k = k0 + lane;
-      int32_t p = -1;
-      uint32_t code = 0;
-      if (k < pc) {
-        p = static_cast<int32_t>(in_pairs[it.pstart + k]);
-        const vx_primitive pr = x.prims[p];
-#pragma unroll
-        for (uint32_t c = 0; c < 8; ++c) {
-          const int64_t ox = (int64_t(2 * cell.x + (c & 1u))) * csize;
-          const int64_t oy = (int64_t(2 * cell.y + ((c >> 1) & 1u))) * csize;
-          const int64_t oz = (int64_t(2 * cell.z + ((c >> 2) & 1u))) * csize;
-          code |= classify(pr, world_exp, ox, oy, oz, csize) << (2 * c);
-        }
-      }
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        const bool take = ((code >> (2 * c)) & 3u) == VX_CELL_MIXED && p > full_max[c];
-        const uint32_t b = __ballot_sync(kFullMask, take);
-        if (take) out_pairs[child_pstart[c] + __popc(b & lanemask_lt())] = static_cast<uint32_t>(p);
-        child_pstart[c] += __popc(b);
-      }
-    }
-    if (lane == 0) {
+    if (c == 0) {
       x.a.items[base + wi].child_base = next_base + item_off;
       x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
     }
@@ -401,6 +349,7 @@ struct DagTree {
 
 // Level depth - 1: evaluate the 8 leaves of every item (8 threads per item)
 // and hash-cons the item.
+template <bool Terrain>
 __global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
   Header *h = x.t.hdr;
   if (ld_relaxed_u32(&h->status) != kDevOk) return;
@@ -430,7 +379,7 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
       bool loaded = false, touched = false;
       for (uint32_t k = 0; k < it.pcount; ++k) {
         const vx_primitive pr = x.prims[pairs[it.pstart + k]];
-        const uint32_t cls = classify(pr, world_exp, ox, oy, oz, 4);
+        const uint32_t cls = classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
         if (cls == VX_CELL_EMPTY) continue;
         const bool add = vx_prim_op(&pr) == VX_OP_ADD;
         touched = true;
@@ -443,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
           mask = read_leaf(x.t, old_child);
           loaded = true;
         }
-        const uint64_t m = leaf_mask(pr, world_exp, ox, oy, oz);
+        const uint64_t m = leaf_mask<Terrain>(pr, world_exp, ox, oy, oz);
         mask = add ? (mask | m) : (mask & ~m);
       }
       result = touched ? canon_leaf(x.t, mask) : old_child;
@@ -599,7 +548,7 @@ inline uint64_t next_pow2(uint64_t v) {
 
 vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
                        const uint32_t *d_count, uint32_t host_count,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool terrain = false) {
   Ctx x{d->t, d->a, prims, d_count, host_count};
   const uint32_t depth = d->t.depth;
   const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
@@ -612,12 +561,18 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   DagTree tree{d->t};
   for (uint32_t l = 0; l + 1 < depth; ++l) {
     prof::Scope sc("dag_expand", s);
-    expand_kernel<DagTree><<<grid, kBlock, 0, s>>>(x, tree, l);
+    if (terrain)
+      expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(x, tree, l);
+    else
+      expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(x, tree, l);
     VX_TRY_CUDA(cudaGetLastError());
   }
   {
     prof::Scope sc("dag_leafparent", s);
-    leafparent_kernel<<<grid, kBlock, 0, s>>>(x);
+    if (terrain)
+      leafparent_kernel<true><<<grid, kBlock, 0, s>>>(x);
+    else
+      leafparent_kernel<false><<<grid, kBlock, 0, s>>>(x);
   }
   VX_TRY_CUDA(cudaGetLastError());
   for (uint32_t r = depth - 1; r > 0; --r) {
@@ -831,7 +786,7 @@ vx_status vx_dag_build_terrain(vx_dag *d, const vx_terrain *terrain,
   VX_TRY(vx_dag_reset(d, stream));
   VX_TRY_CUDA(cudaMemcpyAsync(d->tmp_prim, &p, sizeof(p), cudaMemcpyHostToDevice, s));
   VX_TRY_CUDA(cudaStreamSynchronize(s));
-  return run_pipeline(d, d->tmp_prim, nullptr, 1, s);
+  return run_pipeline(d, d->tmp_prim, nullptr, 1, s, true);
 }
 
 vx_status vx_dag_query(const vx_dag *d, const vx_voxel *pts, uint32_t count,

@@ -43,13 +43,21 @@ __host__ __device__ __forceinline__ uint64_t child_cell(uint64_t p, uint32_t c) 
                    2 * k.z + ((c >> 2) & 1u));
 }
 
-// Classify primitive p against the voxel cube [o, o + n)^3.
+// Classify primitive p against the voxel cube [o, o + n)^3.  Kernels that
+// only ever see sphere / box / leaf-mask primitives instantiate Terrain =
+// false and carry none of the terrain generator's code.
+template <bool Terrain>
 __device__ __forceinline__ uint32_t classify(const vx_primitive &p,
                                              uint32_t world_exp, int64_t ox,
                                              int64_t oy, int64_t oz, int64_t n) {
   const uint32_t shape = vx_prim_shape(&p);
-  if (shape == VX_SHAPE_SPHERE || shape == VX_SHAPE_BOX)
-    return vx_prim_classify(&p, ox, oy, oz, n);
+  if (Terrain && shape == kShapeTerrain) {
+    const vx_terrain t{static_cast<uint32_t>(p.c[0]), static_cast<uint32_t>(p.c[1]),
+                       static_cast<uint32_t>(p.c[2]), world_exp};
+    return vx_terrain_classify(&t, static_cast<uint32_t>(ox),
+                               static_cast<uint32_t>(oy),
+                               static_cast<uint32_t>(oz), static_cast<uint32_t>(n));
+  }
   if (shape == kShapeLeafMask) {
     const int64_t lx = p.c[0], ly = p.c[1], lz = p.c[2];
     if (lx < ox || lx >= ox + n || ly < oy || ly >= oy + n || lz < oz ||
@@ -57,29 +65,26 @@ __device__ __forceinline__ uint32_t classify(const vx_primitive &p,
       return VX_CELL_EMPTY;
     return VX_CELL_MIXED;
   }
-  // terrain
-  const vx_terrain t{static_cast<uint32_t>(p.c[0]), static_cast<uint32_t>(p.c[1]),
-                     static_cast<uint32_t>(p.c[2]), world_exp};
-  return vx_terrain_classify(&t, static_cast<uint32_t>(ox),
-                             static_cast<uint32_t>(oy), static_cast<uint32_t>(oz),
-                             static_cast<uint32_t>(n));
+  return vx_prim_classify(&p, ox, oy, oz, n);
 }
 
 // Voxels of the 4^3 leaf at o that the primitive covers.
+template <bool Terrain>
 __device__ __forceinline__ uint64_t leaf_mask(const vx_primitive &p,
                                               uint32_t world_exp, int64_t ox,
                                               int64_t oy, int64_t oz) {
   const uint32_t shape = vx_prim_shape(&p);
-  if (shape == VX_SHAPE_SPHERE || shape == VX_SHAPE_BOX)
-    return vx_prim_leaf_mask(&p, ox, oy, oz);
+  if (Terrain && shape == kShapeTerrain) {
+    const vx_terrain t{static_cast<uint32_t>(p.c[0]), static_cast<uint32_t>(p.c[1]),
+                       static_cast<uint32_t>(p.c[2]), world_exp};
+    return vx_terrain_leaf_mask(&t, static_cast<uint32_t>(ox),
+                                static_cast<uint32_t>(oy), static_cast<uint32_t>(oz));
+  }
   if (shape == kShapeLeafMask) {
     if (p.c[0] != ox || p.c[1] != oy || p.c[2] != oz) return 0;
     return static_cast<uint64_t>(p.r[0]) | (static_cast<uint64_t>(p.r[1]) << 32);
   }
-  const vx_terrain t{static_cast<uint32_t>(p.c[0]), static_cast<uint32_t>(p.c[1]),
-                     static_cast<uint32_t>(p.c[2]), world_exp};
-  return vx_terrain_leaf_mask(&t, static_cast<uint32_t>(ox),
-                              static_cast<uint32_t>(oy), static_cast<uint32_t>(oz));
+  return vx_prim_leaf_mask(&p, ox, oy, oz);
 }
 
 // One work item of the top-down expansion (32 bytes).
