@@ -201,6 +201,7 @@ __global__ void init_kernel(Ctx x) {
       h->item_off[l] = 0;
       h->item_count[l] = 0;
       h->pair_count[l] = 0;
+      h->big_count[l] = 0;
     }
     h->prim_count = n;
     const uint32_t ok = h->status == kDevOk && n <= x.a.pair_cap;
@@ -254,6 +255,16 @@ __global__ void __launch_bounds__(kBlock)
     const bool have = wi < W;
     Item it{};
     if (have) it = x.a.items[base + wi];
+    const bool big = have && it.pcount > kBigItem;
+    if (big) {
+      // Long lists go to expand_big_kernel (one block per item).
+      if (c == 0) {
+        const uint32_t slot = atomicAdd(&h->big_count[l], 1u);
+        if (slot < x.a.big_cap) x.a.big[slot] = wi;
+        else set_status(&h->status, kDevCapacity);
+      }
+      it.pcount = 0;
+    }
     const Cell cell = unpack_cell(it.cell);
     const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
     const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
@@ -289,8 +300,8 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t const_mask = (__ballot_sync(kFullMask, last_full >= 0) >> gshift) & 0xffu;
     const uint32_t const_full = (__ballot_sync(kFullMask, full_add) >> gshift) & 0xffu;
     if (c == 0) {
-      s_items[group] = have ? group_items : 0u;
-      s_pairs[group] = have ? group_pairs : 0u;
+      s_items[group] = have && !big ? group_items : 0u;
+      s_pairs[group] = have && !big ? group_pairs : 0u;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -314,7 +325,7 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t item_off = s_item_base + s_items[group];
     const uint32_t pair_off = s_pair_base + s_pairs[group];
     __syncthreads(); // s_* are reused by the next tile
-    if (!have || !room) continue;
+    if (!have || big || !room) continue;
 
     if (cnt) {
       const uint32_t my_pairs = pair_off + inc_pairs - cnt;
@@ -337,6 +348,167 @@ __global__ void __launch_bounds__(kBlock)
       x.a.items[base + wi].child_base = next_base + item_off;
       x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
     }
+  }
+}
+
+// Expansion of the long-list items of level l: one block per item.  Three
+// walks over the list: the last fully-covering primitive per child (block
+// max), the partial primitives after it per child (block sum), then an
+// order-preserving block-wide compaction of those into each child's list.
+template <class Tree, bool Terrain>
+__global__ void __launch_bounds__(kBlock)
+    expand_big_kernel(Ctx x, Tree tree, uint32_t l) {
+  Header *h = x.t.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t nbig = min(h->big_count[l], x.a.big_cap);
+  const uint32_t depth = x.t.depth;
+  const uint32_t base = h->item_off[l];
+  const uint32_t next_base = base + h->item_count[l];
+  const uint32_t *in_pairs = x.a.pairs[l & 1u];
+  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
+  const int64_t csize = int64_t(4) << (depth - l - 1);
+  const uint32_t world_exp = depth + 2;
+  constexpr uint32_t kWarps = kBlock / kWarp;
+  __shared__ int32_t s_last[8];
+  __shared__ uint32_t s_cnt[8], s_start[8];
+  __shared__ uint32_t s_warp[8][kWarps];
+  __shared__ uint32_t s_item_base, s_pair_base;
+  __shared__ bool s_room;
+  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
+
+  for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const uint32_t wi = x.a.big[b];
+    const Item it = x.a.items[base + wi];
+    const Cell cell = unpack_cell(it.cell);
+    if (t < 8) {
+      s_last[t] = -1;
+      s_cnt[t] = 0;
+    }
+    __syncthreads();
+    // Walk 1: last FULL per child.
+    int32_t last[8];
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) last[c] = -1;
+    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const vx_primitive pr = x.prims[p];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+        if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_FULL)
+          last[c] = max(last[c], static_cast<int32_t>(p));
+      }
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const int32_t m = __reduce_max_sync(kFullMask, last[c]);
+      if (lane == 0 && m >= 0) atomicMax(&s_last[c], m);
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) last[c] = s_last[c];
+    // Walk 2: partial primitives after the last full one.
+    uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const vx_primitive pr = x.prims[p];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        if (static_cast<int32_t>(p) <= last[c]) continue;
+        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+        if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED) ++cnt[c];
+      }
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const uint32_t v = __reduce_add_sync(kFullMask, cnt[c]);
+      if (lane == 0 && v) atomicAdd(&s_cnt[c], v);
+    }
+    __syncthreads();
+    if (t == 0) {
+      uint32_t ni = 0, np = 0, cm = 0, km = 0, kf = 0;
+      for (uint32_t c = 0; c < 8; ++c) {
+        s_start[c] = np;
+        if (s_cnt[c]) {
+          cm |= 1u << c;
+          ++ni;
+          np += s_cnt[c];
+        }
+        if (s_last[c] >= 0) {
+          km |= 1u << c;
+          if (vx_prim_op(&x.prims[s_last[c]]) == VX_OP_ADD) kf |= 1u << c;
+        }
+      }
+      s_item_base = ni ? atomicAdd(&h->item_count[l + 1], ni) : 0;
+      s_pair_base = np ? atomicAdd(&h->pair_count[l + 1], np) : 0;
+      if (ni && static_cast<uint64_t>(next_base) + s_item_base + ni > x.a.item_cap)
+        set_status(&h->status, kDevCapacity);
+      if (np && static_cast<uint64_t>(s_pair_base) + np > x.a.pair_cap)
+        set_status(&h->status, kDevCapacity);
+      x.a.items[base + wi].child_base = next_base + s_item_base;
+      x.a.items[base + wi].masks = cm | (km << 8) | (kf << 16);
+      s_room = ld_relaxed_u32(&h->status) == kDevOk;
+    }
+    __syncthreads();
+    const bool room = s_room; // block-uniform: it guards barriers below
+    if (room && t < 8 && s_cnt[t]) {
+      uint32_t k = 0;
+      for (uint32_t c = 0; c < t; ++c) k += s_cnt[c] ? 1u : 0u;
+      Item ci{};
+      ci.cell = child_cell(it.cell, t);
+      ci.old = s_last[t] >= 0
+                   ? (vx_prim_op(&x.prims[s_last[t]]) == VX_OP_ADD ? kFullRef : kEmptyRef)
+                   : tree.child(l, it.old, t);
+      ci.pstart = s_pair_base + s_start[t];
+      ci.pcount = s_cnt[t];
+      x.a.items[next_base + s_item_base + k] = ci;
+    }
+    // Walk 3: order-preserving compaction, one 256-pair chunk at a time.
+    uint32_t run[8];
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) run[c] = s_pair_base + s_start[c];
+    for (uint32_t k0 = 0; k0 < it.pcount && room; k0 += kBlock) {
+      const uint32_t k = k0 + t;
+      uint32_t take = 0, p = 0;
+      if (k < it.pcount) {
+        p = in_pairs[it.pstart + k];
+        const vx_primitive pr = x.prims[p];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          if (static_cast<int32_t>(p) <= last[c]) continue;
+          const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+          const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+          const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+          if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
+            take |= 1u << c;
+        }
+      }
+      uint32_t ballots[8];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        ballots[c] = __ballot_sync(kFullMask, (take >> c) & 1u);
+        if (lane == 0) s_warp[c][warp] = __popc(ballots[c]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < kWarps; ++w) {
+          const uint32_t v = s_warp[c][w];
+          before += w < warp ? v : 0u;
+          total += v;
+        }
+        if ((take >> c) & 1u)
+          out_pairs[run[c] + before + __popc(ballots[c] & lanemask_lt())] = p;
+        run[c] += total;
+      }
+      __syncthreads();
+    }
+    __syncthreads();
   }
 }
 
@@ -560,11 +732,21 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   VX_TRY_CUDA(cudaGetLastError());
   DagTree tree{d->t};
   for (uint32_t l = 0; l + 1 < depth; ++l) {
-    prof::Scope sc("dag_expand", s);
-    if (terrain)
-      expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(x, tree, l);
-    else
-      expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(x, tree, l);
+    {
+      prof::Scope sc("dag_expand", s);
+      if (terrain)
+        expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(x, tree, l);
+      else
+        expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(x, tree, l);
+    }
+    VX_TRY_CUDA(cudaGetLastError());
+    {
+      prof::Scope sc("dag_expand_big", s);
+      if (terrain)
+        expand_big_kernel<DagTree, true><<<sm_count() * 2, kBlock, 0, s>>>(x, tree, l);
+      else
+        expand_big_kernel<DagTree, false><<<sm_count() * 2, kBlock, 0, s>>>(x, tree, l);
+    }
     VX_TRY_CUDA(cudaGetLastError());
   }
   {
@@ -677,10 +859,13 @@ vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
   d->bytes += arena;
   // Items take 60 % of the arena, the two pair buffers the rest; every
   // sub-buffer starts on a 256-byte boundary.
-  const uint64_t item_bytes = arena / 10 * 6 / 256 * 256;
+  const uint64_t big_bytes = std::min<uint64_t>(arena / 64, 4ull << 20) / 256 * 256;
+  const uint64_t item_bytes = (arena - big_bytes) / 10 * 6 / 256 * 256;
   d->a.items = static_cast<vx::edit::Item *>(d->arena_mem);
   d->a.item_cap = static_cast<uint32_t>(std::min<uint64_t>(item_bytes / sizeof(vx::edit::Item), 0xffffffffull));
-  const uint64_t pair_bytes = (arena - item_bytes) / 2 / 256 * 256;
+  const uint64_t pair_bytes = (arena - big_bytes - item_bytes) / 2 / 256 * 256;
+  d->a.big = reinterpret_cast<uint32_t *>(static_cast<char *>(d->arena_mem) + item_bytes + 2 * pair_bytes);
+  d->a.big_cap = static_cast<uint32_t>(big_bytes / 4);
   d->a.pairs[0] = reinterpret_cast<uint32_t *>(static_cast<char *>(d->arena_mem) + item_bytes);
   d->a.pairs[1] = reinterpret_cast<uint32_t *>(static_cast<char *>(d->arena_mem) + item_bytes + pair_bytes);
   d->a.pair_cap = static_cast<uint32_t>(std::min<uint64_t>(pair_bytes / 4, 0xffffffffull));

@@ -110,13 +110,19 @@ struct Header {
   uint32_t pair_count[16];      // pairs of each level
   uint64_t node_count[16];      // items inserted per table (DAG)
   uint32_t pool_used[16];       // words used per level pool (DAG)
+  uint32_t big_count[16];       // items deferred to the block-per-item path
 };
 
 struct Arena {
   Item *items;
   uint32_t *pairs[2];
+  uint32_t *big;       // indices of items with long primitive lists
   uint32_t item_cap;
   uint32_t pair_cap;
+  uint32_t big_cap;
 };
+
+// Items with more primitives than this are expanded by a whole block.
+constexpr uint32_t kBigItem = 64;
 
 } // namespace vx::edit
