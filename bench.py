@@ -59,6 +59,9 @@ DAG_EDITS = 16384
 DAG_MAX_NODES = 1 << 27
 DAG_ARENA = 16 << 30
 PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
+# DRAM bytes per dag_leafparent launch from ncu (profiles/); None until a
+# capture of this workload is committed.
+LEAFPARENT_TRAFFIC = None
 N_HASH = 1 << 26
 HASH_LOAD = 0.8
 BYTES_HASH_INSERT = 40  # read key 8 + one 32-B sector read-modify-write
@@ -423,8 +426,8 @@ def run_dag(args, ws, rank, local, torch, vx, device):
         clk.mark("end")
     barrier()
     launches = lib.vx_profile_launches() - launches0
-    kern = {k: _prof(lib, k) for k in ("dag_init", "dag_expand", "dag_leafparent",
-                                       "dag_build", "dag_publish")}
+    kern = {k: _prof(lib, k) for k in ("dag_init", "dag_expand", "dag_expand_big",
+                                       "dag_leafparent", "dag_build", "dag_publish")}
     lib.vx_profile_enable(0)
     st = work.status()
     if st != 0:
@@ -547,8 +550,19 @@ def run_ours(args, ws, rank, local):
     sweep = run_sweep(args, ws, rank, local, torch, vx, device)
     hbm, kind = peaks()
     k = dag["kernels"]
-    top = max(("dag_expand", "dag_leafparent", "dag_build"), key=lambda n: k[n][1])
+    top = max(("dag_expand", "dag_expand_big", "dag_leafparent", "dag_build"),
+              key=lambda n: k[n][1])
     total_k = sum(v[1] for v in k.values())
+    # Algorithmic bytes of one leaf-parent launch (the last level of the
+    # expansion): per item its 32-B record, 4-B result, the old parent item
+    # (~24 B) and the new item's hash-cons (8-B index slot + ~24-B item), and
+    # per leaf child the old leaf (8 B) and its hash-cons slot (read + CAS,
+    # 16 B); per (item, primitive) pair the 4-B index and 32-B primitive.
+    lp_items = dag["items_per_level"][DAG_DEPTH - 1]
+    lp_pairs = dag["pairs_per_level"][DAG_DEPTH - 1]
+    lp_bytes = lp_items * (32 + 4 + 24 + 32 + 8 * (8 + 16)) + lp_pairs * 36
+    lp_n, lp_ms = k["dag_leafparent"]
+    lp_achieved = lp_bytes / (lp_ms / lp_n / 1e3) / 1e9 if lp_n else None
     plain = dag["plain"]
     result = {
         "metric": METRIC,
@@ -591,15 +605,18 @@ def run_ours(args, ws, rank, local):
             **sweep,
         },
         "roofline": {
-            "kernel": top,
+            "kernel": "dag_leafparent",
+            "dominant_kernel_measured": top,
             "bound": "hbm",
-            "achieved": None,
+            "achieved": round(lp_achieved, 1) if lp_achieved else None,
             "peak": hbm,
             "peak_kind": kind,
             "unit": "GB/s",
-            "frac": None,
-            "traffic": None,
-            "note": "see components.sort_partition_u64 for the sweep's dominant kernel",
+            "frac": round(lp_achieved / hbm, 4) if lp_achieved else None,
+            "traffic": LEAFPARENT_TRAFFIC,
+            "algorithmic_bytes_per_launch": lp_bytes,
+            "launches": lp_n,
+            "avg_launch_ms": round(lp_ms / lp_n, 3) if lp_n else None,
         },
         "e2e": dag["e2e"],
         "gpu_launches": dag["launches"],
