@@ -822,7 +822,7 @@ def run_case(args):
         else:
             # dag: 4096^3 cave terrain (scale 16) + n spheres of the C4 mix
             depth = 10
-            dag = vx.HashDag(depth, 1 << 25, 4 << 30)
+            dag = vx.HashDag(depth, 1 << 23, 1 << 30)
             dag.build_terrain(7, 16, True)
             st = dag.status()
             ts = dag.stats()
