@@ -1,0 +1,35 @@
+"""The C++ compatibility header (the reference's call shapes over the C ABI)
+compiles and links against the library; nothing runs on a device."""
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+SRC = r'''
+#include "voxel_b200_compat.hpp"
+int main() {
+  namespace hdg = algo::svt::hash_dag_gpu;
+  std::uint32_t *d = nullptr; std::uint64_t *k = nullptr;
+  (void)algo::cuda::scan::required_workspace_size<std::uint32_t>(10);
+  (void)algo::cuda::scan::exclusive_sum(d, 0, nullptr, 0);
+  (void)algo::cuda::sort::sort_by_key(k, algo::cuda::sort::value_arrays(d), 0, nullptr, 0);
+  (void)hdg::apply_voxel_edits_workspace_size(4);
+  hdg::VoxelEdit e{1, 2, 3};
+  (void)e;
+  return 0;
+}
+'''
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no g++")
+def test_compat_header_compiles_and_links(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text(SRC)
+    exe = tmp_path / "use"
+    cmd = ["g++", "-std=c++17", str(src), "-I", str(ROOT / "include"),
+           "-I", "/usr/local/cuda/include", "-L", str(ROOT / "voxel_b200"),
+           "-lvoxel_b200", "-L", "/usr/local/cuda/lib64", "-lcudart", "-o", str(exe)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
