@@ -272,6 +272,72 @@ typedef struct vx_dag_stats {
 vx_status vx_dag_get_stats(const vx_dag *dag, vx_dag_stats *host_stats,
                            vx_stream stream);
 
+/* ------------------------------------------------------------------ SVO --
+ * Pointer-based sparse voxel octree with free lists.  World side 4 << depth,
+ * 1 <= depth <= 12 (the reference GPU SVO is fixed at depth 10,
+ * svt/cuda/config.cuh:17-31).  Node = 8 x u32 child_data: bits 0-29 child
+ * index, bit 30 child present, bit 31 filled-when-absent (svt/cuda/config.cuh:
+ * 36-42).  Leaves are u64 masks, bit = x + 4y + 16z.  With materials enabled
+ * each leaf also holds 64 material bytes, a uniform filled child stores its
+ * material in bits 0-7, and a region collapses only when occupancy and
+ * material are both uniform; with materials disabled the structure is exactly
+ * the reference's (svt/svo.hpp, svt/cuda/voxel/detail/collapse).
+ * Replaces GpuSvo / DeviceGpuSvo / reset_svo (svt/cuda/storage.cuh:12-122,
+ * svt/cuda/device_view.cuh:11-44, svt/cuda/svo.cuh:17-22). */
+typedef struct vx_svo vx_svo;
+
+typedef struct vx_svo_config {
+    uint32_t depth;           /* inner levels, 1..12 */
+    uint32_t materials;       /* 0 = occupancy only, 1 = uint8 material per voxel */
+    uint32_t max_nodes;
+    uint32_t max_leaves;
+    uint64_t arena_bytes;     /* scratch for batched / terrain builds (0 = default) */
+} vx_svo_config;
+
+vx_status vx_svo_create(const vx_svo_config *config, vx_svo **out);
+vx_status vx_svo_destroy(vx_svo *svo);
+vx_status vx_svo_reset(vx_svo *svo, vx_stream stream);
+
+/* Plain per-call path: place (with a material) or destroy a voxel list.
+ * Replaces svt::cuda::{place,destroy}_voxel_edits and
+ * apply_voxel_edits_workspace_size (svt/cuda/voxel/edit.cuh:14-92). */
+size_t vx_svo_voxel_workspace_size(uint32_t count);
+vx_status vx_svo_apply_voxels(vx_svo *svo, const vx_voxel *edits,
+                              uint32_t count, uint32_t op, uint32_t material,
+                              void *workspace, size_t workspace_bytes,
+                              vx_stream stream);
+/* Batched primitives, sequential semantics in array order (see the DAG). */
+vx_status vx_svo_apply_primitives(vx_svo *svo, const vx_primitive *prims,
+                                  uint32_t count, vx_stream stream);
+vx_status vx_svo_status(vx_svo *svo, vx_stream stream);
+vx_status vx_svo_build_terrain(vx_svo *svo, const vx_terrain *terrain,
+                               vx_stream stream);
+/* out[i] = material of voxel pts[i] (0 = empty; 1 for solid without
+ * materials) (svt::cuda::get_voxel, svt/cuda/query.cuh:11-35). */
+vx_status vx_svo_query(const vx_svo *svo, const vx_voxel *pts, uint32_t count,
+                       uint8_t *out, vx_stream stream);
+/* Canonical dump (host, synchronises): DFS first-visit renumbering of nodes
+ * and leaves; host_nodes gets 8 words per node with child indices replaced by
+ * canonical ones and bits 30/31 (and materials) kept; host_leaves gets the u64
+ * masks; host_materials (may be NULL) 64 bytes per leaf.  NULL arrays query
+ * the counts. */
+vx_status vx_svo_export_canonical(const vx_svo *svo, uint32_t *host_node_count,
+                                  uint32_t *host_leaf_count,
+                                  uint32_t *host_nodes, uint32_t nodes_capacity,
+                                  uint64_t *host_leaves,
+                                  uint8_t *host_materials,
+                                  uint32_t leaves_capacity, vx_stream stream);
+
+/* Counters (GpuSvoCounters, svt/cuda/device_view.cuh:24-29). */
+typedef struct vx_svo_counters {
+    uint32_t node_count;
+    uint32_t leaf_count;
+    uint32_t free_node_count;
+    uint32_t free_leaf_count;
+} vx_svo_counters;
+vx_status vx_svo_get_counters(const vx_svo *svo, vx_svo_counters *host_counters,
+                              vx_stream stream);
+
 /* ---------------------------------------------------------- rasterising --
  * Expand primitives into voxel lists (the plain path's input shape).
  * out_offsets[i] = first voxel of primitive i (exclusive scan of counts);

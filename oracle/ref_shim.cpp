@@ -72,8 +72,9 @@ struct DagDump {
 };
 
 // DFS pre-order canonical form of an SVO: node ids in first-visit order (root
-// = 0), leaf ids in first-visit order, child words keep bits 30/31 and carry
-// the canonical index (svo.hpp:19-91, CHILD_* constants at svo.hpp:11-16).
+// = 0), leaf ids in first-visit order; an absent child keeps its word (bit 31
+// = filled), a present child is bit 30 | canonical index (svo.hpp:19-91,
+// CHILD_* constants at svo.hpp:11-16).
 struct SvoDump {
   const SVO &svo;
   std::vector<u32> nodes;
@@ -97,7 +98,9 @@ struct SvoDump {
           cid = static_cast<u32>(leaves.size());
           leaves.push_back(svo.leaves_[child].voxel_data);
         }
-        rec[c] = (info & ~algo::svt::CHILD_INDEX_MASK) | cid;
+        // Bit 31 of a child-present word is a don't-care (the reference
+        // reads it only when bit 30 is clear); canonical form drops it.
+        rec[c] = algo::svt::CHILD_MASK_BIT | cid;
       } else {
         rec[c] = info;
       }

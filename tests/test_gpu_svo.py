@@ -1,0 +1,128 @@
+"""GPU SVO against the oracle (pinned to the reference's CPU SVO): canonical
+node arrays, leaves and materials bit-exact after batched primitives, the
+plain voxel path, terrain builds; queries; counters; capacity."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import voxel_b200 as vx
+
+pytestmark = pytest.mark.gpu
+
+
+def canon(s: vx.Svo) -> oracle.SvoCanon:
+    return oracle.SvoCanon(*s.canonical())
+
+
+def rand_prims(rng, n, world, rmax, sphere_frac=0.6, add_frac=0.55, materials=True):
+    p = np.zeros(n, oracle.PRIM_DTYPE)
+    for i in range(n):
+        shape = 0 if rng.random() < sphere_frac else 1
+        op = int(rng.random() < add_frac)
+        r = rng.integers(0, rmax + 1, 3)
+        mat = int(rng.integers(1, 256)) if (op and materials) else (1 if op else 0)
+        p[i] = (rng.integers(-3, world + 3, 3), (r[0], r[1] if shape else 0, r[2] if shape else 0),
+                shape | (op << 8) | (mat << 16), 0)
+    return p
+
+
+@pytest.mark.parametrize("depth,n,seed,mats", [(1, 12, 0, False), (2, 30, 1, False),
+                                               (3, 80, 2, True), (5, 200, 3, False),
+                                               (5, 200, 4, True), (6, 300, 5, True)])
+def test_batched_primitives_match_oracle(cuda, depth, n, seed, mats):
+    rng = np.random.default_rng(seed)
+    world = 4 << depth
+    prims = rand_prims(rng, n, world, max(2, world // 5), materials=mats)
+    s = vx.Svo(depth, 1 << 18, 1 << 18, materials=mats, arena_bytes=64 << 20)
+    s.apply_primitives(vx.prims_to_device(prims, cuda))
+    assert s.status() == 0
+    assert canon(s) == oracle.Grid(depth, materials=mats).apply_prims(prims).svo()
+
+
+@pytest.mark.parametrize("depth,caves,mats", [(4, False, False), (5, True, True),
+                                              (6, True, False)])
+def test_terrain_build_matches_oracle(cuda, depth, caves, mats):
+    t = oracle.terrain(seed=1, scale=1, caves=caves)
+    s = vx.Svo(depth, 1 << 20, 1 << 20, materials=mats, arena_bytes=64 << 20)
+    s.build_terrain(1, 1, caves)
+    assert s.status() == 0
+    assert canon(s) == oracle.Grid(depth, materials=mats).terrain(t).svo()
+
+
+@pytest.mark.parametrize("mats", [False, True])
+def test_terrain_then_batches_queries_and_gc(cuda, mats):
+    depth = 6
+    world = 4 << depth
+    rng = np.random.default_rng(12)
+    t = oracle.terrain(seed=7, scale=1, caves=True)
+    s = vx.Svo(depth, 1 << 18, 1 << 18, materials=mats, arena_bytes=64 << 20)
+    s.build_terrain(7, 1, True)
+    g = oracle.Grid(depth, materials=mats).terrain(t)
+    all_prims = []
+    for _ in range(4):
+        prims = rand_prims(rng, 120, world, 30, materials=mats)
+        all_prims.append(prims)
+        s.apply_primitives(vx.prims_to_device(prims, cuda))
+        g.apply_prims(prims)
+        assert s.status() == 0
+        assert canon(s) == g.svo()
+    pts = rng.integers(0, world + 8, (5000, 3)).astype(np.uint32)
+    got = s.query(vx.voxels_to_device(pts, cuda)).cpu().numpy()
+    inside = (pts < world).all(axis=1)
+    expect = np.zeros(len(pts), np.uint8)
+    expect[inside] = oracle.eval_voxels(t, depth + 2, np.concatenate(all_prims), pts[inside],
+                                        materials=mats)
+    assert np.array_equal(got, expect)
+    # live structure = counters minus free lists
+    c = s.counters()
+    nodes, leaves, _ = s.canonical()
+    assert c.node_count - c.free_node_count == nodes.size // 8
+    assert c.leaf_count - c.free_leaf_count == leaves.size
+
+
+def test_plain_voxels_match_reference_semantics(cuda):
+    """The plain path (one op per voxel list) against the oracle, which is
+    pinned to the reference SVO::set_voxel; config C1's 256^3 world."""
+    depth = 6
+    world = 4 << depth
+    rng = np.random.default_rng(8)
+    s = vx.Svo(depth, 1 << 16, 1 << 16, arena_bytes=32 << 20)
+    g = oracle.Grid(depth)
+    for i in range(12):
+        c = rng.integers(0, world, 3)
+        r = int(rng.integers(2, 17))
+        ax = np.arange(-r, r + 1)
+        zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+        ins = xx ** 2 + yy ** 2 + zz ** 2 <= r * r
+        vox = np.stack([xx[ins], yy[ins], zz[ins]], 1) + c
+        vox = vox[(vox >= 0).all(1) & (vox < world).all(1)].astype(np.uint32)
+        op = i % 2 == 0 or i % 3 == 0
+        assert s.apply_voxels(vx.voxels_to_device(vox, cuda), int(op)) == 0
+        g.apply_voxels(vox, int(op))
+        assert canon(s) == g.svo()
+
+
+def test_plain_out_of_world_and_rejections(cuda):
+    depth = 4
+    s = vx.Svo(depth, 1 << 12, 1 << 12, arena_bytes=8 << 20)
+    e = np.array([[1, 2, 3], [70, 1, 1], [1, 999, 1], [4, 4, 4]], np.uint32)
+    assert s.apply_voxels(vx.voxels_to_device(e, cuda), vx.EDIT_PLACE) == 0
+    g = oracle.Grid(depth).apply_voxels(e, 1)
+    assert canon(s) == g.svo()
+    lib = vx.lib()
+    st = vx.stream_handle()
+    assert lib.vx_svo_apply_voxels(s._h, None, 3, 1, 1, None, 0, st) == vx.VX_ERR_INVALID_VALUE
+    assert lib.vx_svo_apply_voxels(s._h, None, 0, 1, 1, None, 0, st) == vx.VX_OK
+    assert canon(s) == g.svo()
+
+
+def test_capacity_overflow_changes_nothing(cuda):
+    depth = 6
+    s = vx.Svo(depth, 64, 64, arena_bytes=8 << 20)
+    small = np.array([[1, 1, 1]], np.uint32)
+    assert s.apply_voxels(vx.voxels_to_device(small, cuda), vx.EDIT_PLACE) == 0
+    before = canon(s)
+    many = np.random.default_rng(2).integers(0, 4 << depth, (3000, 3)).astype(np.uint32)
+    assert s.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE) == vx.VX_ERR_CAPACITY
+    assert canon(s) == before

@@ -18,7 +18,7 @@ __all__ = [
     "workspace_status", "SlabHashSet", "CuckooMap", "PRIM_DTYPE",
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
-    "config_c4_edits", "rasterize",
+    "config_c4_edits", "rasterize", "Svo",
 ]
 
 
@@ -352,3 +352,88 @@ def rasterize(prims: torch.Tensor, world_exp: int):
     check(lib().vx_rasterize(ptr(prims), n, world_exp, ptr(offsets), ptr(out),
                              stream_handle()), "vx_rasterize")
     return out[:total], offsets
+
+
+class Svo:
+    """Pointer sparse voxel octree on the GPU (GpuSvo / DeviceGpuSvo,
+    svt/cuda/storage.cuh:12-122, widened to depth 1..12 and optional uint8
+    materials)."""
+
+    def __init__(self, depth: int, max_nodes: int = 1 << 20, max_leaves: int = 1 << 20,
+                 materials: bool = False, arena_bytes: int = 0):
+        from . import vx_svo_config
+        cfg = vx_svo_config(depth, int(materials), max_nodes, max_leaves, arena_bytes)
+        h = C.c_void_p()
+        check(lib().vx_svo_create(C.byref(cfg), C.byref(h)), "vx_svo_create")
+        self._h = h
+        self.depth = depth
+        self.materials = materials
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_svo_destroy(h)
+            self._h = None
+
+    @property
+    def world(self) -> int:
+        return 4 << self.depth
+
+    def reset(self):
+        check(lib().vx_svo_reset(self._h, stream_handle()), "vx_svo_reset")
+
+    def apply_voxels(self, voxels: torch.Tensor, op: int, material: int = 1,
+                     workspace: torch.Tensor | None = None) -> int:
+        """Plain path (svt::cuda::{place,destroy}_voxel_edits,
+        svt/cuda/voxel/edit.cuh:76-92); returns the status."""
+        n = voxels.numel() // 3
+        ws = workspace
+        if ws is None and n:
+            ws = torch.empty(lib().vx_svo_voxel_workspace_size(n), dtype=torch.uint8,
+                             device=voxels.device)
+        return lib().vx_svo_apply_voxels(self._h, ptr(voxels) if n else None, n, op,
+                                         material, ptr(ws) if n else None,
+                                         ws.numel() if n else 0, stream_handle())
+
+    def apply_primitives(self, prims: torch.Tensor) -> None:
+        n = prims.numel() // 8
+        check(lib().vx_svo_apply_primitives(self._h, ptr(prims) if n else None, n,
+                                            stream_handle()), "vx_svo_apply_primitives")
+
+    def status(self) -> int:
+        return lib().vx_svo_status(self._h, stream_handle())
+
+    def build_terrain(self, seed: int, scale: int, caves: bool) -> None:
+        from . import vx_terrain
+        t = vx_terrain(seed, scale, int(caves), self.depth + 2)
+        check(lib().vx_svo_build_terrain(self._h, C.byref(t), stream_handle()),
+              "vx_svo_build_terrain")
+
+    def query(self, voxels: torch.Tensor) -> torch.Tensor:
+        n = voxels.numel() // 3
+        out = torch.empty(n, dtype=torch.uint8, device=voxels.device)
+        check(lib().vx_svo_query(self._h, ptr(voxels), n, ptr(out), stream_handle()),
+              "vx_svo_query")
+        return out
+
+    def counters(self):
+        from . import vx_svo_counters
+        c = vx_svo_counters()
+        check(lib().vx_svo_get_counters(self._h, C.byref(c), stream_handle()),
+              "vx_svo_get_counters")
+        return c
+
+    def canonical(self):
+        """(nodes [8 words each], leaves, materials or None): DFS pre-order."""
+        nn, nl = C.c_uint32(0), C.c_uint32(0)
+        f = lib().vx_svo_export_canonical
+        check(f(self._h, C.byref(nn), C.byref(nl), None, 0, None, None, 0,
+                stream_handle()), "export sizes")
+        nodes = np.zeros(max(nn.value * 8, 1), np.uint32)
+        leaves = np.zeros(max(nl.value, 1), np.uint64)
+        mats = np.zeros(max(nl.value * 64, 1), np.uint8) if self.materials else None
+        check(f(self._h, C.byref(nn), C.byref(nl), nodes.ctypes.data, nn.value,
+                leaves.ctypes.data, None if mats is None else mats.ctypes.data,
+                nl.value, stream_handle()), "export")
+        return (nodes[:nn.value * 8], leaves[:nl.value],
+                None if mats is None else mats[:nl.value * 64])

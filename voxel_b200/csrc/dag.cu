@@ -193,329 +193,19 @@ struct Ctx {
   uint32_t host_prim_count;
 };
 
-__global__ void init_kernel(Ctx x) {
-  Header *h = x.t.hdr;
-  const uint32_t n = x.d_prim_count ? *x.d_prim_count : x.host_prim_count;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    for (uint32_t l = 0; l < 16; ++l) {
-      h->item_off[l] = 0;
-      h->item_count[l] = 0;
-      h->pair_count[l] = 0;
-      h->big_count[l] = 0;
-    }
-    h->prim_count = n;
-    const uint32_t ok = h->status == kDevOk && n <= x.a.pair_cap;
-    if (h->status == kDevOk && n > x.a.pair_cap) h->status = kDevCapacity;
-    if (ok) {
-      h->item_count[0] = 1;
-      h->pair_count[0] = n;
-      Item it{};
-      it.cell = 0;
-      it.old = h->root;
-      it.pstart = 0;
-      it.pcount = n;
-      x.a.items[0] = it;
-    }
-  }
-  if (n > x.a.pair_cap) return;
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-    x.a.pairs[0][i] = static_cast<uint32_t>(i);
-}
-
-// Top-down expansion of level l into level l + 1 (l + 1 < depth).  Eight
-// lanes per work item, one per child cell: lane c walks the item's ordered
-// primitive list once, remembering the last primitive that covers child c
-// entirely (which resets the count of partial ones before it) and counting the
-// partial ones after it; a second walk writes those to the child's list.
-// Output space for a block's 32 items is taken with one atomicAdd per counter.
-template <class Tree, bool Terrain>
-__global__ void __launch_bounds__(kBlock)
-    expand_kernel(Ctx x, Tree tree, uint32_t l) {
-  Header *h = x.t.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
-  const uint32_t depth = x.t.depth;
-  const uint32_t W = h->item_count[l];
-  const uint32_t base = h->item_off[l];
-  const uint32_t next_base = base + W;
-  if (blockIdx.x == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
-  const uint32_t *in_pairs = x.a.pairs[l & 1u];
-  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
-  const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
-  const uint32_t world_exp = depth + 2;
-  constexpr uint32_t kGroups = kBlock / 8;
-
-  __shared__ uint32_t s_items[kGroups], s_pairs[kGroups];
-  __shared__ uint32_t s_item_base, s_pair_base;
-  const uint32_t group = threadIdx.x >> 3, c = threadIdx.x & 7u;
-  const uint32_t gshift = (lane_id() >> 3) * 8u; // this group's byte in a ballot
-
-  for (uint64_t tile = blockIdx.x; tile * kGroups < W; tile += gridDim.x) {
-    const uint32_t wi = static_cast<uint32_t>(tile * kGroups) + group;
-    const bool have = wi < W;
-    Item it{};
-    if (have) it = x.a.items[base + wi];
-    const bool big = have && it.pcount > kBigItem;
-    if (big) {
-      // Long lists go to expand_big_kernel (one block per item).
-      if (c == 0) {
-        const uint32_t slot = atomicAdd(&h->big_count[l], 1u);
-        if (slot < x.a.big_cap) x.a.big[slot] = wi;
-        else set_status(&h->status, kDevCapacity);
-      }
-      it.pcount = 0;
-    }
-    const Cell cell = unpack_cell(it.cell);
-    const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
-    const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
-    const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
-    int32_t last_full = -1;
-    uint32_t cnt = 0;
-    for (uint32_t k = 0; k < it.pcount; ++k) {
-      const uint32_t p = in_pairs[it.pstart + k];
-      const uint32_t cls = classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize);
-      if (cls == VX_CELL_FULL) {
-        last_full = static_cast<int32_t>(p);
-        cnt = 0;
-      } else if (cls == VX_CELL_MIXED) {
-        ++cnt;
-      }
-    }
-    // Prefix sums over the 8 lanes of the group.
-    uint32_t inc_items = cnt ? 1u : 0u, inc_pairs = cnt;
-#pragma unroll
-    for (uint32_t d = 1; d < 8; d <<= 1) {
-      const uint32_t a = __shfl_up_sync(kFullMask, inc_items, d, 8);
-      const uint32_t b = __shfl_up_sync(kFullMask, inc_pairs, d, 8);
-      if (c >= d) {
-        inc_items += a;
-        inc_pairs += b;
-      }
-    }
-    const uint32_t group_items = __shfl_sync(kFullMask, inc_items, 7, 8);
-    const uint32_t group_pairs = __shfl_sync(kFullMask, inc_pairs, 7, 8);
-    const bool full_add =
-        last_full >= 0 && vx_prim_op(&x.prims[last_full]) == VX_OP_ADD;
-    const uint32_t child_mask = (__ballot_sync(kFullMask, cnt != 0) >> gshift) & 0xffu;
-    const uint32_t const_mask = (__ballot_sync(kFullMask, last_full >= 0) >> gshift) & 0xffu;
-    const uint32_t const_full = (__ballot_sync(kFullMask, full_add) >> gshift) & 0xffu;
-    if (c == 0) {
-      s_items[group] = have && !big ? group_items : 0u;
-      s_pairs[group] = have && !big ? group_pairs : 0u;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t ti = 0, tp = 0;
-      for (uint32_t g = 0; g < kGroups; ++g) {
-        const uint32_t a = s_items[g], b = s_pairs[g];
-        s_items[g] = ti;
-        s_pairs[g] = tp;
-        ti += a;
-        tp += b;
-      }
-      s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
-      s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
-      if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
-        set_status(&h->status, kDevCapacity);
-      if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
-        set_status(&h->status, kDevCapacity);
-    }
-    __syncthreads();
-    const bool room = ld_relaxed_u32(&h->status) == kDevOk;
-    const uint32_t item_off = s_item_base + s_items[group];
-    const uint32_t pair_off = s_pair_base + s_pairs[group];
-    __syncthreads(); // s_* are reused by the next tile
-    if (!have || big || !room) continue;
-
-    if (cnt) {
-      const uint32_t my_pairs = pair_off + inc_pairs - cnt;
-      Item ci{};
-      ci.cell = child_cell(it.cell, c);
-      ci.old = last_full >= 0 ? (full_add ? kFullRef : kEmptyRef)
-                              : tree.child(l, it.old, c);
-      ci.pstart = my_pairs;
-      ci.pcount = cnt;
-      x.a.items[next_base + item_off + inc_items - 1] = ci;
-      uint32_t j = 0;
-      for (uint32_t k = 0; k < it.pcount && j < cnt; ++k) {
-        const uint32_t p = in_pairs[it.pstart + k];
-        if (static_cast<int32_t>(p) <= last_full) continue;
-        if (classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
-          out_pairs[my_pairs + j++] = p;
-      }
-    }
-    if (c == 0) {
-      x.a.items[base + wi].child_base = next_base + item_off;
-      x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
-    }
-  }
-}
-
-// Expansion of the long-list items of level l: one block per item.  Three
-// walks over the list: the last fully-covering primitive per child (block
-// max), the partial primitives after it per child (block sum), then an
-// order-preserving block-wide compaction of those into each child's list.
-template <class Tree, bool Terrain>
-__global__ void __launch_bounds__(kBlock)
-    expand_big_kernel(Ctx x, Tree tree, uint32_t l) {
-  Header *h = x.t.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
-  const uint32_t nbig = min(h->big_count[l], x.a.big_cap);
-  const uint32_t depth = x.t.depth;
-  const uint32_t base = h->item_off[l];
-  const uint32_t next_base = base + h->item_count[l];
-  const uint32_t *in_pairs = x.a.pairs[l & 1u];
-  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
-  const int64_t csize = int64_t(4) << (depth - l - 1);
-  const uint32_t world_exp = depth + 2;
-  constexpr uint32_t kWarps = kBlock / kWarp;
-  __shared__ int32_t s_last[8];
-  __shared__ uint32_t s_cnt[8], s_start[8];
-  __shared__ uint32_t s_warp[8][kWarps];
-  __shared__ uint32_t s_item_base, s_pair_base;
-  __shared__ bool s_room;
-  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
-
-  for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
-    const uint32_t wi = x.a.big[b];
-    const Item it = x.a.items[base + wi];
-    const Cell cell = unpack_cell(it.cell);
-    if (t < 8) {
-      s_last[t] = -1;
-      s_cnt[t] = 0;
-    }
-    __syncthreads();
-    // Walk 1: last FULL per child.
-    int32_t last[8];
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) last[c] = -1;
-    for (uint32_t k = t; k < it.pcount; k += kBlock) {
-      const uint32_t p = in_pairs[it.pstart + k];
-      const vx_primitive pr = x.prims[p];
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
-        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
-        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
-        if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_FULL)
-          last[c] = max(last[c], static_cast<int32_t>(p));
-      }
-    }
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      const int32_t m = __reduce_max_sync(kFullMask, last[c]);
-      if (lane == 0 && m >= 0) atomicMax(&s_last[c], m);
-    }
-    __syncthreads();
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) last[c] = s_last[c];
-    // Walk 2: partial primitives after the last full one.
-    uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t k = t; k < it.pcount; k += kBlock) {
-      const uint32_t p = in_pairs[it.pstart + k];
-      const vx_primitive pr = x.prims[p];
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        if (static_cast<int32_t>(p) <= last[c]) continue;
-        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
-        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
-        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
-        if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED) ++cnt[c];
-      }
-    }
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      const uint32_t v = __reduce_add_sync(kFullMask, cnt[c]);
-      if (lane == 0 && v) atomicAdd(&s_cnt[c], v);
-    }
-    __syncthreads();
-    if (t == 0) {
-      uint32_t ni = 0, np = 0, cm = 0, km = 0, kf = 0;
-      for (uint32_t c = 0; c < 8; ++c) {
-        s_start[c] = np;
-        if (s_cnt[c]) {
-          cm |= 1u << c;
-          ++ni;
-          np += s_cnt[c];
-        }
-        if (s_last[c] >= 0) {
-          km |= 1u << c;
-          if (vx_prim_op(&x.prims[s_last[c]]) == VX_OP_ADD) kf |= 1u << c;
-        }
-      }
-      s_item_base = ni ? atomicAdd(&h->item_count[l + 1], ni) : 0;
-      s_pair_base = np ? atomicAdd(&h->pair_count[l + 1], np) : 0;
-      if (ni && static_cast<uint64_t>(next_base) + s_item_base + ni > x.a.item_cap)
-        set_status(&h->status, kDevCapacity);
-      if (np && static_cast<uint64_t>(s_pair_base) + np > x.a.pair_cap)
-        set_status(&h->status, kDevCapacity);
-      x.a.items[base + wi].child_base = next_base + s_item_base;
-      x.a.items[base + wi].masks = cm | (km << 8) | (kf << 16);
-      s_room = ld_relaxed_u32(&h->status) == kDevOk;
-    }
-    __syncthreads();
-    const bool room = s_room; // block-uniform: it guards barriers below
-    if (room && t < 8 && s_cnt[t]) {
-      uint32_t k = 0;
-      for (uint32_t c = 0; c < t; ++c) k += s_cnt[c] ? 1u : 0u;
-      Item ci{};
-      ci.cell = child_cell(it.cell, t);
-      ci.old = s_last[t] >= 0
-                   ? (vx_prim_op(&x.prims[s_last[t]]) == VX_OP_ADD ? kFullRef : kEmptyRef)
-                   : tree.child(l, it.old, t);
-      ci.pstart = s_pair_base + s_start[t];
-      ci.pcount = s_cnt[t];
-      x.a.items[next_base + s_item_base + k] = ci;
-    }
-    // Walk 3: order-preserving compaction, one 256-pair chunk at a time.
-    uint32_t run[8];
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) run[c] = s_pair_base + s_start[c];
-    for (uint32_t k0 = 0; k0 < it.pcount && room; k0 += kBlock) {
-      const uint32_t k = k0 + t;
-      uint32_t take = 0, p = 0;
-      if (k < it.pcount) {
-        p = in_pairs[it.pstart + k];
-        const vx_primitive pr = x.prims[p];
-#pragma unroll
-        for (uint32_t c = 0; c < 8; ++c) {
-          if (static_cast<int32_t>(p) <= last[c]) continue;
-          const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
-          const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
-          const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
-          if (classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
-            take |= 1u << c;
-        }
-      }
-      uint32_t ballots[8];
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        ballots[c] = __ballot_sync(kFullMask, (take >> c) & 1u);
-        if (lane == 0) s_warp[c][warp] = __popc(ballots[c]);
-      }
-      __syncthreads();
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) {
-        uint32_t before = 0, total = 0;
-        for (uint32_t w = 0; w < kWarps; ++w) {
-          const uint32_t v = s_warp[c][w];
-          before += w < warp ? v : 0u;
-          total += v;
-        }
-        if ((take >> c) & 1u)
-          out_pairs[run[c] + before + __popc(ballots[c] & lanemask_lt())] = p;
-        run[c] += total;
-      }
-      __syncthreads();
-    }
-    __syncthreads();
-  }
-}
-
 struct DagTree {
   Tables t;
+  static constexpr bool kItemsForConst = false;
   __device__ uint32_t child(uint32_t l, uint32_t ref, uint32_t c) const {
     return child_ref(t, l, ref, c);
+  }
+  template <bool Terrain>
+  __device__ uint32_t classify(const vx_primitive &p, uint32_t world_exp,
+                               int64_t ox, int64_t oy, int64_t oz, int64_t n) const {
+    return vx::edit::classify<Terrain>(p, world_exp, ox, oy, oz, n);
+  }
+  __device__ uint32_t const_value(const vx_primitive &p, int64_t, int64_t) const {
+    return vx_prim_op(&p) == VX_OP_ADD ? kFullRef : kEmptyRef;
   }
 };
 
@@ -667,7 +357,7 @@ __global__ void run_flags_kernel(const uint64_t *keys, uint32_t n, uint32_t dept
 // Each run start ORs its run's bits into one leaf-mask primitive.
 __global__ void reduce_runs_kernel(const uint64_t *keys, const uint32_t *bits,
                                    const uint32_t *offsets, uint32_t n,
-                                   uint32_t depth, uint32_t op,
+                                   uint32_t depth, uint32_t op, uint32_t material,
                                    vx_primitive *out, uint32_t *out_count) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
@@ -690,7 +380,7 @@ __global__ void reduce_runs_kernel(const uint64_t *keys, const uint32_t *bits,
     p.c[2] = static_cast<int32_t>(lz * 4);
     p.r[0] = static_cast<uint32_t>(mask);
     p.r[1] = static_cast<uint32_t>(mask >> 32);
-    p.flags = vx_make_flags(kShapeLeafMask, op, 0);
+    p.flags = vx_make_flags(kShapeLeafMask, op, material);
     out[offsets[i]] = p;
   }
   if (i == n - 1) *out_count = offsets[i] + (start ? 1u : 0u);
@@ -722,12 +412,13 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
                        const uint32_t *d_count, uint32_t host_count,
                        cudaStream_t s, bool terrain = false) {
   Ctx x{d->t, d->a, prims, d_count, host_count};
+  const EditCtx e{d->t.hdr, d->a, prims, d_count, host_count, d->t.depth};
   const uint32_t depth = d->t.depth;
   const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
   {
     prof::Scope sc("dag_init", s);
     init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),
-                  kBlock, 0, s>>>(x);
+                  kBlock, 0, s>>>(e, kUseHeaderRoot);
   }
   VX_TRY_CUDA(cudaGetLastError());
   DagTree tree{d->t};
@@ -735,17 +426,17 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
     {
       prof::Scope sc("dag_expand", s);
       if (terrain)
-        expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(x, tree, l);
+        expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(e, tree, l);
       else
-        expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(x, tree, l);
+        expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(e, tree, l);
     }
     VX_TRY_CUDA(cudaGetLastError());
     {
       prof::Scope sc("dag_expand_big", s);
       if (terrain)
-        expand_big_kernel<DagTree, true><<<sm_count() * 2, kBlock, 0, s>>>(x, tree, l);
+        expand_big_kernel<DagTree, true><<<sm_count() * 2, kBlock, 0, s>>>(e, tree, l);
       else
-        expand_big_kernel<DagTree, false><<<sm_count() * 2, kBlock, 0, s>>>(x, tree, l);
+        expand_big_kernel<DagTree, false><<<sm_count() * 2, kBlock, 0, s>>>(e, tree, l);
     }
     VX_TRY_CUDA(cudaGetLastError());
   }
@@ -816,6 +507,51 @@ struct NullCarver {
 };
 
 } // namespace vx::dag
+
+namespace vx::plain {
+
+size_t workspace_size(uint32_t count) {
+  if (count == 0) return 0;
+  vx::dag::NullCarver c;
+  vx::dag::plain_layout(c, count);
+  return c.offset;
+}
+
+// Voxel list -> one leaf-mask primitive per touched leaf (op, material),
+// written into the workspace; *out_prims / *out_count point into it.
+vx_status prepare(const vx_voxel *edits, uint32_t count, uint32_t depth,
+                  uint32_t op, uint32_t material, void *workspace,
+                  const vx_primitive **out_prims, const uint32_t **out_count,
+                  cudaStream_t s) {
+  using namespace vx::dag;
+  vx::Carver c(workspace);
+  const PlainLayout p = plain_layout(c, count);
+  const uint32_t blocks = vx::ceil_div(count, kBlock);
+  {
+    vx::prof::Scope sc("plain_pack_voxels", s);
+    pack_voxels_kernel<<<blocks, kBlock, 0, s>>>(edits, count, depth, p.keys, p.bits);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_sort_pairs_u64(p.keys, p.bits, count, 3 * depth + 1, p.sort_ws,
+                           p.sort_ws_bytes, s));
+  {
+    vx::prof::Scope sc("plain_run_flags", s);
+    run_flags_kernel<<<blocks, kBlock, 0, s>>>(p.keys, count, depth, p.offsets);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_scan_exclusive_sum_u32(p.offsets, count, p.scan_ws, p.scan_ws_bytes, s));
+  {
+    vx::prof::Scope sc("plain_reduce_runs", s);
+    reduce_runs_kernel<<<blocks, kBlock, 0, s>>>(p.keys, p.bits, p.offsets, count,
+                                                 depth, op, material, p.prims, p.count);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  *out_prims = p.prims;
+  *out_count = p.count;
+  return VX_OK;
+}
+
+} // namespace vx::plain
 
 using namespace vx::dag;
 
@@ -906,10 +642,7 @@ vx_status vx_dag_reset(vx_dag *d, vx_stream stream) {
 uint32_t vx_dag_depth(const vx_dag *d) { return d ? d->t.depth : 0; }
 
 size_t vx_dag_voxel_workspace_size(uint32_t count) {
-  if (count == 0) return 0;
-  NullCarver c;
-  plain_layout(c, count);
-  return c.offset;
+  return vx::plain::workspace_size(count);
 }
 
 vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
@@ -921,29 +654,10 @@ vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
   if (workspace == nullptr || workspace_bytes < vx_dag_voxel_workspace_size(count))
     return VX_ERR_INVALID_VALUE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  vx::Carver c(workspace);
-  const PlainLayout p = plain_layout(c, count);
-  const uint32_t blocks = vx::ceil_div(count, kBlock);
-  {
-    vx::prof::Scope sc("dag_pack_voxels", s);
-    pack_voxels_kernel<<<blocks, kBlock, 0, s>>>(edits, count, d->t.depth, p.keys, p.bits);
-  }
-  VX_TRY_CUDA(cudaGetLastError());
-  VX_TRY(vx_sort_pairs_u64(p.keys, p.bits, count, 3 * d->t.depth + 1, p.sort_ws,
-                           p.sort_ws_bytes, s));
-  {
-    vx::prof::Scope sc("dag_run_flags", s);
-    run_flags_kernel<<<blocks, kBlock, 0, s>>>(p.keys, count, d->t.depth, p.offsets);
-  }
-  VX_TRY_CUDA(cudaGetLastError());
-  VX_TRY(vx_scan_exclusive_sum_u32(p.offsets, count, p.scan_ws, p.scan_ws_bytes, s));
-  {
-    vx::prof::Scope sc("dag_reduce_runs", s);
-    reduce_runs_kernel<<<blocks, kBlock, 0, s>>>(p.keys, p.bits, p.offsets, count,
-                                                 d->t.depth, op, p.prims, p.count);
-  }
-  VX_TRY_CUDA(cudaGetLastError());
-  VX_TRY(run_pipeline(d, p.prims, p.count, count, s));
+  const vx_primitive *prims = nullptr;
+  const uint32_t *n = nullptr;
+  VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));
+  VX_TRY(run_pipeline(d, prims, n, count, s));
   return read_status(d, s, true);
 }
 

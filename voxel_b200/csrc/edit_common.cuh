@@ -125,4 +125,349 @@ struct Arena {
 // Items with more primitives than this are expanded by a whole block.
 constexpr uint32_t kBigItem = 64;
 
+
+// init_kernel's root_old value meaning "the root stored in the header".
+constexpr uint32_t kUseHeaderRoot = 0xfffffffeu;
+
+// Device-side edit context shared by the DAG and SVO pipelines.
+struct EditCtx {
+  Header *hdr;
+  Arena a;
+  const vx_primitive *prims;
+  const uint32_t *d_prim_count; // device count (NULL: use host_prim_count)
+  uint32_t host_prim_count;
+  uint32_t depth;
+};
+
+// A tree Policy supplies:
+//   static constexpr bool kItemsForConst  - also create a (primitive-free)
+//       child item where a primitive covers the child entirely, so the
+//       rebuild sees its constant value in the child item's `old`;
+//   child(l, old, c)                      - content of child c of `old` at level l;
+//   classify<Terrain>(prim, world_exp, ox, oy, oz, n);
+//   const_value(prim, oz, n)              - the content a fully covering
+//       primitive leaves in the cube at height oz of side n (1 = full).
+
+static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
+  Header *h = x.hdr;
+  const uint32_t n = x.d_prim_count ? *x.d_prim_count : x.host_prim_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (uint32_t l = 0; l < 16; ++l) {
+      h->item_off[l] = 0;
+      h->item_count[l] = 0;
+      h->pair_count[l] = 0;
+      h->big_count[l] = 0;
+    }
+    h->prim_count = n;
+    const uint32_t ok = h->status == kDevOk && n <= x.a.pair_cap;
+    if (h->status == kDevOk && n > x.a.pair_cap) h->status = kDevCapacity;
+    if (ok) {
+      h->item_count[0] = 1;
+      h->pair_count[0] = n;
+      Item it{};
+      it.cell = 0;
+      it.old = root_old == kUseHeaderRoot ? h->root : root_old;
+      it.pstart = 0;
+      it.pcount = n;
+      x.a.items[0] = it;
+    }
+  }
+  if (n > x.a.pair_cap) return;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    x.a.pairs[0][i] = static_cast<uint32_t>(i);
+}
+
+// Top-down expansion of level l into level l + 1 (l + 1 < depth).  Eight
+// lanes per work item, one per child cell: lane c walks the item's ordered
+// primitive list once, remembering the last primitive that covers child c
+// entirely (which resets the count of partial ones before it) and counting the
+// partial ones after it; a second walk writes those to the child's list.
+// Output space for a block's 32 items is taken with one atomicAdd per counter.
+template <class Policy, bool Terrain>
+__global__ void __launch_bounds__(kBlock)
+    expand_kernel(EditCtx x, Policy pol, uint32_t l) {
+  Header *h = x.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t depth = x.depth;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  const uint32_t next_base = base + W;
+  if (blockIdx.x == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
+  const uint32_t *in_pairs = x.a.pairs[l & 1u];
+  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
+  const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
+  const uint32_t world_exp = depth + 2;
+  constexpr uint32_t kGroups = kBlock / 8;
+
+  __shared__ uint32_t s_items[kGroups], s_pairs[kGroups];
+  __shared__ uint32_t s_item_base, s_pair_base;
+  const uint32_t group = threadIdx.x >> 3, c = threadIdx.x & 7u;
+  const uint32_t gshift = (lane_id() >> 3) * 8u; // this group's byte in a ballot
+
+  for (uint64_t tile = blockIdx.x; tile * kGroups < W; tile += gridDim.x) {
+    const uint32_t wi = static_cast<uint32_t>(tile * kGroups) + group;
+    const bool have = wi < W;
+    Item it{};
+    if (have) it = x.a.items[base + wi];
+    const bool big = have && it.pcount > kBigItem;
+    if (big) {
+      // Long lists go to expand_big_kernel (one block per item).
+      if (c == 0) {
+        const uint32_t slot = atomicAdd(&h->big_count[l], 1u);
+        if (slot < x.a.big_cap) x.a.big[slot] = wi;
+        else set_status(&h->status, kDevCapacity);
+      }
+      it.pcount = 0;
+    }
+    const Cell cell = unpack_cell(it.cell);
+    const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+    const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+    const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+    int32_t last_full = -1;
+    uint32_t cnt = 0;
+    for (uint32_t k = 0; k < it.pcount; ++k) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const uint32_t cls = pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize);
+      if (cls == VX_CELL_FULL) {
+        last_full = static_cast<int32_t>(p);
+        cnt = 0;
+      } else if (cls == VX_CELL_MIXED) {
+        ++cnt;
+      }
+    }
+    // Prefix sums over the 8 lanes of the group.
+    uint32_t inc_items =
+                 (cnt != 0 || (Policy::kItemsForConst && last_full >= 0)) ? 1u : 0u,
+             inc_pairs = cnt;
+#pragma unroll
+    for (uint32_t d = 1; d < 8; d <<= 1) {
+      const uint32_t a = __shfl_up_sync(kFullMask, inc_items, d, 8);
+      const uint32_t b = __shfl_up_sync(kFullMask, inc_pairs, d, 8);
+      if (c >= d) {
+        inc_items += a;
+        inc_pairs += b;
+      }
+    }
+    const uint32_t group_items = __shfl_sync(kFullMask, inc_items, 7, 8);
+    const uint32_t group_pairs = __shfl_sync(kFullMask, inc_pairs, 7, 8);
+    const uint32_t const_val =
+        last_full >= 0 ? pol.const_value(x.prims[last_full], oz, csize) : 0u;
+    const bool full_add = last_full >= 0 && const_val == 1u;
+    const bool has_item = cnt != 0 || (Policy::kItemsForConst && last_full >= 0);
+    const uint32_t child_mask = (__ballot_sync(kFullMask, has_item) >> gshift) & 0xffu;
+    const uint32_t const_mask = (__ballot_sync(kFullMask, last_full >= 0) >> gshift) & 0xffu;
+    const uint32_t const_full = (__ballot_sync(kFullMask, full_add) >> gshift) & 0xffu;
+    if (c == 0) {
+      s_items[group] = have && !big ? group_items : 0u;
+      s_pairs[group] = have && !big ? group_pairs : 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t ti = 0, tp = 0;
+      for (uint32_t g = 0; g < kGroups; ++g) {
+        const uint32_t a = s_items[g], b = s_pairs[g];
+        s_items[g] = ti;
+        s_pairs[g] = tp;
+        ti += a;
+        tp += b;
+      }
+      s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
+      s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
+      if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
+        set_status(&h->status, kDevCapacity);
+      if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
+        set_status(&h->status, kDevCapacity);
+    }
+    __syncthreads();
+    const bool room = ld_relaxed_u32(&h->status) == kDevOk;
+    const uint32_t item_off = s_item_base + s_items[group];
+    const uint32_t pair_off = s_pair_base + s_pairs[group];
+    __syncthreads(); // s_* are reused by the next tile
+    if (!have || big || !room) continue;
+
+    if (has_item) {
+      const uint32_t my_pairs = pair_off + inc_pairs - cnt;
+      Item ci{};
+      ci.cell = child_cell(it.cell, c);
+      ci.old = last_full >= 0 ? const_val : pol.child(l, it.old, c);
+      ci.pstart = my_pairs;
+      ci.pcount = cnt;
+      x.a.items[next_base + item_off + inc_items - 1] = ci;
+      uint32_t j = 0;
+      for (uint32_t k = 0; k < it.pcount && j < cnt; ++k) {
+        const uint32_t p = in_pairs[it.pstart + k];
+        if (static_cast<int32_t>(p) <= last_full) continue;
+        if (pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
+          out_pairs[my_pairs + j++] = p;
+      }
+    }
+    if (c == 0) {
+      x.a.items[base + wi].child_base = next_base + item_off;
+      x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
+    }
+  }
+}
+
+// Expansion of the long-list items of level l: one block per item.  Three
+// walks over the list: the last fully-covering primitive per child (block
+// max), the partial primitives after it per child (block sum), then an
+// order-preserving block-wide compaction of those into each child's list.
+template <class Policy, bool Terrain>
+__global__ void __launch_bounds__(kBlock)
+    expand_big_kernel(EditCtx x, Policy pol, uint32_t l) {
+  Header *h = x.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t nbig = min(h->big_count[l], x.a.big_cap);
+  const uint32_t depth = x.depth;
+  const uint32_t base = h->item_off[l];
+  const uint32_t next_base = base + h->item_count[l];
+  const uint32_t *in_pairs = x.a.pairs[l & 1u];
+  uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
+  const int64_t csize = int64_t(4) << (depth - l - 1);
+  const uint32_t world_exp = depth + 2;
+  constexpr uint32_t kWarps = kBlock / kWarp;
+  __shared__ int32_t s_last[8];
+  __shared__ uint32_t s_cnt[8], s_start[8], s_const[8], s_cm;
+  __shared__ uint32_t s_warp[8][kWarps];
+  __shared__ uint32_t s_item_base, s_pair_base;
+  __shared__ bool s_room;
+  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
+
+  for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const uint32_t wi = x.a.big[b];
+    const Item it = x.a.items[base + wi];
+    const Cell cell = unpack_cell(it.cell);
+    if (t < 8) {
+      s_last[t] = -1;
+      s_cnt[t] = 0;
+    }
+    __syncthreads();
+    // Walk 1: last FULL per child.
+    int32_t last[8];
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) last[c] = -1;
+    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const vx_primitive pr = x.prims[p];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+        if (pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_FULL)
+          last[c] = max(last[c], static_cast<int32_t>(p));
+      }
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const int32_t m = __reduce_max_sync(kFullMask, last[c]);
+      if (lane == 0 && m >= 0) atomicMax(&s_last[c], m);
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) last[c] = s_last[c];
+    // Walk 2: partial primitives after the last full one.
+    uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+      const uint32_t p = in_pairs[it.pstart + k];
+      const vx_primitive pr = x.prims[p];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        if (static_cast<int32_t>(p) <= last[c]) continue;
+        const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+        const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+        const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+        if (pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED) ++cnt[c];
+      }
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const uint32_t v = __reduce_add_sync(kFullMask, cnt[c]);
+      if (lane == 0 && v) atomicAdd(&s_cnt[c], v);
+    }
+    __syncthreads();
+    if (t == 0) {
+      uint32_t ni = 0, np = 0, cm = 0, km = 0, kf = 0;
+      for (uint32_t c = 0; c < 8; ++c) {
+        s_start[c] = np;
+        const int64_t coz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+        s_const[c] = s_last[c] >= 0 ? pol.const_value(x.prims[s_last[c]], coz, csize) : 0u;
+        if (s_cnt[c] || (Policy::kItemsForConst && s_last[c] >= 0)) {
+          cm |= 1u << c;
+          ++ni;
+          np += s_cnt[c];
+        }
+        if (s_last[c] >= 0) {
+          km |= 1u << c;
+          if (s_const[c] == 1u) kf |= 1u << c;
+        }
+      }
+      s_cm = cm;
+      s_item_base = ni ? atomicAdd(&h->item_count[l + 1], ni) : 0;
+      s_pair_base = np ? atomicAdd(&h->pair_count[l + 1], np) : 0;
+      if (ni && static_cast<uint64_t>(next_base) + s_item_base + ni > x.a.item_cap)
+        set_status(&h->status, kDevCapacity);
+      if (np && static_cast<uint64_t>(s_pair_base) + np > x.a.pair_cap)
+        set_status(&h->status, kDevCapacity);
+      x.a.items[base + wi].child_base = next_base + s_item_base;
+      x.a.items[base + wi].masks = cm | (km << 8) | (kf << 16);
+      s_room = ld_relaxed_u32(&h->status) == kDevOk;
+    }
+    __syncthreads();
+    const bool room = s_room; // block-uniform: it guards barriers below
+    if (room && t < 8 && ((s_cm >> t) & 1u)) {
+      const uint32_t k = __popc(s_cm & ((1u << t) - 1u));
+      Item ci{};
+      ci.cell = child_cell(it.cell, t);
+      ci.old = s_last[t] >= 0 ? s_const[t] : pol.child(l, it.old, t);
+      ci.pstart = s_pair_base + s_start[t];
+      ci.pcount = s_cnt[t];
+      x.a.items[next_base + s_item_base + k] = ci;
+    }
+    // Walk 3: order-preserving compaction, one 256-pair chunk at a time.
+    uint32_t run[8];
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) run[c] = s_pair_base + s_start[c];
+    for (uint32_t k0 = 0; k0 < it.pcount && room; k0 += kBlock) {
+      const uint32_t k = k0 + t;
+      uint32_t take = 0, p = 0;
+      if (k < it.pcount) {
+        p = in_pairs[it.pstart + k];
+        const vx_primitive pr = x.prims[p];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          if (static_cast<int32_t>(p) <= last[c]) continue;
+          const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
+          const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
+          const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+          if (pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
+            take |= 1u << c;
+        }
+      }
+      uint32_t ballots[8];
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        ballots[c] = __ballot_sync(kFullMask, (take >> c) & 1u);
+        if (lane == 0) s_warp[c][warp] = __popc(ballots[c]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) {
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < kWarps; ++w) {
+          const uint32_t v = s_warp[c][w];
+          before += w < warp ? v : 0u;
+          total += v;
+        }
+        if ((take >> c) & 1u)
+          out_pairs[run[c] + before + __popc(ballots[c] & lanemask_lt())] = p;
+        run[c] += total;
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
 } // namespace vx::edit

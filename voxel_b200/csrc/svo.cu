@@ -1,0 +1,748 @@
+// Pointer sparse voxel octree on one B200: in-place batched / plain edits,
+// terrain builds, queries, counters, canonical dump.
+//
+// Layout (the reference GpuSvo, svt/cuda/storage.cuh:12-122 and
+// device_view.cuh:11-44): nodes are 8 u32 child words — bits 0-29 child
+// index, bit 30 child present, bit 31 filled when absent (svt/cuda/config.cuh:
+// 36-42); node 0 is the root and always exists.  Leaves are u64 masks
+// (bit = x + 4y + 16z).  With materials each leaf also owns 64 material bytes
+// and an absent filled child keeps its material in bits 0-7; a region
+// collapses only when occupancy and material are both uniform.  Without
+// materials the structure is exactly the reference's: a node or leaf exists
+// iff its region is not uniform (svo.hpp:26-91, GPU collapse
+// svt/cuda/voxel/detail/collapse/kernels.cuh:12-94).
+//
+// Edits use the shared top-down expansion (edit_common.cuh); the rebuild then
+// updates nodes in place bottom-up: a changed region that stays non-uniform
+// reuses its node / leaf, a new one takes an index from the free-list
+// snapshot first and the bump counter after (the reference's rank -> index
+// rule, svt/cuda/voxel/detail/allocation/materialize_common.cuh:72-84), and a
+// region that became uniform detaches its old subtree.  Detached subtrees are
+// reclaimed by a reachability pass that rebuilds the free lists.  Before any
+// write the edit checks that the worst-case allocation fits; if not it
+// reports VX_ERR_CAPACITY and changes nothing.
+#include "edit_common.cuh"
+#include "plain.cuh"
+#include "profile.cuh"
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+namespace vx::svo {
+
+using namespace vx::edit;
+
+constexpr uint32_t kChild = 1u << 30, kFilled = 1u << 31, kIndex = kChild - 1u;
+constexpr uint32_t kMaxDepth = 12;
+
+struct Counters {
+  uint32_t node_count, leaf_count, free_node_count, free_leaf_count;
+  uint32_t base_node_count, base_leaf_count, base_free_nodes, base_free_leaves;
+  uint32_t taken_nodes, taken_leaves;
+  uint32_t detached;
+  uint32_t gc_count[kMaxDepth + 1];
+};
+
+struct Tables {
+  uint32_t depth;
+  uint32_t materials;
+  uint32_t *nodes;
+  uint64_t *leaves;
+  uint8_t *mats;
+  uint32_t *free_nodes;
+  uint32_t *free_leaves;
+  uint8_t *node_mark;
+  uint8_t *leaf_mark;
+  uint32_t *front[2];
+  uint32_t max_nodes, max_leaves;
+  Counters *ctr;
+  Header *hdr;
+};
+
+__device__ __forceinline__ uint32_t word_value(uint32_t w, bool mats) {
+  return (w & kFilled) ? (mats ? (w & 0xffu) : 1u) : 0u;
+}
+__device__ __forceinline__ uint32_t uniform_word(uint32_t v, bool mats) {
+  return v ? (kFilled | (mats ? v : 0u)) : 0u;
+}
+
+// Material an add primitive writes at height z (terrain: its height band).
+__device__ __forceinline__ uint32_t prim_material(const vx_primitive &p, uint32_t world_exp,
+                                                  uint32_t z) {
+  if (vx_prim_shape(&p) == kShapeTerrain) {
+    const vx_terrain t{static_cast<uint32_t>(p.c[0]), static_cast<uint32_t>(p.c[1]),
+                       static_cast<uint32_t>(p.c[2]), world_exp};
+    return vx_terrain_material(&t, z);
+  }
+  const uint32_t m = vx_prim_material(&p);
+  return m ? m : 1u;
+}
+
+struct SvoTree {
+  Tables t;
+  static constexpr bool kItemsForConst = true;
+  __device__ uint32_t child(uint32_t, uint32_t old, uint32_t c) const {
+    if (old & kChild) return t.nodes[static_cast<size_t>(old & kIndex) * 8u + c];
+    return old; // a uniform region's children hold the same value
+  }
+  template <bool Terrain>
+  __device__ uint32_t classify(const vx_primitive &p, uint32_t world_exp, int64_t ox,
+                               int64_t oy, int64_t oz, int64_t n) const {
+    const uint32_t c = vx::edit::classify<Terrain>(p, world_exp, ox, oy, oz, n);
+    if (Terrain && t.materials && c == VX_CELL_FULL && vx_prim_shape(&p) == kShapeTerrain) {
+      // solid terrain is uniform only inside one material band
+      const int64_t band = 8 * static_cast<int64_t>(p.c[1]);
+      if (oz / band != (oz + n - 1) / band) return VX_CELL_MIXED;
+    }
+    return c;
+  }
+  __device__ uint32_t const_value(const vx_primitive &p, int64_t oz, int64_t) const {
+    if (vx_prim_op(&p) != VX_OP_ADD) return 0u;
+    return uniform_word(prim_material(p, t.depth + 2, static_cast<uint32_t>(oz)),
+                        t.materials != 0);
+  }
+};
+
+__device__ __forceinline__ uint32_t alloc_node(const Tables &t) {
+  const uint32_t r = atomicAdd(&t.ctr->taken_nodes, 1u);
+  const uint32_t bf = t.ctr->base_free_nodes;
+  return r < bf ? t.free_nodes[bf - 1u - r] : t.ctr->base_node_count + (r - bf);
+}
+__device__ __forceinline__ uint32_t alloc_leaf(const Tables &t) {
+  const uint32_t r = atomicAdd(&t.ctr->taken_leaves, 1u);
+  const uint32_t bf = t.ctr->base_free_leaves;
+  return r < bf ? t.free_leaves[bf - 1u - r] : t.ctr->base_leaf_count + (r - bf);
+}
+
+// The word a rebuilt cell leaves in its parent: uniform when all 8 children
+// are the same uniform word (never for the root), else a node, reused or new.
+__device__ uint32_t finish_node(const Tables &t, uint32_t old, const uint32_t (&child)[8],
+                                bool is_root) {
+  bool uni = (child[0] & kChild) == 0u;
+#pragma unroll
+  for (uint32_t c = 1; c < 8; ++c) uni = uni && child[c] == child[0];
+  if (uni && !is_root) {
+    if (old & kChild) atomicOr(&t.ctr->detached, 1u);
+    return child[0];
+  }
+  const uint32_t idx = is_root ? 0u : ((old & kChild) ? (old & kIndex) : alloc_node(t));
+  uint4 *dst = reinterpret_cast<uint4 *>(t.nodes + static_cast<size_t>(idx) * 8u);
+  dst[0] = make_uint4(child[0], child[1], child[2], child[3]);
+  dst[1] = make_uint4(child[4], child[5], child[6], child[7]);
+  // A materialised child keeps the fill of the uniform region it replaced in
+  // bit 31, as the reference does (make_child_data, svt/cuda/detail/
+  // node_ops.cuh:24-28; SVO::set_voxel, svo.hpp:54-58); a reused one keeps its.
+  return kChild | idx | (old & kFilled);
+}
+
+__global__ void begin_kernel(Tables t) {
+  Counters *c = t.ctr;
+  c->base_node_count = c->node_count;
+  c->base_leaf_count = c->leaf_count;
+  c->base_free_nodes = c->free_node_count;
+  c->base_free_leaves = c->free_leaf_count;
+  c->taken_nodes = 0;
+  c->taken_leaves = 0;
+}
+
+// Worst case before any write: every item below the root may need a node and
+// every leaf child of the last level a leaf.
+__global__ void check_capacity_kernel(Tables t) {
+  Header *h = t.hdr;
+  if (h->status != kDevOk) return;
+  uint64_t nodes = 0;
+  for (uint32_t l = 1; l < t.depth; ++l) nodes += h->item_count[l];
+  const uint64_t leaves = 8ull * h->item_count[t.depth - 1];
+  const Counters *c = t.ctr;
+  const uint64_t avail_nodes = c->base_free_nodes + uint64_t(t.max_nodes - c->base_node_count);
+  const uint64_t avail_leaves = c->base_free_leaves + uint64_t(t.max_leaves - c->base_leaf_count);
+  if (nodes > avail_nodes || leaves > avail_leaves) h->status = kDevCapacity;
+}
+
+template <bool Terrain>
+__global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t) {
+  Header *h = x.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const SvoTree pol{t};
+  const uint32_t l = t.depth - 1;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  const uint32_t *pairs = x.a.pairs[l & 1u];
+  const uint32_t world_exp = t.depth + 2;
+  const bool mats = t.materials != 0;
+  const uint32_t lane = lane_id();
+  const uint64_t total = static_cast<uint64_t>(W) * 8u;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
+       g0 < total; g0 += stride) {
+    const uint64_t g = g0 + lane;
+    const bool have = g < total;
+    const uint32_t wi = static_cast<uint32_t>(g >> 3), c = lane & 7u;
+    uint32_t result = 0;
+    Item it{};
+    if (have) {
+      it = x.a.items[base + wi];
+      const Cell cell = unpack_cell(it.cell);
+      const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * 4;
+      const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
+      const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
+      const uint32_t oc = pol.child(l, it.old, c);
+      uint64_t mask = 0;
+      uint32_t v[16]; // 64 material bytes, 4 per word; word w holds z = w >> 2
+      bool loaded = false, touched = false;
+      for (uint32_t k = 0; k < it.pcount; ++k) {
+        const vx_primitive pr = x.prims[pairs[it.pstart + k]];
+        const uint32_t cls = pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
+        if (cls == VX_CELL_EMPTY) continue;
+        const bool add = vx_prim_op(&pr) == VX_OP_ADD;
+        if (!loaded && cls == VX_CELL_MIXED) {
+          if (oc & kChild) {
+            const uint32_t li = oc & kIndex;
+            mask = t.leaves[li];
+            if (mats) {
+              const uint4 *src = reinterpret_cast<const uint4 *>(t.mats + static_cast<size_t>(li) * 64u);
+#pragma unroll
+              for (uint32_t q = 0; q < 4; ++q) {
+                const uint4 u = src[q];
+                v[4 * q] = u.x;
+                v[4 * q + 1] = u.y;
+                v[4 * q + 2] = u.z;
+                v[4 * q + 3] = u.w;
+              }
+            }
+          } else {
+            const uint32_t val = word_value(oc, mats);
+            mask = val ? ~0ull : 0ull;
+            if (mats)
+#pragma unroll
+              for (uint32_t w = 0; w < 16; ++w) v[w] = val * 0x01010101u;
+          }
+        }
+        loaded = true;
+        touched = true;
+        const uint64_t m = cls == VX_CELL_FULL ? ~0ull : leaf_mask<Terrain>(pr, world_exp, ox, oy, oz);
+        mask = add ? (mask | m) : (mask & ~m);
+        if (mats) {
+#pragma unroll
+          for (uint32_t w = 0; w < 16; ++w) {
+            const uint32_t nib = static_cast<uint32_t>(m >> (4 * w)) & 0xfu;
+            if (!nib) continue;
+            const uint32_t bm = ((nib & 1u) ? 0xffu : 0u) | ((nib & 2u) ? 0xff00u : 0u) |
+                                ((nib & 4u) ? 0xff0000u : 0u) | ((nib & 8u) ? 0xff000000u : 0u);
+            const uint32_t val =
+                add ? prim_material(pr, world_exp, static_cast<uint32_t>(oz) + (w >> 2)) : 0u;
+            v[w] = (v[w] & ~bm) | ((val * 0x01010101u) & bm);
+          }
+        }
+      }
+      if (!touched) {
+        result = oc;
+      } else {
+        bool uni;
+        uint32_t uval;
+        if (mats) {
+          uni = true;
+#pragma unroll
+          for (uint32_t w = 1; w < 16; ++w) uni = uni && v[w] == v[0];
+          uni = uni && v[0] == (v[0] & 0xffu) * 0x01010101u;
+          uval = v[0] & 0xffu;
+        } else {
+          uni = mask == 0 || mask == ~0ull;
+          uval = mask ? 1u : 0u;
+        }
+        if (uni) {
+          if (oc & kChild) atomicOr(&t.ctr->detached, 1u);
+          result = uniform_word(uval, mats);
+        } else {
+          const uint32_t li = (oc & kChild) ? (oc & kIndex) : alloc_leaf(t);
+          t.leaves[li] = mask;
+          if (mats) {
+            uint4 *dst = reinterpret_cast<uint4 *>(t.mats + static_cast<size_t>(li) * 64u);
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q)
+              dst[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          }
+          result = kChild | li | (oc & kFilled);
+        }
+      }
+    }
+    uint32_t child[8];
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k)
+      child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
+    if (have && c == 0)
+      x.a.items[base + wi].result = finish_node(t, it.old, child, l == 0);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) build_kernel(EditCtx x, Tables t, uint32_t l) {
+  Header *h = x.hdr;
+  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  const uint32_t W = h->item_count[l];
+  const uint32_t base = h->item_off[l];
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < W; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const Item it = x.a.items[base + i];
+    const uint32_t cm = it.masks & 0xffu;
+    uint32_t child[8];
+    if (it.old & kChild) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(t.nodes + static_cast<size_t>(it.old & kIndex) * 8u);
+      const uint4 a = src[0], b = src[1];
+      child[0] = a.x; child[1] = a.y; child[2] = a.z; child[3] = a.w;
+      child[4] = b.x; child[5] = b.y; child[6] = b.z; child[7] = b.w;
+    } else {
+#pragma unroll
+      for (uint32_t c = 0; c < 8; ++c) child[c] = it.old;
+    }
+    uint32_t k = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c)
+      if (cm & (1u << c)) child[c] = x.a.items[it.child_base + k++].result;
+    x.a.items[base + i].result = finish_node(t, it.old, child, l == 0);
+  }
+}
+
+__global__ void finalize_kernel(Tables t) {
+  Counters *c = t.ctr;
+  if (t.hdr->status != kDevOk) return;
+  const uint32_t tn = c->taken_nodes, tl = c->taken_leaves;
+  if (tn <= c->base_free_nodes) {
+    c->free_node_count = c->base_free_nodes - tn;
+  } else {
+    c->free_node_count = 0;
+    c->node_count = c->base_node_count + (tn - c->base_free_nodes);
+  }
+  if (tl <= c->base_free_leaves) {
+    c->free_leaf_count = c->base_free_leaves - tl;
+  } else {
+    c->free_leaf_count = 0;
+    c->leaf_count = c->base_leaf_count + (tl - c->base_free_leaves);
+  }
+}
+
+// ------------------------------------------------------------------- GC --
+
+__global__ void gc_clear_kernel(Tables t) {
+  Counters *c = t.ctr;
+  if (!c->detached) return;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < c->node_count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    t.node_mark[i] = 0;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < c->leaf_count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    t.leaf_mark[i] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (uint32_t l = 0; l <= kMaxDepth; ++l) c->gc_count[l] = 0;
+    c->gc_count[0] = 1;
+    t.front[0][0] = 0; // the root
+  }
+}
+
+__global__ void gc_level_kernel(Tables t, uint32_t l) {
+  Counters *c = t.ctr;
+  if (!c->detached) return;
+  const uint32_t n = c->gc_count[l];
+  const uint32_t *front = t.front[l & 1u];
+  uint32_t *next = t.front[(l + 1) & 1u];
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t node = front[i];
+    t.node_mark[node] = 1;
+    for (uint32_t k = 0; k < 8; ++k) {
+      const uint32_t w = t.nodes[static_cast<size_t>(node) * 8u + k];
+      if (!(w & kChild)) continue;
+      if (l + 1 < t.depth) next[atomicAdd(&c->gc_count[l + 1], 1u)] = w & kIndex;
+      else t.leaf_mark[w & kIndex] = 1;
+    }
+  }
+}
+
+__global__ void gc_zero_free_kernel(Tables t) {
+  Counters *c = t.ctr;
+  if (!c->detached) return;
+  c->free_node_count = 0;
+  c->free_leaf_count = 0;
+}
+
+__global__ void gc_rebuild_kernel(Tables t) {
+  Counters *c = t.ctr;
+  if (!c->detached) return;
+  const uint32_t nn = c->node_count, nl = c->leaf_count;
+  for (uint64_t i = 1 + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nn;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    if (!t.node_mark[i]) t.free_nodes[atomicAdd(&c->free_node_count, 1u)] = static_cast<uint32_t>(i);
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nl;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    if (!t.leaf_mark[i]) t.free_leaves[atomicAdd(&c->free_leaf_count, 1u)] = static_cast<uint32_t>(i);
+}
+
+__global__ void gc_end_kernel(Tables t) { t.ctr->detached = 0; }
+
+__global__ void reset_kernel(Tables t) {
+#pragma unroll
+  for (uint32_t c = 0; c < 8; ++c) t.nodes[c] = 0;
+  Counters *c = t.ctr;
+  c->node_count = 1;
+  c->leaf_count = 0;
+  c->free_node_count = 0;
+  c->free_leaf_count = 0;
+  c->detached = 0;
+  t.hdr->status = kDevOk;
+}
+
+__global__ void query_kernel(Tables t, const vx_voxel *pts, uint32_t n, uint8_t *out) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const vx_voxel p = pts[i];
+  const uint32_t side_exp = t.depth + 2;
+  const bool mats = t.materials != 0;
+  if ((p.x >> side_exp) | (p.y >> side_exp) | (p.z >> side_exp)) {
+    out[i] = 0;
+    return;
+  }
+  uint32_t w = kChild; // root node 0
+  for (uint32_t l = 0; l < t.depth && (w & kChild); ++l) {
+    const uint32_t s = side_exp - 1 - l;
+    const uint32_t c = ((p.x >> s) & 1u) | (((p.y >> s) & 1u) << 1) | (((p.z >> s) & 1u) << 2);
+    w = t.nodes[static_cast<size_t>(w & kIndex) * 8u + c];
+  }
+  if (!(w & kChild)) {
+    out[i] = static_cast<uint8_t>(word_value(w, mats));
+    return;
+  }
+  const uint32_t li = w & kIndex;
+  const uint32_t bit = (p.x & 3u) + 4u * (p.y & 3u) + 16u * (p.z & 3u);
+  if (mats) out[i] = t.mats[static_cast<size_t>(li) * 64u + bit];
+  else out[i] = static_cast<uint8_t>((t.leaves[li] >> bit) & 1ull);
+}
+
+} // namespace vx::svo
+
+// ================================================================ handle ==
+
+struct vx_svo {
+  vx::svo::Tables t{};
+  vx::edit::Arena a{};
+  void *arena_mem = nullptr;
+  vx_primitive *tmp_prim = nullptr;
+};
+
+namespace vx::svo {
+
+vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_count,
+                       uint32_t host_count, cudaStream_t s, bool terrain) {
+  const Tables &t = v->t;
+  const EditCtx e{t.hdr, v->a, prims, d_count, host_count, t.depth};
+  const SvoTree pol{t};
+  const uint32_t depth = t.depth;
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
+  {
+    prof::Scope sc("svo_init", s);
+    begin_kernel<<<1, 1, 0, s>>>(t);
+    init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),
+                  kBlock, 0, s>>>(e, kChild);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  for (uint32_t l = 0; l + 1 < depth; ++l) {
+    {
+      prof::Scope sc("svo_expand", s);
+      if (terrain) expand_kernel<SvoTree, true><<<grid, kBlock, 0, s>>>(e, pol, l);
+      else expand_kernel<SvoTree, false><<<grid, kBlock, 0, s>>>(e, pol, l);
+    }
+    VX_TRY_CUDA(cudaGetLastError());
+    {
+      prof::Scope sc("svo_expand_big", s);
+      if (terrain) expand_big_kernel<SvoTree, true><<<sm_count() * 2, kBlock, 0, s>>>(e, pol, l);
+      else expand_big_kernel<SvoTree, false><<<sm_count() * 2, kBlock, 0, s>>>(e, pol, l);
+    }
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  {
+    prof::Scope sc("svo_check_capacity", s);
+    check_capacity_kernel<<<1, 1, 0, s>>>(t);
+  }
+  {
+    prof::Scope sc("svo_leafparent", s);
+    if (terrain) leafparent_kernel<true><<<grid, kBlock, 0, s>>>(e, t);
+    else leafparent_kernel<false><<<grid, kBlock, 0, s>>>(e, t);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  for (uint32_t r = depth - 1; r > 0; --r) {
+    prof::Scope sc("svo_build", s);
+    build_kernel<<<grid, kBlock, 0, s>>>(e, t, r - 1);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  {
+    prof::Scope sc("svo_finalize", s);
+    finalize_kernel<<<1, 1, 0, s>>>(t);
+  }
+  {
+    prof::Scope sc("svo_gc", s);
+    gc_clear_kernel<<<grid, kBlock, 0, s>>>(t);
+    for (uint32_t l = 0; l < depth; ++l) gc_level_kernel<<<grid, kBlock, 0, s>>>(t, l);
+    gc_zero_free_kernel<<<1, 1, 0, s>>>(t);
+    gc_rebuild_kernel<<<grid, kBlock, 0, s>>>(t);
+    gc_end_kernel<<<1, 1, 0, s>>>(t);
+  }
+  return from_cuda(cudaGetLastError());
+}
+
+vx_status read_status(vx_svo *v, cudaStream_t s) {
+  uint32_t code = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(&code, &v->t.hdr->status, sizeof(code),
+                              cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  if (code != kDevOk) {
+    VX_TRY_CUDA(cudaMemsetAsync(&v->t.hdr->status, 0, sizeof(uint32_t), s));
+    VX_TRY_CUDA(cudaStreamSynchronize(s));
+  }
+  return status_from_device(code);
+}
+
+} // namespace vx::svo
+
+using namespace vx::svo;
+
+extern "C" {
+
+vx_status vx_svo_create(const vx_svo_config *cfg, vx_svo **out) {
+  if (cfg == nullptr || out == nullptr || cfg->depth < 1 || cfg->depth > kMaxDepth ||
+      cfg->max_nodes < 1 || cfg->max_leaves < 1 || cfg->max_nodes > kIndex ||
+      cfg->max_leaves > kIndex)
+    return VX_ERR_INVALID_VALUE;
+  int devs = 0;
+  if (cudaGetDeviceCount(&devs) != cudaSuccess || devs == 0) return VX_ERR_NO_DEVICE;
+  auto *v = new (std::nothrow) vx_svo;
+  if (v == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  Tables &t = v->t;
+  t.depth = cfg->depth;
+  t.materials = cfg->materials ? 1u : 0u;
+  t.max_nodes = cfg->max_nodes;
+  t.max_leaves = cfg->max_leaves;
+  auto fail = [&](cudaError_t e) {
+    vx_svo_destroy(v);
+    return vx::from_cuda(e);
+  };
+  cudaError_t e;
+  const size_t nn = cfg->max_nodes, nl = cfg->max_leaves;
+  if ((e = cudaMalloc(&t.nodes, nn * 32)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.leaves, nl * 8)) != cudaSuccess) return fail(e);
+  if (t.materials && (e = cudaMalloc(&t.mats, nl * 64)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.free_nodes, nn * 4)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.free_leaves, nl * 4)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.node_mark, nn)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.leaf_mark, nl)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.front[0], nn * 4)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.front[1], nn * 4)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.ctr, sizeof(Counters))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&t.hdr, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&v->tmp_prim, sizeof(vx_primitive))) != cudaSuccess) return fail(e);
+  const uint64_t arena = cfg->arena_bytes ? cfg->arena_bytes : (256ull << 20);
+  if ((e = cudaMalloc(&v->arena_mem, arena)) != cudaSuccess) return fail(e);
+  const uint64_t big_bytes = std::min<uint64_t>(arena / 64, 4ull << 20) / 256 * 256;
+  const uint64_t item_bytes = (arena - big_bytes) / 10 * 6 / 256 * 256;
+  const uint64_t pair_bytes = (arena - big_bytes - item_bytes) / 2 / 256 * 256;
+  char *base = static_cast<char *>(v->arena_mem);
+  v->a.items = reinterpret_cast<vx::edit::Item *>(base);
+  v->a.item_cap = static_cast<uint32_t>(std::min<uint64_t>(item_bytes / sizeof(vx::edit::Item), 0xffffffffull));
+  v->a.pairs[0] = reinterpret_cast<uint32_t *>(base + item_bytes);
+  v->a.pairs[1] = reinterpret_cast<uint32_t *>(base + item_bytes + pair_bytes);
+  v->a.pair_cap = static_cast<uint32_t>(std::min<uint64_t>(pair_bytes / 4, 0xffffffffull));
+  v->a.big = reinterpret_cast<uint32_t *>(base + item_bytes + 2 * pair_bytes);
+  v->a.big_cap = static_cast<uint32_t>(big_bytes / 4);
+  if ((e = cudaMemset(t.hdr, 0, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(t.ctr, 0, sizeof(Counters))) != cudaSuccess) return fail(e);
+  const vx_status st = vx_svo_reset(v, nullptr);
+  if (st != VX_OK) {
+    vx_svo_destroy(v);
+    return st;
+  }
+  if ((e = cudaStreamSynchronize(nullptr)) != cudaSuccess) return fail(e);
+  *out = v;
+  return VX_OK;
+}
+
+vx_status vx_svo_destroy(vx_svo *v) {
+  if (v == nullptr) return VX_ERR_INVALID_VALUE;
+  Tables &t = v->t;
+  cudaFree(t.nodes);
+  cudaFree(t.leaves);
+  cudaFree(t.mats);
+  cudaFree(t.free_nodes);
+  cudaFree(t.free_leaves);
+  cudaFree(t.node_mark);
+  cudaFree(t.leaf_mark);
+  cudaFree(t.front[0]);
+  cudaFree(t.front[1]);
+  cudaFree(t.ctr);
+  cudaFree(t.hdr);
+  cudaFree(v->tmp_prim);
+  cudaFree(v->arena_mem);
+  delete v;
+  return VX_OK;
+}
+
+// reset_svo (svt/cuda/svo.cuh:17-22): root = all empty, counters {1,0,0,0}.
+vx_status vx_svo_reset(vx_svo *v, vx_stream stream) {
+  if (v == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope sc("svo_reset", s);
+  reset_kernel<<<1, 1, 0, s>>>(v->t);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+size_t vx_svo_voxel_workspace_size(uint32_t count) {
+  return vx::plain::workspace_size(count);
+}
+
+vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
+                              uint32_t op, uint32_t material, void *workspace,
+                              size_t workspace_bytes, vx_stream stream) {
+  if (v == nullptr || (edits == nullptr && count != 0) || op > 1 || material > 255)
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  if (workspace == nullptr || workspace_bytes < vx_svo_voxel_workspace_size(count))
+    return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const vx_primitive *prims = nullptr;
+  const uint32_t *n = nullptr;
+  const uint32_t mat = op == VX_EDIT_PLACE ? (material ? material : 1u) : 0u;
+  VX_TRY(vx::plain::prepare(edits, count, v->t.depth, op, mat, workspace, &prims, &n, s));
+  VX_TRY(run_pipeline(v, prims, n, count, s, false));
+  return read_status(v, s);
+}
+
+vx_status vx_svo_apply_primitives(vx_svo *v, const vx_primitive *prims,
+                                  uint32_t count, vx_stream stream) {
+  if (v == nullptr || (prims == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  return run_pipeline(v, prims, nullptr, count, static_cast<cudaStream_t>(stream), false);
+}
+
+vx_status vx_svo_status(vx_svo *v, vx_stream stream) {
+  if (v == nullptr) return VX_ERR_INVALID_VALUE;
+  return read_status(v, static_cast<cudaStream_t>(stream));
+}
+
+vx_status vx_svo_build_terrain(vx_svo *v, const vx_terrain *terrain, vx_stream stream) {
+  if (v == nullptr || terrain == nullptr || terrain->scale == 0) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx_primitive p{};
+  p.c[0] = static_cast<int32_t>(terrain->seed);
+  p.c[1] = static_cast<int32_t>(terrain->scale);
+  p.c[2] = static_cast<int32_t>(terrain->caves);
+  p.flags = vx_make_flags(vx::edit::kShapeTerrain, VX_OP_ADD, 0);
+  VX_TRY(vx_svo_reset(v, stream));
+  VX_TRY_CUDA(cudaMemcpyAsync(v->tmp_prim, &p, sizeof(p), cudaMemcpyHostToDevice, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  return run_pipeline(v, v->tmp_prim, nullptr, 1, s, true);
+}
+
+vx_status vx_svo_query(const vx_svo *v, const vx_voxel *pts, uint32_t count,
+                       uint8_t *out, vx_stream stream) {
+  if (v == nullptr || ((pts == nullptr || out == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope sc("svo_query", s);
+  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(v->t, pts, count, out);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_svo_get_counters(const vx_svo *v, vx_svo_counters *host, vx_stream stream) {
+  if (v == nullptr || host == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Counters c;
+  VX_TRY_CUDA(cudaMemcpyAsync(&c, v->t.ctr, sizeof(c), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  // live counts (GpuSvoCounters: allocated high-water and free-stack sizes)
+  host->node_count = c.node_count;
+  host->leaf_count = c.leaf_count;
+  host->free_node_count = c.free_node_count;
+  host->free_leaf_count = c.free_leaf_count;
+  return VX_OK;
+}
+
+vx_status vx_svo_export_canonical(const vx_svo *v, uint32_t *host_node_count,
+                                  uint32_t *host_leaf_count, uint32_t *host_nodes,
+                                  uint32_t nodes_capacity, uint64_t *host_leaves,
+                                  uint8_t *host_materials, uint32_t leaves_capacity,
+                                  vx_stream stream) {
+  if (v == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Tables &t = v->t;
+  Counters c;
+  VX_TRY_CUDA(cudaMemcpyAsync(&c, t.ctr, sizeof(c), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  std::vector<uint32_t> nodes(static_cast<size_t>(c.node_count) * 8);
+  std::vector<uint64_t> leaves(c.leaf_count);
+  std::vector<uint8_t> mats(t.materials ? static_cast<size_t>(c.leaf_count) * 64 : 0);
+  VX_TRY_CUDA(cudaMemcpyAsync(nodes.data(), t.nodes, nodes.size() * 4, cudaMemcpyDeviceToHost, s));
+  if (c.leaf_count) {
+    VX_TRY_CUDA(cudaMemcpyAsync(leaves.data(), t.leaves, leaves.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (t.materials)
+      VX_TRY_CUDA(cudaMemcpyAsync(mats.data(), t.mats, mats.size(), cudaMemcpyDeviceToHost, s));
+  }
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  // DFS pre-order: node ids on first visit, leaves in visit order.
+  std::vector<uint32_t> out_nodes;
+  std::vector<uint64_t> out_leaves;
+  std::vector<uint8_t> out_mats;
+  struct Frame {
+    uint32_t node, depth, c, id;
+    uint32_t rec[8];
+  };
+  std::vector<Frame> st;
+  auto open = [&](uint32_t node, uint32_t depth) {
+    Frame f{};
+    f.node = node;
+    f.depth = depth;
+    f.id = static_cast<uint32_t>(out_nodes.size() / 8);
+    out_nodes.resize(out_nodes.size() + 8, 0);
+    st.push_back(f);
+  };
+  open(0, 0);
+  while (!st.empty()) {
+    Frame &f = st.back();
+    if (f.c == 8) {
+      std::copy(f.rec, f.rec + 8, out_nodes.begin() + static_cast<size_t>(f.id) * 8);
+      const uint32_t id = f.id;
+      st.pop_back();
+      if (!st.empty()) {
+        Frame &p = st.back();
+        p.rec[p.c] = kChild | id; // bit 31 of a present child is a don't-care
+        ++p.c;
+      }
+      continue;
+    }
+    const uint32_t w = nodes[static_cast<size_t>(f.node) * 8 + f.c];
+    if (!(w & kChild)) {
+      f.rec[f.c++] = w;
+    } else if (f.depth + 1 < t.depth) {
+      open(w & kIndex, f.depth + 1); // completes when popped
+    } else {
+      const uint32_t li = w & kIndex;
+      f.rec[f.c++] = kChild | static_cast<uint32_t>(out_leaves.size());
+      out_leaves.push_back(leaves[li]);
+      if (t.materials) out_mats.insert(out_mats.end(), &mats[static_cast<size_t>(li) * 64],
+                                       &mats[static_cast<size_t>(li) * 64] + 64);
+    }
+  }
+  const uint32_t nn = static_cast<uint32_t>(out_nodes.size() / 8);
+  const uint32_t nl = static_cast<uint32_t>(out_leaves.size());
+  if (host_node_count) *host_node_count = nn;
+  if (host_leaf_count) *host_leaf_count = nl;
+  if (host_nodes) {
+    if (nn > nodes_capacity) return VX_ERR_INVALID_VALUE;
+    std::copy(out_nodes.begin(), out_nodes.end(), host_nodes);
+  }
+  if (host_leaves) {
+    if (nl > leaves_capacity) return VX_ERR_INVALID_VALUE;
+    std::copy(out_leaves.begin(), out_leaves.end(), host_leaves);
+  }
+  if (host_materials && t.materials) std::copy(out_mats.begin(), out_mats.end(), host_materials);
+  return VX_OK;
+}
+
+} // extern "C"
