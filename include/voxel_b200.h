@@ -85,6 +85,17 @@ vx_status vx_scan_inclusive_sum_u32(uint32_t *data, uint32_t count,
 vx_status vx_scan_exclusive_sum_u64(uint64_t *data, uint32_t count,
                                     void *workspace, size_t workspace_bytes,
                                     vx_stream stream);
+/* In-place exclusive sum of u32 that allocates nothing and takes no
+ * workspace, for callers that cannot allocate device memory where they need
+ * the scan (a fixed device-memory budget, or code that must not call
+ * cudaMalloc / cudaFree because they synchronise the device).  No counterpart
+ * in the reference: its scans always take a caller workspace.  The scratch is
+ * a 256 KiB array inside this library on each device, so count must be at
+ * most 2^28 (larger counts return VX_ERR_CAPACITY and touch nothing); calls
+ * that can overlap on the GPU share that array and race; the first call on a
+ * device looks up the array's address and should precede any stream capture. */
+vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
+                                            vx_stream stream);
 
 /* ------------------------------------------------------------------ sort --
  * Stable LSD radix sort ("onesweep": one all-pass digit histogram, then one

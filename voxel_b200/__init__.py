@@ -124,6 +124,7 @@ _SIGS = {
     "vx_scan_exclusive_sum_u32": (_ST, [_P, _U32, _P, _SZ, _P]),
     "vx_scan_inclusive_sum_u32": (_ST, [_P, _U32, _P, _SZ, _P]),
     "vx_scan_exclusive_sum_u64": (_ST, [_P, _U32, _P, _SZ, _P]),
+    "vx_scan_exclusive_sum_u32_noalloc": (_ST, [_P, _U32, _P]),
     "vx_sort_workspace_size": (_SZ, [_U32, _U32]),
     "vx_sort_pairs_u32": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_sort_pairs_u64": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),

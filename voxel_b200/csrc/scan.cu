@@ -3,6 +3,8 @@
 #include "profile.cuh"
 #include "scan.cuh"
 
+#include <mutex>
+
 namespace vx {
 
 int sm_count() {
@@ -232,6 +234,85 @@ vx_status vx_scan_exclusive_sum_u64(uint64_t *data, uint32_t count,
   return vx::scan::scan_launch<uint64_t>(data, count, false, workspace,
                                          workspace_bytes,
                                          static_cast<cudaStream_t>(stream));
+}
+
+} // extern "C"
+
+// ------------------------------------------------- allocation-free variant --
+//
+// Some callers cannot allocate device memory at the point where they need a
+// prefix sum: a frame loop or plugin that owns a fixed device-memory budget,
+// or code that must not call cudaMalloc / cudaFree because those calls
+// synchronise the device.  This entry point takes no workspace: its look-back
+// scratch is one array in this library's own device memory, sized for at
+// most kNoAllocMaxCount elements (256 KiB plus a 256-byte header, held on
+// every GPU that loads the library until the process exits).
+
+namespace vx::scan {
+namespace {
+
+constexpr uint32_t kNoAllocMaxCount = 1u << 28;
+constexpr uint32_t kNoAllocTiles =
+    (kNoAllocMaxCount + TileShape<uint32_t>::kTile - 1) / TileShape<uint32_t>::kTile;
+constexpr size_t kNoAllocHeader = 256; // tile counter, status word
+
+// [0, 256): tile counter and status; then one packed look-back record per tile.
+static __device__ __align__(256) unsigned char
+    g_noalloc_scratch[kNoAllocHeader + size_t(kNoAllocTiles) * sizeof(uint64_t)];
+
+// Device address of g_noalloc_scratch per device (the symbol's name is only a
+// host-side stand-in and must never be handed to a kernel).
+void *noalloc_scratch(cudaError_t *err) {
+  static std::mutex mu;
+  static void *addr[64] = {};
+  int dev = 0;
+  *err = cudaGetDevice(&dev);
+  if (*err != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void *p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (*err != cudaSuccess) return nullptr;
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
+} // namespace
+} // namespace vx::scan
+
+extern "C" {
+
+// Allocation-free exclusive sum (see the block comment above): count must be
+// at most 2^28; every call on a device shares one scratch array, so calls that
+// may overlap on the GPU (different streams without ordering) race.  The
+// first call on each device looks the scratch address up and should come
+// before any stream capture.
+vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
+                                            vx_stream stream) {
+  using namespace vx::scan;
+  if (data == nullptr && count != 0) return VX_ERR_INVALID_VALUE;
+  if (count > kNoAllocMaxCount) return VX_ERR_CAPACITY;
+  if (count == 0) return VX_OK;
+  cudaError_t err = cudaSuccess;
+  char *base = static_cast<char *>(noalloc_scratch(&err));
+  if (base == nullptr) return vx::from_cuda(err);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  using S = TileShape<uint32_t>;
+  const uint32_t tiles = vx::ceil_div(count, S::kTile);
+  ScanLayout ws{};
+  ws.tile_counter = reinterpret_cast<uint32_t *>(base);
+  ws.status = ws.tile_counter + 1;
+  ws.rec_a = reinterpret_cast<uint64_t *>(base + kNoAllocHeader);
+  // The previous call's records are still there: clear the part this call uses.
+  VX_TRY_CUDA(cudaMemsetAsync(base, 0, kNoAllocHeader + size_t(tiles) * sizeof(uint64_t), s));
+  PackedRecords32 records{ws.rec_a};
+  vx::prof::Scope scope("scan_u32_noalloc", s);
+  if ((reinterpret_cast<uintptr_t>(data) & 15u) == 0)
+    scan_kernel<uint32_t, false, true><<<tiles, S::kBlock, 0, s>>>(data, count, ws, records);
+  else
+    scan_kernel<uint32_t, false, false><<<tiles, S::kBlock, 0, s>>>(data, count, ws, records);
+  return vx::from_cuda(cudaGetLastError());
 }
 
 } // extern "C"
