@@ -62,6 +62,8 @@ PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
 # DRAM bytes per dag_leafparent launch from ncu (profiles/); None until a
 # capture of this workload is committed.
 LEAFPARENT_TRAFFIC = None
+SVO_C3_DEPTH = 10         # 4096^3
+SVO_C3_EDITS = 65536
 N_HASH = 1 << 26
 HASH_LOAD = 0.8
 BYTES_HASH_INSERT = 40  # read key 8 + one 32-B sector read-modify-write
@@ -536,6 +538,97 @@ def run_plain_sample(torch, vx, device, work, pristine, prims, counts, prims_np,
             "points_checked": int(pts.shape[0])}
 
 
+def run_svo(args, ws, rank, local, torch, vx, device):
+    """C1 (plain per-call SVO edits on 256^3 with materials) and C3 (one
+    batched launch of 65,536 mixed primitives on the 4096^3 cave terrain)."""
+    stream = torch.cuda.current_stream()
+    out = {}
+    # --- C1: 256^3 heightfield, 1,000 spheres, plain path (one call each)
+    depth = 6
+    prims_np = vx.config_c1_edits(1000, seed=1)
+    prims = vx.prims_to_device(prims_np, device)
+    vox, off = vx.rasterize(prims, depth + 2)
+    off_h = off.cpu().numpy()
+    voxels = int(off_h[-1])
+    ws_svo = torch.empty(vx.lib().vx_svo_voxel_workspace_size(int(np.diff(off_h).max())),
+                         dtype=torch.uint8, device=device)
+    ops = [((int(p["flags"]) >> 8) & 0xFF, (int(p["flags"]) >> 16) & 0xFF) for p in prims_np]
+    times = []
+    for rep in range(max(1, args.warmup // 3) + 2):
+        s1 = vx.Svo(depth, 1 << 18, 1 << 18, materials=True, arena_bytes=64 << 20)
+        s1.build_terrain(1, 1, False)
+        assert s1.status() == 0
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for i, (op, mat) in enumerate(ops):
+            st = s1.apply_voxels(vox[off_h[i]:off_h[i + 1]], op, mat, ws_svo)
+            if st != 0:
+                raise RuntimeError(f"C1 plain edit {i} failed: {st}")
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+        del s1
+    out["svo_c1_plain_ms"] = round(min(times[1:] or times), 2)
+    out["svo_c1_plain_voxels_per_s"] = round(voxels / (out["svo_c1_plain_ms"] / 1e3), 1)
+    # the same 1,000 spheres in one batched launch
+    times = []
+    for rep in range(args.warmup + args.steps):
+        s1 = vx.Svo(depth, 1 << 18, 1 << 18, materials=True, arena_bytes=64 << 20)
+        s1.build_terrain(1, 1, False)
+        assert s1.status() == 0
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s1.apply_primitives(prims)
+        b.record(stream)
+        assert s1.status() == 0
+        times.append(a.elapsed_time(b))
+        del s1
+    t_b = sum(times[args.warmup:]) / args.steps
+    out["svo_c1_voxels"] = voxels
+    out["svo_c1_batched_ms"] = round(t_b, 3)
+    out["svo_c1_batched_voxels_per_s"] = round(voxels / (t_b / 1e3), 1)
+    del vox
+    # --- C3: 4096^3 cave terrain (scale 16), 65,536 mixed primitives batched
+    depth = SVO_C3_DEPTH
+    prims = vx.prims_to_device(vx.config_c3_edits(SVO_C3_EDITS, seed=6,
+                                                  world_exp=depth + 2), device)
+    c3_vox = int(count_voxels(torch, vx, prims, depth + 2).sum().item())
+    s3 = vx.Svo(depth, 1 << 25, 1 << 27, materials=True, arena_bytes=8 << 30)
+    times = []
+    build_ms = None
+    for rep in range(args.warmup + args.steps):
+        a0 = torch.cuda.Event(enable_timing=True)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        s3.build_terrain(6, 16, True)      # restore the terrain (untimed)
+        a.record(stream)
+        s3.apply_primitives(prims)
+        b.record(stream)
+        st = s3.status()
+        if st != 0:
+            c = s3.counters()
+            raise RuntimeError(f"C3 batched edit failed: {st} (nodes {c.node_count}, "
+                               f"leaves {c.leaf_count})")
+        build_ms = a0.elapsed_time(a)
+        times.append(a.elapsed_time(b))
+    t3 = sum(times[args.warmup:]) / args.steps
+    c = s3.counters()
+    out["svo_c3_terrain_build_ms"] = round(build_ms, 2)
+    out["svo_c3_voxels"] = c3_vox
+    out["svo_c3_batched_ms"] = round(t3, 3)
+    out["svo_c3_batched_voxels_per_s"] = round(c3_vox / (t3 / 1e3), 1)
+    out["svo_c3_nodes_leaves_live"] = [c.node_count - c.free_node_count,
+                                       c.leaf_count - c.free_leaf_count]
+    del s3
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
     import voxel_b200 as vx
@@ -547,6 +640,7 @@ def run_ours(args, ws, rank, local):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dag = run_dag(args, ws, rank, local, torch, vx, device)
+    svo = run_svo(args, ws, rank, local, torch, vx, device)
     sweep = run_sweep(args, ws, rank, local, torch, vx, device)
     hbm, kind = peaks()
     k = dag["kernels"]
@@ -602,6 +696,7 @@ def run_ours(args, ws, rank, local):
             "dag_kernel_ms": {n: round(v[1], 3) for n, v in k.items()},
             "dag_kernel_share": {n: round(v[1] / total_k, 3) for n, v in k.items()} if total_k else {},
             "dag_bytes_reserved": dag["dag_bytes_reserved"],
+            **svo,
             **sweep,
         },
         "roofline": {

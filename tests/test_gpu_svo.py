@@ -126,3 +126,34 @@ def test_capacity_overflow_changes_nothing(cuda):
     many = np.random.default_rng(2).integers(0, 4 << depth, (3000, 3)).astype(np.uint32)
     assert s.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE) == vx.VX_ERR_CAPACITY
     assert canon(s) == before
+
+
+def test_config_c1_full_size_plain_and_batched_bit_exact(cuda):
+    """Configuration C1 at full size: 256^3 heightfield (materials by height
+    band), 1,000 spheres r in [2, 16] applied in order through the plain
+    per-call path (one voxel list and op per sphere) and through one batched
+    call; both canonical dumps (nodes, leaves, materials) equal the oracle's
+    sequential application."""
+    depth = 6
+    prims = vx.config_c1_edits(1000, seed=1)
+    t = oracle.terrain(seed=1, scale=1, caves=False)
+    g = oracle.Grid(depth, materials=True).terrain(t).apply_prims(prims)
+    expect = g.svo()
+
+    plain = vx.Svo(depth, 1 << 18, 1 << 18, materials=True, arena_bytes=64 << 20)
+    plain.build_terrain(1, 1, False)
+    assert plain.status() == 0
+    dev_prims = vx.prims_to_device(prims, cuda)
+    vox, off = vx.rasterize(dev_prims, depth + 2)
+    off = off.cpu().numpy()
+    for i, p in enumerate(prims):
+        op = (int(p["flags"]) >> 8) & 0xFF
+        mat = (int(p["flags"]) >> 16) & 0xFF
+        assert plain.apply_voxels(vox[off[i]:off[i + 1]].contiguous(), op, mat) == 0
+    assert canon(plain) == expect
+
+    batched = vx.Svo(depth, 1 << 18, 1 << 18, materials=True, arena_bytes=64 << 20)
+    batched.build_terrain(1, 1, False)
+    batched.apply_primitives(dev_prims)
+    assert batched.status() == 0
+    assert canon(batched) == expect
