@@ -43,6 +43,65 @@ __host__ __device__ __forceinline__ uint64_t child_cell(uint64_t p, uint32_t c) 
                    2 * k.z + ((c >> 2) & 1u));
 }
 
+// Exact sphere tests in 32-bit arithmetic for radii below 2^14: a distance
+// that decides anything is at most r (+3 inside a leaf), so every square and
+// every sum of three squares stays below 2^31.  Larger radii take the 64-bit
+// definitions of vx_workload.h; both give identical results.
+constexpr int64_t kFastRadius = int64_t(1) << 14;
+
+__device__ __forceinline__ uint32_t sphere_classify32(const vx_primitive &p, int64_t ox,
+                                                      int64_t oy, int64_t oz, int64_t n) {
+  const int64_t r = p.r[0];
+  const int64_t lo[3] = {ox, oy, oz};
+  uint32_t near2 = 0, far2 = 0;
+  bool far_in = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int64_t c = p.c[a], a0 = lo[a], a1 = lo[a] + n - 1;
+    const int64_t d = c < a0 ? a0 - c : (c > a1 ? c - a1 : 0);
+    if (d > r) return VX_CELL_EMPTY;
+    near2 += static_cast<uint32_t>(d) * static_cast<uint32_t>(d);
+    const int64_t f0 = c - a0 > 0 ? c - a0 : a0 - c;
+    const int64_t f1 = c - a1 > 0 ? c - a1 : a1 - c;
+    const int64_t f = f0 > f1 ? f0 : f1;
+    if (f > r) far_in = false;
+    else far2 += static_cast<uint32_t>(f) * static_cast<uint32_t>(f);
+  }
+  const uint32_t r2 = static_cast<uint32_t>(r) * static_cast<uint32_t>(r);
+  if (near2 > r2) return VX_CELL_EMPTY;
+  return (far_in && far2 <= r2) ? VX_CELL_FULL : VX_CELL_MIXED;
+}
+
+// Sphere mask of the leaf at o; the caller has classified the leaf MIXED, so
+// every coordinate difference is within r + 3 of the centre.
+__device__ __forceinline__ uint64_t sphere_leaf_mask32(const vx_primitive &p, int64_t ox,
+                                                       int64_t oy, int64_t oz) {
+  const int32_t r = static_cast<int32_t>(p.r[0]);
+  const int32_t r2 = r * r;
+  const int32_t dx0 = static_cast<int32_t>(ox - p.c[0]);
+  const int32_t dy0 = static_cast<int32_t>(oy - p.c[1]);
+  const int32_t dz0 = static_cast<int32_t>(oz - p.c[2]);
+  int32_t dx2[4], dy2[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    dx2[i] = (dx0 + i) * (dx0 + i);
+    dy2[i] = (dy0 + i) * (dy0 + i);
+  }
+  uint64_t m = 0;
+#pragma unroll
+  for (int z = 0; z < 4; ++z) {
+    const int32_t rz = r2 - (dz0 + z) * (dz0 + z);
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      const int32_t ry = rz - dy2[y];
+      const uint32_t bits = (dx2[0] <= ry ? 1u : 0u) | (dx2[1] <= ry ? 2u : 0u) |
+                            (dx2[2] <= ry ? 4u : 0u) | (dx2[3] <= ry ? 8u : 0u);
+      m |= static_cast<uint64_t>(ry >= 0 ? bits : 0u) << (4 * y + 16 * z);
+    }
+  }
+  return m;
+}
+
 // Classify primitive p against the voxel cube [o, o + n)^3.  Kernels that
 // only ever see sphere / box / leaf-mask primitives instantiate Terrain =
 // false and carry none of the terrain generator's code.
@@ -65,6 +124,8 @@ __device__ __forceinline__ uint32_t classify(const vx_primitive &p,
       return VX_CELL_EMPTY;
     return VX_CELL_MIXED;
   }
+  if (shape == VX_SHAPE_SPHERE && p.r[0] < kFastRadius)
+    return sphere_classify32(p, ox, oy, oz, n);
   return vx_prim_classify(&p, ox, oy, oz, n);
 }
 
@@ -84,6 +145,8 @@ __device__ __forceinline__ uint64_t leaf_mask(const vx_primitive &p,
     if (p.c[0] != ox || p.c[1] != oy || p.c[2] != oz) return 0;
     return static_cast<uint64_t>(p.r[0]) | (static_cast<uint64_t>(p.r[1]) << 32);
   }
+  if (shape == VX_SHAPE_SPHERE && p.r[0] < kFastRadius)
+    return sphere_leaf_mask32(p, ox, oy, oz);
   return vx_prim_leaf_mask(&p, ox, oy, oz);
 }
 
