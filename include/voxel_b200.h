@@ -271,6 +271,24 @@ vx_status vx_dag_export_canonical(const vx_dag *dag, uint32_t *host_root,
  * reference (its GPU DAG is not copyable, hash_dag_gpu/storage.cuh:40-43). */
 vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream);
 
+/* Compaction: keep only the nodes reachable from the root (edits are
+ * copy-on-write, so superseded items accumulate), re-hash-consing them into
+ * cleared tables; the canonical content is unchanged.  The GPU counterpart of
+ * the reference CPU DAG's collect_garbage (svt/hash_dag.hpp:133-191); the
+ * reference GPU DAG has none (append-only, hash_dag_gpu/storage.cuh:14-15).
+ * Synchronises; uses temporary device buffers. */
+vx_status vx_dag_compact(vx_dag *dag, vx_stream stream);
+
+/* The same dump for an earlier root ref (e.g. one a served batch published):
+ * valid while the tables still hold it, i.e. until the next reset or
+ * compaction.  root = 0xffffffff means the current root. */
+vx_status vx_dag_export_canonical_at(const vx_dag *dag, uint32_t root,
+                                     uint32_t *host_root, uint64_t *host_counts,
+                                     uint32_t *host_nodes,
+                                     uint64_t nodes_capacity_words,
+                                     uint64_t *host_leaves,
+                                     uint64_t leaves_capacity, vx_stream stream);
+
 typedef struct vx_dag_stats {
     uint64_t nodes_per_level[16]; /* items stored (live and superseded) */
     uint64_t words_per_level[16];
@@ -348,6 +366,67 @@ typedef struct vx_svo_counters {
 } vx_svo_counters;
 vx_status vx_svo_get_counters(const vx_svo *svo, vx_svo_counters *host_counters,
                               vx_stream stream);
+
+/* -------------------------------------------------------------- serving --
+ * A request loop over a resident Hash DAG with continuous batching: submitted
+ * requests (lists of primitives) are applied in submission order; queued
+ * requests are coalesced into one batched edit per launch, up to two launches
+ * are in flight, and the DAG is compacted when a table passes
+ * compact_at_fill (admission by memory headroom).  Completions report the
+ * commit time (host clock of vx_serve_now_ns, when the batch's completion was
+ * observed) and the root the batch published.  The server owns the DAG's
+ * stream while it runs.  No counterpart in the reference (no serving path). */
+typedef struct vx_server vx_server;
+
+typedef struct vx_serve_config {
+    uint32_t max_batch_prims;    /* primitives per launch (0 = 65536) */
+    uint32_t max_batch_requests; /* requests per launch (0 = unlimited, 1 = one each) */
+    double compact_at_fill;      /* compact above this table fill (0 = 0.5) */
+    uint32_t max_inflight;       /* launches in flight, 1 or 2 (0 = 2) */
+    uint32_t reserved;
+} vx_serve_config;
+
+typedef struct vx_serve_completion {
+    uint64_t request_id;
+    uint64_t arrival_ns;
+    uint64_t commit_ns;
+    uint32_t status;             /* 0 = committed */
+    uint32_t root;               /* root ref published by the request's batch */
+} vx_serve_completion;
+
+typedef struct vx_serve_stats {
+    uint64_t batches;
+    uint64_t requests;
+    uint64_t prims;
+    uint64_t compactions;
+    uint64_t recoveries;
+    double compact_ms;
+} vx_serve_stats;
+
+uint64_t vx_serve_now_ns(void);
+vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *config, vx_server **out);
+/* Copies the host primitives; thread-safe. */
+vx_status vx_serve_submit(vx_server *server, uint64_t request_id,
+                          const vx_primitive *host_prims, uint32_t count,
+                          uint64_t arrival_ns);
+/* Moves up to `capacity` completions into host_out. */
+vx_status vx_serve_poll(vx_server *server, vx_serve_completion *host_out,
+                        uint32_t capacity, uint32_t *host_count);
+/* Blocks until every submitted request has completed. */
+vx_status vx_serve_drain(vx_server *server);
+vx_status vx_serve_get_stats(vx_server *server, vx_serve_stats *host_stats);
+/* Drains, stops the threads and frees the server (not the DAG). */
+vx_status vx_serve_destroy(vx_server *server);
+
+/* Seeded served-request stream (vx_workload.h): Poisson arrivals at `rate`
+ * per second for `seconds`, Zipf(zipf_s) sizes over [1, max_size], primitives
+ * from `mix`.  NULL arrays return only the counts. */
+vx_status vx_generate_requests(const vx_edit_mix *mix, uint64_t seed, double rate,
+                               double seconds, double zipf_s, uint32_t max_size,
+                               uint64_t max_requests, uint64_t *host_arrival_ns,
+                               uint32_t *host_sizes, uint64_t max_prims,
+                               vx_primitive *host_prims, uint64_t *host_requests,
+                               uint64_t *host_total_prims);
 
 /* ---------------------------------------------------------- rasterising --
  * Expand primitives into voxel lists (the plain path's input shape).

@@ -421,6 +421,7 @@ typedef struct vx_edit_mix {
 } vx_edit_mix;
 
 #include <math.h>
+#include <stdlib.h>
 
 static inline double vx_pcg32_unit(vx_pcg32 *rng) {
     return (double)vx_pcg32_next(rng) * (1.0 / 4294967296.0);
@@ -463,6 +464,52 @@ static inline void vx_generate_primitives_host(const vx_edit_mix *m, uint64_t se
         p.reserved = 0u;
         out[i] = p;
     }
+}
+
+/* ------------------------------------------------------- request stream --
+ * Host-only: a served edit stream.  Arrivals are a Poisson process of `rate`
+ * requests per second (exponential gaps, u = (next + 0.5) / 2^32), request
+ * sizes follow Zipf(s) over [1, max_size] (inverse CDF over the exact
+ * normalised weights k^-s), and each request's primitives come from `mix`
+ * (same per-primitive draw order as vx_generate_primitives_host).  One PCG32
+ * stream serves arrivals and sizes; primitives use a second stream. */
+static inline uint64_t vx_generate_requests_host(
+    const vx_edit_mix *mix, uint64_t seed, double rate, double seconds,
+    double zipf_s, uint32_t max_size, uint64_t max_requests,
+    uint64_t *arrival_ns, uint32_t *sizes, uint64_t max_prims, vx_primitive *prims,
+    uint64_t *total_prims) {
+    vx_pcg32 rng;
+    vx_pcg32_seed(&rng, seed, 11u);
+    double *cdf = (double *)malloc(sizeof(double) * (max_size ? max_size : 1u));
+    if (cdf == NULL) return 0;
+    double norm = 0.0;
+    for (uint32_t k = 1; k <= max_size; ++k) {
+        norm += pow((double)k, -zipf_s);
+        cdf[k - 1] = norm;
+    }
+    double t = 0.0;
+    uint64_t n = 0, np = 0;
+    while (n < max_requests) {
+        const double u = ((double)vx_pcg32_next(&rng) + 0.5) * (1.0 / 4294967296.0);
+        t += -log(u) / rate;
+        if (t >= seconds) break;
+        const double v = ((double)vx_pcg32_next(&rng) + 0.5) * (1.0 / 4294967296.0) * norm;
+        uint32_t lo = 0, hi = max_size - 1u; /* first k with cdf[k - 1] >= v */
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) / 2u;
+            if (cdf[mid] >= v) hi = mid;
+            else lo = mid + 1u;
+        }
+        const uint32_t k = lo + 1u;
+        if (arrival_ns) arrival_ns[n] = (uint64_t)(t * 1e9);
+        if (sizes) sizes[n] = k;
+        np += k;
+        ++n;
+    }
+    free(cdf);
+    if (total_prims) *total_prims = np;
+    if (prims && np <= max_prims) vx_generate_primitives_host(mix, seed, 12u, np, prims);
+    return n;
 }
 
 #ifdef __cplusplus

@@ -214,3 +214,31 @@ def test_copy_restores_snapshot(cuda):
     assert canon(b) == oracle.Grid(depth).terrain(t).apply_prims(prims).dag()
     b.copy_from(a)
     assert canon(b) == canon(a)
+
+
+def test_compaction_keeps_content_and_frees_garbage(cuda):
+    depth = 7
+    rng = np.random.default_rng(31)
+    t = oracle.terrain(seed=4, scale=2, caves=True)
+    dag = vx.HashDag(depth, max_nodes=1 << 20, arena_bytes=64 << 20)
+    dag.build_terrain(4, 2, True)
+    g = oracle.Grid(depth).terrain(t)
+    for _ in range(5):  # several batches: plenty of superseded items
+        prims = rand_prims(rng, 120, 4 << depth, 30)
+        dag.apply_primitives(vx.prims_to_device(prims, cuda))
+        g.apply_prims(prims)
+    assert dag.status() == 0
+    before = dag.stats()
+    dag.compact()
+    after = dag.stats()
+    c = canon(dag)
+    assert c == g.dag()
+    # after compaction the tables hold exactly the live (canonical) nodes
+    assert [int(after.nodes_per_level[l]) for l in range(depth + 1)] == c.counts
+    assert sum(after.nodes_per_level) < sum(before.nodes_per_level)
+    # editing continues normally on the compacted tables
+    prims = rand_prims(rng, 60, 4 << depth, 30)
+    dag.apply_primitives(vx.prims_to_device(prims, cuda))
+    g.apply_prims(prims)
+    assert dag.status() == 0
+    assert canon(dag) == g.dag()

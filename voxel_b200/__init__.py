@@ -89,6 +89,18 @@ class vx_dag_stats(C.Structure):
                 ("status", C.c_uint32)]
 
 
+class vx_serve_config(C.Structure):
+    _fields_ = [("max_batch_prims", C.c_uint32), ("max_batch_requests", C.c_uint32),
+                ("compact_at_fill", C.c_double), ("max_inflight", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class vx_serve_stats(C.Structure):
+    _fields_ = [("batches", C.c_uint64), ("requests", C.c_uint64),
+                ("prims", C.c_uint64), ("compactions", C.c_uint64),
+                ("recoveries", C.c_uint64), ("compact_ms", C.c_double)]
+
+
 class vx_svo_config(C.Structure):
     _fields_ = [("depth", C.c_uint32), ("materials", C.c_uint32),
                 ("max_nodes", C.c_uint32), ("max_leaves", C.c_uint32),
@@ -155,7 +167,20 @@ _SIGS = {
     "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), _P,
                                       _P, _U64, _P, _U64, _P]),
     "vx_dag_get_stats": (_ST, [_P, C.POINTER(vx_dag_stats), _P]),
+    "vx_dag_export_canonical_at": (_ST, [_P, _U32, C.POINTER(_U32), _P, _P, _U64,
+                                         _P, _U64, _P]),
+    "vx_serve_now_ns": (_U64, []),
+    "vx_serve_create": (_ST, [_P, C.POINTER(vx_serve_config), C.POINTER(_P)]),
+    "vx_serve_submit": (_ST, [_P, _U64, _P, _U32, _U64]),
+    "vx_serve_poll": (_ST, [_P, _P, _U32, C.POINTER(_U32)]),
+    "vx_serve_drain": (_ST, [_P]),
+    "vx_serve_get_stats": (_ST, [_P, C.POINTER(vx_serve_stats)]),
+    "vx_serve_destroy": (_ST, [_P]),
+    "vx_generate_requests": (_ST, [C.POINTER(vx_edit_mix), _U64, C.c_double, C.c_double,
+                                   C.c_double, _U32, _U64, _P, _P, _U64, _P,
+                                   C.POINTER(_U64), C.POINTER(_U64)]),
     "vx_dag_copy": (_ST, [_P, _P, _P]),
+    "vx_dag_compact": (_ST, [_P, _P]),
     "vx_svo_create": (_ST, [C.POINTER(vx_svo_config), C.POINTER(_P)]),
     "vx_svo_destroy": (_ST, [_P]),
     "vx_svo_reset": (_ST, [_P, _P]),

@@ -18,7 +18,8 @@ __all__ = [
     "workspace_status", "SlabHashSet", "CuckooMap", "PRIM_DTYPE",
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
-    "config_c4_edits", "rasterize", "Svo",
+    "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
+    "COMPLETION_DTYPE",
 ]
 
 
@@ -274,6 +275,10 @@ class HashDag:
               "vx_dag_query")
         return out
 
+    def compact(self) -> None:
+        """Drop superseded nodes (copy-on-write garbage); content unchanged."""
+        check(lib().vx_dag_compact(self._h, stream_handle()), "vx_dag_compact")
+
     def copy_from(self, other: "HashDag") -> None:
         """Device-side snapshot restore: take other's complete table state."""
         check(lib().vx_dag_copy(self._h, other._h, stream_handle()), "vx_dag_copy")
@@ -285,18 +290,19 @@ class HashDag:
               "vx_dag_get_stats")
         return st
 
-    def canonical(self):
-        """(root, counts, nodes, leaves): DFS first-visit canonical dump."""
+    def canonical(self, at_root: int = 0xFFFFFFFF):
+        """(root, counts, nodes, leaves): DFS first-visit canonical dump of the
+        current root, or of an earlier root ref still held by the tables."""
         root = C.c_uint32(0)
         counts = np.zeros(self.depth + 1, np.uint64)
-        f = lib().vx_dag_export_canonical
-        check(f(self._h, C.byref(root), counts.ctypes.data, None, 0, None, 0,
+        f = lib().vx_dag_export_canonical_at
+        check(f(self._h, at_root, C.byref(root), counts.ctypes.data, None, 0, None, 0,
                 stream_handle()), "export sizes")
         words = int(counts[:self.depth].sum()) * 10
         nodes = np.zeros(max(words, 1), np.uint32)
         nl = int(counts[self.depth])
         leaves = np.zeros(max(nl, 1), np.uint64)
-        check(f(self._h, C.byref(root), counts.ctypes.data, nodes.ctypes.data,
+        check(f(self._h, at_root, C.byref(root), counts.ctypes.data, nodes.ctypes.data,
                 words, leaves.ctypes.data, nl, stream_handle()), "export")
         return root.value, counts, nodes[:words], leaves[:nl]
 
@@ -437,3 +443,80 @@ class Svo:
                 nl.value, stream_handle()), "export")
         return (nodes[:nn.value * 8], leaves[:nl.value],
                 None if mats is None else mats[:nl.value * 64])
+
+
+COMPLETION_DTYPE = np.dtype([("request_id", "<u8"), ("arrival_ns", "<u8"),
+                             ("commit_ns", "<u8"), ("status", "<u4"), ("root", "<u4")])
+
+
+def generate_requests(world_exp: int, rate: float, seconds: float, seed: int, *,
+                      zipf_s: float = 1.2, max_size: int = 4096,
+                      sphere_permille: int = 500, add_permille: int = 500,
+                      r_min: int = 1, r_max: int = 128, log_uniform: bool = True,
+                      max_requests: int = 1 << 40):
+    """Served request stream: (arrival_ns [n], sizes [n], prims [total])."""
+    from . import vx_edit_mix
+    mix = vx_edit_mix(world_exp, sphere_permille, add_permille, r_min, r_max,
+                      int(log_uniform), 1, 255)
+    nreq, nprim = C.c_uint64(0), C.c_uint64(0)
+    f = lib().vx_generate_requests
+    check(f(C.byref(mix), seed, rate, seconds, zipf_s, max_size, max_requests,
+            None, None, 0, None, C.byref(nreq), C.byref(nprim)), "count requests")
+    arr = np.zeros(max(nreq.value, 1), np.uint64)
+    sizes = np.zeros(max(nreq.value, 1), np.uint32)
+    prims = np.zeros(max(nprim.value, 1), PRIM_DTYPE)
+    check(f(C.byref(mix), seed, rate, seconds, zipf_s, max_size, max_requests,
+            arr.ctypes.data, sizes.ctypes.data, prims.size, prims.ctypes.data,
+            C.byref(nreq), C.byref(nprim)), "generate requests")
+    return arr[:nreq.value], sizes[:nreq.value], prims[:nprim.value]
+
+
+class Server:
+    """Request loop over a resident HashDag with continuous batching."""
+
+    def __init__(self, dag: HashDag, max_batch_prims: int = 0, max_batch_requests: int = 0,
+                 compact_at_fill: float = 0.0, max_inflight: int = 0):
+        from . import vx_serve_config
+        cfg = vx_serve_config(max_batch_prims, max_batch_requests, compact_at_fill,
+                              max_inflight, 0)
+        h = C.c_void_p()
+        check(lib().vx_serve_create(dag._h, C.byref(cfg), C.byref(h)), "vx_serve_create")
+        self._h = h
+        self.dag = dag
+
+    @staticmethod
+    def now_ns() -> int:
+        return lib().vx_serve_now_ns()
+
+    def submit(self, request_id: int, prims: np.ndarray, arrival_ns: int) -> None:
+        p = np.ascontiguousarray(prims, PRIM_DTYPE)
+        check(lib().vx_serve_submit(self._h, request_id, p.ctypes.data if p.size else None,
+                                    p.size, arrival_ns), "vx_serve_submit")
+
+    def poll(self, capacity: int = 1 << 16) -> np.ndarray:
+        out = np.zeros(capacity, COMPLETION_DTYPE)
+        n = C.c_uint32(0)
+        check(lib().vx_serve_poll(self._h, out.ctypes.data, capacity, C.byref(n)),
+              "vx_serve_poll")
+        return out[:n.value]
+
+    def drain(self) -> None:
+        check(lib().vx_serve_drain(self._h), "vx_serve_drain")
+
+    def stats(self):
+        from . import vx_serve_stats
+        st = vx_serve_stats()
+        check(lib().vx_serve_get_stats(self._h, C.byref(st)), "vx_serve_get_stats")
+        return st
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            check(lib().vx_serve_destroy(h), "vx_serve_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -725,12 +725,23 @@ vx_status vx_dag_export_canonical(const vx_dag *d, uint32_t *host_root,
                                   uint64_t nodes_capacity_words,
                                   uint64_t *host_leaves,
                                   uint64_t leaves_capacity, vx_stream stream) {
+  return vx_dag_export_canonical_at(d, 0xffffffffu, host_root, host_counts, host_nodes,
+                                    nodes_capacity_words, host_leaves, leaves_capacity,
+                                    stream);
+}
+
+vx_status vx_dag_export_canonical_at(const vx_dag *d, uint32_t root, uint32_t *host_root,
+                                     uint64_t *host_counts, uint32_t *host_nodes,
+                                     uint64_t nodes_capacity_words,
+                                     uint64_t *host_leaves, uint64_t leaves_capacity,
+                                     vx_stream stream) {
   if (d == nullptr) return VX_ERR_INVALID_VALUE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint32_t D = d->t.depth;
   vx::edit::Header h;
   VX_TRY_CUDA(cudaMemcpyAsync(&h, d->t.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
   VX_TRY_CUDA(cudaStreamSynchronize(s));
+  if (root != 0xffffffffu) h.root = root;
   std::vector<std::vector<uint32_t>> pools(D);
   for (uint32_t l = 0; l < D; ++l) {
     const uint64_t used = std::min<uint64_t>(h.pool_used[l], d->t.pool_cap[l]);
@@ -873,3 +884,225 @@ vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream) {
 }
 
 } // extern "C"
+
+// ============================================================ compaction ==
+//
+// Edits are copy-on-write: every changed node gets a new item and the items
+// it replaced stay in the tables until compaction (the reference CPU DAG's
+// collect_garbage, svt/hash_dag.hpp:133-191).  Compaction marks the nodes
+// reachable from the root level by level, stages their items, clears every
+// table and hash-conses the live items back bottom-up, remapping child refs
+// through sorted (old ref -> new ref) arrays of the level below.  It is a
+// maintenance call: it synchronises and uses temporary device buffers.
+
+namespace vx::dag {
+
+__global__ void mark_level_kernel(Tables t, uint32_t l, const uint32_t *front,
+                                  uint32_t n, uint32_t *next, uint32_t *next_count,
+                                  uint32_t next_cap, uint32_t *bitmap) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t *item = t.pool[l] + (front[i] - 2);
+    const uint32_t cm = item[0] & 0xffu;
+    for (uint32_t k = 0; k < static_cast<uint32_t>(__popc(cm)); ++k) {
+      const uint32_t r = item[1 + k];
+      const uint32_t bit = r - 2;
+      const uint32_t old = atomicOr(&bitmap[bit >> 5], 1u << (bit & 31u));
+      if (old & (1u << (bit & 31u))) continue;
+      const uint32_t at = atomicAdd(next_count, 1u);
+      if (at < next_cap) next[at] = r;
+      else set_status(&t.hdr->status, kDevCapacity);
+    }
+  }
+}
+
+__global__ void stage_kernel(Tables t, uint32_t l, const uint32_t *refs, uint32_t n,
+                             uint32_t *staged /* 9 words per item */, uint64_t *leaf_masks) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    if (l == t.depth) {
+      leaf_masks[i] = t.leaves[refs[i] - 2];
+      continue;
+    }
+    const uint32_t *item = t.pool[l] + (refs[i] - 2);
+    const uint32_t w = 1 + __popc(item[0] & 0xffu);
+    for (uint32_t k = 0; k < 9; ++k) staged[i * 9 + k] = k < w ? item[k] : 0u;
+  }
+}
+
+__global__ void reinsert_leaves_kernel(Tables t, const uint64_t *masks, uint32_t n,
+                                       uint32_t *new_refs) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    new_refs[i] = leaf_find_or_insert(t, masks[i]);
+}
+
+__device__ __forceinline__ uint32_t remap(const uint32_t *old_sorted, const uint32_t *new_sorted,
+                                          uint32_t n, uint32_t ref, uint32_t *status) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (old_sorted[mid] < ref) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo < n && old_sorted[lo] == ref) return new_sorted[lo];
+  set_status(status, kDevInvalid); // a live child that was not marked
+  return kEmptyRef;
+}
+
+__global__ void reinsert_nodes_kernel(Tables t, uint32_t l, const uint32_t *staged,
+                                      uint32_t n, const uint32_t *child_old,
+                                      const uint32_t *child_new, uint32_t child_n,
+                                      uint32_t *new_refs) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    uint32_t w[9];
+    w[0] = staged[i * 9];
+    const uint32_t k = __popc(w[0] & 0xffu);
+    for (uint32_t j = 0; j < k; ++j)
+      w[1 + j] = remap(child_old, child_new, child_n, staged[i * 9 + 1 + j], &t.hdr->status);
+    new_refs[i] = node_find_or_insert(t, l, w, 1 + k);
+  }
+}
+
+__global__ void set_root_kernel(Tables t, uint32_t root) { t.hdr->root = root; }
+
+} // namespace vx::dag
+
+extern "C" {
+
+vx_status vx_dag_compact(vx_dag *d, vx_stream stream) {
+  if (d == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t D = d->t.depth;
+  vx::edit::Header h;
+  VX_TRY_CUDA(cudaMemcpyAsync(&h, d->t.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  if (h.status != vx::kDevOk) return vx::status_from_device(h.status);
+  if (h.root < 2) { // empty or full world: nothing is live
+    VX_TRY(vx_dag_reset(d, stream));
+    vx::prof::Scope sc("dag_set_root", s);
+    set_root_kernel<<<1, 1, 0, s>>>(d->t, h.root);
+    return vx::from_cuda(cudaGetLastError());
+  }
+  const uint32_t grid = static_cast<uint32_t>(vx::sm_count()) * 8u;
+  std::vector<void *> owned;
+  auto alloc = [&](size_t bytes) -> void * {
+    void *p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 256)) != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    return p;
+  };
+  auto cleanup = [&]() {
+    for (void *p : owned) cudaFree(p);
+  };
+  // Upper bounds of live items per level: the items each table holds.
+  std::vector<uint32_t *> refs(D + 1), newr(D + 1), sorted_old(D + 1), sorted_new(D + 1);
+  std::vector<uint32_t> live(D + 1, 0);
+  uint32_t *counter = static_cast<uint32_t *>(alloc(4 * (D + 1)));
+  if (!counter) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+  VX_TRY_CUDA(cudaMemsetAsync(counter, 0, 4 * (D + 1), s));
+  for (uint32_t l = 0; l <= D; ++l) {
+    const uint64_t cap = std::max<uint64_t>(h.node_count[l], 1);
+    refs[l] = static_cast<uint32_t *>(alloc(cap * 4));
+    newr[l] = static_cast<uint32_t *>(alloc(cap * 4));
+    sorted_old[l] = static_cast<uint32_t *>(alloc(cap * 4));
+    sorted_new[l] = static_cast<uint32_t *>(alloc(cap * 4));
+    if (!refs[l] || !newr[l] || !sorted_old[l] || !sorted_new[l]) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+  }
+  // Mark, level by level.
+  VX_TRY_CUDA(cudaMemcpyAsync(refs[0], &h.root, 4, cudaMemcpyHostToDevice, s));
+  live[0] = 1;
+  for (uint32_t l = 0; l < D; ++l) {
+    const uint64_t bits = l + 1 < D ? std::max<uint64_t>(h.pool_used[l + 1], 1) : d->leaf_slots;
+    uint32_t *bitmap = static_cast<uint32_t *>(alloc((bits + 31) / 32 * 4));
+    if (!bitmap) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+    VX_TRY_CUDA(cudaMemsetAsync(bitmap, 0, (bits + 31) / 32 * 4, s));
+    {
+      vx::prof::Scope sc("dag_compact_mark", s);
+      mark_level_kernel<<<grid, kBlock, 0, s>>>(d->t, l, refs[l], live[l], refs[l + 1],
+                                                counter + l + 1,
+                                                static_cast<uint32_t>(std::max<uint64_t>(h.node_count[l + 1], 1)),
+                                                bitmap);
+    }
+    VX_TRY_CUDA(cudaGetLastError());
+    VX_TRY_CUDA(cudaMemcpyAsync(&live[l + 1], counter + l + 1, 4, cudaMemcpyDeviceToHost, s));
+    VX_TRY_CUDA(cudaStreamSynchronize(s));
+    cudaFree(bitmap);
+    owned.pop_back();
+  }
+  // Stage every live item, then clear the tables.
+  std::vector<uint32_t *> staged(D, nullptr);
+  uint64_t *leaf_masks = static_cast<uint64_t *>(alloc(std::max<uint32_t>(live[D], 1) * 8ull));
+  if (!leaf_masks) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+  for (uint32_t l = 0; l <= D; ++l) {
+    if (l < D) {
+      staged[l] = static_cast<uint32_t *>(alloc(std::max<uint32_t>(live[l], 1) * 36ull));
+      if (!staged[l]) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+    }
+    if (!live[l]) continue;
+    vx::prof::Scope sc("dag_compact_stage", s);
+    stage_kernel<<<grid, kBlock, 0, s>>>(d->t, l, refs[l], live[l], staged[l < D ? l : 0], leaf_masks);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  VX_TRY(vx_dag_reset(d, stream));
+  // Re-insert bottom-up.
+  size_t sort_bytes = 0;
+  for (uint32_t l = 0; l <= D; ++l) sort_bytes = std::max(sort_bytes, vx_sort_workspace_size(live[l], 4));
+  void *sort_ws = alloc(sort_bytes);
+  if (!sort_ws) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+  for (uint32_t r = D + 1; r > 0; --r) {
+    const uint32_t l = r - 1;
+    if (!live[l]) continue;
+    if (l == D) {
+      vx::prof::Scope sc("dag_compact_reinsert", s);
+      reinsert_leaves_kernel<<<grid, kBlock, 0, s>>>(d->t, leaf_masks, live[l], newr[l]);
+    } else {
+      vx::prof::Scope sc("dag_compact_reinsert", s);
+      reinsert_nodes_kernel<<<grid, kBlock, 0, s>>>(d->t, l, staged[l], live[l], sorted_old[l + 1],
+                                                    sorted_new[l + 1], live[l + 1], newr[l]);
+    }
+    VX_TRY_CUDA(cudaGetLastError());
+    // (old ref -> new ref) of this level, sorted by old ref, for the level above.
+    VX_TRY_CUDA(cudaMemcpyAsync(sorted_old[l], refs[l], live[l] * 4ull, cudaMemcpyDeviceToDevice, s));
+    VX_TRY_CUDA(cudaMemcpyAsync(sorted_new[l], newr[l], live[l] * 4ull, cudaMemcpyDeviceToDevice, s));
+    VX_TRY(vx_sort_pairs_u32(sorted_old[l], sorted_new[l], live[l], 32, sort_ws, sort_bytes, s));
+  }
+  uint32_t root = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(&root, newr[0], 4, cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  {
+    vx::prof::Scope sc("dag_set_root", s);
+    set_root_kernel<<<1, 1, 0, s>>>(d->t, root);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  cleanup();
+  return read_status(d, s, true);
+}
+
+} // extern "C"
+
+// ======================================================= serving hooks ==
+
+#include "dag_internal.cuh"
+
+namespace vx::dag {
+
+const void *device_header(const vx_dag *d) { return d->t.hdr; }
+size_t header_bytes() { return sizeof(vx::edit::Header); }
+uint32_t header_root(const void *hh) { return static_cast<const vx::edit::Header *>(hh)->root; }
+uint32_t header_status(const void *hh) { return static_cast<const vx::edit::Header *>(hh)->status; }
+
+double fill_fraction(const vx_dag *d, const void *hh) {
+  const auto *h = static_cast<const vx::edit::Header *>(hh);
+  double f = 0.0;
+  for (uint32_t l = 0; l < d->t.depth; ++l) {
+    f = std::max(f, static_cast<double>(h->node_count[l]) / (d->index_slots[l] / 2.0));
+    f = std::max(f, static_cast<double>(h->pool_used[l]) / static_cast<double>(d->t.pool_cap[l]));
+  }
+  f = std::max(f, static_cast<double>(h->node_count[d->t.depth]) / (d->leaf_slots / 2.0));
+  return f;
+}
+
+} // namespace vx::dag
