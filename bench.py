@@ -67,6 +67,8 @@ SVO_C3_EDITS = 65536
 SERVE_DEPTH = 11          # 8192^3
 SERVE_RATE = 2000.0       # requests per second (Poisson)
 SERVE_SECONDS = 60.0
+SERVE_MAX_NODES = 1 << 28   # per level; two such DAGs (served + check) ~ 100 GB
+SERVE_ARENA = 16 << 30
 N_HASH = 1 << 26
 HASH_LOAD = 0.8
 BYTES_HASH_INSERT = 40  # read key 8 + one 32-B sector read-modify-write
@@ -642,7 +644,7 @@ def run_serve(args, ws, rank, local, torch, vx, device):
     offs[1:] = np.cumsum(sizes)
     dprims = vx.prims_to_device(prims, device)
     voxels = int(count_voxels(torch, vx, dprims, world_exp).sum().item())
-    dag = vx.HashDag(SERVE_DEPTH, 1 << 27, 8 << 30)
+    dag = vx.HashDag(SERVE_DEPTH, SERVE_MAX_NODES, SERVE_ARENA)
     dag.build_terrain(8, 32, True)
     assert dag.status() == 0
     srv = vx.Server(dag, max_batch_prims=1 << 16, compact_at_fill=0.5)
@@ -673,12 +675,18 @@ def run_serve(args, ws, rank, local, torch, vx, device):
     span_s = (int(done["commit_ns"].max()) - t0) / 1e9
     # Spot check: the same primitives applied with the batched call in
     # sequential chunks on a fresh terrain must give the same voxels.
-    check = vx.HashDag(SERVE_DEPTH, 1 << 27, 8 << 30)
+    check = vx.HashDag(SERVE_DEPTH, SERVE_MAX_NODES, SERVE_ARENA)
     check.build_terrain(8, 32, True)
-    chunk = 1 << 20
+    chunk = 1 << 16
     for a in range(0, dprims.shape[0], chunk):
-        check.apply_primitives(dprims[a:a + chunk].contiguous())
-        if check.status() != 0:
+        part = dprims[a:a + chunk].contiguous()
+        check.apply_primitives(part)
+        if check.status() != 0:      # tables full: compact and apply again
+            check.compact()
+            check.apply_primitives(part)
+            if check.status() != 0:
+                raise RuntimeError("sequential check could not apply a chunk")
+        if (a // chunk) % 16 == 15:
             check.compact()
     g = torch.Generator(device=device)
     g.manual_seed(5)

@@ -276,7 +276,8 @@ vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream);
  * cleared tables; the canonical content is unchanged.  The GPU counterpart of
  * the reference CPU DAG's collect_garbage (svt/hash_dag.hpp:133-191); the
  * reference GPU DAG has none (append-only, hash_dag_gpu/storage.cuh:14-15).
- * Synchronises; uses temporary device buffers. */
+ * Synchronises; its temporaries live in the DAG's edit arena (returns
+ * VX_ERR_CAPACITY, changing nothing, when the arena is too small). */
 vx_status vx_dag_compact(vx_dag *dag, vx_stream stream);
 
 /* The same dump for an earlier root ref (e.g. one a served batch published):

@@ -69,13 +69,19 @@ def test_each_result_same_alone_and_in_the_mix(cuda):
     d_mix, s_mix = run(mixed, arr, sizes, prims, compact_at_fill=1e9)
     assert s_mix.batches < len(arr)
     root_alone = dict(zip(d_alone["request_id"].tolist(), d_alone["root"].tolist()))
-    # the last request of each mixed batch: same content as after it alone
-    by_root = {}
-    for rid, root in zip(d_mix["request_id"].tolist(), d_mix["root"].tolist()):
-        by_root[root] = max(rid, by_root.get(root, -1))
+    # A batch is a run of consecutive requests completed together (same
+    # commit time and root); two batches may publish the same root when the
+    # later one changes nothing.  The last request of each mixed batch must
+    # see the same content as right after it ran alone.
+    order = np.argsort(d_mix["request_id"])
+    rids = d_mix["request_id"][order].tolist()
+    roots = d_mix["root"][order].tolist()
+    commits = d_mix["commit_ns"][order].tolist()
     checked = 0
-    for root, last in sorted(by_root.items(), key=lambda kv: kv[1]):
-        assert canon(mixed, root) == canon(alone, root_alone[last])
+    for i, rid in enumerate(rids):
+        if i + 1 < len(rids) and (roots[i + 1], commits[i + 1]) == (roots[i], commits[i]):
+            continue
+        assert canon(mixed, roots[i]) == canon(alone, root_alone[rid])
         checked += 1
     assert checked == s_mix.batches
 

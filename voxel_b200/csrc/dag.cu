@@ -573,10 +573,14 @@ vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
   cudaError_t e;
   for (uint32_t l = 0; l < cfg->depth; ++l) {
     // Level l holds at most 8^l live nodes, plus superseded ones from earlier
-    // edits; small levels keep room for 2^20 items.
+    // edits: every edit copies the path above what it changes, so the small
+    // levels fill with garbage first. They keep room for max(2^20,
+    // max_nodes / 16) items, which sets how often a long-running editor
+    // (the serving loop) has to compact.
     const double live = l < 21 ? std::pow(8.0, static_cast<double>(l)) : 1e30;
+    const uint64_t floor_cap = std::max<uint64_t>(1u << 20, cfg->max_nodes / 16);
     const uint64_t cap = std::min<uint64_t>(
-        cfg->max_nodes, std::max<uint64_t>(1u << 20, static_cast<uint64_t>(std::min(live * 4, 1e18))));
+        cfg->max_nodes, std::max<uint64_t>(floor_cap, static_cast<uint64_t>(std::min(live * 4, 1e18))));
     d->index_slots[l] = next_pow2(cap * 2);
     d->t.index_mask[l] = d->index_slots[l] - 1;
     d->t.pool_cap[l] = std::min<uint64_t>(cap * 6, 0xfffffff0ull);
@@ -893,79 +897,186 @@ vx_status vx_dag_copy(vx_dag *dst, const vx_dag *src, vx_stream stream) {
 // reachable from the root level by level, stages their items, clears every
 // table and hash-conses the live items back bottom-up, remapping child refs
 // through sorted (old ref -> new ref) arrays of the level below.  It is a
-// maintenance call: it synchronises and uses temporary device buffers.
+// maintenance call: it synchronises, and its temporaries live in the DAG's
+// edit arena (VX_ERR_CAPACITY if the arena cannot hold them).
 
 namespace vx::dag {
 
-__global__ void mark_level_kernel(Tables t, uint32_t l, const uint32_t *front,
-                                  uint32_t n, uint32_t *next, uint32_t *next_count,
-                                  uint32_t next_cap, uint32_t *bitmap) {
+// Compaction.  Every level l gets a mark bitmap over its old ref space (ref
+// - 2 = pool word offset, or leaf slot) and, after an exclusive scan of the
+// bitmap words' popcounts, a rank for every live ref: the live refs of a
+// level, listed in ascending order, are ranks 0..live-1, and the new ref of
+// an old one is new_refs[rank(old)].  Nothing is sized on the host except by
+// upper bounds, so the whole pass is stream-ordered.
+struct LevelMarks {
+  uint32_t *bits;   // mark bitmap
+  uint32_t *prefix; // exclusive prefix of popcount(bits[w])
+  uint32_t *refs;   // live old refs in ascending order (rank order)
+  uint32_t *new_refs;
+  uint32_t *live;   // device count of live refs
+  uint64_t words;   // bitmap words
+  uint32_t cap;     // capacity of refs / new_refs
+};
+
+__device__ __forceinline__ uint32_t rank_of(const LevelMarks &m, uint32_t ref) {
+  const uint32_t b = ref - 2u;
+  return m.prefix[b >> 5] + __popc(m.bits[b >> 5] & ((1u << (b & 31u)) - 1u));
+}
+
+// Marks the children of level l's live items in level l+1's bitmap.
+__global__ void mark_children_kernel(Tables t, uint32_t l, LevelMarks m, LevelMarks next) {
+  const uint32_t n = *m.live;
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint32_t *item = t.pool[l] + (front[i] - 2);
+    const uint32_t *item = t.pool[l] + (m.refs[i] - 2);
     const uint32_t cm = item[0] & 0xffu;
     for (uint32_t k = 0; k < static_cast<uint32_t>(__popc(cm)); ++k) {
-      const uint32_t r = item[1 + k];
-      const uint32_t bit = r - 2;
-      const uint32_t old = atomicOr(&bitmap[bit >> 5], 1u << (bit & 31u));
-      if (old & (1u << (bit & 31u))) continue;
-      const uint32_t at = atomicAdd(next_count, 1u);
-      if (at < next_cap) next[at] = r;
-      else set_status(&t.hdr->status, kDevCapacity);
+      const uint32_t b = item[1 + k] - 2u;
+      const uint32_t bit = 1u << (b & 31u);
+      if (!(ld_relaxed_u32(next.bits + (b >> 5)) & bit)) atomicOr(next.bits + (b >> 5), bit);
     }
   }
 }
 
-__global__ void stage_kernel(Tables t, uint32_t l, const uint32_t *refs, uint32_t n,
+__global__ void popcount_kernel(LevelMarks m) {
+  for (uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; w < m.words;
+       w += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    m.prefix[w] = __popc(m.bits[w]);
+}
+
+// After the scan: the live count and the rank-ordered list of live refs.
+__global__ void list_kernel(Tables t, LevelMarks m) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (first == 0) {
+    const uint64_t last = m.words - 1;
+    const uint32_t total = m.prefix[last] + __popc(m.bits[last]);
+    if (total > m.cap) set_status(&t.hdr->status, kDevCapacity);
+    *m.live = min(total, m.cap);
+  }
+  for (uint64_t w = first; w < m.words; w += stride) {
+    uint32_t bits = m.bits[w];
+    uint32_t at = m.prefix[w];
+    while (bits) {
+      const uint32_t b = __ffs(bits) - 1u;
+      bits &= bits - 1u;
+      if (at < m.cap) m.refs[at] = static_cast<uint32_t>(w * 32u + b + 2u);
+      ++at;
+    }
+  }
+}
+
+__global__ void stage_kernel(Tables t, uint32_t l, LevelMarks m,
                              uint32_t *staged /* 9 words per item */, uint64_t *leaf_masks) {
+  const uint32_t n = *m.live;
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     if (l == t.depth) {
-      leaf_masks[i] = t.leaves[refs[i] - 2];
+      leaf_masks[i] = t.leaves[m.refs[i] - 2];
       continue;
     }
-    const uint32_t *item = t.pool[l] + (refs[i] - 2);
+    const uint32_t *item = t.pool[l] + (m.refs[i] - 2);
     const uint32_t w = 1 + __popc(item[0] & 0xffu);
     for (uint32_t k = 0; k < 9; ++k) staged[i * 9 + k] = k < w ? item[k] : 0u;
   }
 }
 
-__global__ void reinsert_leaves_kernel(Tables t, const uint64_t *masks, uint32_t n,
-                                       uint32_t *new_refs) {
+// Re-insertion.  The live items of a level are distinct by content (the
+// tables hash-cons them) and stay distinct after their children are renamed
+// (renaming is injective), so an item needs no lookup: its pool offset is the
+// exclusive scan of the items' word counts and its index entry takes the
+// first empty slot of its probe sequence.  No shared counter is touched per
+// item; the level's counts are written once at the end.
+__global__ void reinsert_leaves_kernel(Tables t, LevelMarks m, const uint64_t *masks) {
+  const uint32_t n = *m.live;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t mask = masks[i];
+    uint64_t pos = mix64(mask) & t.leaf_mask;
+    uint32_t ref = kEmptyRef;
+    for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+      if (ld_relaxed_u64(t.leaves + pos) == 0 &&
+          atomicCAS(reinterpret_cast<unsigned long long *>(t.leaves + pos), 0ull,
+                    static_cast<unsigned long long>(mask)) == 0ull) {
+        ref = static_cast<uint32_t>(pos + 2);
+        break;
+      }
+      pos = (pos + 1) & t.leaf_mask;
+    }
+    if (ref == kEmptyRef) set_status(&t.hdr->status, kDevCapacity);
+    m.new_refs[i] = ref;
+  }
+}
+
+__global__ void item_words_kernel(LevelMarks m, const uint32_t *staged, uint32_t *words) {
+  const uint32_t n = *m.live;
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-    new_refs[i] = leaf_find_or_insert(t, masks[i]);
+    words[i] = 1u + __popc(staged[i * 9] & 0xffu);
 }
 
-__device__ __forceinline__ uint32_t remap(const uint32_t *old_sorted, const uint32_t *new_sorted,
-                                          uint32_t n, uint32_t ref, uint32_t *status) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (old_sorted[mid] < ref) lo = mid + 1;
-    else hi = mid;
-  }
-  if (lo < n && old_sorted[lo] == ref) return new_sorted[lo];
-  set_status(status, kDevInvalid); // a live child that was not marked
-  return kEmptyRef;
-}
-
-__global__ void reinsert_nodes_kernel(Tables t, uint32_t l, const uint32_t *staged,
-                                      uint32_t n, const uint32_t *child_old,
-                                      const uint32_t *child_new, uint32_t child_n,
-                                      uint32_t *new_refs) {
+__global__ void reinsert_nodes_kernel(Tables t, uint32_t l, LevelMarks m, LevelMarks child,
+                                      const uint32_t *staged, const uint32_t *offsets) {
+  const uint32_t n = *m.live;
+  uint64_t *idx = t.index[l];
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     uint32_t w[9];
     w[0] = staged[i * 9];
     const uint32_t k = __popc(w[0] & 0xffu);
-    for (uint32_t j = 0; j < k; ++j)
-      w[1 + j] = remap(child_old, child_new, child_n, staged[i * 9 + 1 + j], &t.hdr->status);
-    new_refs[i] = node_find_or_insert(t, l, w, 1 + k);
+    for (uint32_t j = 0; j < k; ++j) w[1 + j] = child.new_refs[rank_of(child, staged[i * 9 + 1 + j])];
+    const uint32_t off = offsets[i];
+    if (static_cast<uint64_t>(off) + 1 + k > t.pool_cap[l]) {
+      set_status(&t.hdr->status, kDevCapacity);
+      m.new_refs[i] = kEmptyRef;
+      continue;
+    }
+    uint32_t *dst = t.pool[l] + off;
+    for (uint32_t j = 0; j <= k; ++j) dst[j] = w[j];
+    const uint64_t h = hash_words(w, 1 + k);
+    const uint64_t entry = (static_cast<uint64_t>(static_cast<uint32_t>(h >> 32) | 1u) << 32) |
+                           (off + 2u);
+    uint64_t pos = h & t.index_mask[l];
+    bool placed = false;
+    for (uint32_t probe = 0; probe < kMaxProbes && !placed; ++probe) {
+      placed = ld_relaxed_u64(idx + pos) == 0 &&
+               atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos), 0ull,
+                         static_cast<unsigned long long>(entry)) == 0ull;
+      pos = (pos + 1) & t.index_mask[l];
+    }
+    if (!placed) set_status(&t.hdr->status, kDevCapacity);
+    m.new_refs[i] = off + 2u;
   }
 }
 
+// The level's node count and pool use, once its items are in.
+__global__ void finish_level_kernel(Tables t, uint32_t l, LevelMarks m, const uint32_t *staged,
+                                    const uint32_t *offsets) {
+  const uint32_t n = *m.live;
+  t.hdr->node_count[l] = n;
+  if (l < t.depth)
+    t.hdr->pool_used[l] = n ? offsets[n - 1] + 1u + __popc(staged[(n - 1) * 9ull] & 0xffu) : 0u;
+}
+
+__global__ void seed_root_kernel(LevelMarks m, uint32_t root) {
+  m.refs[0] = root;
+  *m.live = 1;
+}
+
 __global__ void set_root_kernel(Tables t, uint32_t root) { t.hdr->root = root; }
+
+__global__ void publish_compacted_root_kernel(Tables t, LevelMarks m0) {
+  if (t.hdr->status == kDevOk) t.hdr->root = m0.new_refs[0];
+}
+
+// Carver stand-in that only adds up sizes (pointers come back null).
+struct SizingCarver {
+  Sizer z;
+  template <class T> T *take(size_t n) {
+    z.take<T>(n);
+    return nullptr;
+  }
+};
 
 } // namespace vx::dag
 
@@ -986,98 +1097,142 @@ vx_status vx_dag_compact(vx_dag *d, vx_stream stream) {
     return vx::from_cuda(cudaGetLastError());
   }
   const uint32_t grid = static_cast<uint32_t>(vx::sm_count()) * 8u;
-  std::vector<void *> owned;
-  auto alloc = [&](size_t bytes) -> void * {
-    void *p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(bytes, 256)) != cudaSuccess) return nullptr;
-    owned.push_back(p);
-    return p;
-  };
-  auto cleanup = [&]() {
-    for (void *p : owned) cudaFree(p);
-  };
-  // Upper bounds of live items per level: the items each table holds.
-  std::vector<uint32_t *> refs(D + 1), newr(D + 1), sorted_old(D + 1), sorted_new(D + 1);
-  std::vector<uint32_t> live(D + 1, 0);
-  uint32_t *counter = static_cast<uint32_t *>(alloc(4 * (D + 1)));
-  if (!counter) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
-  VX_TRY_CUDA(cudaMemsetAsync(counter, 0, 4 * (D + 1), s));
+  // Temporaries: per level a bitmap and prefix over its old ref space and
+  // live-ref / new-ref lists sized by the level's node count, the scan
+  // workspace, then (once the live counts are known) the staged items.  They
+  // live in the idle edit arena when it is large enough, else in temporary
+  // allocations.
+  std::vector<LevelMarks> m(D + 1);
+  uint64_t max_words = 1;
   for (uint32_t l = 0; l <= D; ++l) {
-    const uint64_t cap = std::max<uint64_t>(h.node_count[l], 1);
-    refs[l] = static_cast<uint32_t *>(alloc(cap * 4));
-    newr[l] = static_cast<uint32_t *>(alloc(cap * 4));
-    sorted_old[l] = static_cast<uint32_t *>(alloc(cap * 4));
-    sorted_new[l] = static_cast<uint32_t *>(alloc(cap * 4));
-    if (!refs[l] || !newr[l] || !sorted_old[l] || !sorted_new[l]) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+    const uint64_t space = l == D ? d->leaf_slots
+                                  : std::min<uint64_t>(h.pool_used[l], d->t.pool_cap[l]);
+    m[l].words = std::max<uint64_t>((space + 31) / 32, 1);
+    m[l].cap = static_cast<uint32_t>(std::max<uint64_t>(h.node_count[l], 1));
+    max_words = std::max(max_words, m[l].words);
   }
-  // Mark, level by level.
-  VX_TRY_CUDA(cudaMemcpyAsync(refs[0], &h.root, 4, cudaMemcpyHostToDevice, s));
-  live[0] = 1;
+  if (max_words > 0xffffffffull) return VX_ERR_CAPACITY;
+  uint64_t max_scan = max_words;
+  for (uint32_t l = 0; l <= D; ++l) max_scan = std::max<uint64_t>(max_scan, m[l].cap);
+  const size_t scan_bytes = vx_scan_workspace_size(static_cast<uint32_t>(max_scan));
+  uint32_t *counts = nullptr;
+  void *scan_ws = nullptr;
+  auto carve_marks = [&](auto &c) {
+    counts = c.template take<uint32_t>(D + 1);
+    scan_ws = c.template take<unsigned char>(scan_bytes);
+    for (uint32_t l = 0; l <= D; ++l) {
+      m[l].live = counts + l;
+      m[l].bits = c.template take<uint32_t>(m[l].words);
+      m[l].prefix = c.template take<uint32_t>(m[l].words);
+      m[l].refs = c.template take<uint32_t>(m[l].cap);
+      m[l].new_refs = c.template take<uint32_t>(m[l].cap);
+    }
+  };
+  const size_t arena_bytes = static_cast<size_t>(d->a.item_cap) * sizeof(vx::edit::Item) +
+                             2ull * d->a.pair_cap * 4;
+  struct TempBlock {
+    void *p = nullptr;
+    ~TempBlock() { if (p) cudaFree(p); }
+  } temp_marks, temp_staged;
+  SizingCarver marks_size;
+  carve_marks(marks_size);
+  void *marks_base = d->arena_mem;
+  if (marks_size.z.offset > arena_bytes) {
+    VX_TRY_CUDA(cudaMalloc(&temp_marks.p, marks_size.z.offset));
+    marks_base = temp_marks.p;
+  }
+  vx::Carver carver(marks_base);
+  carve_marks(carver);
+  for (uint32_t l = 1; l <= D; ++l)
+    VX_TRY_CUDA(cudaMemsetAsync(m[l].bits, 0, m[l].words * 4, s));
+  {
+    vx::prof::Scope sc("dag_compact_mark", s);
+    seed_root_kernel<<<1, 1, 0, s>>>(m[0], h.root);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  // Mark top-down: children of level l's live items, then rank level l+1.
   for (uint32_t l = 0; l < D; ++l) {
-    const uint64_t bits = l + 1 < D ? std::max<uint64_t>(h.pool_used[l + 1], 1) : d->leaf_slots;
-    uint32_t *bitmap = static_cast<uint32_t *>(alloc((bits + 31) / 32 * 4));
-    if (!bitmap) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
-    VX_TRY_CUDA(cudaMemsetAsync(bitmap, 0, (bits + 31) / 32 * 4, s));
     {
       vx::prof::Scope sc("dag_compact_mark", s);
-      mark_level_kernel<<<grid, kBlock, 0, s>>>(d->t, l, refs[l], live[l], refs[l + 1],
-                                                counter + l + 1,
-                                                static_cast<uint32_t>(std::max<uint64_t>(h.node_count[l + 1], 1)),
-                                                bitmap);
+      mark_children_kernel<<<grid, kBlock, 0, s>>>(d->t, l, m[l], m[l + 1]);
+      VX_TRY_CUDA(cudaGetLastError());
     }
-    VX_TRY_CUDA(cudaGetLastError());
-    VX_TRY_CUDA(cudaMemcpyAsync(&live[l + 1], counter + l + 1, 4, cudaMemcpyDeviceToHost, s));
-    VX_TRY_CUDA(cudaStreamSynchronize(s));
-    cudaFree(bitmap);
-    owned.pop_back();
+    {
+      vx::prof::Scope sc("dag_compact_rank", s);
+      popcount_kernel<<<grid, kBlock, 0, s>>>(m[l + 1]);
+      VX_TRY_CUDA(cudaGetLastError());
+    }
+    VX_TRY(vx_scan_exclusive_sum_u32(m[l + 1].prefix, static_cast<uint32_t>(m[l + 1].words),
+                                     scan_ws, scan_bytes, s));
+    {
+      vx::prof::Scope sc("dag_compact_rank", s);
+      list_kernel<<<grid, kBlock, 0, s>>>(d->t, m[l + 1]);
+      VX_TRY_CUDA(cudaGetLastError());
+    }
+  }
+  // Live counts (and a capacity error raised while listing, which must not
+  // be lost to the reset below).
+  std::vector<uint32_t> live(D + 1, 0);
+  uint32_t mark_status = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(live.data(), counts, 4 * (D + 1), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaMemcpyAsync(&mark_status, &d->t.hdr->status, 4, cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  if (mark_status != vx::kDevOk) return vx::status_from_device(mark_status);
+  // Staging, sized by the live counts: 9 words per inner item, leaf masks.
+  std::vector<uint32_t *> staged(D + 1, nullptr), offsets(D + 1, nullptr);
+  uint64_t *leaf_masks = nullptr;
+  auto carve_staged = [&](auto &c) {
+    leaf_masks = c.template take<uint64_t>(std::max<uint32_t>(live[D], 1));
+    for (uint32_t l = 0; l < D; ++l) {
+      staged[l] = c.template take<uint32_t>(std::max<uint32_t>(live[l], 1) * 9ull);
+      offsets[l] = c.template take<uint32_t>(std::max<uint32_t>(live[l], 1));
+    }
+  };
+  SizingCarver staged_size;
+  staged_size.z.offset = marks_base == d->arena_mem ? carver.offset : 0;
+  carve_staged(staged_size);
+  if (marks_base == d->arena_mem && staged_size.z.offset <= arena_bytes) {
+    carve_staged(carver);
+  } else {
+    SizingCarver alone;
+    carve_staged(alone);
+    VX_TRY_CUDA(cudaMalloc(&temp_staged.p, alone.z.offset));
+    vx::Carver c2(temp_staged.p);
+    carve_staged(c2);
   }
   // Stage every live item, then clear the tables.
-  std::vector<uint32_t *> staged(D, nullptr);
-  uint64_t *leaf_masks = static_cast<uint64_t *>(alloc(std::max<uint32_t>(live[D], 1) * 8ull));
-  if (!leaf_masks) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
   for (uint32_t l = 0; l <= D; ++l) {
-    if (l < D) {
-      staged[l] = static_cast<uint32_t *>(alloc(std::max<uint32_t>(live[l], 1) * 36ull));
-      if (!staged[l]) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
-    }
-    if (!live[l]) continue;
     vx::prof::Scope sc("dag_compact_stage", s);
-    stage_kernel<<<grid, kBlock, 0, s>>>(d->t, l, refs[l], live[l], staged[l < D ? l : 0], leaf_masks);
+    stage_kernel<<<grid, kBlock, 0, s>>>(d->t, l, m[l], staged[l], leaf_masks);
     VX_TRY_CUDA(cudaGetLastError());
   }
   VX_TRY(vx_dag_reset(d, stream));
-  // Re-insert bottom-up.
-  size_t sort_bytes = 0;
-  for (uint32_t l = 0; l <= D; ++l) sort_bytes = std::max(sort_bytes, vx_sort_workspace_size(live[l], 4));
-  void *sort_ws = alloc(sort_bytes);
-  if (!sort_ws) { cleanup(); return VX_ERR_MEMORY_ALLOCATION; }
+  // Re-insert bottom-up; a child's new ref is new_refs[rank(old ref)].
   for (uint32_t r = D + 1; r > 0; --r) {
     const uint32_t l = r - 1;
-    if (!live[l]) continue;
-    if (l == D) {
-      vx::prof::Scope sc("dag_compact_reinsert", s);
-      reinsert_leaves_kernel<<<grid, kBlock, 0, s>>>(d->t, leaf_masks, live[l], newr[l]);
-    } else {
-      vx::prof::Scope sc("dag_compact_reinsert", s);
-      reinsert_nodes_kernel<<<grid, kBlock, 0, s>>>(d->t, l, staged[l], live[l], sorted_old[l + 1],
-                                                    sorted_new[l + 1], live[l + 1], newr[l]);
+    if (l < D && live[l]) {
+      {
+        vx::prof::Scope sc("dag_compact_reinsert", s);
+        item_words_kernel<<<grid, kBlock, 0, s>>>(m[l], staged[l], offsets[l]);
+        VX_TRY_CUDA(cudaGetLastError());
+      }
+      VX_TRY(vx_scan_exclusive_sum_u32(offsets[l], live[l], scan_ws, scan_bytes, s));
     }
+    vx::prof::Scope sc("dag_compact_reinsert", s);
+    if (l == D)
+      reinsert_leaves_kernel<<<grid, kBlock, 0, s>>>(d->t, m[D], leaf_masks);
+    else
+      reinsert_nodes_kernel<<<grid, kBlock, 0, s>>>(d->t, l, m[l], m[l + 1], staged[l],
+                                                    offsets[l]);
     VX_TRY_CUDA(cudaGetLastError());
-    // (old ref -> new ref) of this level, sorted by old ref, for the level above.
-    VX_TRY_CUDA(cudaMemcpyAsync(sorted_old[l], refs[l], live[l] * 4ull, cudaMemcpyDeviceToDevice, s));
-    VX_TRY_CUDA(cudaMemcpyAsync(sorted_new[l], newr[l], live[l] * 4ull, cudaMemcpyDeviceToDevice, s));
-    VX_TRY(vx_sort_pairs_u32(sorted_old[l], sorted_new[l], live[l], 32, sort_ws, sort_bytes, s));
+    finish_level_kernel<<<1, 1, 0, s>>>(d->t, l, m[l], staged[l], offsets[l]);
+    VX_TRY_CUDA(cudaGetLastError());
   }
-  uint32_t root = 0;
-  VX_TRY_CUDA(cudaMemcpyAsync(&root, newr[0], 4, cudaMemcpyDeviceToHost, s));
-  VX_TRY_CUDA(cudaStreamSynchronize(s));
   {
     vx::prof::Scope sc("dag_set_root", s);
-    set_root_kernel<<<1, 1, 0, s>>>(d->t, root);
+    publish_compacted_root_kernel<<<1, 1, 0, s>>>(d->t, m[0]);
   }
   VX_TRY_CUDA(cudaGetLastError());
-  VX_TRY_CUDA(cudaStreamSynchronize(s));
-  cleanup();
   return read_status(d, s, true);
 }
 
