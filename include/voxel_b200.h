@@ -327,6 +327,7 @@ typedef struct vx_svo_config {
 vx_status vx_svo_create(const vx_svo_config *config, vx_svo **out);
 vx_status vx_svo_destroy(vx_svo *svo);
 vx_status vx_svo_reset(vx_svo *svo, vx_stream stream);
+uint32_t vx_svo_depth(const vx_svo *svo);
 
 /* Plain per-call path: place (with a material) or destroy a voxel list.
  * Replaces svt::cuda::{place,destroy}_voxel_edits and
@@ -367,6 +368,51 @@ typedef struct vx_svo_counters {
 } vx_svo_counters;
 vx_status vx_svo_get_counters(const vx_svo *svo, vx_svo_counters *host_counters,
                               vx_stream stream);
+
+/* ------------------------------------------------------- terminal edits --
+ * Place or destroy whole octree cells and 4^3 bricks (svt/cuda/terminal/
+ * types.cuh:15-31, detail/pipeline.cuh:27-222).  A node input is the cell at
+ * `depth` (0 = the whole world, `depth` of the structure = one leaf) whose
+ * path from the root is `prefix` (3 bits per level, the root's child in the
+ * highest triple, child = x | y << 1 | z << 2), moved by a voxel offset; a leaf
+ * input is a 4^3 brick (bit x + 4y + 16z of mask64) at the full-depth path
+ * `leaf_prefix`, moved by a voxel offset.  Every voxel of the union of the
+ * moved inputs that lies inside the world becomes filled (place) or empty
+ * (destroy); inputs with depth > structure depth or prefix bits above
+ * 3 * depth are ignored, as in the reference.  Structures of depth <= 10
+ * (prefixes are 32-bit).  Layouts match TerminalNodeInput (20 B) and
+ * TerminalLeafInput (32 B). */
+typedef struct vx_terminal_node {
+    uint32_t depth;
+    uint32_t prefix;
+    int32_t offset[3];
+} vx_terminal_node;
+
+typedef struct vx_terminal_leaf {
+    uint32_t leaf_prefix;
+    uint32_t pad0;
+    uint64_t mask64;
+    int32_t offset[3];
+    uint32_t pad1;
+} vx_terminal_leaf;
+
+/* Workspace for one call (> 0 even for empty inputs: a NULL workspace is
+ * rejected as in the reference, detail/pipeline.cuh:41-46). */
+size_t vx_terminal_workspace_size(uint32_t node_count, uint32_t leaf_count);
+/* Synchronise and return the edit's status (as the reference does).
+ * Replaces place_terminal_edits / destroy_terminal_edits
+ * (svt/cuda/terminal/detail/pipeline.cuh:200-222); `material` is used when
+ * the SVO has materials (0 = 1). */
+vx_status vx_svo_apply_terminal(vx_svo *svo, const vx_terminal_node *nodes,
+                                uint32_t node_count, const vx_terminal_leaf *leaves,
+                                uint32_t leaf_count, uint32_t op, uint32_t material,
+                                void *workspace, size_t workspace_bytes,
+                                vx_stream stream);
+/* The same edit on a Hash DAG (depth <= 10). */
+vx_status vx_dag_apply_terminal(vx_dag *dag, const vx_terminal_node *nodes,
+                                uint32_t node_count, const vx_terminal_leaf *leaves,
+                                uint32_t leaf_count, uint32_t op, void *workspace,
+                                size_t workspace_bytes, vx_stream stream);
 
 /* -------------------------------------------------------------- serving --
  * A request loop over a resident Hash DAG with continuous batching: submitted

@@ -1,8 +1,8 @@
 // voxel_b200_compat.hpp - the reference's C++ call shapes over the C ABI.
 //
 // Existing callers of yamaatsu1112/voxel's algorithm library include
-// <algo/cuda/scan.cuh>, <algo/cuda/sort.cuh> and <algo/svt/hash_dag_gpu.cuh>
-// and call templates such as
+// <algo/cuda/scan.cuh>, <algo/cuda/sort.cuh>, <algo/svt/hash_dag_gpu.cuh> and
+// the GPU SVO headers (<algo/svt/cuda/...>) and call templates such as
 //     algo::cuda::scan::exclusive_sum(d_data, n, ws, ws_size, stream);
 //     algo::cuda::sort::sort_by_key(keys, sort::value_arrays(vals), n, ws, ws_size, stream);
 //     algo::svt::hash_dag_gpu::place_voxel_edits(dag.view(), edits, n, ws, ws_size, stream);
@@ -192,3 +192,131 @@ inline cudaError_t destroy_voxel_edits(DeviceHashDagGpu dag, const VoxelEdit *ed
 }
 
 } // namespace algo::svt::hash_dag_gpu
+
+namespace algo::svt::cuda {
+
+// svt/cuda/voxel/types.cuh, svt/cuda/detail/edit_common.cuh
+struct VoxelEdit {
+  std::uint32_t x, y, z;
+};
+static_assert(sizeof(VoxelEdit) == sizeof(vx_voxel));
+enum class EditOp { Place, Destroy };
+
+// svt/cuda/terminal/types.cuh:15-31 (same layouts)
+using TerminalNodeInput = vx_terminal_node;
+using TerminalLeafInput = vx_terminal_leaf;
+struct TerminalPlainDepthwiseAllocation {};
+struct TerminalCompactAllDepthAllocation {};
+struct TerminalDepthwiseRelease {};
+struct TerminalFrontierRelease {};
+template <class Allocation, class Release> struct TerminalEditConfig {
+  using allocation = Allocation;
+  using release = Release;
+};
+using DefaultTerminalEditConfig =
+    TerminalEditConfig<TerminalCompactAllDepthAllocation, TerminalFrontierRelease>;
+
+// The view passed to edit calls (svt/cuda/device_view.cuh:11-44): a handle.
+struct DeviceGpuSvo {
+  vx_svo *svo;
+};
+
+// svt/cuda/storage.cuh:12-122: RAII owner of a depth-10 (4096^3) SVO with
+// MaxNodeCount nodes and MaxLeafCount leaves; movable, not copyable.
+template <std::uint32_t MaxNodeCount = 131072, std::uint32_t MaxLeafCount = 524288>
+class GpuSvo {
+public:
+  GpuSvo() {
+    vx_svo_config cfg{10, 0, MaxNodeCount, MaxLeafCount, 0};
+    status_ = vx_compat::to_cuda(vx_svo_create(&cfg, &svo_));
+  }
+  ~GpuSvo() {
+    if (svo_) vx_svo_destroy(svo_);
+  }
+  GpuSvo(const GpuSvo &) = delete;
+  GpuSvo &operator=(const GpuSvo &) = delete;
+  GpuSvo(GpuSvo &&o) noexcept : svo_(o.svo_), status_(o.status_) { o.svo_ = nullptr; }
+  GpuSvo &operator=(GpuSvo &&o) noexcept {
+    if (this != &o) {
+      if (svo_) vx_svo_destroy(svo_);
+      svo_ = o.svo_;
+      status_ = o.status_;
+      o.svo_ = nullptr;
+    }
+    return *this;
+  }
+  [[nodiscard]] cudaError_t status() const { return status_; }
+  [[nodiscard]] DeviceGpuSvo view() const { return DeviceGpuSvo{svo_}; }
+
+private:
+  vx_svo *svo_ = nullptr;
+  cudaError_t status_ = cudaSuccess;
+};
+
+// svt/cuda/svo.cuh:17-22
+inline cudaError_t reset_svo(DeviceGpuSvo svo, cudaStream_t stream = nullptr) {
+  return vx_compat::to_cuda(vx_svo_reset(svo.svo, stream));
+}
+
+// svt/cuda/voxel/edit.cuh:38-92 (Config ignored)
+template <class... Config>
+inline std::size_t apply_voxel_edits_workspace_size(std::uint32_t count) {
+  return vx_svo_voxel_workspace_size(count);
+}
+template <class... Config>
+inline cudaError_t place_voxel_edits(DeviceGpuSvo svo, const VoxelEdit *edits,
+                                     std::uint32_t count, void *ws, std::size_t ws_size,
+                                     cudaStream_t stream = nullptr) {
+  return vx_compat::to_cuda(vx_svo_apply_voxels(svo.svo, reinterpret_cast<const vx_voxel *>(edits),
+                                                count, VX_EDIT_PLACE, 1, ws, ws_size, stream));
+}
+template <class... Config>
+inline cudaError_t destroy_voxel_edits(DeviceGpuSvo svo, const VoxelEdit *edits,
+                                       std::uint32_t count, void *ws, std::size_t ws_size,
+                                       cudaStream_t stream = nullptr) {
+  return vx_compat::to_cuda(vx_svo_apply_voxels(svo.svo, reinterpret_cast<const vx_voxel *>(edits),
+                                                count, VX_EDIT_DESTROY, 0, ws, ws_size, stream));
+}
+
+namespace detail {
+// svt/cuda/terminal/detail/workspace/edit.cuh:125-134; the request capacity
+// is not needed here (inputs become a fixed number of primitives).
+template <class Allocation, class Release>
+inline std::size_t apply_terminal_edits_workspace_size(std::uint32_t node_count,
+                                                       std::uint32_t leaf_count,
+                                                       std::uint32_t = 0) {
+  return vx_terminal_workspace_size(node_count, leaf_count);
+}
+template <class Allocation, class Release>
+inline cudaError_t apply_terminal_edits(DeviceGpuSvo svo, const TerminalNodeInput *nodes,
+                                        std::uint32_t node_count,
+                                        const TerminalLeafInput *leaves,
+                                        std::uint32_t leaf_count, EditOp op, void *ws,
+                                        std::size_t ws_size, cudaStream_t stream = nullptr) {
+  return vx_compat::to_cuda(vx_svo_apply_terminal(
+      svo.svo, nodes, node_count, leaves, leaf_count,
+      op == EditOp::Place ? VX_EDIT_PLACE : VX_EDIT_DESTROY, 1, ws, ws_size, stream));
+}
+} // namespace detail
+
+// svt/cuda/terminal/detail/pipeline.cuh:200-222
+template <class Config = DefaultTerminalEditConfig>
+inline cudaError_t place_terminal_edits(DeviceGpuSvo svo, const TerminalNodeInput *nodes,
+                                        std::uint32_t node_count,
+                                        const TerminalLeafInput *leaves,
+                                        std::uint32_t leaf_count, void *ws,
+                                        std::size_t ws_size, cudaStream_t stream = nullptr) {
+  return detail::apply_terminal_edits<typename Config::allocation, typename Config::release>(
+      svo, nodes, node_count, leaves, leaf_count, EditOp::Place, ws, ws_size, stream);
+}
+template <class Config = DefaultTerminalEditConfig>
+inline cudaError_t destroy_terminal_edits(DeviceGpuSvo svo, const TerminalNodeInput *nodes,
+                                          std::uint32_t node_count,
+                                          const TerminalLeafInput *leaves,
+                                          std::uint32_t leaf_count, void *ws,
+                                          std::size_t ws_size, cudaStream_t stream = nullptr) {
+  return detail::apply_terminal_edits<typename Config::allocation, typename Config::release>(
+      svo, nodes, node_count, leaves, leaf_count, EditOp::Destroy, ws, ws_size, stream);
+}
+
+} // namespace algo::svt::cuda

@@ -278,12 +278,15 @@ VX_HD uint32_t vx_terrain_classify(const vx_terrain *t, uint32_t x0,
 
 #define VX_SHAPE_SPHERE 0u
 #define VX_SHAPE_BOX 1u
+#define VX_SHAPE_AABB 4u /* half-open box [c, c + r) per axis */
 #define VX_OP_REMOVE 0u
 #define VX_OP_ADD 1u
 
 /* One edit primitive (32 bytes).  Spheres use r[0] as the radius; boxes use
- * r[0..2] as inclusive half-extents.  flags = shape | op << 8 | material << 16.
- * Within a batch, primitives apply in array order (later ones win). */
+ * r[0..2] as inclusive half-extents around c; axis-aligned boxes (AABB) cover
+ * [c, c + r) per axis, so they can have even sides (aligned octree cells).
+ * flags = shape | op << 8 | material << 16.  Within a batch, primitives
+ * apply in array order (later ones win). */
 typedef struct vx_primitive {
     int32_t c[3];
     uint32_t r[3];
@@ -300,8 +303,29 @@ VX_HD uint32_t vx_make_flags(uint32_t shape, uint32_t op, uint32_t material) {
     return shape | (op << 8) | (material << 16);
 }
 
+/* Inclusive voxel range [lo, hi] of a box or AABB primitive along axis a
+ * (empty when hi < lo). */
+VX_HD void vx_prim_axis_range(const vx_primitive *p, int a, int64_t *lo, int64_t *hi) {
+    if (vx_prim_shape(p) == VX_SHAPE_AABB) {
+        *lo = (int64_t)p->c[a];
+        *hi = (int64_t)p->c[a] + (int64_t)p->r[a] - 1;
+    } else {
+        *lo = (int64_t)p->c[a] - (int64_t)p->r[a];
+        *hi = (int64_t)p->c[a] + (int64_t)p->r[a];
+    }
+}
+
 VX_HD int vx_prim_contains_voxel(const vx_primitive *p, int64_t x, int64_t y,
                                  int64_t z) {
+    if (vx_prim_shape(p) == VX_SHAPE_AABB) {
+        const int64_t v[3] = {x, y, z};
+        for (int a = 0; a < 3; ++a) {
+            int64_t lo, hi;
+            vx_prim_axis_range(p, a, &lo, &hi);
+            if (v[a] < lo || v[a] > hi) return 0;
+        }
+        return 1;
+    }
     const int64_t dx = x - p->c[0], dy = y - p->c[1], dz = z - p->c[2];
     if (vx_prim_shape(p) == VX_SHAPE_SPHERE) {
         const int64_t r = p->r[0];
@@ -335,8 +359,8 @@ VX_HD uint32_t vx_prim_classify(const vx_primitive *p, int64_t x0, int64_t y0,
     }
     int inside = 1;
     for (int a = 0; a < 3; ++a) {
-        const int64_t b0 = (int64_t)p->c[a] - (int64_t)p->r[a];
-        const int64_t b1 = (int64_t)p->c[a] + (int64_t)p->r[a];
+        int64_t b0, b1;
+        vx_prim_axis_range(p, a, &b0, &b1);
         if (b1 < lo[a] || b0 > lo[a] + n - 1) return VX_CELL_EMPTY;
         if (!(b0 <= lo[a] && b1 >= lo[a] + n - 1)) inside = 0;
     }
@@ -349,12 +373,12 @@ VX_HD uint32_t vx_prim_classify(const vx_primitive *p, int64_t x0, int64_t y0,
 VX_HD uint64_t vx_prim_leaf_mask(const vx_primitive *p, int64_t x0, int64_t y0,
                                  int64_t z0) {
     uint64_t m = 0;
-    if (vx_prim_shape(p) == VX_SHAPE_BOX) {
+    if (vx_prim_shape(p) != VX_SHAPE_SPHERE) {
         uint32_t ax[3];
         const int64_t lo[3] = {x0, y0, z0};
         for (int a = 0; a < 3; ++a) {
-            const int64_t b0 = (int64_t)p->c[a] - (int64_t)p->r[a];
-            const int64_t b1 = (int64_t)p->c[a] + (int64_t)p->r[a];
+            int64_t b0, b1;
+            vx_prim_axis_range(p, a, &b0, &b1);
             uint32_t bits = 0;
             for (int i = 0; i < 4; ++i) {
                 const int64_t v = lo[a] + i;

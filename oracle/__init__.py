@@ -138,6 +138,7 @@ _VOXEL_SIGS = [
     ("orc_grid_terrain", None, [_P, _P]),
     ("orc_grid_apply_prims", None, [_P, _P, _U64]),
     ("orc_grid_apply_voxels", None, [_P, _P, _U64, _I, _U32]),
+    ("orc_grid_apply_terminal", None, [_P, _P, _U64, _P, _U64, _I, _U32]),
     ("orc_grid_count", _U64, [_P]),
     ("orc_grid_get", _I, [_P, _U32, _U32, _U32]),
     ("orc_grid_export_dag", _I, [_P, C.POINTER(_U32), _P, _P, _U64, _P, _U64]),
@@ -229,6 +230,19 @@ class Grid:
     def apply_prims(self, prims: np.ndarray):
         p = np.ascontiguousarray(prims, PRIM_DTYPE)
         lib().orc_grid_apply_prims(self._h, p.ctypes.data, p.size)
+        return self
+
+    def apply_terminal(self, nodes, leaves, op: int, material: int = 1):
+        """Terminal edit semantics: nodes / leaves are record arrays with the
+        TerminalNodeInput (20 B) / TerminalLeafInput (32 B) layouts."""
+        n = np.ascontiguousarray(nodes) if nodes is not None and len(nodes) else None
+        lv = np.ascontiguousarray(leaves) if leaves is not None and len(leaves) else None
+        assert n is None or n.dtype.itemsize == 20
+        assert lv is None or lv.dtype.itemsize == 32
+        lib().orc_grid_apply_terminal(self._h, None if n is None else n.ctypes.data,
+                                      0 if n is None else n.size,
+                                      None if lv is None else lv.ctypes.data,
+                                      0 if lv is None else lv.size, op, material)
         return self
 
     def apply_voxels(self, xyz: np.ndarray, op: int, material: int = 1):

@@ -90,9 +90,15 @@ void apply_prim(Grid &g, const vx_primitive &p) {
   const int64_t world = int64_t(4) << g.depth;
   int64_t lo[3], hi[3];
   for (int a = 0; a < 3; ++a) {
-    const int64_t r = vx_prim_shape(&p) == VX_SHAPE_SPHERE ? p.r[0] : p.r[a];
-    lo[a] = std::max<int64_t>(0, int64_t(p.c[a]) - r);
-    hi[a] = std::min<int64_t>(world - 1, int64_t(p.c[a]) + r);
+    int64_t b0, b1;
+    if (vx_prim_shape(&p) == VX_SHAPE_SPHERE) {
+      b0 = int64_t(p.c[a]) - p.r[0];
+      b1 = int64_t(p.c[a]) + p.r[0];
+    } else {
+      vx_prim_axis_range(&p, a, &b0, &b1);
+    }
+    lo[a] = std::max<int64_t>(0, b0);
+    hi[a] = std::min<int64_t>(world - 1, b1);
   }
   const bool add = vx_prim_op(&p) == VX_OP_ADD;
   const u8 m = static_cast<u8>(vx_prim_material(&p));
@@ -329,6 +335,66 @@ void orc_grid_terrain(void *gp, const vx_terrain *t) {
 void orc_grid_apply_prims(void *gp, const vx_primitive *p, u64 n) {
   Grid &g = *static_cast<Grid *>(gp);
   for (u64 i = 0; i < n; ++i) apply_prim(g, p[i]);
+}
+
+// Terminal edits (svt/cuda/terminal/detail/count_requests.cuh:13-158,
+// emit_requests.cuh:1-484, common.cuh): the cell at (depth, prefix) or the
+// brick at the full-depth leaf_prefix, moved by a voxel offset, clipped to
+// the world; every covered voxel is set (op 1) or cleared (op 0).  Inputs
+// with depth > the grid's depth or prefix bits above 3 * depth are ignored
+// (common.cuh terminal_prefix_to_leaf_coord).  Restated per voxel.
+struct OrcTerminalNode {
+  u32 depth, prefix;
+  int32_t offset[3];
+};
+struct OrcTerminalLeaf {
+  u32 leaf_prefix, pad0;
+  u64 mask64;
+  int32_t offset[3];
+  u32 pad1;
+};
+
+static bool orc_prefix_origin(u32 depth, u32 prefix, u32 depth_max, int64_t o[3]) {
+  if (depth > depth_max) return false;
+  if (depth < 11 && (u64(prefix) >> (3 * depth)) != 0) return false;
+  u32 c[3] = {0, 0, 0};
+  for (u32 i = 0; i < depth; ++i) {
+    const u32 child = (prefix >> (3 * (depth - 1 - i))) & 7u;
+    for (int a = 0; a < 3; ++a) c[a] = (c[a] << 1) | ((child >> a) & 1u);
+  }
+  for (int a = 0; a < 3; ++a) o[a] = int64_t(c[a] << (depth_max - depth)) * 4;
+  return true;
+}
+
+void orc_grid_apply_terminal(void *gp, const OrcTerminalNode *nodes, u64 n_nodes,
+                             const OrcTerminalLeaf *leaves, u64 n_leaves, int op,
+                             u32 material) {
+  Grid &g = *static_cast<Grid *>(gp);
+  const int64_t world = int64_t(4) << g.depth;
+  const bool add = op != 0;
+  const u8 m = add ? static_cast<u8>(material ? material : 1) : 0;
+  auto set = [&](int64_t x, int64_t y, int64_t z) {
+    if (x < 0 || y < 0 || z < 0 || x >= world || y >= world || z >= world) return;
+    g.set(u32(x), u32(y), u32(z), add, m);
+  };
+  for (u64 i = 0; i < n_nodes; ++i) {
+    int64_t o[3];
+    if (!orc_prefix_origin(nodes[i].depth, nodes[i].prefix, g.depth, o)) continue;
+    const int64_t side = int64_t(4) << (g.depth - nodes[i].depth);
+    for (int a = 0; a < 3; ++a) o[a] += nodes[i].offset[a];
+    for (int64_t z = std::max<int64_t>(o[2], 0); z < std::min(o[2] + side, world); ++z)
+      for (int64_t y = std::max<int64_t>(o[1], 0); y < std::min(o[1] + side, world); ++y)
+        for (int64_t x = std::max<int64_t>(o[0], 0); x < std::min(o[0] + side, world); ++x)
+          set(x, y, z);
+  }
+  for (u64 i = 0; i < n_leaves; ++i) {
+    int64_t o[3];
+    if (!orc_prefix_origin(g.depth, leaves[i].leaf_prefix, g.depth, o)) continue;
+    for (u32 b = 0; b < 64; ++b)
+      if ((leaves[i].mask64 >> b) & 1ull)
+        set(o[0] + (b & 3u) + leaves[i].offset[0], o[1] + ((b >> 2) & 3u) + leaves[i].offset[1],
+            o[2] + ((b >> 4) & 3u) + leaves[i].offset[2]);
+  }
 }
 
 // Plain-path semantics: one op (1 place, 0 destroy) for a voxel list;

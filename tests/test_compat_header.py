@@ -18,6 +18,20 @@ int main() {
   (void)hdg::apply_voxel_edits_workspace_size(4);
   hdg::VoxelEdit e{1, 2, 3};
   (void)e;
+  namespace svt = algo::svt::cuda;
+  using Cfg = svt::DefaultTerminalEditConfig;
+  (void)svt::detail::apply_terminal_edits_workspace_size<Cfg::allocation, Cfg::release>(1, 1, 16);
+  svt::TerminalNodeInput node{0u, 0u, 0, 0, 0};
+  svt::TerminalLeafInput leaf{};
+  static_assert(sizeof(node) == 20 && sizeof(leaf) == 32, "reference layouts");
+  if (false) {  // link-time check only: needs a device to run
+    svt::GpuSvo<256, 64> svo;
+    (void)svt::reset_svo(svo.view());
+    (void)svt::place_terminal_edits(svo.view(), &node, 1, &leaf, 1, nullptr, 0);
+    (void)svt::destroy_terminal_edits(svo.view(), &node, 1, &leaf, 1, nullptr, 0);
+    (void)svt::place_voxel_edits(svo.view(), nullptr, 0, nullptr, 0);
+    (void)svt::apply_voxel_edits_workspace_size(4);
+  }
   return 0;
 }
 '''

@@ -19,7 +19,8 @@ __all__ = [
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
-    "COMPLETION_DTYPE",
+    "COMPLETION_DTYPE", "TERMINAL_NODE_DTYPE", "TERMINAL_LEAF_DTYPE", "cell_prefix",
+    "terminal_nodes", "terminal_leaves", "records_to_device",
 ]
 
 
@@ -209,6 +210,57 @@ def voxels_to_device(xyz: np.ndarray, device) -> torch.Tensor:
     return torch.from_numpy(a.view(np.int32)).to(device)
 
 
+# Terminal edit inputs (TerminalNodeInput / TerminalLeafInput,
+# svt/cuda/terminal/types.cuh:15-31).
+TERMINAL_NODE_DTYPE = np.dtype([("depth", "<u4"), ("prefix", "<u4"), ("offset", "<i4", 3)])
+TERMINAL_LEAF_DTYPE = np.dtype([("leaf_prefix", "<u4"), ("pad0", "<u4"), ("mask64", "<u8"),
+                                ("offset", "<i4", 3), ("pad1", "<u4")])
+assert TERMINAL_NODE_DTYPE.itemsize == 20 and TERMINAL_LEAF_DTYPE.itemsize == 32
+
+
+def cell_prefix(x: int, y: int, z: int, level: int) -> int:
+    """Path of the cell (x, y, z) at `level` (cell units): 3 bits per level,
+    the root's child in the highest triple, child = x | y << 1 | z << 2
+    (make_leaf_key, svt/cuda/detail/geometry.cuh:12-24, at any level)."""
+    p = 0
+    for i in range(level - 1, -1, -1):
+        p = (p << 3) | ((x >> i) & 1) | (((y >> i) & 1) << 1) | (((z >> i) & 1) << 2)
+    return p
+
+
+def terminal_nodes(rows) -> np.ndarray:
+    """[(depth, prefix, ox, oy, oz), ...] -> TERMINAL_NODE_DTYPE records."""
+    a = np.zeros(len(rows), TERMINAL_NODE_DTYPE)
+    for i, (d, p, ox, oy, oz) in enumerate(rows):
+        a[i] = (d, p, (ox, oy, oz))
+    return a
+
+
+def terminal_leaves(rows) -> np.ndarray:
+    """[(leaf_prefix, mask64, ox, oy, oz), ...] -> TERMINAL_LEAF_DTYPE records."""
+    a = np.zeros(len(rows), TERMINAL_LEAF_DTYPE)
+    for i, (p, m, ox, oy, oz) in enumerate(rows):
+        a[i] = (p, 0, m, (ox, oy, oz), 0)
+    return a
+
+
+def records_to_device(records: np.ndarray, device) -> torch.Tensor:
+    """Any record array -> uint8 CUDA tensor holding its bytes."""
+    a = np.ascontiguousarray(records)
+    return torch.from_numpy(a.view(np.uint8).reshape(-1).copy()).to(device)
+
+
+def _apply_terminal(fn, h, nodes, leaves, extra, workspace, device):
+    nn = 0 if nodes is None else nodes.numel() // TERMINAL_NODE_DTYPE.itemsize
+    nl = 0 if leaves is None else leaves.numel() // TERMINAL_LEAF_DTYPE.itemsize
+    ws = workspace
+    if ws is None:
+        ws = torch.empty(lib().vx_terminal_workspace_size(nn, nl), dtype=torch.uint8,
+                         device=device)
+    return fn(h, ptr(nodes) if nn else None, nn, ptr(leaves) if nl else None, nl, *extra,
+              ptr(ws), ws.numel(), stream_handle())
+
+
 class HashDag:
     """Hash DAG resident on the GPU (HashDagGpu / DeviceHashDagGpu,
     hash_dag_gpu/storage.cuh:16-105, widened to depth 1..14)."""
@@ -250,6 +302,14 @@ class HashDag:
         return lib().vx_dag_apply_voxels(self._h, ptr(voxels) if n else None, n,
                                          op, ptr(ws) if n else None,
                                          ws.numel() if n else 0, stream_handle())
+
+    def apply_terminal(self, nodes: torch.Tensor | None, leaves: torch.Tensor | None,
+                       op: int, workspace: torch.Tensor | None = None,
+                       device="cuda") -> int:
+        """Terminal edit (place_/destroy_terminal_edits): byte tensors of
+        TERMINAL_NODE_DTYPE / TERMINAL_LEAF_DTYPE records; returns the status."""
+        return _apply_terminal(lib().vx_dag_apply_terminal, self._h, nodes, leaves, (op,),
+                               workspace, device)
 
     def apply_primitives(self, prims: torch.Tensor) -> None:
         """Batched path: primitives applied as if in order; asynchronous
@@ -400,6 +460,14 @@ class Svo:
         return lib().vx_svo_apply_voxels(self._h, ptr(voxels) if n else None, n, op,
                                          material, ptr(ws) if n else None,
                                          ws.numel() if n else 0, stream_handle())
+
+    def apply_terminal(self, nodes: torch.Tensor | None, leaves: torch.Tensor | None,
+                       op: int, material: int = 1, workspace: torch.Tensor | None = None,
+                       device="cuda") -> int:
+        """Terminal edit (svt::cuda::place_/destroy_terminal_edits,
+        svt/cuda/terminal/detail/pipeline.cuh:200-222); returns the status."""
+        return _apply_terminal(lib().vx_svo_apply_terminal, self._h, nodes, leaves,
+                               (op, material), workspace, device)
 
     def apply_primitives(self, prims: torch.Tensor) -> None:
         n = prims.numel() // 8

@@ -199,6 +199,8 @@ struct DagTree {
   __device__ uint32_t child(uint32_t l, uint32_t ref, uint32_t c) const {
     return child_ref(t, l, ref, c);
   }
+  // Superseded subtrees stay in the tables until vx_dag_compact.
+  __device__ void replaced(uint32_t, uint32_t, uint32_t) const {}
   template <bool Terrain>
   __device__ uint32_t classify(const vx_primitive &p, uint32_t world_exp,
                                int64_t ox, int64_t oy, int64_t oz, int64_t n) const {

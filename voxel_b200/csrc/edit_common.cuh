@@ -209,7 +209,9 @@ struct EditCtx {
 //   child(l, old, c)                      - content of child c of `old` at level l;
 //   classify<Terrain>(prim, world_exp, ox, oy, oz, n);
 //   const_value(prim, oz, n)              - the content a fully covering
-//       primitive leaves in the cube at height oz of side n (1 = full).
+//       primitive leaves in the cube at height oz of side n (1 = full);
+//   replaced(l, old, c)                   - child c of `old` is overwritten
+//       by a fully covering primitive (its subtree is dropped).
 
 static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
   Header *h = x.hdr;
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t pair_off = s_pair_base + s_pairs[group];
     __syncthreads(); // s_* are reused by the next tile
     if (!have || big || !room) continue;
+    if (last_full >= 0) pol.replaced(l, it.old, c);
 
     if (has_item) {
       const uint32_t my_pairs = pair_off + inc_pairs - cnt;
@@ -479,6 +482,7 @@ __global__ void __launch_bounds__(kBlock)
     }
     __syncthreads();
     const bool room = s_room; // block-uniform: it guards barriers below
+    if (room && t < 8 && s_last[t] >= 0) pol.replaced(l, it.old, t);
     if (room && t < 8 && ((s_cm >> t) & 1u)) {
       const uint32_t k = __popc(s_cm & ((1u << t) - 1u));
       Item ci{};

@@ -34,7 +34,11 @@ __device__ __forceinline__ void row_run(const vx_primitive &p, int64_t world,
     }
     half = isqrt64(rem);
   } else {
-    half = p.r[0];
+    int64_t lo, hi;
+    vx_prim_axis_range(&p, 0, &lo, &hi);
+    x0 = max((int64_t)0, lo);
+    x1 = min((int64_t)(world - 1), hi);
+    return;
   }
   x0 = max((int64_t)0, (int64_t)p.c[0] - half);
   x1 = min((int64_t)(world - 1), (int64_t)p.c[0] + half);
@@ -43,12 +47,20 @@ __device__ __forceinline__ void row_run(const vx_primitive &p, int64_t world,
 __device__ __forceinline__ void row_range(const vx_primitive &p, int64_t world,
                                           int64_t &y0, int64_t &ny, int64_t &z0,
                                           int64_t &nz) {
-  const bool sphere = vx_prim_shape(&p) == VX_SHAPE_SPHERE;
-  const int64_t ry = sphere ? p.r[0] : p.r[1], rz = sphere ? p.r[0] : p.r[2];
-  y0 = max((int64_t)0, (int64_t)p.c[1] - ry);
-  z0 = max((int64_t)0, (int64_t)p.c[2] - rz);
-  const int64_t y1 = min((int64_t)(world - 1), (int64_t)p.c[1] + ry);
-  const int64_t z1 = min((int64_t)(world - 1), (int64_t)p.c[2] + rz);
+  int64_t ylo, yhi, zlo, zhi;
+  if (vx_prim_shape(&p) == VX_SHAPE_SPHERE) {
+    ylo = (int64_t)p.c[1] - p.r[0];
+    yhi = (int64_t)p.c[1] + p.r[0];
+    zlo = (int64_t)p.c[2] - p.r[0];
+    zhi = (int64_t)p.c[2] + p.r[0];
+  } else {
+    vx_prim_axis_range(&p, 1, &ylo, &yhi);
+    vx_prim_axis_range(&p, 2, &zlo, &zhi);
+  }
+  y0 = max((int64_t)0, ylo);
+  z0 = max((int64_t)0, zlo);
+  const int64_t y1 = min((int64_t)(world - 1), yhi);
+  const int64_t z1 = min((int64_t)(world - 1), zhi);
   ny = y1 >= y0 ? y1 - y0 + 1 : 0;
   nz = z1 >= z0 ? z1 - z0 + 1 : 0;
 }

@@ -86,6 +86,11 @@ struct SvoTree {
     if (old & kChild) return t.nodes[static_cast<size_t>(old & kIndex) * 8u + c];
     return old; // a uniform region's children hold the same value
   }
+  // A materialised child overwritten by a covering primitive leaves its
+  // subtree unreachable: flag it for the end-of-edit collection.
+  __device__ void replaced(uint32_t l, uint32_t old, uint32_t c) const {
+    if ((old & kChild) && (child(l, old, c) & kChild)) atomicOr(&t.ctr->detached, 1u);
+  }
   template <bool Terrain>
   __device__ uint32_t classify(const vx_primitive &p, uint32_t world_exp, int64_t ox,
                                int64_t oy, int64_t oz, int64_t n) const {
@@ -612,6 +617,8 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
   VX_TRY(run_pipeline(v, prims, n, count, s, false));
   return read_status(v, s);
 }
+
+uint32_t vx_svo_depth(const vx_svo *v) { return v ? v->t.depth : 0; }
 
 vx_status vx_svo_apply_primitives(vx_svo *v, const vx_primitive *prims,
                                   uint32_t count, vx_stream stream) {
