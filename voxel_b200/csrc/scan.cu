@@ -34,56 +34,67 @@ template <class T> typename RecordsFor<T>::type make_records(const ScanLayout &w
   return r;
 }
 
+// One tile per block, tiles taken in the order of a global counter (a tile
+// only waits on tiles already taken by running blocks).  A full, aligned tile
+// arrives by one bulk copy; the last, partial tile and unaligned data use
+// guarded loads.  Pass 1 reads the rows from shared memory for per-row warp
+// totals, warp 0 scans the block and looks back, pass 2 re-reads the rows,
+// recomputes each thread's offset inside its warp (cheaper than holding it in
+// registers, which bound the resident blocks) and writes the prefix sums
+// straight to global memory.
 template <class T, bool Inclusive, bool Vectorised>
-__global__ void __launch_bounds__(TileShape<T>::kBlock, 2)
+__global__ void __launch_bounds__(TileShape<T>::kBlock, TileShape<T>::kMinBlocks)
     scan_kernel(T *__restrict__ data, uint32_t count, ScanLayout ws,
                 typename RecordsFor<T>::type records) {
   using S = TileShape<T>;
+  constexpr uint32_t kTileBytes = S::kTile * sizeof(T);
+  __shared__ __align__(128) T s_data[S::kTile];
+  __shared__ uint64_t s_bar;
   __shared__ uint32_t s_tile;
   __shared__ T s_warp[S::kWarps][S::kRows];
   __shared__ T s_row_off[S::kRows];
   __shared__ T s_prefix;
 
-  if (threadIdx.x == 0) s_tile = atomicAdd(ws.tile_counter, 1u);
-  __syncthreads();
-  const uint32_t tile = s_tile;
-  const uint64_t base = static_cast<uint64_t>(tile) * S::kTile;
   const uint32_t t = threadIdx.x;
   const uint32_t lane = lane_id();
   const uint32_t warp = t / kWarp;
-
-  T v[S::kRows][S::kPerVec];
-  const bool full = base + S::kTile <= count;
-  if (Vectorised && full) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(data + base);
-#pragma unroll
-    for (uint32_t r = 0; r < S::kRows; ++r) {
-      const uint4 q = ld_stream_u4(src + r * S::kBlock + t);
-      const T *qt = reinterpret_cast<const T *>(&q);
-#pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) v[r][e] = qt[e];
+  if (t == 0) {
+    const uint32_t tile = atomicAdd(ws.tile_counter, 1u);
+    s_tile = tile;
+    if (Vectorised && static_cast<uint64_t>(tile + 1) * S::kTile <= count) {
+      mbar_init(&s_bar, 1);
+      mbar_arrive_expect_tx(&s_bar, kTileBytes);
+      bulk_load(s_data, data + static_cast<uint64_t>(tile) * S::kTile, kTileBytes, &s_bar);
+    }
+  }
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t base = static_cast<uint64_t>(tile) * S::kTile;
+  const bool bulk = Vectorised && base + S::kTile <= count;
+  if (bulk) {
+    if (!mbar_wait(&s_bar, 0)) {
+      // Never expected: report, let the copy land, give up on this tile.
+      if (t == 0) set_status(ws.status, kDevTimeout);
+      mbar_wait(&s_bar, 0);
+      return;
     }
   } else {
-#pragma unroll
-    for (uint32_t r = 0; r < S::kRows; ++r)
-#pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) {
-        const uint64_t i =
-            base + (static_cast<uint64_t>(r) * S::kBlock + t) * S::kPerVec + e;
-        v[r][e] = i < count ? data[i] : T(0);
-      }
+    for (uint32_t i = t; i < S::kTile; i += S::kBlock)
+      s_data[i] = base + i < count ? data[base + i] : T(0);
+    __syncthreads();
   }
+  const uint4 *rows = reinterpret_cast<const uint4 *>(s_data);
 
-  // Row sums per thread, then a warp-inclusive scan of each row.
-  T sum[S::kRows], incl[S::kRows];
-#pragma unroll
+  // Pass 1: per-row warp totals.
+#pragma unroll 4
   for (uint32_t r = 0; r < S::kRows; ++r) {
-    T s = 0;
+    const uint4 q = rows[r * S::kBlock + t];
+    const T *qt = reinterpret_cast<const T *>(&q);
+    T sum = 0;
 #pragma unroll
-    for (uint32_t e = 0; e < S::kPerVec; ++e) s += v[r][e];
-    sum[r] = s;
-    incl[r] = warp_inclusive_sum<T>(s);
-    if (lane == kWarp - 1) s_warp[warp][r] = incl[r];
+    for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
+    sum = warp_sum<T>(sum);
+    if (lane == 0) s_warp[warp][r] = sum;
   }
   __syncthreads();
 
@@ -102,37 +113,35 @@ __global__ void __launch_bounds__(TileShape<T>::kBlock, 2)
   }
   __syncthreads();
 
+  // Pass 2: prefix sums, written straight to global memory.
   const T tile_prefix = s_prefix;
-#pragma unroll
+#pragma unroll 4
   for (uint32_t r = 0; r < S::kRows; ++r) {
-    T run = tile_prefix + s_row_off[r] + s_warp[warp][r] + (incl[r] - sum[r]);
+    uint4 q = rows[r * S::kBlock + t];
+    T *qt = reinterpret_cast<T *>(&q);
+    T sum = 0;
+#pragma unroll
+    for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
+    T run = tile_prefix + s_row_off[r] + s_warp[warp][r] + (warp_inclusive_sum<T>(sum) - sum);
 #pragma unroll
     for (uint32_t e = 0; e < S::kPerVec; ++e) {
-      const T x = v[r][e];
+      const T x = qt[e];
       if (Inclusive) {
         run += x;
-        v[r][e] = run;
+        qt[e] = run;
       } else {
-        v[r][e] = run;
+        qt[e] = run;
         run += x;
       }
     }
-  }
-
-  if (Vectorised && full) {
-    uint4 *dst = reinterpret_cast<uint4 *>(data + base);
+    if (bulk) {
+      reinterpret_cast<uint4 *>(data + base)[r * S::kBlock + t] = q;
+    } else {
+      const uint64_t i0 = base + (static_cast<uint64_t>(r) * S::kBlock + t) * S::kPerVec;
 #pragma unroll
-    for (uint32_t r = 0; r < S::kRows; ++r)
-      dst[r * S::kBlock + t] = *reinterpret_cast<const uint4 *>(v[r]);
-  } else {
-#pragma unroll
-    for (uint32_t r = 0; r < S::kRows; ++r)
-#pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) {
-        const uint64_t i =
-            base + (static_cast<uint64_t>(r) * S::kBlock + t) * S::kPerVec + e;
-        if (i < count) data[i] = v[r][e];
-      }
+      for (uint32_t e = 0; e < S::kPerVec; ++e)
+        if (i0 + e < count) data[i0 + e] = qt[e];
+    }
   }
 }
 

@@ -1,8 +1,9 @@
 // Single-pass prefix sum with decoupled look-back (Merrill & Garland 2016,
 // "Single-pass Parallel Prefix Scan with Decoupled Look-back"), written for
-// sm_100a: 128-bit coalesced row loads, a dynamic tile id so that a tile only
-// ever waits on tiles that are already resident, a warp-parallel look-back
-// over 32 predecessors at a time, and a globaltimer bound on every wait.
+// sm_100a: each tile arrives in shared memory by one bulk copy (TMA), a
+// dynamic tile id makes a tile only ever wait on tiles that are already
+// resident, a warp-parallel look-back reads 64 predecessors per round trip,
+// and a globaltimer bound limits every wait.
 //
 // Replaces the reference's BlockBased<DecoupledLookback<WarpShuffleBlock<512,4>>>
 // (cuda/scan/block_based/decoupled_lookback.cuh:116-221), whose look-back is a
@@ -63,10 +64,15 @@ template <> struct RecordsFor<uint32_t> { using type = PackedRecords32; };
 template <> struct RecordsFor<uint64_t> { using type = SplitRecords64; };
 
 // Warp-parallel look-back, called by one full warp.  Publishes the tile's
-// aggregate, accumulates predecessors 32 at a time until an inclusive record
-// is found, publishes the inclusive prefix and returns the exclusive prefix
-// (valid in every lane).  On timeout sets *status and returns a partial sum.
-template <class T, class Records>
+// aggregate, then reads the records of the previous 32 * R tiles at once
+// (lane l, row j reads distance l + 32 j: R coalesced loads in flight per
+// lane), accumulates back to the nearest inclusive record, publishes the
+// inclusive prefix and returns the exclusive prefix (valid in every lane).
+// A window wider than one warp matters because with hundreds of tiles
+// resident the nearest inclusive record can be far back, and each window
+// costs one round trip to L2.  On timeout sets *status and returns a partial
+// sum.
+template <class T, uint32_t R = 2, class Records>
 __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
                            uint32_t *status) {
   const uint32_t lane = lane_id();
@@ -79,14 +85,30 @@ __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
   int64_t pos = static_cast<int64_t>(tile) - 1;
   const uint64_t t0 = global_ns();
   for (;;) {
-    uint32_t s;
-    T v;
-    records.read(pos - static_cast<int64_t>(lane), s, v);
-    const uint32_t inc_mask = __ballot_sync(kFullMask, s == kInclusive);
-    const uint32_t wait_mask = __ballot_sync(kFullMask, s == kNotReady);
-    const uint32_t limit = inc_mask ? (__ffs(inc_mask) - 1u) : 31u;
-    const uint32_t range = limit == 31u ? kFullMask : ((1u << (limit + 1u)) - 1u);
-    if (wait_mask & range) {
+    uint32_t st[R];
+    T v[R];
+#pragma unroll
+    for (uint32_t j = 0; j < R; ++j)
+      records.read(pos - static_cast<int64_t>(lane + kWarp * j), st[j], v[j]);
+    // Nearest inclusive record: first row with one, first lane in it.
+    int32_t first_row = -1;
+    uint32_t limit = 31;
+    bool wait = false;
+#pragma unroll
+    for (uint32_t j = 0; j < R; ++j) {
+      const uint32_t inc = __ballot_sync(kFullMask, st[j] == kInclusive);
+      const uint32_t nr = __ballot_sync(kFullMask, st[j] == kNotReady);
+      if (first_row < 0) {
+        const uint32_t lim = inc ? (__ffs(inc) - 1u) : 31u;
+        const uint32_t range = lim == 31u ? kFullMask : ((1u << (lim + 1u)) - 1u);
+        wait = wait || (nr & range) != 0;
+        if (inc) {
+          first_row = static_cast<int32_t>(j);
+          limit = lim;
+        }
+      }
+    }
+    if (wait) {
       if (global_ns() - t0 > kWaitLimitNs) {
         if (lane == 0) set_status(status, kDevTimeout);
         break;
@@ -94,20 +116,38 @@ __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
       __nanosleep(32);
       continue;
     }
-    exclusive += warp_sum<T>(lane <= limit ? v : T(0));
-    if (inc_mask) break;
-    pos -= kWarp;
+    T part = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < R; ++j) {
+      const bool in = first_row < 0 || static_cast<int32_t>(j) < first_row ||
+                      (static_cast<int32_t>(j) == first_row && lane <= limit);
+      part += in ? v[j] : T(0);
+    }
+    exclusive += warp_sum<T>(part);
+    if (first_row >= 0) break;
+    pos -= static_cast<int64_t>(kWarp * R);
   }
   if (lane == 0) records.publish(tile, kInclusive, exclusive + aggregate);
   return exclusive;
 }
 
-// Block-wide scan tile geometry: kBlock threads, each owning kRows 16-byte
-// vectors; row r of the tile is the contiguous range of kBlock vectors
-// [r * kBlock, (r + 1) * kBlock), so every row load is fully coalesced.
+// Tile geometry: 256 threads x 8 rows of 16-byte vectors (a 32 KB tile);
+// row r of the tile is the contiguous range of kBlock vectors [r * kBlock,
+// (r + 1) * kBlock) and thread t owns vector t of every row.  The tile is
+// staged in shared memory by one bulk copy and scanned from there in two
+// passes, so a thread keeps only a few registers.  What bounds the bandwidth
+// is the bytes in flight per SM while tiles wait for their loads and
+// look-backs: registers would hold 128 KB of tiles per SM, shared memory
+// holds six 32 KB tiles.  Without the look-back this pipeline streams at
+// ~91 % of a device copy; the look-back chain (each tile waits for the
+// aggregates of all tiles before it) costs the rest.  Measured alternatives
+// on B200 (2^28 u32): 64 KB tiles x 3 per SM 0.63 ms, 128 KB x 1 0.72 ms,
+// 32 KB x 4 0.82 ms, this shape 0.61 ms; 512 threads x 4 rows held in
+// registers (2 per SM) 0.93 ms.
 template <class T> struct TileShape {
-  static constexpr uint32_t kBlock = 512;
-  static constexpr uint32_t kRows = 4;
+  static constexpr uint32_t kBlock = 256;
+  static constexpr uint32_t kRows = 8;
+  static constexpr uint32_t kMinBlocks = 6;
   static constexpr uint32_t kPerVec = 16 / sizeof(T);
   static constexpr uint32_t kTile = kBlock * kRows * kPerVec;
   static constexpr uint32_t kWarps = kBlock / kWarp;
