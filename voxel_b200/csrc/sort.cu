@@ -6,12 +6,13 @@
 //      (shared-memory counters per block, then one global atomicAdd per bin);
 //   2. one partition kernel per 8-bit digit:
 //        - dynamic tile id, so a tile only waits on tiles already running;
-//        - each warp loads 32 x kItems keys with coalesced row loads and ranks
-//          them by digit with __match_any_sync (stable: rank follows the
-//          original order inside the warp);
+//        - the tile's keys and payloads arrive in shared memory by bulk copies
+//          (TMA); each warp takes 32 x kItems of them and ranks them by digit
+//          with __match_any_sync (stable: rank follows the original order
+//          inside the warp);
 //        - warp counts are combined per digit, the tile publishes its digit
-//          counts and looks back over predecessor tiles per digit (bounded
-//          by the GPU timer);
+//          counts and looks back over predecessor tiles per digit, eight
+//          tiles per round trip (bounded by the GPU timer);
 //        - keys and payloads are first sorted inside the tile in shared
 //          memory, then written out in that order so consecutive threads write
 //          consecutive addresses of each digit's run.
@@ -36,9 +37,13 @@ constexpr uint32_t kMaxCount = (1u << 30) - 1u;
 constexpr uint32_t kRecAgg = 1u << 30, kRecInc = 2u << 30;
 constexpr uint32_t kRecValue = (1u << 30) - 1u;
 
+// Items per thread: small enough that four 256-thread blocks fit an SM
+// (64 registers, ~34 KB of shared memory each), which is what hides the
+// latency of the per-key ranking and the look-back.
 template <class K> struct Shape;
-template <> struct Shape<uint32_t> { static constexpr uint32_t kItems = 16; };
-template <> struct Shape<uint64_t> { static constexpr uint32_t kItems = 12; };
+template <> struct Shape<uint32_t> { static constexpr uint32_t kItems = 12; };
+template <> struct Shape<uint64_t> { static constexpr uint32_t kItems = 8; };
+constexpr uint32_t kPartitionBlocksPerSm = 4;
 
 template <class K> __host__ __device__ constexpr uint32_t tile_keys() {
   return kBlock * Shape<K>::kItems;
@@ -155,46 +160,72 @@ __device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
 }
 
 template <class K, bool HasValues>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
     partition_kernel(const K *__restrict__ in_keys,
                      const uint32_t *__restrict__ in_vals,
                      K *__restrict__ out_keys, uint32_t *__restrict__ out_vals,
                      uint32_t count, uint32_t shift, uint32_t mask,
                      const uint32_t *__restrict__ pass_hist,
                      uint32_t *records, uint32_t *tile_counter,
-                     uint32_t *status) {
+                     uint32_t *status, bool aligned) {
   constexpr uint32_t kItems = Shape<K>::kItems;
   constexpr uint32_t kTile = tile_keys<K>();
+  constexpr uint32_t kKeyBytes = kTile * sizeof(K);
+  constexpr uint32_t kValBytes = HasValues ? kTile * 4u : 0u;
+  __shared__ uint64_t s_bar;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_hist[kWarps][kBins];
   __shared__ uint32_t s_digit_off[kBins];
   __shared__ uint32_t s_global[kBins];
   __shared__ uint32_t s_tmp[kWarps];
-  __shared__ K s_keys[kTile];
-  __shared__ uint32_t s_vals[HasValues ? kTile : 1];
+  // The tile arrives here (input order), and later holds it sorted by digit.
+  __shared__ __align__(128) K s_keys[kTile];
+  __shared__ __align__(128) uint32_t s_vals[HasValues ? kTile : 1];
 
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
-  if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+  if (t == 0) {
+    const uint32_t tile = atomicAdd(tile_counter, 1u);
+    s_tile = tile;
+    if (aligned && static_cast<uint64_t>(tile + 1) * kTile <= count) {
+      const uint64_t b = static_cast<uint64_t>(tile) * kTile;
+      mbar_init(&s_bar, 1);
+      mbar_arrive_expect_tx(&s_bar, kKeyBytes + kValBytes);
+      bulk_load(s_keys, in_keys + b, kKeyBytes, &s_bar);
+      if (HasValues) bulk_load(s_vals, in_vals + b, kValBytes, &s_bar);
+    }
+  }
 #pragma unroll
   for (uint32_t w = 0; w < kWarps; ++w) s_warp_hist[w][t] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint64_t tile_base = static_cast<uint64_t>(tile) * kTile;
-  const uint64_t warp_base = tile_base + warp * kWarp * kItems;
+  const uint32_t valid_in_tile =
+      count - tile_base < kTile ? static_cast<uint32_t>(count - tile_base) : kTile;
+  if (aligned && valid_in_tile == kTile) {
+    if (!mbar_wait(&s_bar, 0)) {
+      // Never expected: report, let the copies land, give up on this tile.
+      if (t == 0) set_status(status, kDevTimeout);
+      mbar_wait(&s_bar, 0);
+      return;
+    }
+  } else {
+    for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
+      s_keys[j] = in_keys[tile_base + j];
+      if (HasValues) s_vals[j] = in_vals[tile_base + j];
+    }
+    __syncthreads();
+  }
+  const uint32_t warp_first = warp * kWarp * kItems; // tile-local index of item 0
+  const uint64_t warp_base = tile_base + warp_first;
 
   K key[kItems];
   uint32_t val[kItems];
-  uint32_t rank[kItems];
+  uint32_t rank2[(kItems + 1) / 2]; // two 16-bit ranks per register
 #pragma unroll
   for (uint32_t i = 0; i < kItems; ++i) {
-    const uint64_t idx = warp_base + i * kWarp + lane;
-    if (idx < count) {
-      key[i] = in_keys[idx];
-      if (HasValues) val[i] = in_vals[idx];
-    } else {
-      key[i] = K(0);
-      val[i] = 0;
-    }
+    const uint32_t j = warp_first + i * kWarp + lane;
+    key[i] = j < valid_in_tile ? s_keys[j] : K(0);
+    val[i] = HasValues && j < valid_in_tile ? s_vals[j] : 0u;
   }
 
   // Warp-level multi-split: rank each key among the warp's keys of its digit.
@@ -208,7 +239,9 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t leader = 31u - __clz(peers);
     uint32_t pre = 0;
     if (valid) pre = s_warp_hist[warp][d];
-    rank[i] = pre + below;
+    const uint32_t rk = pre + below;
+    if (i & 1u) rank2[i / 2] |= rk << 16;
+    else rank2[i / 2] = rk;
     __syncwarp();
     if (valid && lane == leader) s_warp_hist[warp][d] = pre + __popc(peers);
     __syncwarp();
@@ -227,18 +260,40 @@ __global__ void __launch_bounds__(kBlock)
   const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
   s_digit_off[t] = digit_off;
 
-  // Per-digit decoupled look-back over predecessor tiles.
+  // Per-digit decoupled look-back over predecessor tiles: thread t (digit t)
+  // reads the records of kWindow predecessors at once (independent loads, one
+  // round trip to L2), sums back to the nearest inclusive record and retries
+  // the window while a tile before that one has not published its count.
   uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
   uint32_t exclusive = 0;
   if (tile == 0) {
     st_relaxed_u32(rec, kRecInc | tile_count);
   } else {
+    constexpr uint32_t kWindow = 8;
     st_relaxed_u32(rec, kRecAgg | tile_count);
     const uint64_t t0 = global_ns();
     int64_t pred = static_cast<int64_t>(tile) - 1;
-    while (pred >= 0) {
-      const uint32_t r = ld_relaxed_u32(records + static_cast<size_t>(pred) * kBins + t);
-      if ((r & ~kRecValue) == 0) {
+    for (;;) {
+      uint32_t r[kWindow];
+#pragma unroll
+      for (uint32_t j = 0; j < kWindow; ++j)
+        r[j] = pred - static_cast<int64_t>(j) >= 0
+                   ? ld_relaxed_u32(records + static_cast<size_t>(pred - j) * kBins + t)
+                   : kRecInc;
+      uint32_t sum = 0;
+      bool found = false, wait = false;
+#pragma unroll
+      for (uint32_t j = 0; j < kWindow; ++j) {
+        if (found || wait) continue;
+        const uint32_t state = r[j] & ~kRecValue;
+        if (state == 0) {
+          wait = true;
+        } else {
+          sum += r[j] & kRecValue;
+          found = state == kRecInc;
+        }
+      }
+      if (wait) {
         if (global_ns() - t0 > kWaitLimitNs) {
           set_status(status, kDevTimeout);
           break;
@@ -246,9 +301,9 @@ __global__ void __launch_bounds__(kBlock)
         __nanosleep(20);
         continue;
       }
-      exclusive += r & kRecValue;
-      if ((r & ~kRecValue) == kRecInc) break;
-      --pred;
+      exclusive += sum;
+      if (found) break;
+      pred -= kWindow;
     }
     st_relaxed_u32(rec, kRecInc | (exclusive + tile_count));
   }
@@ -261,7 +316,8 @@ __global__ void __launch_bounds__(kBlock)
     const uint64_t idx = warp_base + i * kWarp + lane;
     if (idx < count) {
       const uint32_t d = digit_of(key[i], shift, mask);
-      const uint32_t pos = s_digit_off[d] + s_warp_hist[warp][d] + rank[i];
+      const uint32_t rk = (i & 1u) ? (rank2[i / 2] >> 16) : (rank2[i / 2] & 0xffffu);
+      const uint32_t pos = s_digit_off[d] + s_warp_hist[warp][d] + rk;
       s_keys[pos] = key[i];
       if (HasValues) s_vals[pos] = val[i];
     }
@@ -269,8 +325,6 @@ __global__ void __launch_bounds__(kBlock)
   __syncthreads();
 
   // Write the tile's runs out in order.
-  const uint32_t valid_in_tile =
-      count - tile_base < kTile ? static_cast<uint32_t>(count - tile_base) : kTile;
 #pragma unroll 4
   for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
     const K k = s_keys[j];
@@ -315,6 +369,7 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
 
   const uint32_t tiles = ceil_div(count, tile_keys<K>());
   K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
+  auto aligned16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
   uint32_t *src_v = values, *dst_v = l.tmp_vals;
   for (uint32_t p = 0; p < passes; ++p) {
     uint32_t *rec = l.records + static_cast<size_t>(p) * tiles * kBins;
@@ -322,11 +377,12 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
     if (values != nullptr)
       partition_kernel<K, true><<<tiles, kBlock, 0, stream>>>(
           src_k, src_v, dst_k, dst_v, count, info.shift[p], info.mask[p],
-          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1);
+          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1,
+          aligned16(src_k) && aligned16(src_v));
     else
       partition_kernel<K, false><<<tiles, kBlock, 0, stream>>>(
           src_k, nullptr, dst_k, nullptr, count, info.shift[p], info.mask[p],
-          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1);
+          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1, aligned16(src_k));
     VX_TRY_CUDA(cudaGetLastError());
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);
