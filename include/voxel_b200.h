@@ -67,6 +67,23 @@ vx_status vx_generate_primitives(const vx_edit_mix *mix, uint64_t seed,
                                  uint64_t stream, uint64_t count,
                                  vx_primitive *host_out);
 
+/* ---------------------------------------------------------------- tuning --
+ * Launch-shape knobs (partition items per thread and count publishing of the
+ * radix sort, the long-list threshold and grid of the edit pipelines).  Every
+ * allowed value gives the same results; they only trade speed, and
+ * voxel_b200/autotune.py picks them per device by timing.  Settings are
+ * process-wide and apply to launches made after the call.  The reference
+ * fixes these as template policies (cuda/sort/radix/onesweep/host.cuh,
+ * svt/hash_dag_gpu/config.cuh); there is no runtime counterpart. */
+uint32_t vx_tuning_count(void);
+const char *vx_tuning_name(uint32_t index);  /* NULL past the last knob */
+vx_status vx_tuning_options(const char *name, int64_t *host_values,
+                            uint32_t capacity, uint32_t *host_count);
+vx_status vx_tuning_get(const char *name, int64_t *host_value);
+/* VX_ERR_INVALID_VALUE for an unknown knob or a value it does not allow. */
+vx_status vx_tuning_set(const char *name, int64_t value);
+vx_status vx_tuning_reset(void);             /* back to the defaults */
+
 /* ------------------------------------------------------------------ scan --
  * In-place prefix sums over uint32 / uint64 with modular (wrapping)
  * arithmetic.  Replaces algo::cuda::scan::{exclusive,inclusive}_sum<T> and

@@ -1,0 +1,100 @@
+"""Every allowed value of every launch-shape knob computes the same result:
+radix sorts of each partition variant against the oracle's stable sort
+(partial tiles, unaligned arrays, duplicates), batched DAG / SVO edits under
+each edit setting against the oracle's canonical dumps; and a quick autotune
+run writes a valid settings file."""
+import itertools
+import json
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import voxel_b200 as vx
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _defaults():
+    vx.reset_tuning()
+    yield
+    vx.reset_tuning()
+
+
+def to_dev(a, device):
+    return torch.from_numpy(a.view(np.int64 if a.dtype == np.uint64 else np.int32)).to(device)
+
+
+@pytest.mark.parametrize("key_bytes,key_bits,n,offset", [
+    (4, 32, 1_000_003, 0), (4, 32, 100_000, 1), (4, 20, 3072 * 5, 0),
+    (8, 60, 700_001, 0), (8, 64, 65_537, 1), (8, 40, 2048 * 7, 0)])
+def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
+    rng = np.random.default_rng(n + key_bits)
+    dt = np.uint64 if key_bytes == 8 else np.uint32
+    keys = rng.integers(0, 2**63, n, dtype=np.uint64).astype(dt)
+    keys[::5] = keys[3]
+    vals = np.arange(n, dtype=np.uint32)
+    ek, ev = oracle.stable_sort_pairs(keys, vals, key_bits)
+    knob = "sort.items_u32" if key_bytes == 4 else "sort.items_u64"
+    for items, early in itertools.product(vx.tuning_options(knob),
+                                          vx.tuning_options("sort.early_counts")):
+        vx.set_tuning(knob, items)
+        vx.set_tuning("sort.early_counts", early)
+        # offset 1: the arrays start one element into a buffer (not 16-byte aligned)
+        kbuf = to_dev(np.concatenate([np.zeros(offset, dt), keys]), cuda)
+        vbuf = to_dev(np.concatenate([np.zeros(offset, np.uint32), vals]), cuda)
+        dk, dv = kbuf[offset:], vbuf[offset:]
+        vx.sort_pairs(dk, dv, key_bits)
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early)
+        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early)
+        dk = to_dev(keys.copy(), cuda)
+        vx.sort_pairs(dk, None, key_bits)
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, "keys only")
+
+
+def rand_prims(rng, n, world, rmax):
+    p = np.zeros(n, oracle.PRIM_DTYPE)
+    for i in range(n):
+        shape = int(rng.random() < 0.4)
+        op = int(rng.random() < 0.55)
+        r = rng.integers(0, rmax + 1, 3)
+        p[i] = (rng.integers(-3, world + 3, 3), (r[0], r[1] if shape else 0, r[2] if shape else 0),
+                shape | (op << 8) | ((1 if op else 0) << 16), 0)
+    return p
+
+
+def test_edit_settings_match_oracle(cuda):
+    depth = 6
+    world = 4 << depth
+    rng = np.random.default_rng(21)
+    prims = rand_prims(rng, 300, world, world // 4)
+    # a long primitive list at the root exercises the block-per-item path
+    t = oracle.terrain(seed=4, scale=1, caves=True)
+    expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
+    for big, bps in [(16, 2), (64, 8), (512, 16), (32, 4)]:
+        vx.set_tuning("edit.big_item", big)
+        vx.set_tuning("edit.blocks_per_sm", bps)
+        d = vx.HashDag(depth, 1 << 18, 64 << 20)
+        d.build_terrain(4, 1, True)
+        d.apply_primitives(vx.prims_to_device(prims, cuda))
+        assert d.status() == 0
+        assert oracle.DagCanon(*d.canonical()) == expect.dag(), (big, bps)
+        s = vx.Svo(depth, 1 << 18, 1 << 18, arena_bytes=64 << 20)
+        s.build_terrain(4, 1, True)
+        s.apply_primitives(vx.prims_to_device(prims, cuda))
+        assert s.status() == 0
+        assert oracle.SvoCanon(*s.canonical()) == expect.svo(), (big, bps)
+
+
+def test_quick_autotune_writes_settings(cuda, tmp_path):
+    from voxel_b200 import autotune
+    out = tmp_path / "tune.json"
+    res = autotune.main(["--quick", "--quiet", "--out", str(out)])
+    saved = json.loads(out.read_text())
+    assert saved["knobs"] == res["knobs"]
+    for name, value in saved["knobs"].items():
+        assert value in vx.tuning_options(name)
+    assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0,
+                           "edit.big_item": 64, "edit.blocks_per_sm": 16}

@@ -199,6 +199,12 @@ _SIGS = {
     "vx_dag_apply_terminal": (_ST, [_P, _P, _U32, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_rasterize_count": (_ST, [_P, _U32, _U32, _P, _P]),
     "vx_rasterize": (_ST, [_P, _U32, _U32, _P, _P, _P]),
+    "vx_tuning_count": (_U32, []),
+    "vx_tuning_name": (C.c_char_p, [_U32]),
+    "vx_tuning_options": (_ST, [C.c_char_p, C.POINTER(C.c_int64), _U32, C.POINTER(_U32)]),
+    "vx_tuning_get": (_ST, [C.c_char_p, C.POINTER(C.c_int64)]),
+    "vx_tuning_set": (_ST, [C.c_char_p, C.c_int64]),
+    "vx_tuning_reset": (_ST, []),
 }
 
 _lib = None
@@ -220,7 +226,35 @@ def lib() -> C.CDLL:
             fn.restype = res
             fn.argtypes = args
         _lib = l
+        _apply_saved_tuning()
     return _lib
+
+
+TUNING_DIR = Path(__file__).resolve().parent / "tuning"
+
+
+def tuning_file(device_name: str) -> Path:
+    """Where the autotuner keeps the knob settings for one kind of device."""
+    safe = "".join(ch if ch.isalnum() else "_" for ch in device_name).strip("_")
+    return TUNING_DIR / f"{safe}.json"
+
+
+def _apply_saved_tuning() -> None:
+    """Apply the autotuner's settings for the current device, if it has any
+    (voxel_b200/tuning/<device>.json, written by voxel_b200.autotune)."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return
+        path = tuning_file(torch.cuda.get_device_name())
+    except Exception:
+        return
+    if not path.exists():
+        return
+    import json
+    knobs = json.loads(path.read_text()).get("knobs", {})
+    for name, value in knobs.items():
+        _lib.vx_tuning_set(name.encode(), int(value))
 
 
 def exported_symbols() -> list[str]:

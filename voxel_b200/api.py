@@ -21,7 +21,36 @@ __all__ = [
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
     "COMPLETION_DTYPE", "TERMINAL_NODE_DTYPE", "TERMINAL_LEAF_DTYPE", "cell_prefix",
     "terminal_nodes", "terminal_leaves", "records_to_device",
+    "tuning", "tuning_options", "set_tuning", "reset_tuning",
 ]
+
+
+def tuning() -> dict:
+    """Current launch-shape knobs {name: value} (vx_tuning_*)."""
+    out = {}
+    for i in range(lib().vx_tuning_count()):
+        name = lib().vx_tuning_name(i)
+        v = C.c_int64()
+        check(lib().vx_tuning_get(name, C.byref(v)), "vx_tuning_get")
+        out[name.decode()] = v.value
+    return out
+
+
+def tuning_options(name: str) -> list[int]:
+    n = C.c_uint32()
+    check(lib().vx_tuning_options(name.encode(), None, 0, C.byref(n)), "vx_tuning_options")
+    vals = (C.c_int64 * n.value)()
+    check(lib().vx_tuning_options(name.encode(), vals, n.value, C.byref(n)),
+          "vx_tuning_options")
+    return list(vals)
+
+
+def set_tuning(name: str, value: int) -> None:
+    check(lib().vx_tuning_set(name.encode(), int(value)), f"vx_tuning_set({name}={value})")
+
+
+def reset_tuning() -> None:
+    check(lib().vx_tuning_reset(), "vx_tuning_reset")
 
 
 def stream_handle(stream: torch.cuda.Stream | None = None) -> int:

@@ -1,0 +1,185 @@
+"""Autotuner for the library's launch-shape knobs (vx_tuning_*).
+
+    python -m voxel_b200.autotune [--quick] [--out PATH]
+
+Times every allowed value of each knob on a representative workload on the
+current GPU and writes the fastest settings to voxel_b200/tuning/<device>.json,
+which the library applies when it is first loaded on that kind of device:
+
+  * sort.items_u32 / sort.items_u64 / sort.early_counts: radix-sort partition
+    tile size (items per thread, hence blocks per SM) and whether a tile
+    publishes its digit counts before or after ranking; timed on 2^26 u32 and
+    2^25 60-bit u64 key/value pairs;
+  * edit.big_item / edit.blocks_per_sm: the primitive-list length above which
+    a work item is expanded by a whole block, and the grid of the edit
+    pipelines' item kernels; timed on a batched Hash DAG edit (4096^3 cave
+    terrain at scale 16, 4096 spheres of radius log-uniform in [1, 256],
+    60 % add).
+
+Every setting's output is compared with the default setting's (the sorted
+arrays bit for bit, the edited DAG by 2^20 point queries) before its time
+counts, so a setting that computed something else is reported, not chosen.
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import lib
+from . import api as vx
+from . import tuning_file
+
+
+def _time(fn, reps: int, before=None) -> float:
+    """Median device time of fn() in ms (before() runs untimed each rep)."""
+    ts = []
+    for i in range(reps + 1):
+        if before is not None:
+            before()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        if i:  # the first run warms up
+            ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def tune_sort(n32: int, n64: int, reps: int, log) -> tuple[dict, dict]:
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    cases = {
+        "u32": (torch.randint(-(1 << 31), (1 << 31) - 1, (n32,), dtype=torch.int32,
+                              device="cuda", generator=g), 32, "sort.items_u32"),
+        "u64": (torch.randint(0, 1 << 60, (n64,), dtype=torch.int64, device="cuda",
+                              generator=g), 60, "sort.items_u64"),
+    }
+    times: dict = {}
+    for label, (keys0, bits, knob) in cases.items():
+        n = keys0.numel()
+        vals0 = torch.arange(n, dtype=torch.int32, device="cuda")
+        ws = torch.empty(lib().vx_sort_workspace_size(n, keys0.element_size()),
+                         dtype=torch.uint8, device="cuda")
+        k, v = keys0.clone(), vals0.clone()
+
+        def restore():
+            k.copy_(keys0)
+            v.copy_(vals0)
+
+        vx.reset_tuning()
+        restore()
+        vx.sort_pairs(k, v, bits, ws)
+        ref_k, ref_v = k.clone(), v.clone()
+        for items, early in itertools.product(vx.tuning_options(knob),
+                                              vx.tuning_options("sort.early_counts")):
+            vx.set_tuning(knob, items)
+            vx.set_tuning("sort.early_counts", early)
+            restore()
+            vx.sort_pairs(k, v, bits, ws)
+            same = bool(torch.equal(k, ref_k) and torch.equal(v, ref_v))
+            ms = _time(lambda: vx.sort_pairs(k, v, bits, ws), reps, restore) if same else None
+            times[f"{label} items={items} early={early}"] = ms
+            log(f"  sort {label} items={items} early={early}: "
+                + (f"{ms:.3f} ms" if same else "DIFFERENT OUTPUT (not used)"))
+    vx.reset_tuning()
+    best: dict = {}
+    early_opts = vx.tuning_options("sort.early_counts")
+    score = {}
+    for early in early_opts:
+        tot = 0.0
+        for label, (_, _, knob) in cases.items():
+            cand = [times[f"{label} items={i} early={early}"] for i in vx.tuning_options(knob)]
+            cand = [c for c in cand if c is not None]
+            tot = tot + min(cand) if cand else float("inf")
+        score[early] = tot
+    best["sort.early_counts"] = min(score, key=score.get)
+    for label, (_, _, knob) in cases.items():
+        opts = {i: times[f"{label} items={i} early={best['sort.early_counts']}"]
+                for i in vx.tuning_options(knob)}
+        opts = {i: t for i, t in opts.items() if t is not None}
+        best[knob] = min(opts, key=opts.get)
+    return best, times
+
+
+def tune_edit(depth: int, count: int, reps: int, log, max_nodes: int,
+              arena: int) -> tuple[dict, dict]:
+    prims = vx.prims_to_device(vx.config_c4_edits(count, seed=5, world_exp=depth + 2), "cuda")
+    pristine = vx.HashDag(depth, max_nodes, arena)
+    pristine.build_terrain(7, max(1, (4 << depth) // 256), True)  # C3's scale rule
+    if pristine.status() != 0:
+        raise RuntimeError("terrain build failed")
+    work = vx.HashDag(depth, max_nodes, arena)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(12)
+    pts = torch.randint(0, 4 << depth, (1 << 20, 3), dtype=torch.int32, device="cuda",
+                        generator=g)
+    vx.reset_tuning()
+    work.copy_from(pristine)
+    work.apply_primitives(prims)
+    if work.status() != 0:
+        raise RuntimeError("reference edit failed")
+    ref = work.query(pts)
+    times: dict = {}
+    for big, bps in itertools.product(vx.tuning_options("edit.big_item"),
+                                      vx.tuning_options("edit.blocks_per_sm")):
+        vx.set_tuning("edit.big_item", big)
+        vx.set_tuning("edit.blocks_per_sm", bps)
+        work.copy_from(pristine)
+        work.apply_primitives(prims)
+        ok = work.status() == 0 and bool(torch.equal(work.query(pts), ref))
+        ms = _time(lambda: work.apply_primitives(prims), reps,
+                   lambda: work.copy_from(pristine)) if ok else None
+        if ok and work.status() != 0:
+            ms = None
+        times[f"big_item={big} blocks_per_sm={bps}"] = ms
+        log(f"  edit big_item={big} blocks_per_sm={bps}: "
+            + (f"{ms:.3f} ms" if ms is not None else "FAILED OR DIFFERENT (not used)"))
+    vx.reset_tuning()
+    valid = {k: t for k, t in times.items() if t is not None}
+    key = min(valid, key=valid.get)
+    big = int(key.split()[0].split("=")[1])
+    bps = int(key.split()[1].split("=")[1])
+    return {"edit.big_item": big, "edit.blocks_per_sm": bps}, times
+
+
+def main(argv=None) -> dict:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--quick", action="store_true", help="small sizes (a test run)")
+    ap.add_argument("--out", default=None, help="output JSON (default: the device's file)")
+    ap.add_argument("--quiet", action="store_true")
+    args = ap.parse_args(argv)
+    log = (lambda m: None) if args.quiet else (lambda m: print(m, flush=True))
+    if not torch.cuda.is_available():
+        raise SystemExit("autotune needs a CUDA device")
+    dev = torch.cuda.get_device_name()
+    t0 = time.time()
+    if args.quick:
+        sort_best, sort_t = tune_sort(1 << 20, 1 << 19, 2, log)
+        edit_best, edit_t = tune_edit(6, 256, 2, log, 1 << 18, 64 << 20)
+    else:
+        sort_best, sort_t = tune_sort(1 << 26, 1 << 25, 5, log)
+        edit_best, edit_t = tune_edit(10, 4096, 5, log, 1 << 26, 4 << 30)
+    result = {
+        "device": dev,
+        "quick": bool(args.quick),
+        "seconds": round(time.time() - t0, 1),
+        "knobs": {**sort_best, **edit_best},
+        "timings_ms": {"sort": sort_t, "edit": edit_t},
+    }
+    out = args.out or str(tuning_file(dev))
+    from pathlib import Path
+    Path(out).parent.mkdir(parents=True, exist_ok=True)
+    Path(out).write_text(json.dumps(result, indent=1) + "\n")
+    log(f"best {result['knobs']} -> {out}")
+    return result
+
+
+if __name__ == "__main__":
+    main()

@@ -35,8 +35,10 @@ vx_status vx_workspace_status(const void *workspace, vx_stream stream) {
 // ------------------------------------------------------------ profiling --
 
 #include "profile.cuh"
+#include "tuning.cuh"
 
 #include <atomic>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -146,6 +148,84 @@ vx_status vx_generate_primitives(const vx_edit_mix *mix, uint64_t seed,
       mix->r_max < mix->r_min || mix->material_max < mix->material_min)
     return VX_ERR_INVALID_VALUE;
   vx_generate_primitives_host(mix, seed, stream, count, host_out);
+  return VX_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- tuning --
+
+namespace vx::tune {
+namespace {
+struct Knob {
+  const char *name;
+  int64_t def;
+  int64_t allowed[6];
+  uint32_t n_allowed;
+};
+// Defaults = the autotuner's choice on B200 (voxel_b200/tuning/NVIDIA_B200.json).
+constexpr Knob kKnobs[kKnobCount] = {
+    {"sort.items_u32", 16, {12, 16}, 2},
+    {"sort.items_u64", 12, {8, 12}, 2},
+    {"sort.early_counts", 0, {0, 1}, 2},
+    {"edit.big_item", 64, {16, 32, 64, 128, 256, 512}, 6},
+    {"edit.blocks_per_sm", 16, {2, 4, 8, 16, 32}, 5},
+};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {64}, {16}};
+
+int find(const char *name) {
+  if (name == nullptr) return -1;
+  for (uint32_t i = 0; i < kKnobCount; ++i)
+    if (std::strcmp(kKnobs[i].name, name) == 0) return static_cast<int>(i);
+  return -1;
+}
+} // namespace
+
+int64_t get(Id id) { return g_values[id].load(std::memory_order_relaxed); }
+
+} // namespace vx::tune
+
+extern "C" {
+
+uint32_t vx_tuning_count(void) { return vx::tune::kKnobCount; }
+
+const char *vx_tuning_name(uint32_t index) {
+  return index < vx::tune::kKnobCount ? vx::tune::kKnobs[index].name : nullptr;
+}
+
+vx_status vx_tuning_options(const char *name, int64_t *host_values, uint32_t capacity,
+                            uint32_t *host_count) {
+  const int i = vx::tune::find(name);
+  if (i < 0 || host_count == nullptr) return VX_ERR_INVALID_VALUE;
+  const auto &k = vx::tune::kKnobs[i];
+  *host_count = k.n_allowed;
+  if (host_values != nullptr)
+    for (uint32_t j = 0; j < k.n_allowed && j < capacity; ++j) host_values[j] = k.allowed[j];
+  return VX_OK;
+}
+
+vx_status vx_tuning_get(const char *name, int64_t *host_value) {
+  const int i = vx::tune::find(name);
+  if (i < 0 || host_value == nullptr) return VX_ERR_INVALID_VALUE;
+  *host_value = vx::tune::g_values[i].load();
+  return VX_OK;
+}
+
+vx_status vx_tuning_set(const char *name, int64_t value) {
+  const int i = vx::tune::find(name);
+  if (i < 0) return VX_ERR_INVALID_VALUE;
+  const auto &k = vx::tune::kKnobs[i];
+  for (uint32_t j = 0; j < k.n_allowed; ++j)
+    if (k.allowed[j] == value) {
+      vx::tune::g_values[i].store(value);
+      return VX_OK;
+    }
+  return VX_ERR_INVALID_VALUE;
+}
+
+vx_status vx_tuning_reset(void) {
+  for (uint32_t i = 0; i < vx::tune::kKnobCount; ++i)
+    vx::tune::g_values[i].store(vx::tune::kKnobs[i].def);
   return VX_OK;
 }
 

@@ -17,6 +17,7 @@
 // have the same ref, so an edit copies only the paths it changes.
 #include "edit_common.cuh"
 #include "profile.cuh"
+#include "tuning.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -414,9 +415,11 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
                        const uint32_t *d_count, uint32_t host_count,
                        cudaStream_t s, bool terrain = false) {
   Ctx x{d->t, d->a, prims, d_count, host_count};
-  const EditCtx e{d->t.hdr, d->a, prims, d_count, host_count, d->t.depth};
+  const EditCtx e{d->t.hdr, d->a, prims, d_count, host_count, d->t.depth,
+                  static_cast<uint32_t>(tune::get(tune::kEditBigItem))};
   const uint32_t depth = d->t.depth;
-  const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) *
+                        static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm));
   {
     prof::Scope sc("dag_init", s);
     init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),

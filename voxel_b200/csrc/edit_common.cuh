@@ -185,8 +185,8 @@ struct Arena {
   uint32_t big_cap;
 };
 
-// Items with more primitives than this are expanded by a whole block.
-constexpr uint32_t kBigItem = 64;
+// Items with more primitives than EditCtx::big_item (the tuning knob
+// "edit.big_item", 64 by default) are expanded by a whole block.
 
 
 // init_kernel's root_old value meaning "the root stored in the header".
@@ -200,6 +200,7 @@ struct EditCtx {
   const uint32_t *d_prim_count; // device count (NULL: use host_prim_count)
   uint32_t host_prim_count;
   uint32_t depth;
+  uint32_t big_item; // longer primitive lists go to expand_big_kernel
 };
 
 // A tree Policy supplies:
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(kBlock)
     const bool have = wi < W;
     Item it{};
     if (have) it = x.a.items[base + wi];
-    const bool big = have && it.pcount > kBigItem;
+    const bool big = have && it.pcount > x.big_item;
     if (big) {
       // Long lists go to expand_big_kernel (one block per item).
       if (c == 0) {

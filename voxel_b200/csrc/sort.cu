@@ -23,6 +23,7 @@
 // uncoalesced and whose look-back spin is unbounded.
 #include "common.cuh"
 #include "profile.cuh"
+#include "tuning.cuh"
 
 namespace vx::sort {
 
@@ -37,16 +38,24 @@ constexpr uint32_t kMaxCount = (1u << 30) - 1u;
 constexpr uint32_t kRecAgg = 1u << 30, kRecInc = 2u << 30;
 constexpr uint32_t kRecValue = (1u << 30) - 1u;
 
-// Items per thread: small enough that four 256-thread blocks fit an SM
-// (64 registers, ~34 KB of shared memory each), which is what hides the
-// latency of the per-key ranking and the look-back.
+// Items per thread of the partition kernel (the tile is 256 x items keys):
+// the small setting fits four blocks per SM (64 registers, ~35 KB of shared
+// memory each), the large one three with more keys per tile (on B200 the
+// large one is faster: 2.72 vs 3.13 ms for 2^26 u32 pairs).  The tuning
+// knobs "sort.items_u32" / "sort.items_u64" pick one per device.
 template <class K> struct Shape;
-template <> struct Shape<uint32_t> { static constexpr uint32_t kItems = 12; };
-template <> struct Shape<uint64_t> { static constexpr uint32_t kItems = 8; };
-constexpr uint32_t kPartitionBlocksPerSm = 4;
-
-template <class K> __host__ __device__ constexpr uint32_t tile_keys() {
-  return kBlock * Shape<K>::kItems;
+template <> struct Shape<uint32_t> {
+  static constexpr uint32_t kSmall = 12, kLarge = 16;
+};
+template <> struct Shape<uint64_t> {
+  static constexpr uint32_t kSmall = 8, kLarge = 12;
+};
+template <uint32_t Items, class K> constexpr uint32_t min_blocks() {
+  return Items == Shape<K>::kSmall ? 4u : 3u;
+}
+// Tiles of the small setting: the most tiles, so the workspace covers both.
+template <class K> inline uint32_t max_tiles(uint32_t count) {
+  return ceil_div(count, kBlock * Shape<K>::kSmall);
 }
 
 inline uint32_t pass_count(uint32_t key_bits) {
@@ -74,7 +83,7 @@ struct Layout {
 };
 
 template <class K> Layout carve(void *ws, uint32_t count, uint32_t passes) {
-  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  const uint32_t tiles = max_tiles<K>(count);
   Carver c(ws);
   Layout l;
   l.counters = c.take<uint32_t>(kMaxPasses + 2);
@@ -87,7 +96,7 @@ template <class K> Layout carve(void *ws, uint32_t count, uint32_t passes) {
 }
 
 template <class K> size_t workspace_bytes(uint32_t count, uint32_t passes) {
-  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  const uint32_t tiles = max_tiles<K>(count);
   Sizer s;
   s.take<uint32_t>(kMaxPasses + 2);
   s.take<uint32_t>(kMaxPasses * kBins);
@@ -159,8 +168,11 @@ __device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
   return r;
 }
 
-template <class K, bool HasValues>
-__global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
+// Early = publish the tile's digit counts (from a shared-atomic histogram)
+// before ranking, so later tiles' look-backs wait less; otherwise they are
+// published after ranking, from the per-warp counts.
+template <class K, bool HasValues, uint32_t kItems, bool Early>
+__global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     partition_kernel(const K *__restrict__ in_keys,
                      const uint32_t *__restrict__ in_vals,
                      K *__restrict__ out_keys, uint32_t *__restrict__ out_vals,
@@ -168,13 +180,13 @@ __global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
                      const uint32_t *__restrict__ pass_hist,
                      uint32_t *records, uint32_t *tile_counter,
                      uint32_t *status, bool aligned) {
-  constexpr uint32_t kItems = Shape<K>::kItems;
-  constexpr uint32_t kTile = tile_keys<K>();
+  constexpr uint32_t kTile = kBlock * kItems;
   constexpr uint32_t kKeyBytes = kTile * sizeof(K);
   constexpr uint32_t kValBytes = HasValues ? kTile * 4u : 0u;
   __shared__ uint64_t s_bar;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_hist[kWarps][kBins];
+  __shared__ uint32_t s_count[Early ? kBins : 1];
   __shared__ uint32_t s_digit_off[kBins];
   __shared__ uint32_t s_global[kBins];
   __shared__ uint32_t s_tmp[kWarps];
@@ -196,6 +208,7 @@ __global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
   }
 #pragma unroll
   for (uint32_t w = 0; w < kWarps; ++w) s_warp_hist[w][t] = 0;
+  if (Early) s_count[t] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint64_t tile_base = static_cast<uint64_t>(tile) * kTile;
@@ -228,6 +241,16 @@ __global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
     val[i] = HasValues && j < valid_in_tile ? s_vals[j] : 0u;
   }
 
+  uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
+  if (Early) {
+#pragma unroll
+    for (uint32_t i = 0; i < kItems; ++i)
+      if (warp_base + i * kWarp + lane < count)
+        atomicAdd(&s_count[digit_of(key[i], shift, mask)], 1u);
+    __syncthreads();
+    st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | s_count[t]);
+  }
+
   // Warp-level multi-split: rank each key among the warp's keys of its digit.
 #pragma unroll
   for (uint32_t i = 0; i < kItems; ++i) {
@@ -256,21 +279,19 @@ __global__ void __launch_bounds__(kBlock, kPartitionBlocksPerSm)
     s_warp_hist[w][t] = tile_count;
     tile_count += c;
   }
+  if (!Early) st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | tile_count);
   const uint32_t digit_off = block_exclusive_256(tile_count, s_tmp);
   const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
   s_digit_off[t] = digit_off;
 
-  // Per-digit decoupled look-back over predecessor tiles: thread t (digit t)
-  // reads the records of kWindow predecessors at once (independent loads, one
+  // Per-digit decoupled look-back over predecessor tiles (this tile's count
+  // is published): thread t (digit t) reads the records of kWindow
+  // predecessors at once (independent loads, one
   // round trip to L2), sums back to the nearest inclusive record and retries
   // the window while a tile before that one has not published its count.
-  uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
   uint32_t exclusive = 0;
-  if (tile == 0) {
-    st_relaxed_u32(rec, kRecInc | tile_count);
-  } else {
+  if (tile != 0) {
     constexpr uint32_t kWindow = 8;
-    st_relaxed_u32(rec, kRecAgg | tile_count);
     const uint64_t t0 = global_ns();
     int64_t pred = static_cast<int64_t>(tile) - 1;
     for (;;) {
@@ -367,22 +388,31 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
   }
   VX_TRY_CUDA(cudaGetLastError());
 
-  const uint32_t tiles = ceil_div(count, tile_keys<K>());
+  const bool large = tune::get(sizeof(K) == 4 ? tune::kSortItemsU32 : tune::kSortItemsU64) ==
+                     static_cast<int64_t>(Shape<K>::kLarge);
+  const bool early = tune::get(tune::kSortEarlyCounts) != 0;
+  const uint32_t items = large ? Shape<K>::kLarge : Shape<K>::kSmall;
+  const uint32_t tiles = ceil_div(count, kBlock * items);
   K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
-  auto aligned16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
   uint32_t *src_v = values, *dst_v = l.tmp_vals;
+  auto aligned16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
   for (uint32_t p = 0; p < passes; ++p) {
     uint32_t *rec = l.records + static_cast<size_t>(p) * tiles * kBins;
     prof::Scope scope(sizeof(K) == 4 ? "sort_partition_u32" : "sort_partition_u64", stream);
-    if (values != nullptr)
-      partition_kernel<K, true><<<tiles, kBlock, 0, stream>>>(
-          src_k, src_v, dst_k, dst_v, count, info.shift[p], info.mask[p],
-          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1,
-          aligned16(src_k) && aligned16(src_v));
-    else
-      partition_kernel<K, false><<<tiles, kBlock, 0, stream>>>(
-          src_k, nullptr, dst_k, nullptr, count, info.shift[p], info.mask[p],
-          l.hist + p * kBins, rec, l.counters + 2 + p, l.counters + 1, aligned16(src_k));
+    const bool aligned = aligned16(src_k) && (values == nullptr || aligned16(src_v));
+    auto launch = [&](auto kernel) {
+      kernel<<<tiles, kBlock, 0, stream>>>(src_k, src_v, dst_k, dst_v, count, info.shift[p],
+                                           info.mask[p], l.hist + p * kBins, rec,
+                                           l.counters + 2 + p, l.counters + 1, aligned);
+    };
+    constexpr uint32_t S = Shape<K>::kSmall, L = Shape<K>::kLarge;
+    if (values != nullptr) {
+      if (large) early ? launch(partition_kernel<K, true, L, true>) : launch(partition_kernel<K, true, L, false>);
+      else early ? launch(partition_kernel<K, true, S, true>) : launch(partition_kernel<K, true, S, false>);
+    } else {
+      if (large) early ? launch(partition_kernel<K, false, L, true>) : launch(partition_kernel<K, false, L, false>);
+      else early ? launch(partition_kernel<K, false, S, true>) : launch(partition_kernel<K, false, S, false>);
+    }
     VX_TRY_CUDA(cudaGetLastError());
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);

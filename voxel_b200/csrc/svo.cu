@@ -24,6 +24,7 @@
 #include "edit_common.cuh"
 #include "plain.cuh"
 #include "profile.cuh"
+#include "tuning.cuh"
 
 #include <algorithm>
 #include <new>
@@ -438,10 +439,12 @@ namespace vx::svo {
 vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_count,
                        uint32_t host_count, cudaStream_t s, bool terrain) {
   const Tables &t = v->t;
-  const EditCtx e{t.hdr, v->a, prims, d_count, host_count, t.depth};
+  const EditCtx e{t.hdr, v->a, prims, d_count, host_count, t.depth,
+                  static_cast<uint32_t>(tune::get(tune::kEditBigItem))};
   const SvoTree pol{t};
   const uint32_t depth = t.depth;
-  const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) *
+                        static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm));
   {
     prof::Scope sc("svo_init", s);
     begin_kernel<<<1, 1, 0, s>>>(t);

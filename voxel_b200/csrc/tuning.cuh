@@ -1,0 +1,21 @@
+// Launch-shape knobs read at launch time (process-wide; an autotuner sets
+// them per device through vx_tuning_set).  Every allowed value is a correct
+// configuration; the knobs only trade speed.
+#pragma once
+
+#include <cstdint>
+
+namespace vx::tune {
+
+enum Id : uint32_t {
+  kSortItemsU32,    // partition items per thread, u32 keys: 12 or 16
+  kSortItemsU64,    // partition items per thread, u64 keys: 8 or 12
+  kSortEarlyCounts, // publish tile digit counts before ranking: 0 or 1
+  kEditBigItem,     // items with more primitives go to the block-per-item expansion
+  kEditBlocksPerSm, // grid of the edit pipelines' item kernels, in blocks per SM
+  kKnobCount
+};
+
+int64_t get(Id id);
+
+} // namespace vx::tune
