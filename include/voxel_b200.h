@@ -386,6 +386,36 @@ typedef struct vx_svo_counters {
 vx_status vx_svo_get_counters(const vx_svo *svo, vx_svo_counters *host_counters,
                               vx_stream stream);
 
+/* --------------------------------------------------------------- graphs --
+ * A batched edit as a CUDA graph: the capture records every kernel, memset
+ * and copy of one edit; each vx_graph_launch replays them with one launch.
+ * The graph reads its input from the given device addresses when it runs
+ * (rewrite the buffers between launches; same addresses), keeps the
+ * structure's table addresses (valid while it lives, through resets,
+ * copies into it and compactions) and the tuning knobs of capture time.
+ * vx_*_graph_primitives: the list at `prims` of *device_count primitives
+ * (read on the device at each launch; at most `capacity`, else the edit is
+ * rejected with VX_ERR_INVALID_VALUE), or of `capacity` primitives when
+ * device_count is NULL.  vx_dag_graph_voxels: the plain path (sort, merge into
+ * leaf masks, rebuild) for `count` voxels at `edits` with op and workspace.
+ * Check results with vx_*_status after a launch.  The reference runs its
+ * pipelines as separate launches with host synchronisations (svt/hash_dag_gpu/
+ * detail/edit_pipeline.cuh:31-97); there is no counterpart. */
+typedef struct vx_graph vx_graph;
+vx_status vx_dag_graph_primitives(vx_dag *dag, const vx_primitive *prims,
+                                  const uint32_t *device_count, uint32_t capacity,
+                                  vx_graph **out);
+vx_status vx_dag_graph_voxels(vx_dag *dag, const vx_voxel *edits, uint32_t count,
+                              uint32_t op, void *workspace, size_t workspace_bytes,
+                              vx_graph **out);
+vx_status vx_svo_graph_primitives(vx_svo *svo, const vx_primitive *prims,
+                                  const uint32_t *device_count, uint32_t capacity,
+                                  vx_graph **out);
+vx_status vx_graph_launch(vx_graph *graph, vx_stream stream);
+/* Kernel launches one replay performs. */
+vx_status vx_graph_kernels(const vx_graph *graph, uint64_t *host_kernels);
+vx_status vx_graph_destroy(vx_graph *graph);
+
 /* ------------------------------------------------------- terminal edits --
  * Place or destroy whole octree cells and 4^3 bricks (svt/cuda/terminal/
  * types.cuh:15-31, detail/pipeline.cuh:27-222).  A node input is the cell at

@@ -199,6 +199,12 @@ _SIGS = {
     "vx_dag_apply_terminal": (_ST, [_P, _P, _U32, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_rasterize_count": (_ST, [_P, _U32, _U32, _P, _P]),
     "vx_rasterize": (_ST, [_P, _U32, _U32, _P, _P, _P]),
+    "vx_dag_graph_primitives": (_ST, [_P, _P, _P, _U32, C.POINTER(_P)]),
+    "vx_dag_graph_voxels": (_ST, [_P, _P, _U32, _U32, _P, _SZ, C.POINTER(_P)]),
+    "vx_svo_graph_primitives": (_ST, [_P, _P, _P, _U32, C.POINTER(_P)]),
+    "vx_graph_launch": (_ST, [_P, _P]),
+    "vx_graph_kernels": (_ST, [_P, C.POINTER(_U64)]),
+    "vx_graph_destroy": (_ST, [_P]),
     "vx_tuning_count": (_U32, []),
     "vx_tuning_name": (C.c_char_p, [_U32]),
     "vx_tuning_options": (_ST, [C.c_char_p, C.POINTER(C.c_int64), _U32, C.POINTER(_U32)]),

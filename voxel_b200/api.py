@@ -21,7 +21,7 @@ __all__ = [
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
     "COMPLETION_DTYPE", "TERMINAL_NODE_DTYPE", "TERMINAL_LEAF_DTYPE", "cell_prefix",
     "terminal_nodes", "terminal_leaves", "records_to_device",
-    "tuning", "tuning_options", "set_tuning", "reset_tuning",
+    "tuning", "tuning_options", "set_tuning", "reset_tuning", "Graph",
 ]
 
 
@@ -290,6 +290,46 @@ def _apply_terminal(fn, h, nodes, leaves, extra, workspace, device):
               ptr(ws), ws.numel(), stream_handle())
 
 
+class Graph:
+    """A captured edit (vx_*_graph_*): launch() replays it with one launch.
+    Keeps the captured buffers alive; the structure must outlive it."""
+
+    def __init__(self, handle, keep):
+        self._h = handle
+        self._keep = keep
+
+    def launch(self) -> None:
+        check(lib().vx_graph_launch(self._h, stream_handle()), "vx_graph_launch")
+
+    @property
+    def kernels(self) -> int:
+        n = C.c_uint64()
+        check(lib().vx_graph_kernels(self._h, C.byref(n)), "vx_graph_kernels")
+        return n.value
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_graph_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _graph_primitives(fn, owner, prims, device_count, capacity):
+    n = prims.numel() // 8
+    cap = capacity if capacity is not None else n
+    if cap > n:
+        raise ValueError("capacity exceeds the primitive buffer")
+    h = C.c_void_p()
+    check(fn(owner._h, ptr(prims), ptr(device_count), cap, C.byref(h)), "graph capture")
+    return Graph(h, (owner, prims, device_count))
+
+
 class HashDag:
     """Hash DAG resident on the GPU (HashDagGpu / DeviceHashDagGpu,
     hash_dag_gpu/storage.cuh:16-105, widened to depth 1..14)."""
@@ -339,6 +379,25 @@ class HashDag:
         TERMINAL_NODE_DTYPE / TERMINAL_LEAF_DTYPE records; returns the status."""
         return _apply_terminal(lib().vx_dag_apply_terminal, self._h, nodes, leaves, (op,),
                                workspace, device)
+
+    def graph_primitives(self, prims: torch.Tensor, device_count: torch.Tensor | None = None,
+                         capacity: int | None = None) -> "Graph":
+        """Capture the batched edit of `prims` (int32 [n, 8]) as a CUDA graph;
+        with device_count (one int32 on the device) each launch edits that
+        many primitives (at most capacity)."""
+        return _graph_primitives(lib().vx_dag_graph_primitives, self, prims, device_count,
+                                 capacity)
+
+    def graph_voxels(self, voxels: torch.Tensor, op: int,
+                     workspace: torch.Tensor | None = None) -> "Graph":
+        """Capture the plain path (sort, merge, rebuild) for a voxel list."""
+        n = voxels.numel() // 3
+        ws = workspace if workspace is not None else torch.empty(
+            self.workspace_size(n), dtype=torch.uint8, device=voxels.device)
+        h = C.c_void_p()
+        check(lib().vx_dag_graph_voxels(self._h, ptr(voxels), n, op, ptr(ws), ws.numel(),
+                                        C.byref(h)), "vx_dag_graph_voxels")
+        return Graph(h, (self, voxels, ws))
 
     def apply_primitives(self, prims: torch.Tensor) -> None:
         """Batched path: primitives applied as if in order; asynchronous
@@ -497,6 +556,11 @@ class Svo:
         svt/cuda/terminal/detail/pipeline.cuh:200-222); returns the status."""
         return _apply_terminal(lib().vx_svo_apply_terminal, self._h, nodes, leaves,
                                (op, material), workspace, device)
+
+    def graph_primitives(self, prims: torch.Tensor, device_count: torch.Tensor | None = None,
+                         capacity: int | None = None) -> "Graph":
+        return _graph_primitives(lib().vx_svo_graph_primitives, self, prims, device_count,
+                                 capacity)
 
     def apply_primitives(self, prims: torch.Tensor) -> None:
         n = prims.numel() // 8

@@ -69,8 +69,16 @@ bool enabled() { return reg().on; }
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void add_launches(int64_t n) {
+  g_launches.fetch_add(static_cast<uint64_t>(n), std::memory_order_relaxed);
+}
 
 void record(const char *name, cudaStream_t stream, bool start) {
+  // Inside a stream capture (a CUDA graph being built) nothing is timed.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return;
   Registry &r = reg();
   std::lock_guard<std::mutex> lock(r.mu);
   cudaEvent_t ev;

@@ -16,6 +16,7 @@
 // Structural sharing is by content: two equal subtrees of a level always
 // have the same ref, so an edit copies only the paths it changes.
 #include "edit_common.cuh"
+#include "graph.cuh"
 #include "profile.cuh"
 #include "tuning.cuh"
 
@@ -675,6 +676,31 @@ vx_status vx_dag_apply_primitives(vx_dag *d, const vx_primitive *prims,
   if (d == nullptr || (prims == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
   if (count == 0) return VX_OK;
   return run_pipeline(d, prims, nullptr, count, static_cast<cudaStream_t>(stream));
+}
+
+vx_status vx_dag_graph_primitives(vx_dag *d, const vx_primitive *prims,
+                                  const uint32_t *device_count, uint32_t capacity,
+                                  vx_graph **out) {
+  if (d == nullptr || out == nullptr || prims == nullptr || capacity == 0)
+    return VX_ERR_INVALID_VALUE;
+  return vx::graph::capture(
+      [&](cudaStream_t s) { return run_pipeline(d, prims, device_count, capacity, s); }, out);
+}
+
+vx_status vx_dag_graph_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count, uint32_t op,
+                              void *workspace, size_t workspace_bytes, vx_graph **out) {
+  if (d == nullptr || out == nullptr || edits == nullptr || count == 0 || op > 1)
+    return VX_ERR_INVALID_VALUE;
+  if (workspace == nullptr || workspace_bytes < vx_dag_voxel_workspace_size(count))
+    return VX_ERR_INVALID_VALUE;
+  return vx::graph::capture(
+      [&](cudaStream_t s) {
+        const vx_primitive *prims = nullptr;
+        const uint32_t *n = nullptr;
+        VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));
+        return run_pipeline(d, prims, n, count, s);
+      },
+      out);
 }
 
 vx_status vx_dag_status(vx_dag *d, vx_stream stream) {

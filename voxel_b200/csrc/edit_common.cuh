@@ -216,7 +216,13 @@ struct EditCtx {
 
 static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
   Header *h = x.hdr;
-  const uint32_t n = x.d_prim_count ? *x.d_prim_count : x.host_prim_count;
+  // With a device-side count, host_prim_count is the capacity of the list.
+  const uint32_t dn = x.d_prim_count ? *x.d_prim_count : 0u;
+  if (x.d_prim_count && dn > x.host_prim_count) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_status(&h->status, kDevInvalid);
+    return;
+  }
+  const uint32_t n = x.d_prim_count ? dn : x.host_prim_count;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     for (uint32_t l = 0; l < 16; ++l) {
       h->item_off[l] = 0;

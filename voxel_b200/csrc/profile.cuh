@@ -8,11 +8,15 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 namespace vx::prof {
 
 bool enabled();
 void record(const char *name, cudaStream_t stream, bool start);
 void count_launch();
+uint64_t launch_count();
+void add_launches(int64_t n); // graph replays add, captures take back
 
 struct Scope {
   const char *name;

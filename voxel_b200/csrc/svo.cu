@@ -23,6 +23,7 @@
 // reports VX_ERR_CAPACITY and changes nothing.
 #include "edit_common.cuh"
 #include "plain.cuh"
+#include "graph.cuh"
 #include "profile.cuh"
 #include "tuning.cuh"
 
@@ -628,6 +629,16 @@ vx_status vx_svo_apply_primitives(vx_svo *v, const vx_primitive *prims,
   if (v == nullptr || (prims == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
   if (count == 0) return VX_OK;
   return run_pipeline(v, prims, nullptr, count, static_cast<cudaStream_t>(stream), false);
+}
+
+vx_status vx_svo_graph_primitives(vx_svo *v, const vx_primitive *prims,
+                                  const uint32_t *device_count, uint32_t capacity,
+                                  vx_graph **out) {
+  if (v == nullptr || out == nullptr || prims == nullptr || capacity == 0)
+    return VX_ERR_INVALID_VALUE;
+  return vx::graph::capture(
+      [&](cudaStream_t s) { return run_pipeline(v, prims, device_count, capacity, s, false); },
+      out);
 }
 
 vx_status vx_svo_status(vx_svo *v, vx_stream stream) {
