@@ -478,6 +478,23 @@ def run_dag(args, ws, rank, local, torch, vx, device):
     e2e = {"value": round(voxels_batch * e_steps / (e2e_ms / 1e3), 1),
            "unit": "voxels/s", "h2d_bytes_per_step": int(prims.numel() * 4),
            "d2h_bytes_per_step": 4, "ms_per_step": round(e2e_ms / e_steps, 3)}
+    # The same batch replayed as a CUDA graph (one launch per edit).
+    graph = work.graph_primitives(prims)
+    g_ms = 0.0
+    for i in range(steps + 1):
+        work.copy_from(pristine)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        graph.launch()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i:
+            g_ms += a.elapsed_time(b)
+    if work.status() != 0:
+        raise RuntimeError("graph replay of the batched edit failed")
+    graph_kernels = graph.kernels
+    graph.close()
     dag_bytes = ts.bytes_reserved
     del work, pristine
     torch.cuda.empty_cache()
@@ -488,6 +505,7 @@ def run_dag(args, ws, rank, local, torch, vx, device):
         "pairs_per_level": pairs, "kernels": kern, "plain": plain, "e2e": e2e,
         "launches": int(launches), "clocks": clk.summary(),
         "dag_bytes_reserved": int(dag_bytes),
+        "graph_ms": g_ms / steps, "graph_kernels": int(graph_kernels),
     }
 
 
@@ -784,6 +802,10 @@ def run_ours(args, ws, rank, local):
             "dag_kernel_ms": {n: round(v[1], 3) for n, v in k.items()},
             "dag_kernel_share": {n: round(v[1] / total_k, 3) for n, v in k.items()} if total_k else {},
             "dag_bytes_reserved": dag["dag_bytes_reserved"],
+            "batched_graph_ms_per_batch": round(dag["graph_ms"], 3),
+            "batched_graph_voxels_per_s": round(dag["voxels_batch"] / (dag["graph_ms"] / 1e3), 1),
+            "batched_graph_kernels": dag["graph_kernels"],
+            "tuning": vx.tuning(),
             **svo,
             **serve,
             **sweep,

@@ -477,7 +477,8 @@ typedef struct vx_serve_config {
     uint32_t max_batch_requests; /* requests per launch (0 = unlimited, 1 = one each) */
     double compact_at_fill;      /* compact above this table fill (0 = 0.5) */
     uint32_t max_inflight;       /* launches in flight, 1 or 2 (0 = 2) */
-    uint32_t reserved;
+    uint32_t launch_mode;        /* 0 = one CUDA graph launch per batch,
+                                    1 = the pipeline's kernels one by one */
 } vx_serve_config;
 
 typedef struct vx_serve_completion {

@@ -94,3 +94,14 @@ def test_serving_with_compaction_between_batches(cuda):
     assert stats.compactions > 0
     t = oracle.terrain(5, 1, True)
     assert canon(dag) == oracle.Grid(DEPTH).terrain(t).apply_prims(prims).dag()
+
+
+def test_graph_and_direct_launches_agree(cuda):
+    """The per-slot CUDA graphs and the kernel-by-kernel launches serve the
+    same stream to the same final DAG."""
+    arr, sizes, prims = stream(seed=23)
+    a = fresh_dag()
+    run(a, arr, sizes, prims, graphs=True)
+    b = fresh_dag()
+    run(b, arr, sizes, prims, graphs=False)
+    assert canon(a) == canon(b)

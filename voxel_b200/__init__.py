@@ -92,7 +92,7 @@ class vx_dag_stats(C.Structure):
 class vx_serve_config(C.Structure):
     _fields_ = [("max_batch_prims", C.c_uint32), ("max_batch_requests", C.c_uint32),
                 ("compact_at_fill", C.c_double), ("max_inflight", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("launch_mode", C.c_uint32)]
 
 
 class vx_serve_stats(C.Structure):

@@ -636,10 +636,10 @@ class Server:
     """Request loop over a resident HashDag with continuous batching."""
 
     def __init__(self, dag: HashDag, max_batch_prims: int = 0, max_batch_requests: int = 0,
-                 compact_at_fill: float = 0.0, max_inflight: int = 0):
+                 compact_at_fill: float = 0.0, max_inflight: int = 0, graphs: bool = True):
         from . import vx_serve_config
         cfg = vx_serve_config(max_batch_prims, max_batch_requests, compact_at_fill,
-                              max_inflight, 0)
+                              max_inflight, 0 if graphs else 1)
         h = C.c_void_p()
         check(lib().vx_serve_create(dag._h, C.byref(cfg), C.byref(h)), "vx_serve_create")
         self._h = h

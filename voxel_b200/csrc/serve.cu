@@ -5,7 +5,9 @@
 // order.  A worker thread coalesces every queued request into one batch (up
 // to max_batch_prims primitives / max_batch_requests requests), copies it
 // from pinned host memory and launches the batched edit on the server's
-// stream; up to max_inflight batches are in flight, so requests that arrive
+// stream (one CUDA graph per upload slot, captured at creation, which reads
+// the batch size from device memory, so a batch is two copies and one
+// launch); up to max_inflight batches are in flight, so requests that arrive
 // while the GPU works on one batch are admitted into the next as soon as a
 // slot frees, and their upload overlaps the running edit.  A completion
 // thread waits for each batch's event, stamps every request of the batch with
@@ -66,6 +68,10 @@ struct vx_server {
   // two upload slots: pinned host buffer, device buffer, header copy
   vx_primitive *h_buf[2] = {nullptr, nullptr};
   vx_primitive *d_buf[2] = {nullptr, nullptr};
+  // per slot: a graph of the batched edit reading its batch size from d_count
+  uint32_t *h_count = nullptr; // pinned, one word per slot
+  uint32_t *d_count = nullptr; // one word per slot
+  vx_graph *graph[2] = {nullptr, nullptr};
   unsigned char *h_hdr[2] = {nullptr, nullptr};
   bool slot_busy[2] = {false, false};
   std::vector<unsigned char> last_hdr; // header copy of the last completed batch
@@ -168,7 +174,16 @@ void worker_loop(vx_server *s) {
     cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
     cudaMemcpyAsync(s->d_buf[b.slot], s->h_buf[b.slot], b.nprims * sizeof(vx_primitive),
                     cudaMemcpyHostToDevice, s->stream);
-    if (b.nprims) vx_dag_apply_primitives(s->dag, s->d_buf[b.slot], b.nprims, s->stream);
+    if (s->graph[b.slot] != nullptr) {
+      // The slot is not reused before this batch completes, so its pinned
+      // count word is stable until the copy runs.
+      s->h_count[b.slot] = b.nprims;
+      cudaMemcpyAsync(s->d_count + b.slot, s->h_count + b.slot, sizeof(uint32_t),
+                      cudaMemcpyHostToDevice, s->stream);
+      vx_graph_launch(s->graph[b.slot], s->stream);
+    } else if (b.nprims) {
+      vx_dag_apply_primitives(s->dag, s->d_buf[b.slot], b.nprims, s->stream);
+    }
     cudaMemcpyAsync(s->h_hdr[b.slot], vx::dag::device_header(s->dag), vx::dag::header_bytes(),
                     cudaMemcpyDeviceToHost, s->stream);
     cudaEventRecord(b.done, s->stream);
@@ -286,9 +301,21 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
     if (e == cudaSuccess) e = cudaMalloc(&s->d_buf[k], s->hard_cap * sizeof(vx_primitive));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_hdr[k], vx::dag::header_bytes());
   }
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_count, 2 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&s->d_count, 2 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     vx_serve_destroy(s);
     return vx::from_cuda(e);
+  }
+  if (s->cfg.launch_mode == 0) {
+    for (int k = 0; k < 2; ++k) {
+      const vx_status st = vx_dag_graph_primitives(dag, s->d_buf[k], s->d_count + k,
+                                                    s->hard_cap, &s->graph[k]);
+      if (st != VX_OK) {
+        vx_serve_destroy(s);
+        return st;
+      }
+    }
   }
   s->worker = std::thread(worker_loop, s);
   s->completer = std::thread(completer_loop, s);
@@ -355,10 +382,13 @@ vx_status vx_serve_destroy(vx_server *s) {
   if (s->completer.joinable()) s->completer.join();
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (int k = 0; k < 2; ++k) {
+    if (s->graph[k]) vx_graph_destroy(s->graph[k]);
     if (s->h_buf[k]) cudaFreeHost(s->h_buf[k]);
     if (s->d_buf[k]) cudaFree(s->d_buf[k]);
     if (s->h_hdr[k]) cudaFreeHost(s->h_hdr[k]);
   }
+  if (s->h_count) cudaFreeHost(s->h_count);
+  if (s->d_count) cudaFree(s->d_count);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return VX_OK;
