@@ -49,9 +49,11 @@ BYTES_SORT_U64 = 200    # 8 passes x (read 12 + write 12) + 8 histogram read
 # Per-launch algorithmic bytes of the dominant kernel (one u64 partition
 # pass: read key 8 + value 4, write key 8 + value 4 per element).
 PART_U64_BYTES = N_SORT * 24
-# DRAM bytes per sort_partition_u64 launch from ncu (profiles/), scaled to
-# 2^28 elements; None until a capture is committed.
-PART_U64_TRAFFIC = None
+# DRAM bytes per sort_partition_u64 launch: the ncu capture of a 2^24-key
+# pass (profiles/sort_partition_u64_2p24.md: 202.8 + 158.7 MB) scaled by the
+# keys of a launch here (2^28).  At 2^24 part of the input stays in L2, so
+# this is a lower bound for the full size.
+PART_U64_TRAFFIC = round((202.8e6 + 158.7e6) / (1 << 24) * N_SORT)
 DAG_DEPTH = 12            # inner levels: world side 4 << 12 = 16384
 DAG_SCALE = 64            # terrain generator scale (height 8192 + 2560 v)
 DAG_SEED = 7
@@ -59,9 +61,11 @@ DAG_EDITS = 16384
 DAG_MAX_NODES = 1 << 27
 DAG_ARENA = 16 << 30
 PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
-# DRAM bytes per dag_leafparent launch from ncu (profiles/); None until a
-# capture of this workload is committed.
-LEAFPARENT_TRAFFIC = None
+# DRAM bytes per dag_leafparent work item: the ncu capture of the small case
+# (profiles/dag_leafparent_4096cube.md: 438.1 + 216.8 MB) divided by that
+# launch's 5,280,796 items (bench.py --case dag --elements 4096); the
+# roofline's `traffic` scales it by the full launch's items.
+LEAFPARENT_TRAFFIC_PER_ITEM = (438.1e6 + 216.8e6) / 5280796
 SVO_C3_DEPTH = 10         # 4096^3
 SVO_C3_EDITS = 65536
 SERVE_DEPTH = 11          # 8192^3
@@ -819,7 +823,8 @@ def run_ours(args, ws, rank, local):
             "peak_kind": kind,
             "unit": "GB/s",
             "frac": round(lp_achieved / hbm, 4) if lp_achieved else None,
-            "traffic": LEAFPARENT_TRAFFIC,
+            "traffic": (round(LEAFPARENT_TRAFFIC_PER_ITEM * lp_items)
+                        if LEAFPARENT_TRAFFIC_PER_ITEM else None),
             "algorithmic_bytes_per_launch": lp_bytes,
             "launches": lp_n,
             "avg_launch_ms": round(lp_ms / lp_n, 3) if lp_n else None,
@@ -1041,6 +1046,9 @@ def run_case(args):
             t = time.perf_counter()
             dag.apply_primitives(prims)
             assert dag.status() == 0
+            es = dag.stats()
+            print(json.dumps({"edit_items": list(es.items_per_level)[:depth],
+                              "edit_pairs": list(es.pairs_per_level)[:depth]}))
         torch.cuda.synchronize()
         ms.append((time.perf_counter() - t) * 1e3)
     print(json.dumps({"case": args.case, "elements": n, "ms": ms}))

@@ -38,20 +38,22 @@ def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
     vals = np.arange(n, dtype=np.uint32)
     ek, ev = oracle.stable_sort_pairs(keys, vals, key_bits)
     knob = "sort.items_u32" if key_bytes == 4 else "sort.items_u64"
-    for items, early in itertools.product(vx.tuning_options(knob),
-                                          vx.tuning_options("sort.early_counts")):
+    for items, early, ballots in itertools.product(vx.tuning_options(knob),
+                                                   vx.tuning_options("sort.early_counts"),
+                                                   vx.tuning_options("sort.rank_ballots")):
         vx.set_tuning(knob, items)
         vx.set_tuning("sort.early_counts", early)
+        vx.set_tuning("sort.rank_ballots", ballots)
         # offset 1: the arrays start one element into a buffer (not 16-byte aligned)
         kbuf = to_dev(np.concatenate([np.zeros(offset, dt), keys]), cuda)
         vbuf = to_dev(np.concatenate([np.zeros(offset, np.uint32), vals]), cuda)
         dk, dv = kbuf[offset:], vbuf[offset:]
         vx.sort_pairs(dk, dv, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early)
-        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early)
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots)
+        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early, ballots)
         dk = to_dev(keys.copy(), cuda)
         vx.sort_pairs(dk, None, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, "keys only")
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, "keys only")
 
 
 def rand_prims(rng, n, world, rmax):
@@ -96,5 +98,5 @@ def test_quick_autotune_writes_settings(cuda, tmp_path):
     assert saved["knobs"] == res["knobs"]
     for name, value in saved["knobs"].items():
         assert value in vx.tuning_options(name)
-    assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0,
-                           "edit.big_item": 64, "edit.blocks_per_sm": 16}
+    assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0, "sort.rank_ballots": 1,
+                           "edit.big_item": 32, "edit.blocks_per_sm": 32}

@@ -176,10 +176,11 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.items_u32", 16, {12, 16}, 2},
     {"sort.items_u64", 12, {8, 12}, 2},
     {"sort.early_counts", 0, {0, 1}, 2},
-    {"edit.big_item", 64, {16, 32, 64, 128, 256, 512}, 6},
-    {"edit.blocks_per_sm", 16, {2, 4, 8, 16, 32}, 5},
+    {"sort.rank_ballots", 1, {0, 1}, 2},
+    {"edit.big_item", 32, {16, 32, 64, 128, 256, 512}, 6},
+    {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
 };
-std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {64}, {16}};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {32}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

@@ -186,7 +186,7 @@ struct Arena {
 };
 
 // Items with more primitives than EditCtx::big_item (the tuning knob
-// "edit.big_item", 64 by default) are expanded by a whole block.
+// "edit.big_item", 32 by default) are expanded by a whole block.
 
 
 // init_kernel's root_old value meaning "the root stored in the header".

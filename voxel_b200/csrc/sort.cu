@@ -25,6 +25,8 @@
 #include "profile.cuh"
 #include "tuning.cuh"
 
+#include <type_traits>
+
 namespace vx::sort {
 
 constexpr uint32_t kRadixBits = 8;
@@ -171,7 +173,11 @@ __device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
 // Early = publish the tile's digit counts (from a shared-atomic histogram)
 // before ranking, so later tiles' look-backs wait less; otherwise they are
 // published after ranking, from the per-warp counts.
-template <class K, bool HasValues, uint32_t kItems, bool Early>
+// Ballots = find a key's peers (the lanes of its warp with the same digit)
+// with one ballot per digit bit (warp-level multi-split, Adinets & Merrill)
+// instead of __match_any_sync, which executes on a narrow pipe and bounds
+// the pass when every key is ranked with it.
+template <class K, bool HasValues, uint32_t kItems, bool Early, bool Ballots>
 __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     partition_kernel(const K *__restrict__ in_keys,
                      const uint32_t *__restrict__ in_vals,
@@ -257,7 +263,19 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     const uint64_t idx = warp_base + i * kWarp + lane;
     const bool valid = idx < count;
     const uint32_t d = valid ? digit_of(key[i], shift, mask) : kBins;
-    const uint32_t peers = __match_any_sync(kFullMask, d);
+    uint32_t peers;
+    if (Ballots) {
+      const uint32_t vb = __ballot_sync(kFullMask, valid);
+      peers = valid ? vb : ~vb;
+#pragma unroll
+      for (uint32_t b = 0; b < kRadixBits; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bb = __ballot_sync(kFullMask, bit);
+        peers &= bit ? bb : ~bb;
+      }
+    } else {
+      peers = __match_any_sync(kFullMask, d);
+    }
     const uint32_t below = __popc(peers & lanemask_lt());
     const uint32_t leader = 31u - __clz(peers);
     uint32_t pre = 0;
@@ -391,6 +409,7 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
   const bool large = tune::get(sizeof(K) == 4 ? tune::kSortItemsU32 : tune::kSortItemsU64) ==
                      static_cast<int64_t>(Shape<K>::kLarge);
   const bool early = tune::get(tune::kSortEarlyCounts) != 0;
+  const bool ballots = tune::get(tune::kSortRankBallots) != 0;
   const uint32_t items = large ? Shape<K>::kLarge : Shape<K>::kSmall;
   const uint32_t tiles = ceil_div(count, kBlock * items);
   K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
@@ -406,13 +425,23 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
                                            l.counters + 2 + p, l.counters + 1, aligned);
     };
     constexpr uint32_t S = Shape<K>::kSmall, L = Shape<K>::kLarge;
-    if (values != nullptr) {
-      if (large) early ? launch(partition_kernel<K, true, L, true>) : launch(partition_kernel<K, true, L, false>);
-      else early ? launch(partition_kernel<K, true, S, true>) : launch(partition_kernel<K, true, S, false>);
-    } else {
-      if (large) early ? launch(partition_kernel<K, false, L, true>) : launch(partition_kernel<K, false, L, false>);
-      else early ? launch(partition_kernel<K, false, S, true>) : launch(partition_kernel<K, false, S, false>);
-    }
+    // (values, items, early, ballots) -> one of 16 instantiations
+    auto pick = [&](auto hv) {
+      constexpr bool HV = decltype(hv)::value;
+      if (large) {
+        if (early) ballots ? launch(partition_kernel<K, HV, L, true, true>)
+                           : launch(partition_kernel<K, HV, L, true, false>);
+        else ballots ? launch(partition_kernel<K, HV, L, false, true>)
+                     : launch(partition_kernel<K, HV, L, false, false>);
+      } else {
+        if (early) ballots ? launch(partition_kernel<K, HV, S, true, true>)
+                           : launch(partition_kernel<K, HV, S, true, false>);
+        else ballots ? launch(partition_kernel<K, HV, S, false, true>)
+                     : launch(partition_kernel<K, HV, S, false, false>);
+      }
+    };
+    if (values != nullptr) pick(std::true_type{});
+    else pick(std::false_type{});
     VX_TRY_CUDA(cudaGetLastError());
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);

@@ -11,6 +11,7 @@ enum Id : uint32_t {
   kSortItemsU32,    // partition items per thread, u32 keys: 12 or 16
   kSortItemsU64,    // partition items per thread, u64 keys: 8 or 12
   kSortEarlyCounts, // publish tile digit counts before ranking: 0 or 1
+  kSortRankBallots, // rank keys with per-bit ballots (1) or match_any (0)
   kEditBigItem,     // items with more primitives go to the block-per-item expansion
   kEditBlocksPerSm, // grid of the edit pipelines' item kernels, in blocks per SM
   kKnobCount
