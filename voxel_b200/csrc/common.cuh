@@ -93,6 +93,12 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Acquire / release fence at GPU scope: after a relaxed load that observed a
+// release store, it makes the writer's earlier stores visible.
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
 // Streaming 128-bit load that does not allocate in L1 (read-once data).
 __device__ __forceinline__ uint4 ld_stream_u4(const uint4 *p) {
   uint4 v;

@@ -102,15 +102,22 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
   return kEmptyRef;
 }
 
+// Probes use relaxed loads.  An item found through a published entry is
+// read after an acquire fence only when it was inserted by this edit (its
+// offset is at or above pool_mark, the pool use when the edit's inserts
+// began): items from earlier launches are visible without one, and most
+// matches of an edit are such pre-existing subtrees.  Inserts publish with a
+// release store.
 __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
                                         const uint32_t *w, uint32_t n) {
   const uint64_t h = hash_words(w, n);
   const uint32_t tag = static_cast<uint32_t>(h >> 32) | 1u;
   uint64_t *idx = t.index[l];
   uint32_t *pool = t.pool[l];
+  const uint32_t mark = t.hdr->pool_mark[l];
   uint64_t pos = h & t.index_mask[l];
   for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
-    uint64_t v = ld_acquire_u64(idx + pos);
+    uint64_t v = ld_relaxed_u64(idx + pos);
     if (v == 0) {
       const uint64_t claim = (static_cast<uint64_t>(tag) << 32) | kBusy;
       const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos),
@@ -140,10 +147,11 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
             return kEmptyRef;
           }
           __nanosleep(64);
-          r = static_cast<uint32_t>(ld_acquire_u64(idx + pos));
+          r = static_cast<uint32_t>(ld_relaxed_u64(idx + pos));
         }
       }
       if (r >= 2u) {
+        if (r - 2u >= mark) fence_acq_rel_gpu(); // inserted by this edit
         const uint32_t *item = pool + (r - 2u);
         bool eq = true;
         for (uint32_t i = 0; i < n && eq; ++i) eq = item[i] == w[i];
@@ -213,10 +221,15 @@ struct DagTree {
   }
 };
 
+// pool_mark = pool_used of every level, before the edit inserts anything.
+__global__ void mark_pools_kernel(Tables t) {
+  if (threadIdx.x < kMaxDepth) t.hdr->pool_mark[threadIdx.x] = t.hdr->pool_used[threadIdx.x];
+}
+
 // Level depth - 1: evaluate the 8 leaves of every item (8 threads per item)
 // and hash-cons the item.
 template <bool Terrain>
-__global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
+__global__ void __launch_bounds__(kBlock, 4) leafparent_kernel(Ctx x) {
   Header *h = x.t.hdr;
   if (ld_relaxed_u32(&h->status) != kDevOk) return;
   const uint32_t l = x.t.depth - 1;
@@ -227,10 +240,15 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
   const uint32_t lane = lane_id();
   const uint64_t total = static_cast<uint64_t>(W) * 8u;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  // The item's primitives, 8 at a time: lane c of the group loads the c-th
+  // (one parallel load instead of 8 lanes walking the list).
+  __shared__ vx_primitive s_pr[kBlock / 8][8];
+  const uint32_t grp = threadIdx.x >> 3;
+  const uint32_t gmask = 0xffu << (lane & ~7u);
   for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
        g0 < total; g0 += stride) {
     const uint64_t g = g0 + lane;
-    const bool have = g < total;
+    const bool have = g < total; // the same for the 8 lanes of a group
     const uint32_t wi = static_cast<uint32_t>(g >> 3), c = lane & 7u;
     uint32_t result = kEmptyRef;
     Item it{};
@@ -244,7 +262,12 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(Ctx x) {
       uint64_t mask = 0;
       bool loaded = false, touched = false;
       for (uint32_t k = 0; k < it.pcount; ++k) {
-        const vx_primitive pr = x.prims[pairs[it.pstart + k]];
+        if ((k & 7u) == 0) {
+          __syncwarp(gmask); // the previous chunk is no longer read
+          if (k + c < it.pcount) s_pr[grp][c] = x.prims[pairs[it.pstart + k + c]];
+          __syncwarp(gmask);
+        }
+        const vx_primitive pr = s_pr[grp][k & 7u];
         const uint32_t cls = classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
         if (cls == VX_CELL_EMPTY) continue;
         const bool add = vx_prim_op(&pr) == VX_OP_ADD;
@@ -446,6 +469,11 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
     }
     VX_TRY_CUDA(cudaGetLastError());
   }
+  {
+    prof::Scope sc("dag_mark_pools", s);
+    mark_pools_kernel<<<1, 32, 0, s>>>(d->t);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
   {
     prof::Scope sc("dag_leafparent", s);
     if (terrain)

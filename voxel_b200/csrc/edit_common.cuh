@@ -174,6 +174,7 @@ struct Header {
   uint64_t node_count[16];      // items inserted per table (DAG)
   uint32_t pool_used[16];       // words used per level pool (DAG)
   uint32_t big_count[16];       // items deferred to the block-per-item path
+  uint32_t pool_mark[16];       // pool_used before this edit's inserts (DAG)
 };
 
 struct Arena {
