@@ -99,4 +99,4 @@ def test_quick_autotune_writes_settings(cuda, tmp_path):
     for name, value in saved["knobs"].items():
         assert value in vx.tuning_options(name)
     assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0, "sort.rank_ballots": 1,
-                           "edit.big_item": 32, "edit.blocks_per_sm": 32}
+                           "edit.big_item": 32, "edit.blocks_per_sm": 16}

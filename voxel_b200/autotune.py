@@ -149,9 +149,18 @@ def tune_edit(depth: int, count: int, reps: int, log, max_nodes: int,
             + (f"{ms:.3f} ms" if ms is not None else "FAILED OR DIFFERENT (not used)"))
     vx.reset_tuning()
     valid = {k: t for k, t in times.items() if t is not None}
-    key = min(valid, key=valid.get)
-    big = int(key.split()[0].split("=")[1])
-    bps = int(key.split()[1].split("=")[1])
+    # Among settings within 2 % of the fastest, take the smallest grid: on a
+    # large batch more blocks gain little, while on small batches (the
+    # serving loop's) every extra block is launch overhead.
+    fastest = min(valid.values())
+    near = [k for k, t in valid.items() if t <= 1.02 * fastest]
+
+    def parse(k):
+        big, bps = (int(f.split("=")[1]) for f in k.split())
+        return big, bps
+
+    key = min(near, key=lambda k: (parse(k)[1], valid[k]))
+    big, bps = parse(key)
     return {"edit.big_item": big, "edit.blocks_per_sm": bps}, times
 
 

@@ -178,9 +178,9 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.early_counts", 0, {0, 1}, 2},
     {"sort.rank_ballots", 1, {0, 1}, 2},
     {"edit.big_item", 32, {16, 32, 64, 128, 256, 512}, 6},
-    {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
+    {"edit.blocks_per_sm", 16, {2, 4, 8, 16, 32}, 5},
 };
-std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {32}};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {16}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;
