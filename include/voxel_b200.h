@@ -386,6 +386,48 @@ typedef struct vx_svo_counters {
 vx_status vx_svo_get_counters(const vx_svo *svo, vx_svo_counters *host_counters,
                               vx_stream stream);
 
+/* ------------------------------------------------------- device views --
+ * Trivially copyable views for user kernels that read the structures with
+ * the __device__ functions of voxel_b200_device.cuh (vx_dag_get_voxel,
+ * vx_svo_get_voxel, vx_slab_set_contains_warp, vx_cuckoo_find), the
+ * counterparts of the reference's view() / device_view() and its device read
+ * functions (svt/hash_dag_gpu/device_view.cuh:14-31, svt/cuda/device_view.cuh:
+ * 11-44, cuda/hash_table/slab_hash/set/device.cuh).  All pointers are device
+ * pointers, valid while the structure lives; the DAG view reads the current
+ * root at each lookup. */
+typedef struct vx_dag_view {
+    uint32_t depth;
+    uint32_t reserved;
+    const uint32_t *root;      /* the published root ref */
+    const uint32_t *pool[14];  /* inner items of levels 0..depth-1 */
+    const uint64_t *leaves;    /* leaf masks (ref - 2 = slot) */
+} vx_dag_view;
+
+typedef struct vx_svo_view {
+    uint32_t depth;
+    uint32_t materials;
+    const uint32_t *nodes;          /* 8 child words per node, root = node 0 */
+    const uint64_t *leaves;         /* leaf masks */
+    const uint8_t *materials_data;  /* 64 bytes per leaf (materials only) */
+} vx_svo_view;
+
+typedef struct vx_slab_set_view {
+    const void *slabs;       /* buckets then overflow slabs, 128 bytes each */
+    uint32_t bucket_count;
+    uint32_t capacity;       /* overflow slabs */
+} vx_slab_set_view;
+
+typedef struct vx_cuckoo_view {
+    const void *slots;       /* 16-byte slots {key, value | hash id << 32} */
+    uint32_t slot_count;
+    uint32_t reserved;
+} vx_cuckoo_view;
+
+vx_status vx_dag_device_view(const vx_dag *dag, vx_dag_view *out);
+vx_status vx_svo_device_view(const vx_svo *svo, vx_svo_view *out);
+vx_status vx_slab_set_device_view(const vx_slab_set *set, vx_slab_set_view *out);
+vx_status vx_cuckoo_device_view(const vx_cuckoo *map, vx_cuckoo_view *out);
+
 /* --------------------------------------------------------------- graphs --
  * A batched edit as a CUDA graph: the capture records every kernel, memset
  * and copy of one edit; each vx_graph_launch replays them with one launch.

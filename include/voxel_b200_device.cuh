@@ -1,0 +1,177 @@
+/* voxel_b200_device.cuh - device-side lookups for user kernels (nvcc only).
+ *
+ * The reference's read paths are __device__ functions that user kernels call
+ * directly: svt::hash_dag_gpu::get_voxel (svt/hash_dag_gpu/query.cuh:12-39),
+ * svt::cuda::get_voxel (svt/cuda/query.cuh:11-35), the warp-cooperative
+ * DeviceSlabHashSetU32::contains (cuda/hash_table/slab_hash/set/
+ * device.cuh:148-234) and cuckoo_find (cuda/cuckoo_hash.cuh:101-120).  This
+ * header gives the same reads over this library's structures: get a view on
+ * the host (vx_dag_device_view, vx_svo_device_view, vx_slab_set_device_view,
+ * vx_cuckoo_device_view in voxel_b200.h), pass it to a kernel by value and
+ * call the functions below.  The library's own query kernels use these same
+ * functions.  A view stays valid while its structure lives; concurrent edits
+ * of the structure race with reads, as in the reference.
+ */
+#ifndef VOXEL_B200_DEVICE_CUH
+#define VOXEL_B200_DEVICE_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "voxel_b200.h"
+
+#define VX_SVO_CHILD_BIT (1u << 30)  /* child_data: a child node / leaf exists */
+#define VX_SVO_FILLED_BIT (1u << 31) /* child_data: uniform region is filled */
+#define VX_SVO_INDEX_MASK ((1u << 30) - 1u)
+
+/* ---------------------------------------------------------------- hashing */
+
+/* splitmix64 finaliser (Steele, Lea & Flood 2014): the tables' hash. */
+__host__ __device__ __forceinline__ uint64_t vx_mix64(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+
+/* A 64-bit hash mapped onto [0, n) by a multiply-high. */
+__device__ __forceinline__ uint32_t vx_reduce_hash(uint64_t h, uint32_t n) {
+  return (uint32_t)__umul64hi(h, (uint64_t)n);
+}
+
+/* Slot of key under cuckoo hash function hid (0..3) in a table of n slots. */
+__device__ __forceinline__ uint32_t vx_cuckoo_slot(uint64_t key, uint32_t hid, uint32_t n) {
+  const uint64_t salt = hid == 0 ? 0x9e3779b97f4a7c15ull
+                      : hid == 1 ? 0xc2b2ae3d27d4eb4full
+                      : hid == 2 ? 0x165667b19e3779f9ull
+                                 : 0x27d4eb2f165667c5ull;
+  return vx_reduce_hash(vx_mix64(key ^ salt), n);
+}
+
+__device__ __forceinline__ uint64_t vx_ld_relaxed_u64(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+/* ------------------------------------------------------------- Hash DAG -- */
+
+/* Child c (x | y << 1 | z << 2) of the inner item at `item`:
+ * [child_mask | fill_mask << 8, child refs of child_mask in order].
+ * Returns a ref (0 empty, 1 full, else item / leaf slot + 2). */
+__device__ __forceinline__ uint32_t vx_dag_item_child(const uint32_t *item, uint32_t c) {
+  const uint32_t header = item[0];
+  const uint32_t cm = header & 0xffu, fm = (header >> 8) & 0xffu;
+  const uint32_t bit = 1u << c;
+  if (cm & bit) return item[1 + __popc(cm & (bit - 1u))];
+  return (fm & bit) ? 1u : 0u;
+}
+
+/* 1 if voxel (x, y, z) is filled, 0 if empty or outside the world. */
+__device__ __forceinline__ uint8_t vx_dag_get_voxel(const vx_dag_view &v, uint32_t x,
+                                                    uint32_t y, uint32_t z) {
+  const uint32_t side_exp = v.depth + 2;
+  if ((x >> side_exp) | (y >> side_exp) | (z >> side_exp)) return 0;
+  uint32_t ref = *v.root;
+  for (uint32_t l = 0; l < v.depth && ref >= 2u; ++l) {
+    const uint32_t s = side_exp - 1 - l;
+    const uint32_t c = ((x >> s) & 1u) | (((y >> s) & 1u) << 1) | (((z >> s) & 1u) << 2);
+    ref = vx_dag_item_child(v.pool[l] + (ref - 2u), c);
+  }
+  if (ref <= 1u) return (uint8_t)ref;
+  const uint32_t bit = (x & 3u) + 4u * (y & 3u) + 16u * (z & 3u);
+  return (uint8_t)((v.leaves[ref - 2u] >> bit) & 1ull);
+}
+
+/* ------------------------------------------------------------------ SVO -- */
+
+/* Value of a child word without a child: material (or 1 without materials)
+ * when filled, 0 when empty. */
+__device__ __forceinline__ uint32_t vx_svo_word_value(uint32_t w, bool materials) {
+  return (w & VX_SVO_FILLED_BIT) ? (materials ? (w & 0xffu) : 1u) : 0u;
+}
+
+/* Material of voxel (x, y, z) (1 for filled without materials), 0 if empty
+ * or outside the world. */
+__device__ __forceinline__ uint8_t vx_svo_get_voxel(const vx_svo_view &v, uint32_t x,
+                                                    uint32_t y, uint32_t z) {
+  const uint32_t side_exp = v.depth + 2;
+  const bool mats = v.materials != 0;
+  if ((x >> side_exp) | (y >> side_exp) | (z >> side_exp)) return 0;
+  uint32_t w = VX_SVO_CHILD_BIT; /* root node 0 */
+  for (uint32_t l = 0; l < v.depth && (w & VX_SVO_CHILD_BIT); ++l) {
+    const uint32_t s = side_exp - 1 - l;
+    const uint32_t c = ((x >> s) & 1u) | (((y >> s) & 1u) << 1) | (((z >> s) & 1u) << 2);
+    w = v.nodes[(size_t)(w & VX_SVO_INDEX_MASK) * 8u + c];
+  }
+  if (!(w & VX_SVO_CHILD_BIT)) return (uint8_t)vx_svo_word_value(w, mats);
+  const uint32_t li = w & VX_SVO_INDEX_MASK;
+  const uint32_t bit = (x & 3u) + 4u * (y & 3u) + 16u * (z & 3u);
+  if (mats) return v.materials_data[(size_t)li * 64u + bit];
+  return (uint8_t)((v.leaves[li] >> bit) & 1ull);
+}
+
+/* ---------------------------------------------------------- hash tables -- */
+
+/* Cuckoo find: true and *value if key is present. */
+__device__ __forceinline__ bool vx_cuckoo_find(const vx_cuckoo_view &v, uint64_t key,
+                                               uint32_t *value) {
+  if (key == VX_HASH_EMPTY_KEY || key == VX_HASH_DELETED_KEY) return false;
+  const ulonglong2 *slots = (const ulonglong2 *)v.slots;
+#pragma unroll
+  for (uint32_t h = 0; h < 4; ++h) {
+    const uint32_t s = vx_cuckoo_slot(key, h, v.slot_count);
+    ulonglong2 e;
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+                 : "=l"(e.x), "=l"(e.y)
+                 : "l"(slots + s)
+                 : "memory");
+    if (e.x == key) {
+      *value = (uint32_t)e.y;
+      return true;
+    }
+  }
+  return false;
+}
+
+/* Slab set membership, warp-cooperative: all 32 lanes of a warp call it
+ * together (the reference's contract), each with its key and whether it is
+ * active; each half-warp walks one key's chain at a time, a 128-byte slab
+ * (15 keys + link) per coalesced read.  Returns true for an active lane whose
+ * key is present. */
+__device__ __forceinline__ bool vx_slab_set_contains_warp(const vx_slab_set_view &v,
+                                                          uint64_t key, bool active) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t sub = lane & 15u;
+  const uint32_t half = lane >> 4;
+  const uint32_t hmask = half ? 0xffff0000u : 0x0000ffffu;
+  const uint64_t *slabs = (const uint64_t *)v.slabs;
+  if (key == VX_HASH_EMPTY_KEY || key == VX_HASH_DELETED_KEY) active = false;
+  bool found = false;
+  uint32_t queue = __ballot_sync(0xffffffffu, active) & hmask;
+  while (queue) {
+    const uint32_t src = __ffs(queue) - 1u;
+    const uint64_t k = __shfl_sync(hmask, key, src);
+    uint64_t slab = vx_reduce_hash(vx_mix64(k), v.bucket_count);
+    bool hit = false;
+    /* a chain is at most the pool long: the loop ends even on a damaged table */
+    for (uint64_t step = 0; step <= (uint64_t)v.capacity; ++step) {
+      const uint64_t w = vx_ld_relaxed_u64(slabs + slab * 16u + sub);
+      hit = (__ballot_sync(hmask, sub < 15u && w == k) & hmask) != 0;
+      if (hit) break;
+      const uint64_t link = __shfl_sync(hmask, w, (half << 4) + 15u);
+      if (link == ~0ull) break;
+      slab = link;
+    }
+    if (lane == src) {
+      found = hit;
+      active = false;
+    }
+    queue = __ballot_sync(hmask, active) & hmask;
+  }
+  return found;
+}
+
+#endif /* VOXEL_B200_DEVICE_CUH */

@@ -47,3 +47,14 @@ def test_compat_header_compiles_and_links(tmp_path):
            "-lvoxel_b200", "-L", "/usr/local/cuda/lib64", "-lcudart", "-o", str(exe)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+@pytest.mark.skipif(shutil.which("nvcc") is None, reason="no nvcc")
+def test_device_header_compiles_for_sm100a(tmp_path):
+    """A user kernel built against voxel_b200_device.cuh (cross-compiled for
+    sm_100a here; run by tests/test_gpu_device_api.py on a GPU)."""
+    obj = tmp_path / "user.o"
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-c",
+           str(ROOT / "tests" / "user_kernels.cu"), "-I", str(ROOT / "include"), "-o", str(obj)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr

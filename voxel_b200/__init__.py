@@ -89,6 +89,24 @@ class vx_dag_stats(C.Structure):
                 ("status", C.c_uint32)]
 
 
+class vx_dag_view(C.Structure):
+    _fields_ = [("depth", C.c_uint32), ("reserved", C.c_uint32), ("root", C.c_void_p),
+                ("pool", C.c_void_p * 14), ("leaves", C.c_void_p)]
+
+
+class vx_svo_view(C.Structure):
+    _fields_ = [("depth", C.c_uint32), ("materials", C.c_uint32), ("nodes", C.c_void_p),
+                ("leaves", C.c_void_p), ("materials_data", C.c_void_p)]
+
+
+class vx_slab_set_view(C.Structure):
+    _fields_ = [("slabs", C.c_void_p), ("bucket_count", C.c_uint32), ("capacity", C.c_uint32)]
+
+
+class vx_cuckoo_view(C.Structure):
+    _fields_ = [("slots", C.c_void_p), ("slot_count", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class vx_serve_config(C.Structure):
     _fields_ = [("max_batch_prims", C.c_uint32), ("max_batch_requests", C.c_uint32),
                 ("compact_at_fill", C.c_double), ("max_inflight", C.c_uint32),
@@ -205,6 +223,10 @@ _SIGS = {
     "vx_graph_launch": (_ST, [_P, _P]),
     "vx_graph_kernels": (_ST, [_P, C.POINTER(_U64)]),
     "vx_graph_destroy": (_ST, [_P]),
+    "vx_dag_device_view": (_ST, [_P, C.POINTER(vx_dag_view)]),
+    "vx_svo_device_view": (_ST, [_P, C.POINTER(vx_svo_view)]),
+    "vx_slab_set_device_view": (_ST, [_P, C.POINTER(vx_slab_set_view)]),
+    "vx_cuckoo_device_view": (_ST, [_P, C.POINTER(vx_cuckoo_view)]),
     "vx_tuning_count": (_U32, []),
     "vx_tuning_name": (C.c_char_p, [_U32]),
     "vx_tuning_options": (_ST, [C.c_char_p, C.POINTER(C.c_int64), _U32, C.POINTER(_U32)]),

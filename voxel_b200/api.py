@@ -140,6 +140,13 @@ class SlabHashSet:
         self.bucket_count = bucket_count
         self.slab_capacity = slab_capacity
 
+    def device_view(self):
+        """View for user kernels (voxel_b200_device.cuh vx_slab_set_contains_warp)."""
+        from . import vx_slab_set_view
+        v = vx_slab_set_view()
+        check(lib().vx_slab_set_device_view(self._h, C.byref(v)), "vx_slab_set_device_view")
+        return v
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
@@ -185,6 +192,13 @@ class CuckooMap:
               "vx_cuckoo_create")
         self._h = h
         self.slot_count = slot_count
+
+    def device_view(self):
+        """View for user kernels (voxel_b200_device.cuh vx_cuckoo_find)."""
+        from . import vx_cuckoo_view
+        v = vx_cuckoo_view()
+        check(lib().vx_cuckoo_device_view(self._h, C.byref(v)), "vx_cuckoo_device_view")
+        return v
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -341,6 +355,13 @@ class HashDag:
         check(lib().vx_dag_create(C.byref(cfg), C.byref(h)), "vx_dag_create")
         self._h = h
         self.depth = depth
+
+    def device_view(self):
+        """View for user kernels (voxel_b200_device.cuh vx_dag_get_voxel)."""
+        from . import vx_dag_view
+        v = vx_dag_view()
+        check(lib().vx_dag_device_view(self._h, C.byref(v)), "vx_dag_device_view")
+        return v
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -522,6 +543,13 @@ class Svo:
         self._h = h
         self.depth = depth
         self.materials = materials
+
+    def device_view(self):
+        """View for user kernels (voxel_b200_device.cuh vx_svo_get_voxel)."""
+        from . import vx_svo_view
+        v = vx_svo_view()
+        check(lib().vx_svo_device_view(self._h, C.byref(v)), "vx_svo_device_view")
+        return v
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -29,7 +29,7 @@ FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 
 
 def _headers_mtime() -> float:
-    paths = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
+    paths = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h")) + list((ROOT / "include").glob("*.cuh"))
     return max((p.stat().st_mtime for p in paths), default=0.0)
 
 

@@ -16,6 +16,7 @@
 // Structural sharing is by content: two equal subtrees of a level always
 // have the same ref, so an edit copies only the paths it changes.
 #include "edit_common.cuh"
+#include "voxel_b200_device.cuh"
 #include "graph.cuh"
 #include "profile.cuh"
 #include "tuning.cuh"
@@ -68,16 +69,12 @@ __device__ __forceinline__ uint64_t read_leaf(const Tables &t, uint32_t ref) {
   return t.leaves[ref - 2];
 }
 
-// Child c of the node `ref` at inner level l (refs 0/1 are uniform subtrees).
+// Child c of the node `ref` at inner level l (refs 0/1 are uniform subtrees);
+// the item format is read by voxel_b200_device.cuh's vx_dag_item_child.
 __device__ __forceinline__ uint32_t child_ref(const Tables &t, uint32_t l,
                                               uint32_t ref, uint32_t c) {
   if (ref <= kFullRef) return ref;
-  const uint32_t *item = t.pool[l] + (ref - 2);
-  const uint32_t header = item[0];
-  const uint32_t cm = header & 0xffu, fm = (header >> 8) & 0xffu;
-  const uint32_t bit = 1u << c;
-  if (cm & bit) return item[1 + __popc(cm & (bit - 1u))];
-  return (fm & bit) ? kFullRef : kEmptyRef;
+  return vx_dag_item_child(t.pool[l] + (ref - 2), c);
 }
 
 // ---------------------------------------------------------- hash-consing --
@@ -323,28 +320,12 @@ __global__ void publish_kernel(Ctx x) {
   if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;
 }
 
-__global__ void query_kernel(Tables t, const vx_voxel *pts, uint32_t n,
+__global__ void query_kernel(vx_dag_view v, const vx_voxel *pts, uint32_t n,
                              uint8_t *out) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   const vx_voxel p = pts[i];
-  const uint32_t side_exp = t.depth + 2;
-  if ((p.x >> side_exp) | (p.y >> side_exp) | (p.z >> side_exp)) {
-    out[i] = 0;
-    return;
-  }
-  uint32_t ref = t.hdr->root;
-  for (uint32_t l = 0; l < t.depth && ref >= 2u; ++l) {
-    const uint32_t s = side_exp - 1 - l;
-    const uint32_t c = ((p.x >> s) & 1u) | (((p.y >> s) & 1u) << 1) | (((p.z >> s) & 1u) << 2);
-    ref = child_ref(t, l, ref, c);
-  }
-  if (ref <= kFullRef) {
-    out[i] = static_cast<uint8_t>(ref);
-    return;
-  }
-  const uint32_t bit = (p.x & 3u) + 4u * (p.y & 3u) + 16u * (p.z & 3u);
-  out[i] = static_cast<uint8_t>((t.leaves[ref - 2] >> bit) & 1ull);
+  out[i] = vx_dag_get_voxel(v, p.x, p.y, p.z);
 }
 
 // ------------------------------------------------------- plain path prep --
@@ -758,8 +739,20 @@ vx_status vx_dag_query(const vx_dag *d, const vx_voxel *pts, uint32_t count,
   if (count == 0) return VX_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   vx::prof::Scope sc("dag_query", s);
-  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(d->t, pts, count, out);
+  vx_dag_view view;
+  VX_TRY(vx_dag_device_view(d, &view));
+  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, pts, count, out);
   return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_dag_device_view(const vx_dag *d, vx_dag_view *out) {
+  if (d == nullptr || out == nullptr) return VX_ERR_INVALID_VALUE;
+  *out = vx_dag_view{};
+  out->depth = d->t.depth;
+  out->root = &d->t.hdr->root;
+  for (uint32_t l = 0; l < d->t.depth; ++l) out->pool[l] = d->t.pool[l];
+  out->leaves = d->t.leaves;
+  return VX_OK;
 }
 
 vx_status vx_dag_get_stats(const vx_dag *d, vx_dag_stats *st, vx_stream stream) {

@@ -19,6 +19,7 @@
 // hand, reports VX_HASH_OVERFLOW and counts it.
 #include "common.cuh"
 #include "profile.cuh"
+#include "voxel_b200_device.cuh"
 
 #include <new>
 
@@ -31,19 +32,10 @@ constexpr uint32_t kSlotsPerSlab = 15;
 constexpr uint32_t kMaxContentionRetries = 65536;
 constexpr uint32_t kBlock = 256;
 
-__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
-  // splitmix64 finaliser (Steele, Lea & Flood 2014)
-  x ^= x >> 30;
-  x *= 0xbf58476d1ce4e5b9ull;
-  x ^= x >> 27;
-  x *= 0x94d049bb133111ebull;
-  x ^= x >> 31;
-  return x;
-}
-
-// Map a 64-bit hash onto [0, n) without a division (multiply-high).
+// The hashes are voxel_b200_device.cuh's, which user kernels share.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) { return vx_mix64(x); }
 __device__ __forceinline__ uint32_t reduce(uint64_t h, uint32_t n) {
-  return static_cast<uint32_t>(__umul64hi(h, n));
+  return vx_reduce_hash(h, n);
 }
 
 struct Slab {
@@ -213,10 +205,7 @@ constexpr uint32_t kCuckooHashes = 4;
 
 __device__ __forceinline__ uint32_t cuckoo_slot(uint64_t key, uint32_t hid,
                                                 uint32_t n) {
-  constexpr uint64_t salts[kCuckooHashes] = {
-      0x9e3779b97f4a7c15ull, 0xc2b2ae3d27d4eb4full, 0x165667b19e3779f9ull,
-      0x27d4eb2f165667c5ull};
-  return reduce(mix64(key ^ salts[hid]), n);
+  return vx_cuckoo_slot(key, hid, n);
 }
 
 __device__ __forceinline__ ulonglong2 exch128(ulonglong2 *p, ulonglong2 v) {
@@ -314,9 +303,8 @@ __global__ void __launch_bounds__(kBlock)
                        uint32_t *values) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (i >= count) return;
-  uint32_t v = VX_HASH_NOT_FOUND_VALUE, where;
-  const uint64_t key = keys[i];
-  if (key != kEmpty && key != kDeleted) cuckoo_lookup(slots, n, key, v, where);
+  uint32_t v = VX_HASH_NOT_FOUND_VALUE;
+  vx_cuckoo_find(vx_cuckoo_view{slots, n, 0}, keys[i], &v);
   values[i] = v;
 }
 
@@ -415,6 +403,18 @@ vx_status vx_slab_set_erase(vx_slab_set *s, const uint64_t *keys,
                             vx_stream stream) {
   return slab_launch<SetOp::Erase>(s, keys, count, nullptr, statuses, stream,
                                    "slab_erase");
+}
+
+vx_status vx_slab_set_device_view(const vx_slab_set *s, vx_slab_set_view *out) {
+  if (s == nullptr || out == nullptr) return VX_ERR_INVALID_VALUE;
+  *out = vx_slab_set_view{s->slabs, s->bucket_count, s->capacity};
+  return VX_OK;
+}
+
+vx_status vx_cuckoo_device_view(const vx_cuckoo *c, vx_cuckoo_view *out) {
+  if (c == nullptr || out == nullptr) return VX_ERR_INVALID_VALUE;
+  *out = vx_cuckoo_view{c->slots, c->slot_count, 0};
+  return VX_OK;
 }
 
 size_t vx_slab_set_bytes(const vx_slab_set *s) {

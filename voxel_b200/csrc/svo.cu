@@ -22,6 +22,7 @@
 // write the edit checks that the worst-case allocation fits; if not it
 // reports VX_ERR_CAPACITY and changes nothing.
 #include "edit_common.cuh"
+#include "voxel_b200_device.cuh"
 #include "plain.cuh"
 #include "graph.cuh"
 #include "profile.cuh"
@@ -398,30 +399,11 @@ __global__ void reset_kernel(Tables t) {
   t.hdr->status = kDevOk;
 }
 
-__global__ void query_kernel(Tables t, const vx_voxel *pts, uint32_t n, uint8_t *out) {
+__global__ void query_kernel(vx_svo_view v, const vx_voxel *pts, uint32_t n, uint8_t *out) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   const vx_voxel p = pts[i];
-  const uint32_t side_exp = t.depth + 2;
-  const bool mats = t.materials != 0;
-  if ((p.x >> side_exp) | (p.y >> side_exp) | (p.z >> side_exp)) {
-    out[i] = 0;
-    return;
-  }
-  uint32_t w = kChild; // root node 0
-  for (uint32_t l = 0; l < t.depth && (w & kChild); ++l) {
-    const uint32_t s = side_exp - 1 - l;
-    const uint32_t c = ((p.x >> s) & 1u) | (((p.y >> s) & 1u) << 1) | (((p.z >> s) & 1u) << 2);
-    w = t.nodes[static_cast<size_t>(w & kIndex) * 8u + c];
-  }
-  if (!(w & kChild)) {
-    out[i] = static_cast<uint8_t>(word_value(w, mats));
-    return;
-  }
-  const uint32_t li = w & kIndex;
-  const uint32_t bit = (p.x & 3u) + 4u * (p.y & 3u) + 16u * (p.z & 3u);
-  if (mats) out[i] = t.mats[static_cast<size_t>(li) * 64u + bit];
-  else out[i] = static_cast<uint8_t>((t.leaves[li] >> bit) & 1ull);
+  out[i] = vx_svo_get_voxel(v, p.x, p.y, p.z);
 }
 
 } // namespace vx::svo
@@ -624,6 +606,12 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
 
 uint32_t vx_svo_depth(const vx_svo *v) { return v ? v->t.depth : 0; }
 
+vx_status vx_svo_device_view(const vx_svo *v, vx_svo_view *out) {
+  if (v == nullptr || out == nullptr) return VX_ERR_INVALID_VALUE;
+  *out = vx_svo_view{v->t.depth, v->t.materials, v->t.nodes, v->t.leaves, v->t.mats};
+  return VX_OK;
+}
+
 vx_status vx_svo_apply_primitives(vx_svo *v, const vx_primitive *prims,
                                   uint32_t count, vx_stream stream) {
   if (v == nullptr || (prims == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
@@ -667,7 +655,9 @@ vx_status vx_svo_query(const vx_svo *v, const vx_voxel *pts, uint32_t count,
   if (count == 0) return VX_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   vx::prof::Scope sc("svo_query", s);
-  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(v->t, pts, count, out);
+  vx_svo_view view;
+  VX_TRY(vx_svo_device_view(v, &view));
+  query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, pts, count, out);
   return vx::from_cuda(cudaGetLastError());
 }
 
