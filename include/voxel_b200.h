@@ -172,6 +172,33 @@ vx_status vx_slab_set_erase(vx_slab_set *set, const uint64_t *keys,
 /* Bytes of device memory the table holds (buckets + overflow pool). */
 size_t vx_slab_set_bytes(const vx_slab_set *set);
 
+/* Slab hash map u32 -> u32 (SlabHashMapU32, cuda/hash_table/slab_hash/map/
+ * host.cuh, common.cuh:40-94, device.cuh:49-372): 128-byte slabs of 15
+ * packed key/value slots and a link.  Keys VX_MAP_EMPTY_KEY /
+ * VX_MAP_DELETED_KEY are reserved (VX_HASH_INVALID_KEY).  insert_or_replace
+ * takes the first slot of the chain that holds the key, is empty or deleted
+ * (VX_HASH_INSERTED / VX_HASH_REPLACED / VX_HASH_OVERFLOW); duplicates of a
+ * key in one batch apply in array order within a warp.  find writes the value
+ * of the first match or VX_HASH_NOT_FOUND_VALUE (VX_HASH_FOUND /
+ * VX_HASH_NOT_FOUND); erase_all deletes every match (VX_HASH_ERASED /
+ * VX_HASH_NOT_FOUND).  statuses may be NULL. */
+#define VX_MAP_EMPTY_KEY 0xFFFFFFFFu
+#define VX_MAP_DELETED_KEY 0xFFFFFFFEu
+typedef struct vx_slab_map vx_slab_map;
+vx_status vx_slab_map_create(uint32_t bucket_count, uint32_t slab_capacity,
+                             vx_slab_map **out);
+vx_status vx_slab_map_destroy(vx_slab_map *map);
+vx_status vx_slab_map_clear(vx_slab_map *map, vx_stream stream);
+vx_status vx_slab_map_insert_or_replace(vx_slab_map *map, const uint32_t *keys,
+                                        const uint32_t *values, uint32_t count,
+                                        uint32_t *statuses, vx_stream stream);
+vx_status vx_slab_map_find(const vx_slab_map *map, const uint32_t *keys,
+                           uint32_t count, uint32_t *values, uint32_t *statuses,
+                           vx_stream stream);
+vx_status vx_slab_map_erase_all(vx_slab_map *map, const uint32_t *keys,
+                                uint32_t count, uint32_t *statuses, vx_stream stream);
+size_t vx_slab_map_bytes(const vx_slab_map *map);
+
 /* Cuckoo hash map u64 -> u32 with 4 hash functions over one slot array and a
  * bounded eviction chain (max_evictions).  The u64-keyed, inline-key
  * widening of cuckoo_insert / cuckoo_find / initialize_cuckoo_table

@@ -21,6 +21,12 @@ LIB_PATH = _PKG / "libvoxel_b200.so"
 
 VX_OK = 0
 VX_ERR_INVALID_VALUE = 1
+# hash-table statuses (the reference's kSlabHashStatus* values) and keys
+VX_HASH_NOT_FOUND, VX_HASH_INSERTED, VX_HASH_REPLACED, VX_HASH_ERASED = 0, 1, 2, 3
+VX_HASH_OVERFLOW, VX_HASH_INVALID_KEY, VX_HASH_FOUND, VX_HASH_ALREADY_PRESENT = 4, 5, 6, 7
+VX_HASH_NOT_FOUND_VALUE = 0xFFFFFFFF
+VX_MAP_EMPTY_KEY = 0xFFFFFFFF
+VX_MAP_DELETED_KEY = 0xFFFFFFFE
 VX_ERR_MEMORY_ALLOCATION = 2
 VX_ERR_TIMEOUT = 1001
 VX_ERR_CAPACITY = 1002
@@ -165,6 +171,13 @@ _SIGS = {
     "vx_slab_set_contains": (_ST, [_P, _P, _U32, _P, _P, _P]),
     "vx_slab_set_erase": (_ST, [_P, _P, _U32, _P, _P]),
     "vx_slab_set_bytes": (_SZ, [_P]),
+    "vx_slab_map_create": (_ST, [_U32, _U32, C.POINTER(_P)]),
+    "vx_slab_map_destroy": (_ST, [_P]),
+    "vx_slab_map_clear": (_ST, [_P, _P]),
+    "vx_slab_map_insert_or_replace": (_ST, [_P, _P, _P, _U32, _P, _P]),
+    "vx_slab_map_find": (_ST, [_P, _P, _U32, _P, _P, _P]),
+    "vx_slab_map_erase_all": (_ST, [_P, _P, _U32, _P, _P]),
+    "vx_slab_map_bytes": (_SZ, [_P]),
     "vx_cuckoo_create": (_ST, [_U32, _U32, C.POINTER(_P)]),
     "vx_cuckoo_destroy": (_ST, [_P]),
     "vx_cuckoo_clear": (_ST, [_P, _P]),

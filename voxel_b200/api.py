@@ -15,7 +15,7 @@ from . import check, lib
 
 __all__ = [
     "stream_handle", "ptr", "exclusive_sum", "inclusive_sum", "sort_pairs",
-    "workspace_status", "SlabHashSet", "CuckooMap", "PRIM_DTYPE",
+    "workspace_status", "SlabHashSet", "SlabHashMap", "CuckooMap", "PRIM_DTYPE",
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
@@ -179,6 +179,50 @@ class SlabHashSet:
         check(lib().vx_slab_set_erase(self._h, ptr(keys), keys.numel(),
                                       ptr(statuses), stream_handle()),
               "slab erase")
+        return statuses
+
+
+class SlabHashMap:
+    """u32 -> u32 slab hash map (SlabHashMapU32,
+    cuda/hash_table/slab_hash/map/host.cuh)."""
+
+    def __init__(self, bucket_count: int, slab_capacity: int):
+        h = C.c_void_p()
+        check(lib().vx_slab_map_create(bucket_count, slab_capacity, C.byref(h)),
+              "vx_slab_map_create")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_slab_map_destroy(h)
+            self._h = None
+
+    @property
+    def nbytes(self) -> int:
+        return lib().vx_slab_map_bytes(self._h)
+
+    def clear(self):
+        check(lib().vx_slab_map_clear(self._h, stream_handle()), "slab map clear")
+
+    def insert_or_replace(self, keys: torch.Tensor, values: torch.Tensor,
+                          statuses: torch.Tensor | None = None):
+        check(lib().vx_slab_map_insert_or_replace(self._h, ptr(keys), ptr(values),
+                                                  keys.numel(), ptr(statuses),
+                                                  stream_handle()), "slab map insert")
+        return statuses
+
+    def find(self, keys: torch.Tensor, out: torch.Tensor | None = None,
+             statuses: torch.Tensor | None = None):
+        if out is None:
+            out = torch.empty(keys.numel(), dtype=torch.int32, device=keys.device)
+        check(lib().vx_slab_map_find(self._h, ptr(keys), keys.numel(), ptr(out),
+                                     ptr(statuses), stream_handle()), "slab map find")
+        return out
+
+    def erase_all(self, keys: torch.Tensor, statuses: torch.Tensor | None = None):
+        check(lib().vx_slab_map_erase_all(self._h, ptr(keys), keys.numel(), ptr(statuses),
+                                          stream_handle()), "slab map erase")
         return statuses
 
 

@@ -10,6 +10,8 @@
 // bump counter.  Statuses are the reference's kSlabHashStatus* values.  Every
 // retry loop is bounded (the reference's kSlabHashMaxContentionRetries).
 //
+// Slab map: u32 -> u32, the reference's SlabHashMapU32 (below).
+//
 // Cuckoo map: the u64-keyed widening of cuckoo_insert / cuckoo_find
 // (cuda/cuckoo_hash.cuh:54-120).  Four hash functions address one array of
 // 16-byte slots {key, value | hash id << 32}; an eviction moves a whole slot
@@ -48,6 +50,13 @@ static_assert(sizeof(Slab) == 128, "slab must be one 128-byte line");
 struct vx_slab_set {
   vx::hash::Slab *slabs = nullptr; // buckets, then the overflow pool
   uint32_t *alloc = nullptr;       // overflow slabs handed out
+  uint32_t bucket_count = 0;
+  uint32_t capacity = 0;
+};
+
+struct vx_slab_map {
+  vx::hash::Slab *slabs = nullptr; // buckets, then the overflow pool
+  uint32_t *alloc = nullptr;
   uint32_t bucket_count = 0;
   uint32_t capacity = 0;
 };
@@ -199,6 +208,158 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// ---------------------------------------------------------- slab map --
+//
+// u32 -> u32 map (the reference's SlabHashMapU32, cuda/hash_table/slab_hash/
+// map/device.cuh:49-372): a 128-byte slab holds 15 slots packed as
+// key | value << 32 and a link, so a slot changes with one 64-bit CAS.  As in
+// the reference a warp serves its keys one at a time in lane order (later
+// duplicates of a key in a batch replace earlier ones), an insert takes the
+// first slot of the chain that holds the key, is empty or is deleted, a find
+// returns the first match, and erase_all deletes every match.
+
+constexpr uint32_t kMapEmpty = VX_MAP_EMPTY_KEY, kMapDeleted = VX_MAP_DELETED_KEY;
+
+__device__ __forceinline__ uint64_t map_pack(uint32_t k, uint32_t v) {
+  return static_cast<uint64_t>(k) | (static_cast<uint64_t>(v) << 32);
+}
+
+__global__ void map_init_kernel(SetView t, uint64_t words) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < words; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    reinterpret_cast<uint64_t *>(t.slabs)[i] = (i & 15u) == 15u ? kNullLink : map_pack(kMapEmpty, 0);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *t.alloc = 0;
+}
+
+enum class MapOp { InsertOrReplace, Find, EraseAll };
+
+template <MapOp Op>
+__global__ void __launch_bounds__(kBlock)
+    slab_map_kernel(SetView t, const uint32_t *__restrict__ keys,
+                    const uint32_t *__restrict__ values, uint32_t count,
+                    uint32_t *out_values, uint32_t *statuses) {
+  const uint32_t lane = lane_id();
+  const uint32_t sub = lane & 15u;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t warp_first = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) - lane;
+  for (uint64_t base = warp_first; base < count; base += stride) {
+    const uint64_t idx = base + lane;
+    bool active = idx < count;
+    const uint32_t key = active ? keys[idx] : 0u;
+    const uint32_t val = (active && Op == MapOp::InsertOrReplace) ? values[idx] : 0u;
+    uint32_t status = VX_HASH_NOT_FOUND, out = VX_HASH_NOT_FOUND_VALUE;
+    if (active && (key == kMapEmpty || key == kMapDeleted)) {
+      status = VX_HASH_INVALID_KEY;
+      active = false;
+    }
+    uint32_t queue = __ballot_sync(kFullMask, active);
+    while (queue) {
+      const uint32_t src = __ffs(queue) - 1u;
+      const uint32_t k = __shfl_sync(kFullMask, key, src);
+      const uint32_t v = __shfl_sync(kFullMask, val, src);
+      Slab *slab = &t.slabs[reduce(mix64(k), t.bucket_count)];
+      uint32_t result = VX_HASH_OVERFLOW, found_value = VX_HASH_NOT_FOUND_VALUE;
+      bool erased_any = false;
+      const uint64_t max_steps =
+          Op == MapOp::Find ? t.capacity + 1ull
+                            : (t.capacity + 1ull) * static_cast<uint64_t>(kMaxContentionRetries);
+      for (uint64_t step = 0; step < max_steps; ++step) {
+        // lanes 0..15 read the slab (16 words); lanes 16..31 mirror them
+        const uint64_t w = ld_relaxed_u64(&slab->w[sub]);
+        const bool slot = lane < kSlotsPerSlab;
+        const uint32_t wk = static_cast<uint32_t>(w);
+        if (Op == MapOp::Find) {
+          const uint32_t hit = __ballot_sync(kFullMask, slot && wk == k);
+          if (hit) {
+            const uint64_t hw = __shfl_sync(kFullMask, w, __ffs(hit) - 1u);
+            found_value = static_cast<uint32_t>(hw >> 32);
+            result = VX_HASH_FOUND;
+            break;
+          }
+        } else if (Op == MapOp::EraseAll) {
+          const uint32_t hit = __ballot_sync(kFullMask, slot && wk == k);
+          if (hit) {
+            const uint32_t dst = __ffs(hit) - 1u;
+            const uint64_t expect = __shfl_sync(kFullMask, w, dst);
+            unsigned long long old = 0;
+            if (lane == dst)
+              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]), expect,
+                              map_pack(kMapDeleted, static_cast<uint32_t>(expect >> 32)));
+            old = __shfl_sync(kFullMask, old, dst);
+            if (old == expect) erased_any = true;
+            continue; // re-read this slab for further matches
+          }
+        } else {
+          const uint32_t cand = __ballot_sync(
+              kFullMask, slot && (wk == k || wk == kMapEmpty || wk == kMapDeleted));
+          if (cand) {
+            const uint32_t dst = __ffs(cand) - 1u;
+            const uint64_t expect = __shfl_sync(kFullMask, w, dst);
+            unsigned long long old = 0;
+            if (lane == dst)
+              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]), expect,
+                              map_pack(k, v));
+            old = __shfl_sync(kFullMask, old, dst);
+            if (old == expect) {
+              result = static_cast<uint32_t>(expect) == k ? VX_HASH_REPLACED : VX_HASH_INSERTED;
+              break;
+            }
+            continue; // slot changed meanwhile: re-read this slab
+          }
+        }
+        const uint64_t link = __shfl_sync(kFullMask, w, 15u);
+        if (link != kNullLink) {
+          slab = &t.slabs[link];
+          continue;
+        }
+        if (Op == MapOp::Find) {
+          result = VX_HASH_NOT_FOUND;
+          break;
+        }
+        if (Op == MapOp::EraseAll) {
+          result = erased_any ? VX_HASH_ERASED : VX_HASH_NOT_FOUND;
+          break;
+        }
+        // Grow the chain: take a pool slab, initialise it, link it with CAS.
+        uint32_t ord = 0;
+        if (lane == 0) ord = atomicAdd(t.alloc, 1u);
+        ord = __shfl_sync(kFullMask, ord, 0);
+        if (ord >= t.capacity) {
+          uint64_t again = 0;
+          if (lane == 15u) again = ld_relaxed_u64(&slab->w[15]);
+          again = __shfl_sync(kFullMask, again, 15u);
+          if (again != kNullLink) {
+            slab = &t.slabs[again];
+            continue;
+          }
+          result = VX_HASH_OVERFLOW;
+          break;
+        }
+        Slab *fresh = &t.slabs[t.bucket_count + ord];
+        if (lane < 16u) fresh->w[sub] = sub == 15u ? kNullLink : map_pack(kMapEmpty, 0);
+        __threadfence();
+        __syncwarp();
+        unsigned long long observed = 0;
+        if (lane == 15u)
+          observed = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[15]),
+                               kNullLink, t.bucket_count + ord);
+        observed = __shfl_sync(kFullMask, observed, 15u);
+        slab = &t.slabs[observed == kNullLink ? t.bucket_count + ord : observed];
+      }
+      if (lane == src) {
+        status = result;
+        out = found_value;
+        active = false;
+      }
+      queue = __ballot_sync(kFullMask, active);
+    }
+    if (idx < count) {
+      if (statuses) statuses[idx] = status;
+      if (Op == MapOp::Find && out_values) out_values[idx] = out;
+    }
+  }
+}
+
 // ------------------------------------------------------------ cuckoo --
 
 constexpr uint32_t kCuckooHashes = 4;
@@ -339,6 +500,24 @@ static vx_status slab_launch(const vx_slab_set *s, const uint64_t *keys,
 }
 
 
+template <MapOp Op>
+static vx_status map_launch(const vx_slab_map *m, const uint32_t *keys, const uint32_t *values,
+                            uint32_t count, uint32_t *out_values, uint32_t *statuses,
+                            vx_stream stream, const char *name) {
+  if (m == nullptr || (keys == nullptr && count != 0)) return VX_ERR_INVALID_VALUE;
+  if (Op == MapOp::InsertOrReplace && values == nullptr && count != 0)
+    return VX_ERR_INVALID_VALUE;
+  if (Op == MapOp::Find && out_values == nullptr && count != 0) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope(name, st);
+  slab_map_kernel<Op><<<grid_for(count), kBlock, 0, st>>>(
+      SetView{m->slabs, m->alloc, m->bucket_count, m->capacity}, keys, values, count,
+      out_values, statuses);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+
 extern "C" {
 
 vx_status vx_slab_set_clear(vx_slab_set *s, vx_stream stream) {
@@ -403,6 +582,71 @@ vx_status vx_slab_set_erase(vx_slab_set *s, const uint64_t *keys,
                             vx_stream stream) {
   return slab_launch<SetOp::Erase>(s, keys, count, nullptr, statuses, stream,
                                    "slab_erase");
+}
+
+vx_status vx_slab_map_create(uint32_t bucket_count, uint32_t slab_capacity,
+                             vx_slab_map **out) {
+  if (out == nullptr || bucket_count == 0) return VX_ERR_INVALID_VALUE;
+  auto *m = new (std::nothrow) vx_slab_map;
+  if (m == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  m->bucket_count = bucket_count;
+  m->capacity = slab_capacity;
+  const size_t slabs = static_cast<size_t>(bucket_count) + slab_capacity;
+  cudaError_t e = cudaMalloc(&m->slabs, slabs * sizeof(Slab));
+  if (e == cudaSuccess) e = cudaMalloc(&m->alloc, sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    vx_slab_map_destroy(m);
+    return vx::from_cuda(e);
+  }
+  const vx_status st = vx_slab_map_clear(m, nullptr);
+  if (st != VX_OK) {
+    vx_slab_map_destroy(m);
+    return st;
+  }
+  VX_TRY_CUDA(cudaStreamSynchronize(nullptr));
+  *out = m;
+  return VX_OK;
+}
+
+vx_status vx_slab_map_destroy(vx_slab_map *m) {
+  if (m == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaFree(m->slabs);
+  cudaFree(m->alloc);
+  delete m;
+  return VX_OK;
+}
+
+vx_status vx_slab_map_clear(vx_slab_map *m, vx_stream stream) {
+  if (m == nullptr) return VX_ERR_INVALID_VALUE;
+  const uint64_t words = (static_cast<uint64_t>(m->bucket_count) + m->capacity) * 16u;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope scope("slab_map_init", st);
+  map_init_kernel<<<grid_for(words), kBlock, 0, st>>>(
+      SetView{m->slabs, m->alloc, m->bucket_count, m->capacity}, words);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_slab_map_insert_or_replace(vx_slab_map *m, const uint32_t *keys,
+                                        const uint32_t *values, uint32_t count,
+                                        uint32_t *statuses, vx_stream stream) {
+  return map_launch<MapOp::InsertOrReplace>(m, keys, values, count, nullptr, statuses, stream,
+                                            "slab_map_insert");
+}
+
+vx_status vx_slab_map_find(const vx_slab_map *m, const uint32_t *keys, uint32_t count,
+                           uint32_t *values, uint32_t *statuses, vx_stream stream) {
+  return map_launch<MapOp::Find>(m, keys, nullptr, count, values, statuses, stream,
+                                 "slab_map_find");
+}
+
+vx_status vx_slab_map_erase_all(vx_slab_map *m, const uint32_t *keys, uint32_t count,
+                                uint32_t *statuses, vx_stream stream) {
+  return map_launch<MapOp::EraseAll>(m, keys, nullptr, count, nullptr, statuses, stream,
+                                     "slab_map_erase");
+}
+
+size_t vx_slab_map_bytes(const vx_slab_map *m) {
+  return m ? (static_cast<size_t>(m->bucket_count) + m->capacity) * sizeof(Slab) : 0;
 }
 
 vx_status vx_slab_set_device_view(const vx_slab_set *s, vx_slab_set_view *out) {
