@@ -58,3 +58,14 @@ def test_device_header_compiles_for_sm100a(tmp_path):
            str(ROOT / "tests" / "user_kernels.cu"), "-I", str(ROOT / "include"), "-o", str(obj)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+@pytest.mark.skipif(shutil.which("nvcc") is None, reason="no nvcc")
+def test_fused_scan_header_compiles_for_sm100a(tmp_path):
+    """User fused scans against voxel_b200_fused_scan.cuh (cross-compiled for
+    sm_100a; run by tests/test_gpu_fused_scan.py on a GPU)."""
+    obj = tmp_path / "fused.o"
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-c",
+           str(ROOT / "tests" / "user_fused_scan.cu"), "-I", str(ROOT / "include"), "-o", str(obj)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
