@@ -40,6 +40,7 @@ typedef void *vx_stream; /* a cudaStream_t; NULL = legacy default stream */
 #define VX_ERR_TIMEOUT 1001         /* a bounded device wait gave up */
 #define VX_ERR_CAPACITY 1002        /* a node pool / table / arena is full */
 #define VX_ERR_NO_DEVICE 1003       /* no CUDA device is visible */
+#define VX_ERR_IO 1004         /* a file could not be read or written */
 
 /* Library version and a human-readable name for a status code. */
 uint32_t vx_version(void);
@@ -309,6 +310,23 @@ vx_status vx_dag_export_canonical(const vx_dag *dag, uint32_t *host_root,
                                   uint64_t nodes_capacity_words,
                                   uint64_t *host_leaves,
                                   uint64_t leaves_capacity, vx_stream stream);
+
+/* Rebuild the DAG from a canonical dump in host memory (the format of
+ * vx_dag_export_canonical: root 0 / 1 / 2, per-level counts, 10-word node
+ * records of levels 0..depth-1 in order, leaf masks).  The tables are reset
+ * first; VX_ERR_CAPACITY if a level does not fit, VX_ERR_INVALID_VALUE for a
+ * malformed dump.  Synchronises. */
+vx_status vx_dag_import_canonical(vx_dag *dag, uint32_t root, const uint64_t *host_counts,
+                                  const uint32_t *host_nodes, const uint64_t *host_leaves,
+                                  vx_stream stream);
+/* Checkpoint / resume of a resident DAG: the canonical dump as a file
+ * ("VXDAGCN1", version, depth, root, counts, node records, leaf masks;
+ * little-endian) and its import into a DAG of the same depth (any capacity
+ * that holds it).  The on-disk counterpart of the reference CPU DAG's
+ * compaction (svt/hash_dag.hpp:133-191); the reference has no file format.
+ * VX_ERR_IO when the file cannot be read or written. */
+vx_status vx_dag_save(const vx_dag *dag, const char *path, vx_stream stream);
+vx_status vx_dag_load(vx_dag *dag, const char *path, vx_stream stream);
 
 /* Copy the complete table state of src into dst (same configuration): a
  * device-side snapshot / restore of a resident DAG.  No counterpart in the

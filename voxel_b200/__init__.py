@@ -31,6 +31,7 @@ VX_ERR_MEMORY_ALLOCATION = 2
 VX_ERR_TIMEOUT = 1001
 VX_ERR_CAPACITY = 1002
 VX_ERR_NO_DEVICE = 1003
+VX_ERR_IO = 1004
 
 HASH_NOT_FOUND = 0
 HASH_INSERTED = 1
@@ -240,6 +241,9 @@ _SIGS = {
     "vx_svo_device_view": (_ST, [_P, C.POINTER(vx_svo_view)]),
     "vx_slab_set_device_view": (_ST, [_P, C.POINTER(vx_slab_set_view)]),
     "vx_cuckoo_device_view": (_ST, [_P, C.POINTER(vx_cuckoo_view)]),
+    "vx_dag_import_canonical": (_ST, [_P, _U32, _P, _P, _P, _P]),
+    "vx_dag_save": (_ST, [_P, C.c_char_p, _P]),
+    "vx_dag_load": (_ST, [_P, C.c_char_p, _P]),
     "vx_tuning_count": (_U32, []),
     "vx_tuning_name": (C.c_char_p, [_U32]),
     "vx_tuning_options": (_ST, [C.c_char_p, C.POINTER(C.c_int64), _U32, C.POINTER(_U32)]),

@@ -464,6 +464,14 @@ class HashDag:
                                         C.byref(h)), "vx_dag_graph_voxels")
         return Graph(h, (self, voxels, ws))
 
+    def save(self, path) -> None:
+        """Checkpoint: the canonical dump as a file (vx_dag_save)."""
+        check(lib().vx_dag_save(self._h, str(path).encode(), stream_handle()), "vx_dag_save")
+
+    def load(self, path) -> int:
+        """Resume from a file written by save(); returns the status."""
+        return lib().vx_dag_load(self._h, str(path).encode(), stream_handle())
+
     def apply_primitives(self, prims: torch.Tensor) -> None:
         """Batched path: primitives applied as if in order; asynchronous
         (check with status())."""

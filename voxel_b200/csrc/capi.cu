@@ -13,6 +13,7 @@ const char *vx_status_string(vx_status status) {
   case VX_ERR_TIMEOUT: return "a bounded device wait timed out";
   case VX_ERR_CAPACITY: return "capacity exceeded (node pool, table or arena full)";
   case VX_ERR_NO_DEVICE: return "no CUDA device";
+  case VX_ERR_IO: return "file could not be read or written";
   default: return cudaGetErrorString(static_cast<cudaError_t>(status));
   }
 }

@@ -22,6 +22,8 @@
 #include "tuning.cuh"
 
 #include <algorithm>
+#include <cstring>
+#include <cstdio>
 #include <cmath>
 #include <new>
 #include <vector>
@@ -1039,25 +1041,51 @@ __global__ void stage_kernel(Tables t, uint32_t l, LevelMarks m,
 // exclusive scan of the items' word counts and its index entry takes the
 // first empty slot of its probe sequence.  No shared counter is touched per
 // item; the level's counts are written once at the end.
+// Unique inserts (the item is known not to be in the table): the leaf takes
+// the first empty slot of its probe sequence; the node is written at its
+// pool offset and its index entry takes the first empty slot.
+__device__ uint32_t unique_insert_leaf(const Tables &t, uint64_t mask) {
+  uint64_t pos = mix64(mask) & t.leaf_mask;
+  for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+    if (ld_relaxed_u64(t.leaves + pos) == 0 &&
+        atomicCAS(reinterpret_cast<unsigned long long *>(t.leaves + pos), 0ull,
+                  static_cast<unsigned long long>(mask)) == 0ull)
+      return static_cast<uint32_t>(pos + 2);
+    pos = (pos + 1) & t.leaf_mask;
+  }
+  set_status(&t.hdr->status, kDevCapacity);
+  return kEmptyRef;
+}
+
+__device__ uint32_t unique_insert_node(const Tables &t, uint32_t l, const uint32_t *w,
+                                       uint32_t n, uint32_t off) {
+  if (static_cast<uint64_t>(off) + n > t.pool_cap[l]) {
+    set_status(&t.hdr->status, kDevCapacity);
+    return kEmptyRef;
+  }
+  uint32_t *dst = t.pool[l] + off;
+  for (uint32_t j = 0; j < n; ++j) dst[j] = w[j];
+  const uint64_t h = hash_words(w, n);
+  const uint64_t entry =
+      (static_cast<uint64_t>(static_cast<uint32_t>(h >> 32) | 1u) << 32) | (off + 2u);
+  uint64_t *idx = t.index[l];
+  uint64_t pos = h & t.index_mask[l];
+  for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+    if (ld_relaxed_u64(idx + pos) == 0 &&
+        atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos), 0ull,
+                  static_cast<unsigned long long>(entry)) == 0ull)
+      return off + 2u;
+    pos = (pos + 1) & t.index_mask[l];
+  }
+  set_status(&t.hdr->status, kDevCapacity);
+  return off + 2u;
+}
+
 __global__ void reinsert_leaves_kernel(Tables t, LevelMarks m, const uint64_t *masks) {
   const uint32_t n = *m.live;
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint64_t mask = masks[i];
-    uint64_t pos = mix64(mask) & t.leaf_mask;
-    uint32_t ref = kEmptyRef;
-    for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
-      if (ld_relaxed_u64(t.leaves + pos) == 0 &&
-          atomicCAS(reinterpret_cast<unsigned long long *>(t.leaves + pos), 0ull,
-                    static_cast<unsigned long long>(mask)) == 0ull) {
-        ref = static_cast<uint32_t>(pos + 2);
-        break;
-      }
-      pos = (pos + 1) & t.leaf_mask;
-    }
-    if (ref == kEmptyRef) set_status(&t.hdr->status, kDevCapacity);
-    m.new_refs[i] = ref;
-  }
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    m.new_refs[i] = unique_insert_leaf(t, masks[i]);
 }
 
 __global__ void item_words_kernel(LevelMarks m, const uint32_t *staged, uint32_t *words) {
@@ -1070,35 +1098,79 @@ __global__ void item_words_kernel(LevelMarks m, const uint32_t *staged, uint32_t
 __global__ void reinsert_nodes_kernel(Tables t, uint32_t l, LevelMarks m, LevelMarks child,
                                       const uint32_t *staged, const uint32_t *offsets) {
   const uint32_t n = *m.live;
-  uint64_t *idx = t.index[l];
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     uint32_t w[9];
     w[0] = staged[i * 9];
     const uint32_t k = __popc(w[0] & 0xffu);
     for (uint32_t j = 0; j < k; ++j) w[1 + j] = child.new_refs[rank_of(child, staged[i * 9 + 1 + j])];
-    const uint32_t off = offsets[i];
-    if (static_cast<uint64_t>(off) + 1 + k > t.pool_cap[l]) {
-      set_status(&t.hdr->status, kDevCapacity);
-      m.new_refs[i] = kEmptyRef;
+    m.new_refs[i] = unique_insert_node(t, l, w, 1 + k, offsets[i]);
+  }
+}
+
+// ---- import of a canonical dump (records of 10 words per inner node:
+// [child_mask, fill_mask, child ids x 8], id k + 2 = node k of the next
+// level; leaves as u64 masks).  Canonical nodes are distinct per level, so
+// the unique inserts above apply; child ids are checked against the next
+// level's count (a malformed dump raises kDevInvalid, never an out-of-range
+// read).
+
+__global__ void import_leaves_kernel(Tables t, const uint64_t *masks, uint32_t n,
+                                     uint32_t *new_refs) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t m = masks[i];
+    if (m == 0 || m == ~0ull) {
+      set_status(&t.hdr->status, kDevInvalid);
+      new_refs[i] = kEmptyRef;
       continue;
     }
-    uint32_t *dst = t.pool[l] + off;
-    for (uint32_t j = 0; j <= k; ++j) dst[j] = w[j];
-    const uint64_t h = hash_words(w, 1 + k);
-    const uint64_t entry = (static_cast<uint64_t>(static_cast<uint32_t>(h >> 32) | 1u) << 32) |
-                           (off + 2u);
-    uint64_t pos = h & t.index_mask[l];
-    bool placed = false;
-    for (uint32_t probe = 0; probe < kMaxProbes && !placed; ++probe) {
-      placed = ld_relaxed_u64(idx + pos) == 0 &&
-               atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos), 0ull,
-                         static_cast<unsigned long long>(entry)) == 0ull;
-      pos = (pos + 1) & t.index_mask[l];
-    }
-    if (!placed) set_status(&t.hdr->status, kDevCapacity);
-    m.new_refs[i] = off + 2u;
+    new_refs[i] = unique_insert_leaf(t, m);
   }
+}
+
+__global__ void import_words_kernel(const uint32_t *rec, uint32_t n, uint32_t *words) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    words[i] = 1u + __popc(rec[i * 10] & 0xffu);
+}
+
+__global__ void import_nodes_kernel(Tables t, uint32_t l, const uint32_t *rec, uint32_t n,
+                                    const uint32_t *child_refs, uint32_t child_count,
+                                    const uint32_t *offsets, uint32_t *new_refs) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t *r = rec + i * 10;
+    const uint32_t cm = r[0] & 0xffu, fm = r[1] & 0xffu;
+    uint32_t w[9];
+    w[0] = cm | (fm << 8);
+    uint32_t k = 0;
+    bool ok = (cm & fm) == 0 && (cm != 0 || (fm != 0 && fm != 0xffu));
+    for (uint32_t c = 0; c < 8; ++c) {
+      if (!(cm & (1u << c))) continue;
+      const uint32_t id = r[2 + c];
+      ok = ok && id >= 2u && id - 2u < child_count;
+      w[1 + k++] = ok ? child_refs[id - 2u] : kEmptyRef;
+    }
+    if (!ok) {
+      set_status(&t.hdr->status, kDevInvalid);
+      new_refs[i] = kEmptyRef;
+      continue;
+    }
+    new_refs[i] = unique_insert_node(t, l, w, 1 + k, offsets[i]);
+  }
+}
+
+__global__ void import_finish_kernel(Tables t, uint32_t l, uint32_t n, const uint32_t *rec,
+                                     const uint32_t *offsets) {
+  t.hdr->node_count[l] = n;
+  if (l < t.depth)
+    t.hdr->pool_used[l] = n ? offsets[n - 1] + 1u + __popc(rec[(n - 1) * 10ull] & 0xffu) : 0u;
+}
+
+__global__ void import_root_kernel(Tables t, const uint32_t *level0_refs, uint32_t root_id) {
+  if (t.hdr->status != kDevOk) return;
+  t.hdr->root = root_id >= 2u ? level0_refs[root_id - 2u] : root_id;
 }
 
 // The level's node count and pool use, once its items are in.
@@ -1133,6 +1205,150 @@ struct SizingCarver {
 } // namespace vx::dag
 
 extern "C" {
+
+vx_status vx_dag_import_canonical(vx_dag *d, uint32_t root, const uint64_t *host_counts,
+                                  const uint32_t *host_nodes, const uint64_t *host_leaves,
+                                  vx_stream stream) {
+  if (d == nullptr || host_counts == nullptr || root > 2u) return VX_ERR_INVALID_VALUE;
+  const uint32_t D = d->t.depth;
+  uint64_t total_nodes = 0, max_n = 1;
+  for (uint32_t l = 0; l <= D; ++l) {
+    if (host_counts[l] > 0xffffffffull) return VX_ERR_CAPACITY;
+    if (l < D) total_nodes += host_counts[l];
+    max_n = std::max<uint64_t>(max_n, host_counts[l]);
+  }
+  if ((total_nodes && host_nodes == nullptr) || (host_counts[D] && host_leaves == nullptr))
+    return VX_ERR_INVALID_VALUE;
+  if (root == 2u && host_counts[0] != 1) return VX_ERR_INVALID_VALUE;
+  if (root < 2u && total_nodes + host_counts[D] != 0) return VX_ERR_INVALID_VALUE;
+  uint64_t rec0 = 0;
+  for (uint32_t l = 0; l < D; ++l) {
+    uint64_t words = 0; // exact pool words of the level
+    for (uint64_t i = 0; i < host_counts[l]; ++i)
+      words += 1 + __builtin_popcount(host_nodes[(rec0 + i) * 10] & 0xffu);
+    rec0 += host_counts[l];
+    if (host_counts[l] > d->index_slots[l] / 2 || words > d->t.pool_cap[l])
+      return VX_ERR_CAPACITY;
+  }
+  if (host_counts[D] > d->leaf_slots / 2) return VX_ERR_CAPACITY;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t grid = static_cast<uint32_t>(vx::sm_count()) * 8u;
+  // One temporary block: records of the largest level, its offsets, new
+  // refs of two adjacent levels, the leaf masks and the scan workspace.
+  const size_t scan_bytes = vx_scan_workspace_size(static_cast<uint32_t>(max_n));
+  vx::Sizer z;
+  z.take<uint32_t>(max_n * 10);
+  z.take<uint32_t>(max_n);
+  z.take<uint32_t>(max_n);
+  z.take<uint32_t>(max_n);
+  z.take<uint64_t>(std::max<uint64_t>(host_counts[D], 1));
+  z.take<unsigned char>(scan_bytes);
+  struct TempBlock {
+    void *p = nullptr;
+    ~TempBlock() { if (p) cudaFree(p); }
+  } temp;
+  VX_TRY_CUDA(cudaMalloc(&temp.p, z.offset));
+  vx::Carver c(temp.p);
+  uint32_t *rec = c.take<uint32_t>(max_n * 10);
+  uint32_t *offsets = c.take<uint32_t>(max_n);
+  uint32_t *refs[2] = {c.take<uint32_t>(max_n), c.take<uint32_t>(max_n)};
+  uint64_t *masks = c.take<uint64_t>(std::max<uint64_t>(host_counts[D], 1));
+  void *scan_ws = c.take<unsigned char>(scan_bytes);
+  VX_TRY(vx_dag_reset(d, stream));
+  const uint32_t nl = static_cast<uint32_t>(host_counts[D]);
+  if (nl) {
+    VX_TRY_CUDA(cudaMemcpyAsync(masks, host_leaves, nl * 8ull, cudaMemcpyHostToDevice, s));
+    vx::prof::Scope sc("dag_import", s);
+    import_leaves_kernel<<<grid, kBlock, 0, s>>>(d->t, masks, nl, refs[D & 1u]);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  import_finish_kernel<<<1, 1, 0, s>>>(d->t, D, nl, nullptr, nullptr);
+  VX_TRY_CUDA(cudaGetLastError());
+  std::vector<uint64_t> first(D + 1, 0); // first record of each level
+  for (uint32_t l = 1; l < D; ++l) first[l] = first[l - 1] + host_counts[l - 1] * 10;
+  for (uint32_t r = D; r > 0; --r) {
+    const uint32_t l = r - 1;
+    const uint32_t n = static_cast<uint32_t>(host_counts[l]);
+    if (n) {
+      VX_TRY_CUDA(cudaMemcpyAsync(rec, host_nodes + first[l], n * 40ull, cudaMemcpyHostToDevice,
+                                  s));
+      {
+        vx::prof::Scope sc("dag_import", s);
+        import_words_kernel<<<grid, kBlock, 0, s>>>(rec, n, offsets);
+        VX_TRY_CUDA(cudaGetLastError());
+      }
+      VX_TRY(vx_scan_exclusive_sum_u32(offsets, n, scan_ws, scan_bytes, s));
+      vx::prof::Scope sc("dag_import", s);
+      import_nodes_kernel<<<grid, kBlock, 0, s>>>(d->t, l, rec, n, refs[(l + 1) & 1u],
+                                                  static_cast<uint32_t>(host_counts[l + 1]),
+                                                  offsets, refs[l & 1u]);
+      VX_TRY_CUDA(cudaGetLastError());
+    }
+    import_finish_kernel<<<1, 1, 0, s>>>(d->t, l, n, rec, offsets);
+    VX_TRY_CUDA(cudaGetLastError());
+  }
+  import_root_kernel<<<1, 1, 0, s>>>(d->t, refs[0], root);
+  VX_TRY_CUDA(cudaGetLastError());
+  return read_status(d, s, true);
+}
+
+namespace {
+constexpr char kDagFileMagic[8] = {'V', 'X', 'D', 'A', 'G', 'C', 'N', '1'};
+} // namespace
+
+vx_status vx_dag_save(const vx_dag *d, const char *path, vx_stream stream) {
+  if (d == nullptr || path == nullptr) return VX_ERR_INVALID_VALUE;
+  const uint32_t D = d->t.depth;
+  uint32_t root = 0;
+  std::vector<uint64_t> counts(D + 1, 0);
+  VX_TRY(vx_dag_export_canonical(d, &root, counts.data(), nullptr, 0, nullptr, 0, stream));
+  uint64_t words = 0;
+  for (uint32_t l = 0; l < D; ++l) words += counts[l] * 10;
+  std::vector<uint32_t> nodes(words);
+  std::vector<uint64_t> leaves(counts[D]);
+  VX_TRY(vx_dag_export_canonical(d, &root, counts.data(), nodes.data(), words, leaves.data(),
+                                 leaves.size(), stream));
+  FILE *f = std::fopen(path, "wb");
+  if (f == nullptr) return VX_ERR_IO;
+  const uint32_t head[4] = {1u /* version */, D, root, 0u};
+  bool ok = std::fwrite(kDagFileMagic, 1, 8, f) == 8 && std::fwrite(head, 4, 4, f) == 4 &&
+            std::fwrite(counts.data(), 8, counts.size(), f) == counts.size() &&
+            std::fwrite(nodes.data(), 4, nodes.size(), f) == nodes.size() &&
+            std::fwrite(leaves.data(), 8, leaves.size(), f) == leaves.size();
+  ok = std::fclose(f) == 0 && ok;
+  return ok ? VX_OK : VX_ERR_IO;
+}
+
+vx_status vx_dag_load(vx_dag *d, const char *path, vx_stream stream) {
+  if (d == nullptr || path == nullptr) return VX_ERR_INVALID_VALUE;
+  FILE *f = std::fopen(path, "rb");
+  if (f == nullptr) return VX_ERR_IO;
+  struct Closer {
+    FILE *f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  char magic[8];
+  uint32_t head[4];
+  if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kDagFileMagic, 8) != 0 ||
+      std::fread(head, 4, 4, f) != 4 || head[0] != 1u)
+    return VX_ERR_INVALID_VALUE;
+  const uint32_t D = head[1], root = head[2];
+  if (D != d->t.depth || root > 2u) return VX_ERR_INVALID_VALUE;
+  std::vector<uint64_t> counts(D + 1);
+  if (std::fread(counts.data(), 8, counts.size(), f) != counts.size()) return VX_ERR_IO;
+  uint64_t words = 0;
+  for (uint32_t l = 0; l < D; ++l) {
+    if (counts[l] > (1ull << 32)) return VX_ERR_INVALID_VALUE;
+    words += counts[l] * 10;
+  }
+  if (counts[D] > (1ull << 32)) return VX_ERR_INVALID_VALUE;
+  std::vector<uint32_t> nodes(words);
+  std::vector<uint64_t> leaves(counts[D]);
+  if (std::fread(nodes.data(), 4, nodes.size(), f) != nodes.size() ||
+      std::fread(leaves.data(), 8, leaves.size(), f) != leaves.size())
+    return VX_ERR_IO;
+  return vx_dag_import_canonical(d, root, counts.data(), nodes.data(), leaves.data(), stream);
+}
 
 vx_status vx_dag_compact(vx_dag *d, vx_stream stream) {
   if (d == nullptr) return VX_ERR_INVALID_VALUE;
