@@ -200,6 +200,33 @@ vx_status vx_slab_map_erase_all(vx_slab_map *map, const uint32_t *keys,
                                 uint32_t count, uint32_t *statuses, vx_stream stream);
 size_t vx_slab_map_bytes(const vx_slab_map *map);
 
+/* Content-addressed store of fixed-width items (1..9 u32 words): the
+ * reference's AccelerationHashSet32<ItemWords> (cuda/hash_table/
+ * acceleration_hash/set/host.cuh:15-117, device.cuh:29-321), built on one
+ * hash-consing table of the Hash DAG's kind (open-addressing index of
+ * {tag, ref} over a word pool).  Items are count x width words; pointers
+ * are item index + 1, 0 = null (kAccelerationHashNullPtr).  find: FOUND /
+ * NOT_FOUND; insert_unique_unchecked (the caller guarantees no equal item is
+ * present or concurrently inserted): INSERTED / OVERFLOW; find_or_insert
+ * (hash-consing, safe under concurrent equal inserts): FOUND / INSERTED /
+ * OVERFLOW; read copies the words of each pointer (NOT_FOUND and zeros for
+ * null or unknown pointers).  statuses may be NULL. */
+typedef struct vx_itemset vx_itemset;
+vx_status vx_itemset_create(uint32_t width, uint32_t max_items, vx_itemset **out);
+vx_status vx_itemset_destroy(vx_itemset *set);
+vx_status vx_itemset_clear(vx_itemset *set, vx_stream stream);
+vx_status vx_itemset_find(const vx_itemset *set, const uint32_t *items, uint32_t count,
+                          uint32_t *ptrs, uint32_t *statuses, vx_stream stream);
+vx_status vx_itemset_find_or_insert(vx_itemset *set, const uint32_t *items, uint32_t count,
+                                    uint32_t *ptrs, uint32_t *statuses, vx_stream stream);
+vx_status vx_itemset_insert_unique_unchecked(vx_itemset *set, const uint32_t *items,
+                                             uint32_t count, uint32_t *ptrs,
+                                             uint32_t *statuses, vx_stream stream);
+vx_status vx_itemset_read(const vx_itemset *set, const uint32_t *ptrs, uint32_t count,
+                          uint32_t *items, uint32_t *statuses, vx_stream stream);
+/* Items stored (host read, synchronises). */
+vx_status vx_itemset_count(const vx_itemset *set, uint64_t *host_count, vx_stream stream);
+
 /* Cuckoo hash map u64 -> u32 with 4 hash functions over one slot array and a
  * bounded eviction chain (max_evictions).  The u64-keyed, inline-key
  * widening of cuckoo_insert / cuckoo_find / initialize_cuckoo_table

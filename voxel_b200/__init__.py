@@ -179,6 +179,14 @@ _SIGS = {
     "vx_slab_map_find": (_ST, [_P, _P, _U32, _P, _P, _P]),
     "vx_slab_map_erase_all": (_ST, [_P, _P, _U32, _P, _P]),
     "vx_slab_map_bytes": (_SZ, [_P]),
+    "vx_itemset_create": (_ST, [_U32, _U32, C.POINTER(_P)]),
+    "vx_itemset_destroy": (_ST, [_P]),
+    "vx_itemset_clear": (_ST, [_P, _P]),
+    "vx_itemset_find": (_ST, [_P, _P, _U32, _P, _P, _P]),
+    "vx_itemset_find_or_insert": (_ST, [_P, _P, _U32, _P, _P, _P]),
+    "vx_itemset_insert_unique_unchecked": (_ST, [_P, _P, _U32, _P, _P, _P]),
+    "vx_itemset_read": (_ST, [_P, _P, _U32, _P, _P, _P]),
+    "vx_itemset_count": (_ST, [_P, C.POINTER(_U64), _P]),
     "vx_cuckoo_create": (_ST, [_U32, _U32, C.POINTER(_P)]),
     "vx_cuckoo_destroy": (_ST, [_P]),
     "vx_cuckoo_clear": (_ST, [_P, _P]),

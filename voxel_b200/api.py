@@ -15,7 +15,7 @@ from . import check, lib
 
 __all__ = [
     "stream_handle", "ptr", "exclusive_sum", "inclusive_sum", "sort_pairs",
-    "workspace_status", "SlabHashSet", "SlabHashMap", "CuckooMap", "PRIM_DTYPE",
+    "workspace_status", "SlabHashSet", "SlabHashMap", "CuckooMap", "ItemSet", "PRIM_DTYPE",
     "make_flags", "prims_to_device", "voxels_to_device", "HashDag",
     "generate_primitives", "config_c1_edits", "config_c3_edits",
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
@@ -224,6 +224,52 @@ class SlabHashMap:
         check(lib().vx_slab_map_erase_all(self._h, ptr(keys), keys.numel(), ptr(statuses),
                                           stream_handle()), "slab map erase")
         return statuses
+
+
+class ItemSet:
+    """Content-addressed fixed-width item store (AccelerationHashSet32,
+    cuda/hash_table/acceleration_hash/set/host.cuh); pointers = index + 1."""
+
+    def __init__(self, width: int, max_items: int):
+        h = C.c_void_p()
+        check(lib().vx_itemset_create(width, max_items, C.byref(h)), "vx_itemset_create")
+        self._h = h
+        self.width = width
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().vx_itemset_destroy(h)
+            self._h = None
+
+    def _op(self, fn, items, name):
+        n = items.numel() // self.width
+        ptrs = torch.empty(n, dtype=torch.int32, device=items.device)
+        st = torch.empty(n, dtype=torch.int32, device=items.device)
+        check(fn(self._h, ptr(items), n, ptr(ptrs), ptr(st), stream_handle()), name)
+        return ptrs, st
+
+    def find(self, items: torch.Tensor):
+        return self._op(lib().vx_itemset_find, items, "itemset find")
+
+    def find_or_insert(self, items: torch.Tensor):
+        return self._op(lib().vx_itemset_find_or_insert, items, "itemset find_or_insert")
+
+    def insert_unique_unchecked(self, items: torch.Tensor):
+        return self._op(lib().vx_itemset_insert_unique_unchecked, items, "itemset insert")
+
+    def read(self, ptrs: torch.Tensor):
+        n = ptrs.numel()
+        out = torch.empty(n * self.width, dtype=torch.int32, device=ptrs.device)
+        st = torch.empty(n, dtype=torch.int32, device=ptrs.device)
+        check(lib().vx_itemset_read(self._h, ptr(ptrs), n, ptr(out), ptr(st), stream_handle()),
+              "itemset read")
+        return out, st
+
+    def count(self) -> int:
+        v = C.c_uint64(0)
+        check(lib().vx_itemset_count(self._h, C.byref(v), stream_handle()), "itemset count")
+        return v.value
 
 
 class CuckooMap:

@@ -108,7 +108,8 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
 // matches of an edit are such pre-existing subtrees.  Inserts publish with a
 // release store.
 __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
-                                        const uint32_t *w, uint32_t n) {
+                                        const uint32_t *w, uint32_t n,
+                                        bool *inserted = nullptr) {
   const uint64_t h = hash_words(w, n);
   const uint32_t tag = static_cast<uint32_t>(h >> 32) | 1u;
   uint64_t *idx = t.index[l];
@@ -132,6 +133,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
         for (uint32_t i = 0; i < n; ++i) pool[off + i] = w[i];
         st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | (off + 2u));
         atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]), 1ull);
+        if (inserted) *inserted = true;
         return off + 2u;
       }
       v = old;
@@ -1202,9 +1204,191 @@ struct SizingCarver {
   }
 };
 
+// ------------------------------------------------------------ item set --
+// A standalone content-addressed store of fixed-width items (the reference's
+// AccelerationHashSet32, cuda/hash_table/acceleration_hash/set/*): one table
+// of the same kind as a DAG level.  Pointers are item index + 1 (0 = null).
+
+__device__ __forceinline__ uint32_t item_ptr(uint32_t ref, uint32_t width) {
+  return ref >= 2u ? (ref - 2u) / width + 1u : 0u;
+}
+
+// Probe only: the ref of an equal item, or 0.
+__device__ uint32_t node_find(const Tables &t, uint32_t l, const uint32_t *w, uint32_t n) {
+  const uint64_t h = hash_words(w, n);
+  const uint32_t tag = static_cast<uint32_t>(h >> 32) | 1u;
+  const uint64_t *idx = t.index[l];
+  const uint32_t *pool = t.pool[l];
+  uint64_t pos = h & t.index_mask[l];
+  for (uint32_t probe = 0; probe < kMaxProbes; ++probe) {
+    const uint64_t v = ld_relaxed_u64(idx + pos);
+    if (v == 0) return 0u;
+    const uint32_t r = static_cast<uint32_t>(v);
+    if (static_cast<uint32_t>(v >> 32) == tag && r >= 2u && r != kBusy) {
+      fence_acq_rel_gpu();
+      bool eq = true;
+      for (uint32_t i = 0; i < n && eq; ++i) eq = pool[r - 2u + i] == w[i];
+      if (eq) return r;
+    }
+    pos = (pos + 1) & t.index_mask[l];
+  }
+  return 0u;
+}
+
+enum class ItemOp { Find, FindOrInsert, InsertUnique };
+
+template <ItemOp Op>
+__global__ void itemset_kernel(Tables t, uint32_t width, const uint32_t *items, uint32_t n,
+                               uint32_t *ptrs, uint32_t *statuses) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    uint32_t w[9];
+    for (uint32_t j = 0; j < width; ++j) w[j] = items[i * width + j];
+    uint32_t ref = 0, status = VX_HASH_NOT_FOUND;
+    if (Op == ItemOp::Find) {
+      ref = node_find(t, 0, w, width);
+      status = ref ? VX_HASH_FOUND : VX_HASH_NOT_FOUND;
+    } else if (Op == ItemOp::FindOrInsert) {
+      bool inserted = false;
+      ref = node_find_or_insert(t, 0, w, width, &inserted);
+      status = ref >= 2u ? (inserted ? VX_HASH_INSERTED : VX_HASH_FOUND) : VX_HASH_OVERFLOW;
+      if (ref < 2u) ref = 0;
+    } else {
+      const uint32_t off = atomicAdd(&t.hdr->pool_used[0], width);
+      if (static_cast<uint64_t>(off) + width > t.pool_cap[0]) {
+        status = VX_HASH_OVERFLOW;
+      } else {
+        ref = unique_insert_node(t, 0, w, width, off);
+        status = VX_HASH_INSERTED;
+        atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[0]), 1ull);
+      }
+    }
+    ptrs[i] = item_ptr(ref, width);
+    if (statuses) statuses[i] = status;
+  }
+}
+
+__global__ void itemset_read_kernel(Tables t, uint32_t width, const uint32_t *ptrs, uint32_t n,
+                                    uint32_t *out, uint32_t *statuses) {
+  const uint32_t stored = t.hdr->pool_used[0] / width;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t p = ptrs[i];
+    const bool ok = p >= 1u && p <= stored;
+    for (uint32_t j = 0; j < width; ++j)
+      out[i * width + j] = ok ? t.pool[0][(p - 1u) * static_cast<uint64_t>(width) + j] : 0u;
+    if (statuses) statuses[i] = ok ? VX_HASH_FOUND : VX_HASH_NOT_FOUND;
+  }
+}
+
 } // namespace vx::dag
 
+struct vx_itemset {
+  vx::dag::Tables t{};
+  uint32_t width = 0;
+  uint64_t index_slots = 0;
+};
+
+namespace {
+template <vx::dag::ItemOp Op>
+vx_status itemset_launch(const vx_itemset *s, const uint32_t *items, uint32_t count,
+                         uint32_t *ptrs, uint32_t *statuses, vx_stream stream) {
+  if (s == nullptr || ((items == nullptr || ptrs == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint32_t grid = std::min<uint32_t>(vx::ceil_div(count, vx::dag::kBlock),
+                                           static_cast<uint32_t>(vx::sm_count()) * 16u);
+  vx::prof::Scope sc("itemset", st);
+  vx::dag::itemset_kernel<Op><<<grid, vx::dag::kBlock, 0, st>>>(s->t, s->width, items, count,
+                                                                 ptrs, statuses);
+  return vx::from_cuda(cudaGetLastError());
+}
+} // namespace
+
 extern "C" {
+
+vx_status vx_itemset_clear(vx_itemset *s, vx_stream stream) {
+  if (s == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  VX_TRY_CUDA(cudaMemsetAsync(s->t.index[0], 0, s->index_slots * 8, st));
+  VX_TRY_CUDA(cudaMemsetAsync(s->t.hdr, 0, sizeof(vx::edit::Header), st));
+  return VX_OK;
+}
+
+vx_status vx_itemset_destroy(vx_itemset *s) {
+  if (s == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaFree(s->t.index[0]);
+  cudaFree(s->t.pool[0]);
+  cudaFree(s->t.hdr);
+  delete s;
+  return VX_OK;
+}
+
+vx_status vx_itemset_create(uint32_t width, uint32_t max_items, vx_itemset **out) {
+  if (out == nullptr || width < 1 || width > 9 || max_items == 0) return VX_ERR_INVALID_VALUE;
+  auto *s = new (std::nothrow) vx_itemset;
+  if (s == nullptr) return VX_ERR_MEMORY_ALLOCATION;
+  s->width = width;
+  s->t.depth = 1;
+  s->index_slots = vx::dag::next_pow2(2ull * max_items);
+  s->t.index_mask[0] = s->index_slots - 1;
+  s->t.pool_cap[0] = std::min<uint64_t>(static_cast<uint64_t>(max_items) * width, 0xfffffff0ull);
+  cudaError_t e = cudaMalloc(&s->t.index[0], s->index_slots * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&s->t.pool[0], s->t.pool_cap[0] * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->t.hdr, sizeof(vx::edit::Header));
+  if (e != cudaSuccess) {
+    vx_itemset_destroy(s);
+    return vx::from_cuda(e);
+  }
+  const vx_status st = vx_itemset_clear(s, nullptr);
+  if (st != VX_OK) {
+    vx_itemset_destroy(s);
+    return st;
+  }
+  VX_TRY_CUDA(cudaStreamSynchronize(nullptr));
+  *out = s;
+  return VX_OK;
+}
+
+
+vx_status vx_itemset_find(const vx_itemset *s, const uint32_t *items, uint32_t count,
+                          uint32_t *ptrs, uint32_t *statuses, vx_stream stream) {
+  return itemset_launch<vx::dag::ItemOp::Find>(s, items, count, ptrs, statuses, stream);
+}
+
+vx_status vx_itemset_find_or_insert(vx_itemset *s, const uint32_t *items, uint32_t count,
+                                    uint32_t *ptrs, uint32_t *statuses, vx_stream stream) {
+  return itemset_launch<vx::dag::ItemOp::FindOrInsert>(s, items, count, ptrs, statuses, stream);
+}
+
+vx_status vx_itemset_insert_unique_unchecked(vx_itemset *s, const uint32_t *items,
+                                             uint32_t count, uint32_t *ptrs,
+                                             uint32_t *statuses, vx_stream stream) {
+  return itemset_launch<vx::dag::ItemOp::InsertUnique>(s, items, count, ptrs, statuses, stream);
+}
+
+vx_status vx_itemset_read(const vx_itemset *s, const uint32_t *ptrs, uint32_t count,
+                          uint32_t *items, uint32_t *statuses, vx_stream stream) {
+  if (s == nullptr || ((items == nullptr || ptrs == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint32_t grid = std::min<uint32_t>(vx::ceil_div(count, vx::dag::kBlock),
+                                           static_cast<uint32_t>(vx::sm_count()) * 16u);
+  vx::prof::Scope sc("itemset_read", st);
+  vx::dag::itemset_read_kernel<<<grid, vx::dag::kBlock, 0, st>>>(s->t, s->width, ptrs, count,
+                                                                 items, statuses);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_itemset_count(const vx_itemset *s, uint64_t *host_count, vx_stream stream) {
+  if (s == nullptr || host_count == nullptr) return VX_ERR_INVALID_VALUE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  VX_TRY_CUDA(cudaMemcpyAsync(host_count, &s->t.hdr->node_count[0], 8, cudaMemcpyDeviceToHost, st));
+  VX_TRY_CUDA(cudaStreamSynchronize(st));
+  return VX_OK;
+}
 
 vx_status vx_dag_import_canonical(vx_dag *d, uint32_t root, const uint64_t *host_counts,
                                   const uint32_t *host_nodes, const uint64_t *host_leaves,
