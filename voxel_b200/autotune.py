@@ -11,11 +11,12 @@ which the library applies when it is first loaded on that kind of device:
     whether a tile publishes its digit counts before or after ranking, and
     whether keys are ranked with per-bit ballots or match_any; timed on 2^26
     u32 and 2^25 60-bit u64 key/value pairs;
-  * edit.big_item / edit.blocks_per_sm: the primitive-list length above which
-    a work item is expanded by a whole block, and the grid of the edit
-    pipelines' item kernels; timed on a batched Hash DAG edit (4096^3 cave
-    terrain at scale 16, 4096 spheres of radius log-uniform in [1, 256],
-    60 % add).
+  * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks: the
+    primitive-list length above which a work item is expanded by a whole
+    block, the grid of the edit pipelines' item kernels, and the resident
+    blocks the DAG leaf-parent kernel is built for; timed on the batched Hash
+    DAG edit of the benchmark (16384^3 cave terrain at scale 64, 16,384
+    spheres of radius log-uniform in [1, 256], 60 % add).
 
 Every setting's output is compared with the default setting's (the sorted
 arrays bit for bit, the edited DAG by 2^20 point queries) before its time
@@ -114,11 +115,11 @@ def tune_sort(n32: int, n64: int, reps: int, log) -> tuple[dict, dict]:
                   for (l, i, e, b), t in times.items()}
 
 
-def tune_edit(depth: int, count: int, reps: int, log, max_nodes: int,
+def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int,
               arena: int) -> tuple[dict, dict]:
-    prims = vx.prims_to_device(vx.config_c4_edits(count, seed=5, world_exp=depth + 2), "cuda")
+    prims = vx.prims_to_device(vx.config_c4_edits(count, seed=7, world_exp=depth + 2), "cuda")
     pristine = vx.HashDag(depth, max_nodes, arena)
-    pristine.build_terrain(7, max(1, (4 << depth) // 256), True)  # C3's scale rule
+    pristine.build_terrain(7, scale, True)
     if pristine.status() != 0:
         raise RuntimeError("terrain build failed")
     work = vx.HashDag(depth, max_nodes, arena)
@@ -133,10 +134,11 @@ def tune_edit(depth: int, count: int, reps: int, log, max_nodes: int,
         raise RuntimeError("reference edit failed")
     ref = work.query(pts)
     times: dict = {}
-    for big, bps in itertools.product(vx.tuning_options("edit.big_item"),
-                                      vx.tuning_options("edit.blocks_per_sm")):
+
+    def measure(big, bps, lpb):
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
+        vx.set_tuning("edit.leafparent_blocks", lpb)
         work.copy_from(pristine)
         work.apply_primitives(prims)
         ok = work.status() == 0 and bool(torch.equal(work.query(pts), ref))
@@ -144,24 +146,66 @@ def tune_edit(depth: int, count: int, reps: int, log, max_nodes: int,
                    lambda: work.copy_from(pristine)) if ok else None
         if ok and work.status() != 0:
             ms = None
-        times[f"big_item={big} blocks_per_sm={bps}"] = ms
-        log(f"  edit big_item={big} blocks_per_sm={bps}: "
+        times[f"big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb}"] = ms
+        log(f"  edit big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb}: "
             + (f"{ms:.3f} ms" if ms is not None else "FAILED OR DIFFERENT (not used)"))
+        return ms
+
+    # Stage 1: long-list threshold and grid.  Among settings within 2 % of
+    # the fastest, take the smallest grid: on a large batch more blocks gain
+    # little, while on small batches (the serving loop's) every extra block
+    # is launch overhead.
+    lpb0 = vx.tuning()["edit.leafparent_blocks"]
+    stage1 = {}
+    for big, bps in itertools.product(vx.tuning_options("edit.big_item"),
+                                      vx.tuning_options("edit.blocks_per_sm")):
+        ms = measure(big, bps, lpb0)
+        if ms is not None:
+            stage1[(big, bps)] = ms
+    fastest = min(stage1.values())
+    near = [k for k, t in stage1.items() if t <= 1.02 * fastest]
+    big, bps = min(near, key=lambda k: (k[1], stage1[k]))
+    # Stage 2: resident blocks of the leaf-parent kernel at that setting.
+    stage2 = {}
+    for lpb in vx.tuning_options("edit.leafparent_blocks"):
+        ms = measure(big, bps, lpb)
+        if ms is not None:
+            stage2[lpb] = ms
+    lpb = min(stage2, key=stage2.get)
     vx.reset_tuning()
-    valid = {k: t for k, t in times.items() if t is not None}
-    # Among settings within 2 % of the fastest, take the smallest grid: on a
-    # large batch more blocks gain little, while on small batches (the
-    # serving loop's) every extra block is launch overhead.
-    fastest = min(valid.values())
-    near = [k for k, t in valid.items() if t <= 1.02 * fastest]
+    return {"edit.big_item": big, "edit.blocks_per_sm": bps,
+            "edit.leafparent_blocks": lpb}, times
 
-    def parse(k):
-        big, bps = (int(f.split("=")[1]) for f in k.split())
-        return big, bps
 
-    key = min(near, key=lambda k: (parse(k)[1], valid[k]))
-    big, bps = parse(key)
-    return {"edit.big_item": big, "edit.blocks_per_sm": bps}, times
+def tune_serve(depth: int, scale: int, batch: int, reps: int, log, max_nodes: int,
+               arena: int) -> tuple[dict, dict]:
+    """serve.blocks_per_sm: latency of one small batch (the serving loop's
+    typical size) replayed as a graph with a device-side count, on the served
+    terrain; the same pipeline the serving loop captures."""
+    prims = vx.generate_primitives(depth + 2, batch, 8, sphere_permille=500, add_permille=500,
+                                   r_min=1, r_max=128, log_uniform=True)
+    buf = vx.prims_to_device(prims, "cuda")
+    cnt = torch.tensor([batch], dtype=torch.int32, device="cuda")
+    pristine = vx.HashDag(depth, max_nodes, arena)
+    pristine.build_terrain(8, scale, True)
+    if pristine.status() != 0:
+        raise RuntimeError("terrain build failed")
+    work = vx.HashDag(depth, max_nodes, arena)
+    times: dict = {}
+    for bps in vx.tuning_options("serve.blocks_per_sm"):
+        vx.set_tuning("edit.blocks_per_sm", bps)  # the serving graphs' grid
+        graph = work.graph_primitives(buf, cnt, batch)
+        work.copy_from(pristine)
+        graph.launch()
+        ok = work.status() == 0
+        ms = _time(graph.launch, reps, lambda: work.copy_from(pristine)) if ok else None
+        graph.close()
+        times[f"blocks_per_sm={bps}"] = ms
+        log(f"  serve batch of {batch} blocks_per_sm={bps}: "
+            + (f"{ms:.3f} ms" if ms is not None else "FAILED (not used)"))
+    vx.reset_tuning()
+    valid = {int(k.split("=")[1]): t for k, t in times.items() if t is not None}
+    return {"serve.blocks_per_sm": min(valid, key=valid.get)}, times
 
 
 def main(argv=None) -> dict:
@@ -177,16 +221,18 @@ def main(argv=None) -> dict:
     t0 = time.time()
     if args.quick:
         sort_best, sort_t = tune_sort(1 << 20, 1 << 19, 2, log)
-        edit_best, edit_t = tune_edit(6, 256, 2, log, 1 << 18, 64 << 20)
+        edit_best, edit_t = tune_edit(6, 1, 256, 2, log, 1 << 18, 64 << 20)
+        serve_best, serve_t = tune_serve(6, 1, 64, 2, log, 1 << 18, 64 << 20)
     else:
         sort_best, sort_t = tune_sort(1 << 26, 1 << 25, 5, log)
-        edit_best, edit_t = tune_edit(10, 4096, 5, log, 1 << 26, 4 << 30)
+        edit_best, edit_t = tune_edit(12, 64, 16384, 5, log, 1 << 27, 16 << 30)
+        serve_best, serve_t = tune_serve(11, 32, 400, 9, log, 1 << 27, 8 << 30)
     result = {
         "device": dev,
         "quick": bool(args.quick),
         "seconds": round(time.time() - t0, 1),
-        "knobs": {**sort_best, **edit_best},
-        "timings_ms": {"sort": sort_t, "edit": edit_t},
+        "knobs": {**sort_best, **edit_best, **serve_best},
+        "timings_ms": {"sort": sort_t, "edit": edit_t, "serve": serve_t},
     }
     out = args.out or str(tuning_file(dev))
     from pathlib import Path

@@ -179,9 +179,11 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.early_counts", 0, {0, 1}, 2},
     {"sort.rank_ballots", 1, {0, 1}, 2},
     {"edit.big_item", 32, {16, 32, 64, 128, 256, 512}, 6},
-    {"edit.blocks_per_sm", 16, {2, 4, 8, 16, 32}, 5},
+    {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
+    {"edit.leafparent_blocks", 6, {4, 5, 6}, 3},
+    {"serve.blocks_per_sm", 8, {2, 4, 8, 16, 32}, 5},
 };
-std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {16}};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {32}, {6}, {8}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

@@ -229,8 +229,11 @@ __global__ void mark_pools_kernel(Tables t) {
 
 // Level depth - 1: evaluate the 8 leaves of every item (8 threads per item)
 // and hash-cons the item.
-template <bool Terrain>
-__global__ void __launch_bounds__(kBlock, 4) leafparent_kernel(Ctx x) {
+// MinBlocks (the tuning knob "edit.leafparent_blocks") trades registers for
+// resident blocks: the kernel is bound by chains of dependent loads, so more
+// items in flight can outweigh a few spilled values.
+template <bool Terrain, int MinBlocks>
+__global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
   Header *h = x.t.hdr;
   if (ld_relaxed_u32(&h->status) != kDevOk) return;
   const uint32_t l = x.t.depth - 1;
@@ -422,13 +425,15 @@ inline uint64_t next_pow2(uint64_t v) {
 
 vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
                        const uint32_t *d_count, uint32_t host_count,
-                       cudaStream_t s, bool terrain = false) {
+                       cudaStream_t s, bool terrain = false,
+                       uint32_t blocks_per_sm = 0 /* 0: the edit.blocks_per_sm knob */) {
   Ctx x{d->t, d->a, prims, d_count, host_count};
   const EditCtx e{d->t.hdr, d->a, prims, d_count, host_count, d->t.depth,
                   static_cast<uint32_t>(tune::get(tune::kEditBigItem))};
   const uint32_t depth = d->t.depth;
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
-                        static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm));
+                        (blocks_per_sm ? blocks_per_sm
+                                       : static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm)));
   {
     prof::Scope sc("dag_init", s);
     init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),
@@ -461,10 +466,15 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   VX_TRY_CUDA(cudaGetLastError());
   {
     prof::Scope sc("dag_leafparent", s);
+    const int64_t lb = tune::get(tune::kEditLeafparentBlocks);
     if (terrain)
-      leafparent_kernel<true><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<true, 4><<<grid, kBlock, 0, s>>>(x);
+    else if (lb == 6)
+      leafparent_kernel<false, 6><<<grid, kBlock, 0, s>>>(x);
+    else if (lb == 5)
+      leafparent_kernel<false, 5><<<grid, kBlock, 0, s>>>(x);
     else
-      leafparent_kernel<false><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<false, 4><<<grid, kBlock, 0, s>>>(x);
   }
   VX_TRY_CUDA(cudaGetLastError());
   for (uint32_t r = depth - 1; r > 0; --r) {
@@ -699,6 +709,23 @@ vx_status vx_dag_graph_primitives(vx_dag *d, const vx_primitive *prims,
   return vx::graph::capture(
       [&](cudaStream_t s) { return run_pipeline(d, prims, device_count, capacity, s); }, out);
 }
+
+} // extern "C"
+
+namespace vx::dag {
+vx_status graph_primitives_grid(vx_dag *d, const vx_primitive *prims, const uint32_t *d_count,
+                                uint32_t capacity, uint32_t blocks_per_sm, vx_graph **out) {
+  if (d == nullptr || out == nullptr || prims == nullptr || capacity == 0)
+    return VX_ERR_INVALID_VALUE;
+  return vx::graph::capture(
+      [&](cudaStream_t s) {
+        return run_pipeline(d, prims, d_count, capacity, s, false, blocks_per_sm);
+      },
+      out);
+}
+} // namespace vx::dag
+
+extern "C" {
 
 vx_status vx_dag_graph_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count, uint32_t op,
                               void *workspace, size_t workspace_bytes, vx_graph **out) {

@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "dag_internal.cuh"
 #include "profile.cuh"
+#include "tuning.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -309,8 +310,9 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
   }
   if (s->cfg.launch_mode == 0) {
     for (int k = 0; k < 2; ++k) {
-      const vx_status st = vx_dag_graph_primitives(dag, s->d_buf[k], s->d_count + k,
-                                                    s->hard_cap, &s->graph[k]);
+      const vx_status st = vx::dag::graph_primitives_grid(
+          dag, s->d_buf[k], s->d_count + k, s->hard_cap,
+          static_cast<uint32_t>(vx::tune::get(vx::tune::kServeBlocksPerSm)), &s->graph[k]);
       if (st != VX_OK) {
         vx_serve_destroy(s);
         return st;

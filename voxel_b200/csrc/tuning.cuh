@@ -14,6 +14,8 @@ enum Id : uint32_t {
   kSortRankBallots, // rank keys with per-bit ballots (1) or match_any (0)
   kEditBigItem,     // items with more primitives go to the block-per-item expansion
   kEditBlocksPerSm, // grid of the edit pipelines' item kernels, in blocks per SM
+  kEditLeafparentBlocks, // resident blocks the DAG leaf-parent kernel is built for
+  kServeBlocksPerSm, // grid of the serving loop's edit graphs, in blocks per SM
   kKnobCount
 };
 
