@@ -7,7 +7,7 @@
 // from pinned host memory and launches the batched edit on the server's
 // stream (one CUDA graph per upload slot, captured at creation, which reads
 // the batch size from device memory, so a batch is two copies and one
-// launch); up to max_inflight batches are in flight, so requests that arrive
+// launch; the copies run on a second stream and overlap the previous edit); up to max_inflight batches are in flight, so requests that arrive
 // while the GPU works on one batch are admitted into the next as soon as a
 // slot frees, and their upload overlaps the running edit.  A completion
 // thread waits for each batch's event, stamps every request of the batch with
@@ -73,6 +73,10 @@ struct vx_server {
   uint32_t *h_count = nullptr; // pinned, one word per slot
   uint32_t *d_count = nullptr; // one word per slot
   vx_graph *graph[2] = {nullptr, nullptr};
+  // uploads run on their own stream, so a batch's copy overlaps the edit
+  // of the batch before it; the edit waits on the slot's upload event
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t uploaded[2] = {nullptr, nullptr};
   unsigned char *h_hdr[2] = {nullptr, nullptr};
   bool slot_busy[2] = {false, false};
   std::vector<unsigned char> last_hdr; // header copy of the last completed batch
@@ -173,14 +177,16 @@ void worker_loop(vx_server *s) {
       off += static_cast<uint32_t>(r.prims.size());
     }
     cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
+    // The slot is not reused before this batch completes, so its buffers
+    // (pinned and device) are stable until the copies and the edit ran.
     cudaMemcpyAsync(s->d_buf[b.slot], s->h_buf[b.slot], b.nprims * sizeof(vx_primitive),
-                    cudaMemcpyHostToDevice, s->stream);
+                    cudaMemcpyHostToDevice, s->copy_stream);
+    s->h_count[b.slot] = b.nprims;
+    cudaMemcpyAsync(s->d_count + b.slot, s->h_count + b.slot, sizeof(uint32_t),
+                    cudaMemcpyHostToDevice, s->copy_stream);
+    cudaEventRecord(s->uploaded[b.slot], s->copy_stream);
+    cudaStreamWaitEvent(s->stream, s->uploaded[b.slot], 0);
     if (s->graph[b.slot] != nullptr) {
-      // The slot is not reused before this batch completes, so its pinned
-      // count word is stable until the copy runs.
-      s->h_count[b.slot] = b.nprims;
-      cudaMemcpyAsync(s->d_count + b.slot, s->h_count + b.slot, sizeof(uint32_t),
-                      cudaMemcpyHostToDevice, s->stream);
       vx_graph_launch(s->graph[b.slot], s->stream);
     } else if (b.nprims) {
       vx_dag_apply_primitives(s->dag, s->d_buf[b.slot], b.nprims, s->stream);
@@ -297,6 +303,9 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
   s->batch_cap = s->cfg.max_batch_prims;
   cudaGetDevice(&s->device);
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+    e = cudaEventCreateWithFlags(&s->uploaded[k], cudaEventDisableTiming);
   for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
     e = cudaMallocHost(&s->h_buf[k], s->hard_cap * sizeof(vx_primitive));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_buf[k], s->hard_cap * sizeof(vx_primitive));
@@ -382,6 +391,7 @@ vx_status vx_serve_destroy(vx_server *s) {
   }
   s->cv.notify_all();
   if (s->completer.joinable()) s->completer.join();
+  if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (int k = 0; k < 2; ++k) {
     if (s->graph[k]) vx_graph_destroy(s->graph[k]);
@@ -391,6 +401,9 @@ vx_status vx_serve_destroy(vx_server *s) {
   }
   if (s->h_count) cudaFreeHost(s->h_count);
   if (s->d_count) cudaFree(s->d_count);
+  for (int k = 0; k < 2; ++k)
+    if (s->uploaded[k]) cudaEventDestroy(s->uploaded[k]);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return VX_OK;
