@@ -1004,6 +1004,40 @@ def run_reference(args, ws, rank):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_case_dag_full(args, torch, vx, dev):
+    """The C4 batch alone (16384^3 terrain, 16,384 spheres): device time per
+    batch and per kernel over --steps batches, each from the restored
+    terrain; for measuring and profiling the headline edit."""
+    lib = vx.lib()
+    world_exp = DAG_DEPTH + 2
+    pristine = vx.HashDag(DAG_DEPTH, DAG_MAX_NODES, DAG_ARENA)
+    pristine.build_terrain(DAG_SEED, DAG_SCALE, True)
+    assert pristine.status() == 0
+    work = vx.HashDag(DAG_DEPTH, DAG_MAX_NODES, DAG_ARENA)
+    prims = vx.prims_to_device(vx.config_c4_edits(DAG_EDITS, seed=DAG_SEED, world_exp=world_exp),
+                               dev)
+    stream = torch.cuda.current_stream()
+    ms = []
+    lib.vx_profile_reset()
+    for i in range(args.steps + 1):
+        work.copy_from(pristine)
+        lib.vx_profile_enable(1 if i else 0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        work.apply_primitives(prims)
+        b.record(stream)
+        torch.cuda.synchronize()
+        lib.vx_profile_enable(0)
+        assert work.status() == 0
+        if i:
+            ms.append(a.elapsed_time(b))
+    kern = {k: round(_prof(lib, k)[1] / args.steps, 3)
+            for k in ("dag_expand", "dag_expand_big", "dag_leafparent", "dag_build")}
+    print(json.dumps({"case": "dag_full", "ms": [round(x, 3) for x in ms],
+                      "kernel_ms_per_batch": kern, "tuning": vx.tuning()}))
+
+
 def run_case(args):
     """One operation on a small input, for profiler captures:
     --case scan|sort_u32|sort_u64 --elements N (runs --steps launches)."""
@@ -1012,6 +1046,8 @@ def run_case(args):
     dev = torch.device("cuda:0")
     n = args.elements
     ms = []
+    if args.case == "dag_full":
+        return run_case_dag_full(args, torch, vx, dev)
     for _ in range(args.steps):
         if args.case == "scan":
             x = torch.randint(0, 256, (n,), dtype=torch.int32, device=dev)
@@ -1060,7 +1096,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64", "dag"], default=None)
+    ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64", "dag", "dag_full"],
+                    default=None)
     ap.add_argument("--elements", type=int, default=1 << 24)
     ap.add_argument("--serve-seconds", type=float, default=SERVE_SECONDS,
                     help="length of the served arrival stream (0 skips serving)")

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
     const uint64_t g = g0 + lane;
     const bool have = g < total; // the same for the 8 lanes of a group
     const uint32_t wi = static_cast<uint32_t>(g >> 3), c = lane & 7u;
-    uint32_t result = kEmptyRef;
+    uint32_t result = kEmptyRef, old_child = kEmptyRef;
     Item it{};
     if (have) {
       it = x.a.items[base + wi];
@@ -262,11 +262,22 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
       const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * 4;
       const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
       const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
-      const uint32_t old_child = child_ref(x.t, l, it.old, c);
+      // Independent loads side by side: the first chunk's pair index and the
+      // old node, then its primitive and the old leaf (read speculatively:
+      // the kernel is bound by dependent round trips, not by bandwidth).
+      const uint32_t n0 = it.pcount < 8u ? it.pcount : 8u;
+      const uint32_t pidx = c < n0 ? pairs[it.pstart + c] : 0u;
+      old_child = child_ref(x.t, l, it.old, c);
+      vx_primitive first{};
+      if (c < n0) first = x.prims[pidx];
+      const uint64_t old_mask = read_leaf(x.t, old_child);
+      __syncwarp(gmask); // the group's previous item no longer reads s_pr
+      s_pr[grp][c] = first;
+      __syncwarp(gmask);
       uint64_t mask = 0;
       bool loaded = false, touched = false;
       for (uint32_t k = 0; k < it.pcount; ++k) {
-        if ((k & 7u) == 0) {
+        if ((k & 7u) == 0 && k != 0) {
           __syncwarp(gmask); // the previous chunk is no longer read
           if (k + c < it.pcount) s_pr[grp][c] = x.prims[pairs[it.pstart + k + c]];
           __syncwarp(gmask);
@@ -282,19 +293,24 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
           continue;
         }
         if (!loaded) {
-          mask = read_leaf(x.t, old_child);
+          mask = old_mask;
           loaded = true;
         }
         const uint64_t m = leaf_mask<Terrain>(pr, world_exp, ox, oy, oz);
         mask = add ? (mask | m) : (mask & ~m);
       }
-      result = touched ? canon_leaf(x.t, mask) : old_child;
+      // An unchanged mask keeps its canonical ref: no probe of the leaf set.
+      result = (touched && mask != old_mask) ? canon_leaf(x.t, mask) : old_child;
     }
+    // A node whose 8 children all kept their refs is the old node itself
+    // (refs are canonical), so its hash-consing is skipped.
+    const uint32_t changed = __ballot_sync(kFullMask, result != old_child);
+    const bool same = ((changed >> (lane & ~7u)) & 0xffu) == 0u;
     uint32_t child[8];
 #pragma unroll
     for (uint32_t k = 0; k < 8; ++k)
       child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
-    if (have && c == 0) x.a.items[base + wi].result = canon_node(x.t, l, child);
+    if (have && c == 0) x.a.items[base + wi].result = same ? it.old : canon_node(x.t, l, child);
   }
 }
 
@@ -318,7 +334,12 @@ __global__ void __launch_bounds__(kBlock) build_kernel(Ctx x, uint32_t l) {
       else if (km & bit) child[c] = (kf & bit) ? kFullRef : kEmptyRef;
       else child[c] = child_ref(x.t, l, it.old, c);
     }
-    x.a.items[base + i].result = canon_node(x.t, l, child);
+    // Every child kept its ref: the node is the old one (refs are canonical).
+    bool same = true;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c)
+      if ((cm | km) & (1u << c)) same = same && child[c] == child_ref(x.t, l, it.old, c);
+    x.a.items[base + i].result = same ? it.old : canon_node(x.t, l, child);
   }
 }
 
