@@ -57,11 +57,74 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
   return x;
 }
 
+// Hash of an item's n words, fed one word at a time: each word is folded in
+// by an xor, a multiply by an odd constant and a rotation (a bijection of
+// the state for every word, so items that differ in one word never
+// collide), and splitmix64's finaliser spreads the state over all 64 bits.
+struct WordHash {
+  uint64_t h;
+  __device__ __forceinline__ explicit WordHash(uint32_t n) : h(0x243f6a8885a308d3ull ^ n) {}
+  __device__ __forceinline__ void add(uint32_t w) {
+    const uint64_t x = (h ^ w) * 0x9fb21c651e98df25ull;
+    h = (x << 29) | (x >> 35);
+  }
+  __device__ __forceinline__ uint64_t finish() const { return mix64(h); }
+};
+
 __device__ __forceinline__ uint64_t hash_words(const uint32_t *w, uint32_t n) {
-  uint64_t h = 0x243f6a8885a308d3ull ^ n;
-  for (uint32_t i = 0; i < n; ++i) h = mix64(h ^ (static_cast<uint64_t>(w[i]) + (static_cast<uint64_t>(i) << 32)));
-  return h;
+  WordHash s(n);
+  for (uint32_t i = 0; i < n; ++i) s.add(w[i]);
+  return s.finish();
 }
+
+// The words of an item as node_find_or_insert sees them: a plain array ...
+struct ArrayWords {
+  const uint32_t *w;
+  uint32_t n;
+  __device__ __forceinline__ uint32_t size() const { return n; }
+  __device__ __forceinline__ uint64_t hash() const { return hash_words(w, n); }
+  __device__ __forceinline__ bool equals(const uint32_t *item) const {
+    bool eq = true;
+    for (uint32_t i = 0; i < n && eq; ++i) eq = item[i] == w[i];
+    return eq;
+  }
+  __device__ __forceinline__ void write(uint32_t *dst) const {
+    for (uint32_t i = 0; i < n; ++i) dst[i] = w[i];
+  }
+};
+
+// ... or a node's header and its 8 child refs, of which those in the child
+// mask follow the header.  Kept in registers: every loop over the children
+// unrolls, so no word array goes to local memory.
+struct ChildWords {
+  uint32_t header; // child_mask | fill_mask << 8
+  const uint32_t (&child)[8];
+  __device__ __forceinline__ uint32_t size() const { return 1u + __popc(header & 0xffu); }
+  __device__ __forceinline__ uint64_t hash() const {
+    WordHash s(size());
+    s.add(header);
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c)
+      if (header & (1u << c)) s.add(child[c]);
+    return s.finish();
+  }
+  __device__ __forceinline__ bool equals(const uint32_t *item) const {
+    if (item[0] != header) return false; // equal headers: equal lengths
+    bool eq = true;
+    uint32_t k = 1;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c)
+      if (header & (1u << c)) eq &= item[k++] == child[c];
+    return eq;
+  }
+  __device__ __forceinline__ void write(uint32_t *dst) const {
+    dst[0] = header;
+    uint32_t k = 1;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c)
+      if (header & (1u << c)) dst[k++] = child[c];
+  }
+};
 
 // ------------------------------------------------------------- reading --
 
@@ -107,10 +170,11 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
 // began): items from earlier launches are visible without one, and most
 // matches of an edit are such pre-existing subtrees.  Inserts publish with a
 // release store.
-__device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
-                                        const uint32_t *w, uint32_t n,
+template <class Words>
+__device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words &w,
                                         bool *inserted = nullptr) {
-  const uint64_t h = hash_words(w, n);
+  const uint32_t n = w.size();
+  const uint64_t h = w.hash();
   const uint32_t tag = static_cast<uint32_t>(h >> 32) | 1u;
   uint64_t *idx = t.index[l];
   uint32_t *pool = t.pool[l];
@@ -130,7 +194,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
           st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | kFullRef);
           return kEmptyRef;
         }
-        for (uint32_t i = 0; i < n; ++i) pool[off + i] = w[i];
+        w.write(pool + off);
         st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | (off + 2u));
         atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]), 1ull);
         if (inserted) *inserted = true;
@@ -153,10 +217,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
       }
       if (r >= 2u) {
         if (r - 2u >= mark) fence_acq_rel_gpu(); // inserted by this edit
-        const uint32_t *item = pool + (r - 2u);
-        bool eq = true;
-        for (uint32_t i = 0; i < n && eq; ++i) eq = item[i] == w[i];
-        if (eq) return r;
+        if (w.equals(pool + (r - 2u))) return r;
       }
     }
     pos = (pos + 1) & t.index_mask[l];
@@ -169,23 +230,18 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l,
 // the sentinels, everything else is hash-consed into level l's table.
 __device__ uint32_t canon_node(const Tables &t, uint32_t l,
                                const uint32_t (&child)[8]) {
-  uint32_t w[9];
-  uint32_t cm = 0, fm = 0, n = 1;
+  uint32_t cm = 0, fm = 0;
 #pragma unroll
   for (uint32_t c = 0; c < 8; ++c) {
     const uint32_t r = child[c];
     if (r == kFullRef) fm |= 1u << c;
-    else if (r >= 2u) {
-      cm |= 1u << c;
-      w[n++] = r;
-    }
+    else if (r >= 2u) cm |= 1u << c;
   }
   if (cm == 0) {
     if (fm == 0) return kEmptyRef;
     if (fm == 0xffu) return kFullRef;
   }
-  w[0] = cm | (fm << 8);
-  return node_find_or_insert(t, l, w, n);
+  return node_find_or_insert(t, l, ChildWords{cm | (fm << 8), child});
 }
 
 __device__ __forceinline__ uint32_t canon_leaf(const Tables &t, uint64_t mask) {
@@ -1298,7 +1354,7 @@ __global__ void itemset_kernel(Tables t, uint32_t width, const uint32_t *items, 
       status = ref ? VX_HASH_FOUND : VX_HASH_NOT_FOUND;
     } else if (Op == ItemOp::FindOrInsert) {
       bool inserted = false;
-      ref = node_find_or_insert(t, 0, w, width, &inserted);
+      ref = node_find_or_insert(t, 0, ArrayWords{w, width}, &inserted);
       status = ref >= 2u ? (inserted ? VX_HASH_INSERTED : VX_HASH_FOUND) : VX_HASH_OVERFLOW;
       if (ref < 2u) ref = 0;
     } else {
