@@ -161,6 +161,34 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+// atomicAdd of v (below 32) to a counter by the lanes that arrive here
+// together, as one atomic per warp: each lane gets the counter's old value
+// plus the sum of the lanes below it, as from its own atomicAdd.  Counters
+// that every insert of a hash table bumps serialise in L2 when each lane
+// adds on its own.
+__device__ __forceinline__ uint32_t warp_atomic_add_small(uint32_t *ctr, uint32_t v) {
+  const uint32_t am = __activemask();
+  const uint32_t below = am & lanemask_lt();
+  uint32_t prefix = 0, total = 0;
+#pragma unroll
+  for (uint32_t b = 0; b < 5; ++b) {
+    const uint32_t bits = __ballot_sync(am, (v >> b) & 1u);
+    prefix += static_cast<uint32_t>(__popc(bits & below)) << b;
+    total += static_cast<uint32_t>(__popc(bits)) << b;
+  }
+  const uint32_t leader = __ffs(am) - 1u;
+  uint32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(ctr, total);
+  return __shfl_sync(am, base, leader) + prefix;
+}
+
+// atomicAdd of 1 to a 64-bit counter by the lanes that arrive together, as
+// one atomic per warp.
+__device__ __forceinline__ void warp_count_u64(unsigned long long *ctr) {
+  const uint32_t am = __activemask();
+  if (lane_id() == __ffs(am) - 1u) atomicAdd(ctr, static_cast<unsigned long long>(__popc(am)));
+}
+
 template <class T> __device__ __forceinline__ T warp_inclusive_sum(T v) {
 #pragma unroll
   for (uint32_t d = 1; d < kWarp; d <<= 1) {

@@ -153,7 +153,7 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
       const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(t.leaves + pos),
                                      0ull, static_cast<unsigned long long>(mask));
       if (old == 0) {
-        atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[t.depth]), 1ull);
+        warp_count_u64(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[t.depth]));
         return static_cast<uint32_t>(pos + 2);
       }
       if (old == mask) return static_cast<uint32_t>(pos + 2);
@@ -187,7 +187,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
       const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos),
                                      0ull, static_cast<unsigned long long>(claim));
       if (old == 0) {
-        const uint32_t off = atomicAdd(&t.hdr->pool_used[l], n);
+        const uint32_t off = warp_atomic_add_small(&t.hdr->pool_used[l], n);
         if (static_cast<uint64_t>(off) + n > t.pool_cap[l]) {
           set_status(&t.hdr->status, kDevCapacity);
           // Leave a dead entry (ref 1 never matches an item) so waiters move on.
@@ -196,7 +196,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
         }
         w.write(pool + off);
         st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | (off + 2u));
-        atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]), 1ull);
+        warp_count_u64(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]));
         if (inserted) *inserted = true;
         return off + 2u;
       }

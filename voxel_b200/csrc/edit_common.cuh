@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(kBlock)
   const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
   const uint32_t world_exp = depth + 2;
   constexpr uint32_t kGroups = kBlock / 8;
+  static_assert(kGroups == kWarp, "one warp scans the groups' counts");
 
   __shared__ uint32_t s_items[kGroups], s_pairs[kGroups];
   __shared__ uint32_t s_item_base, s_pair_base;
@@ -297,6 +298,9 @@ __global__ void __launch_bounds__(kBlock)
     const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
     const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
     const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
+    // The child's previous content, read before the list walk so that the
+    // two chains of loads overlap (unused when a primitive covers the child).
+    const uint32_t old_child = have && !big ? pol.child(l, it.old, c) : 0u;
     int32_t last_full = -1;
     uint32_t cnt = 0;
     for (uint32_t k = 0; k < it.pcount; ++k) {
@@ -336,21 +340,21 @@ __global__ void __launch_bounds__(kBlock)
       s_pairs[group] = have && !big ? group_pairs : 0u;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t ti = 0, tp = 0;
-      for (uint32_t g = 0; g < kGroups; ++g) {
-        const uint32_t a = s_items[g], b = s_pairs[g];
-        s_items[g] = ti;
-        s_pairs[g] = tp;
-        ti += a;
-        tp += b;
+    if (threadIdx.x < kWarp) { // one group per lane: exclusive offsets by shuffles
+      const uint32_t a = s_items[threadIdx.x], b = s_pairs[threadIdx.x];
+      const uint32_t ia = warp_inclusive_sum(a), ib = warp_inclusive_sum(b);
+      s_items[threadIdx.x] = ia - a;
+      s_pairs[threadIdx.x] = ib - b;
+      const uint32_t ti = __shfl_sync(kFullMask, ia, kWarp - 1);
+      const uint32_t tp = __shfl_sync(kFullMask, ib, kWarp - 1);
+      if (threadIdx.x == 0) {
+        s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
+        s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
+        if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
+          set_status(&h->status, kDevCapacity);
+        if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
+          set_status(&h->status, kDevCapacity);
       }
-      s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
-      s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
-      if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
-        set_status(&h->status, kDevCapacity);
-      if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
-        set_status(&h->status, kDevCapacity);
     }
     __syncthreads();
     const bool room = ld_relaxed_u32(&h->status) == kDevOk;
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(kBlock)
       const uint32_t my_pairs = pair_off + inc_pairs - cnt;
       Item ci{};
       ci.cell = child_cell(it.cell, c);
-      ci.old = last_full >= 0 ? const_val : pol.child(l, it.old, c);
+      ci.old = last_full >= 0 ? const_val : old_child;
       ci.pstart = my_pairs;
       ci.pcount = cnt;
       x.a.items[next_base + item_off + inc_items - 1] = ci;

@@ -113,12 +113,12 @@ struct SvoTree {
 };
 
 __device__ __forceinline__ uint32_t alloc_node(const Tables &t) {
-  const uint32_t r = atomicAdd(&t.ctr->taken_nodes, 1u);
+  const uint32_t r = warp_atomic_add_small(&t.ctr->taken_nodes, 1u);
   const uint32_t bf = t.ctr->base_free_nodes;
   return r < bf ? t.free_nodes[bf - 1u - r] : t.ctr->base_node_count + (r - bf);
 }
 __device__ __forceinline__ uint32_t alloc_leaf(const Tables &t) {
-  const uint32_t r = atomicAdd(&t.ctr->taken_leaves, 1u);
+  const uint32_t r = warp_atomic_add_small(&t.ctr->taken_leaves, 1u);
   const uint32_t bf = t.ctr->base_free_leaves;
   return r < bf ? t.free_leaves[bf - 1u - r] : t.ctr->base_leaf_count + (r - bf);
 }
