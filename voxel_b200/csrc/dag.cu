@@ -170,7 +170,10 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
 // began): items from earlier launches are visible without one, and most
 // matches of an edit are such pre-existing subtrees.  Inserts publish with a
 // release store.
-template <class Words>
+// WarpCounters: bump the level's pool and node counters with one atomic per
+// warp (warp_atomic_add_small), for kernels whose lanes insert side by side;
+// a kernel with a few inserting lanes per warp does better with plain ones.
+template <class Words, bool WarpCounters = true>
 __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words &w,
                                         bool *inserted = nullptr) {
   const uint32_t n = w.size();
@@ -187,7 +190,8 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
       const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long *>(idx + pos),
                                      0ull, static_cast<unsigned long long>(claim));
       if (old == 0) {
-        const uint32_t off = warp_atomic_add_small(&t.hdr->pool_used[l], n);
+        const uint32_t off = WarpCounters ? warp_atomic_add_small(&t.hdr->pool_used[l], n)
+                                          : atomicAdd(&t.hdr->pool_used[l], n);
         if (static_cast<uint64_t>(off) + n > t.pool_cap[l]) {
           set_status(&t.hdr->status, kDevCapacity);
           // Leave a dead entry (ref 1 never matches an item) so waiters move on.
@@ -196,7 +200,10 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
         }
         w.write(pool + off);
         st_release_u64(idx + pos, (static_cast<uint64_t>(tag) << 32) | (off + 2u));
-        warp_count_u64(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]));
+        if (WarpCounters)
+          warp_count_u64(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]));
+        else
+          atomicAdd(reinterpret_cast<unsigned long long *>(&t.hdr->node_count[l]), 1ull);
         if (inserted) *inserted = true;
         return off + 2u;
       }
@@ -228,6 +235,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
 
 // Canonical ref of a node given its 8 child refs: uniform nodes collapse to
 // the sentinels, everything else is hash-consed into level l's table.
+template <bool WarpCounters = true>
 __device__ uint32_t canon_node(const Tables &t, uint32_t l,
                                const uint32_t (&child)[8]) {
   uint32_t cm = 0, fm = 0;
@@ -241,7 +249,7 @@ __device__ uint32_t canon_node(const Tables &t, uint32_t l,
     if (fm == 0) return kEmptyRef;
     if (fm == 0xffu) return kFullRef;
   }
-  return node_find_or_insert(t, l, ChildWords{cm | (fm << 8), child});
+  return node_find_or_insert<ChildWords, WarpCounters>(t, l, ChildWords{cm | (fm << 8), child});
 }
 
 __device__ __forceinline__ uint32_t canon_leaf(const Tables &t, uint64_t mask) {
@@ -366,7 +374,9 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
 #pragma unroll
     for (uint32_t k = 0; k < 8; ++k)
       child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
-    if (have && c == 0) x.a.items[base + wi].result = same ? it.old : canon_node(x.t, l, child);
+    // At most 4 lanes of a warp insert a node here: plain counters.
+    if (have && c == 0)
+      x.a.items[base + wi].result = same ? it.old : canon_node<false>(x.t, l, child);
   }
 }
 
