@@ -75,20 +75,22 @@ def test_edit_settings_match_oracle(cuda):
     # a long primitive list at the root exercises the block-per-item path
     t = oracle.terrain(seed=4, scale=1, caves=True)
     expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
-    for big, bps, lpb in [(16, 2, 4), (64, 8, 5), (512, 16, 6), (32, 32, 4)]:
+    for big, bps, lpb, lanes in [(16, 2, 4, 4), (64, 8, 5, 8), (512, 16, 6, 4), (32, 32, 4, 8),
+                                 (32, 32, 5, 4)]:
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)
+        vx.set_tuning("edit.leafparent_lanes", lanes)
         d = vx.HashDag(depth, 1 << 18, 64 << 20)
         d.build_terrain(4, 1, True)
         d.apply_primitives(vx.prims_to_device(prims, cuda))
         assert d.status() == 0
-        assert oracle.DagCanon(*d.canonical()) == expect.dag(), (big, bps, lpb)
+        assert oracle.DagCanon(*d.canonical()) == expect.dag(), (big, bps, lpb, lanes)
         s = vx.Svo(depth, 1 << 18, 1 << 18, arena_bytes=64 << 20)
         s.build_terrain(4, 1, True)
         s.apply_primitives(vx.prims_to_device(prims, cuda))
         assert s.status() == 0
-        assert oracle.SvoCanon(*s.canonical()) == expect.svo(), (big, bps, lpb)
+        assert oracle.SvoCanon(*s.canonical()) == expect.svo(), (big, bps, lpb, lanes)
 
 
 def test_quick_autotune_writes_settings(cuda, tmp_path):
@@ -101,4 +103,5 @@ def test_quick_autotune_writes_settings(cuda, tmp_path):
         assert value in vx.tuning_options(name)
     assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0, "sort.rank_ballots": 1,
                            "edit.big_item": 32, "edit.blocks_per_sm": 32,
-            "edit.leafparent_blocks": 6, "serve.blocks_per_sm": 8}
+            "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 8,
+            "edit.leafparent_lanes": 4}

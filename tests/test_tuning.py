@@ -4,7 +4,8 @@ import voxel_b200 as vx
 
 EXPECTED = {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0, "sort.rank_ballots": 1,
             "edit.big_item": 32, "edit.blocks_per_sm": 32,
-            "edit.leafparent_blocks": 6, "serve.blocks_per_sm": 8}
+            "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 8,
+            "edit.leafparent_lanes": 4}
 
 
 def test_knobs_and_defaults():

@@ -11,10 +11,11 @@ which the library applies when it is first loaded on that kind of device:
     whether a tile publishes its digit counts before or after ranking, and
     whether keys are ranked with per-bit ballots or match_any; timed on 2^26
     u32 and 2^25 60-bit u64 key/value pairs;
-  * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks: the
-    primitive-list length above which a work item is expanded by a whole
-    block, the grid of the edit pipelines' item kernels, and the resident
-    blocks the DAG leaf-parent kernel is built for; timed on the batched Hash
+  * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks /
+    edit.leafparent_lanes: the primitive-list length above which a work item
+    is expanded by a whole block, the grid of the edit pipelines' item
+    kernels, and the resident blocks and threads per item of the DAG
+    leaf-parent kernel; timed on the batched Hash
     DAG edit of the benchmark (16384^3 cave terrain at scale 64, 16,384
     spheres of radius log-uniform in [1, 256], 60 % add).
 
@@ -135,10 +136,11 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
     ref = work.query(pts)
     times: dict = {}
 
-    def measure(big, bps, lpb):
+    def measure(big, bps, lpb, lanes):
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)
+        vx.set_tuning("edit.leafparent_lanes", lanes)
         work.copy_from(pristine)
         work.apply_primitives(prims)
         ok = work.status() == 0 and bool(torch.equal(work.query(pts), ref))
@@ -146,8 +148,9 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
                    lambda: work.copy_from(pristine)) if ok else None
         if ok and work.status() != 0:
             ms = None
-        times[f"big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb}"] = ms
-        log(f"  edit big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb}: "
+        key = f"big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb} leafparent_lanes={lanes}"
+        times[key] = ms
+        log(f"  edit {key}: "
             + (f"{ms:.3f} ms" if ms is not None else "FAILED OR DIFFERENT (not used)"))
         return ms
 
@@ -156,25 +159,28 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
     # little, while on small batches (the serving loop's) every extra block
     # is launch overhead.
     lpb0 = vx.tuning()["edit.leafparent_blocks"]
+    lanes0 = vx.tuning()["edit.leafparent_lanes"]
     stage1 = {}
     for big, bps in itertools.product(vx.tuning_options("edit.big_item"),
                                       vx.tuning_options("edit.blocks_per_sm")):
-        ms = measure(big, bps, lpb0)
+        ms = measure(big, bps, lpb0, lanes0)
         if ms is not None:
             stage1[(big, bps)] = ms
     fastest = min(stage1.values())
     near = [k for k, t in stage1.items() if t <= 1.02 * fastest]
     big, bps = min(near, key=lambda k: (k[1], stage1[k]))
-    # Stage 2: resident blocks of the leaf-parent kernel at that setting.
+    # Stage 2: threads per item and resident blocks of the leaf-parent
+    # kernel at that setting.
     stage2 = {}
-    for lpb in vx.tuning_options("edit.leafparent_blocks"):
-        ms = measure(big, bps, lpb)
+    for lpb, lanes in itertools.product(vx.tuning_options("edit.leafparent_blocks"),
+                                        vx.tuning_options("edit.leafparent_lanes")):
+        ms = measure(big, bps, lpb, lanes)
         if ms is not None:
-            stage2[lpb] = ms
-    lpb = min(stage2, key=stage2.get)
+            stage2[(lpb, lanes)] = ms
+    lpb, lanes = min(stage2, key=stage2.get)
     vx.reset_tuning()
     return {"edit.big_item": big, "edit.blocks_per_sm": bps,
-            "edit.leafparent_blocks": lpb}, times
+            "edit.leafparent_blocks": lpb, "edit.leafparent_lanes": lanes}, times
 
 
 def tune_serve(depth: int, scale: int, batch: int, reps: int, log, max_nodes: int,

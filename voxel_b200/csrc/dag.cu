@@ -291,13 +291,19 @@ __global__ void mark_pools_kernel(Tables t) {
   if (threadIdx.x < kMaxDepth) t.hdr->pool_mark[threadIdx.x] = t.hdr->pool_used[threadIdx.x];
 }
 
-// Level depth - 1: evaluate the 8 leaves of every item (8 threads per item)
-// and hash-cons the item.
-// MinBlocks (the tuning knob "edit.leafparent_blocks") trades registers for
+// Level depth - 1: evaluate the 8 leaves of every item and hash-cons the
+// item.  Lanes (the tuning knob "edit.leafparent_lanes") threads share an
+// item, each evaluating children q + Lanes * j of it (q its rank in the
+// group): 8 lanes take one leaf each, 4 lanes two, which halves the
+// per-item work that every lane repeats and doubles the items in flight.
+// MinBlocks (the knob "edit.leafparent_blocks") trades registers for
 // resident blocks: the kernel is bound by chains of dependent loads, so more
 // items in flight can outweigh a few spilled values.
-template <bool Terrain, int MinBlocks>
+template <bool Terrain, int MinBlocks, uint32_t Lanes>
 __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
+  static_assert(Lanes == 4 || Lanes == 8, "4 or 8 lanes per item");
+  constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
+  constexpr uint32_t kGroupBits = (1u << Lanes) - 1u;
   Header *h = x.t.hdr;
   if (ld_relaxed_u32(&h->status) != kDevOk) return;
   const uint32_t l = x.t.depth - 1;
@@ -306,76 +312,101 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
   const uint32_t *pairs = x.a.pairs[l & 1u];
   const uint32_t world_exp = x.t.depth + 2;
   const uint32_t lane = lane_id();
-  const uint64_t total = static_cast<uint64_t>(W) * 8u;
+  const uint64_t total = static_cast<uint64_t>(W) * Lanes;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  // The item's primitives, 8 at a time: lane c of the group loads the c-th
-  // (one parallel load instead of 8 lanes walking the list).
-  __shared__ vx_primitive s_pr[kBlock / 8][8];
-  const uint32_t grp = threadIdx.x >> 3;
-  const uint32_t gmask = 0xffu << (lane & ~7u);
+  // The item's primitives, Lanes at a time: lane q of the group loads the
+  // q-th (one parallel load instead of every lane walking the list).
+  __shared__ vx_primitive s_pr[kBlock / Lanes][Lanes];
+  const uint32_t grp = threadIdx.x / Lanes;
+  const uint32_t gbase = lane & ~(Lanes - 1u);
+  const uint32_t gmask = kGroupBits << gbase;
   for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
        g0 < total; g0 += stride) {
     const uint64_t g = g0 + lane;
-    const bool have = g < total; // the same for the 8 lanes of a group
-    const uint32_t wi = static_cast<uint32_t>(g >> 3), c = lane & 7u;
-    uint32_t result = kEmptyRef, old_child = kEmptyRef;
+    const bool have = g < total; // the same for the lanes of a group
+    const uint32_t wi = static_cast<uint32_t>(g / Lanes), q = lane & (Lanes - 1u);
+    uint32_t result[kPer], old_child[kPer];
+#pragma unroll
+    for (uint32_t j = 0; j < kPer; ++j) result[j] = old_child[j] = kEmptyRef;
     Item it{};
     if (have) {
       it = x.a.items[base + wi];
       const Cell cell = unpack_cell(it.cell);
-      const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * 4;
-      const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
-      const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
       // Independent loads side by side: the first chunk's pair index and the
-      // old node, then its primitive and the old leaf (read speculatively:
+      // old node, then its primitive and the old leaves (read speculatively:
       // the kernel is bound by dependent round trips, not by bandwidth).
-      const uint32_t n0 = it.pcount < 8u ? it.pcount : 8u;
-      const uint32_t pidx = c < n0 ? pairs[it.pstart + c] : 0u;
-      old_child = child_ref(x.t, l, it.old, c);
+      int64_t ox[kPer], oy[kPer], oz[kPer];
+#pragma unroll
+      for (uint32_t j = 0; j < kPer; ++j) {
+        const uint32_t c = q + Lanes * j;
+        ox[j] = int64_t(2 * cell.x + (c & 1u)) * 4;
+        oy[j] = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
+        oz[j] = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
+      }
+      const uint32_t n0 = it.pcount < Lanes ? it.pcount : Lanes;
+      const uint32_t pidx = q < n0 ? pairs[it.pstart + q] : 0u;
+#pragma unroll
+      for (uint32_t j = 0; j < kPer; ++j) old_child[j] = child_ref(x.t, l, it.old, q + Lanes * j);
       vx_primitive first{};
-      if (c < n0) first = x.prims[pidx];
-      const uint64_t old_mask = read_leaf(x.t, old_child);
+      if (q < n0) first = x.prims[pidx];
+      uint64_t old_mask[kPer], mask[kPer];
+      bool loaded[kPer], touched[kPer];
+#pragma unroll
+      for (uint32_t j = 0; j < kPer; ++j) {
+        old_mask[j] = read_leaf(x.t, old_child[j]);
+        mask[j] = 0;
+        loaded[j] = touched[j] = false;
+      }
       __syncwarp(gmask); // the group's previous item no longer reads s_pr
-      s_pr[grp][c] = first;
+      s_pr[grp][q] = first;
       __syncwarp(gmask);
-      uint64_t mask = 0;
-      bool loaded = false, touched = false;
       for (uint32_t k = 0; k < it.pcount; ++k) {
-        if ((k & 7u) == 0 && k != 0) {
+        if (k % Lanes == 0 && k != 0) {
           __syncwarp(gmask); // the previous chunk is no longer read
-          if (k + c < it.pcount) s_pr[grp][c] = x.prims[pairs[it.pstart + k + c]];
+          if (k + q < it.pcount) s_pr[grp][q] = x.prims[pairs[it.pstart + k + q]];
           __syncwarp(gmask);
         }
-        const vx_primitive pr = s_pr[grp][k & 7u];
-        const uint32_t cls = classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
-        if (cls == VX_CELL_EMPTY) continue;
+        const vx_primitive pr = s_pr[grp][k % Lanes];
         const bool add = vx_prim_op(&pr) == VX_OP_ADD;
-        touched = true;
-        if (cls == VX_CELL_FULL) {
-          mask = add ? ~0ull : 0ull;
-          loaded = true;
-          continue;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; ++j) {
+          const uint32_t cls = classify<Terrain>(pr, world_exp, ox[j], oy[j], oz[j], 4);
+          if (cls == VX_CELL_EMPTY) continue;
+          touched[j] = true;
+          if (cls == VX_CELL_FULL) {
+            mask[j] = add ? ~0ull : 0ull;
+            loaded[j] = true;
+            continue;
+          }
+          if (!loaded[j]) {
+            mask[j] = old_mask[j];
+            loaded[j] = true;
+          }
+          const uint64_t m = leaf_mask<Terrain>(pr, world_exp, ox[j], oy[j], oz[j]);
+          mask[j] = add ? (mask[j] | m) : (mask[j] & ~m);
         }
-        if (!loaded) {
-          mask = old_mask;
-          loaded = true;
-        }
-        const uint64_t m = leaf_mask<Terrain>(pr, world_exp, ox, oy, oz);
-        mask = add ? (mask | m) : (mask & ~m);
       }
       // An unchanged mask keeps its canonical ref: no probe of the leaf set.
-      result = (touched && mask != old_mask) ? canon_leaf(x.t, mask) : old_child;
+#pragma unroll
+      for (uint32_t j = 0; j < kPer; ++j)
+        result[j] = (touched[j] && mask[j] != old_mask[j]) ? canon_leaf(x.t, mask[j])
+                                                           : old_child[j];
     }
     // A node whose 8 children all kept their refs is the old node itself
     // (refs are canonical), so its hash-consing is skipped.
-    const uint32_t changed = __ballot_sync(kFullMask, result != old_child);
-    const bool same = ((changed >> (lane & ~7u)) & 0xffu) == 0u;
+    bool mine_changed = false;
+#pragma unroll
+    for (uint32_t j = 0; j < kPer; ++j) mine_changed |= result[j] != old_child[j];
+    const uint32_t changed = __ballot_sync(kFullMask, mine_changed);
+    const bool same = ((changed >> gbase) & kGroupBits) == 0u;
     uint32_t child[8];
 #pragma unroll
-    for (uint32_t k = 0; k < 8; ++k)
-      child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
-    // At most 4 lanes of a warp insert a node here: plain counters.
-    if (have && c == 0)
+    for (uint32_t j = 0; j < kPer; ++j)
+#pragma unroll
+      for (uint32_t k = 0; k < Lanes; ++k)
+        child[k + Lanes * j] = __shfl_sync(kFullMask, result[j], gbase + k);
+    // At most 32 / Lanes lanes of a warp insert a node here: plain counters.
+    if (have && q == 0)
       x.a.items[base + wi].result = same ? it.old : canon_node<false>(x.t, l, child);
   }
 }
@@ -554,14 +585,21 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   {
     prof::Scope sc("dag_leafparent", s);
     const int64_t lb = tune::get(tune::kEditLeafparentBlocks);
+    const bool four = tune::get(tune::kEditLeafparentLanes) == 4;
     if (terrain)
-      leafparent_kernel<true, 4><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<true, 4, 8><<<grid, kBlock, 0, s>>>(x);
+    else if (four && lb == 6)
+      leafparent_kernel<false, 6, 4><<<grid, kBlock, 0, s>>>(x);
+    else if (four && lb == 5)
+      leafparent_kernel<false, 5, 4><<<grid, kBlock, 0, s>>>(x);
+    else if (four)
+      leafparent_kernel<false, 4, 4><<<grid, kBlock, 0, s>>>(x);
     else if (lb == 6)
-      leafparent_kernel<false, 6><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<false, 6, 8><<<grid, kBlock, 0, s>>>(x);
     else if (lb == 5)
-      leafparent_kernel<false, 5><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<false, 5, 8><<<grid, kBlock, 0, s>>>(x);
     else
-      leafparent_kernel<false, 4><<<grid, kBlock, 0, s>>>(x);
+      leafparent_kernel<false, 4, 8><<<grid, kBlock, 0, s>>>(x);
   }
   VX_TRY_CUDA(cudaGetLastError());
   for (uint32_t r = depth - 1; r > 0; --r) {
