@@ -62,10 +62,10 @@ DAG_MAX_NODES = 1 << 27
 DAG_ARENA = 16 << 30
 PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
 # DRAM bytes per dag_leafparent work item: the ncu capture of the small case
-# (profiles/dag_leafparent_4096cube.md: 438.1 + 216.8 MB) divided by that
+# (profiles/dag_leafparent_4096cube.md: 451.6 + 226.6 MB) divided by that
 # launch's 5,280,796 items (bench.py --case dag --elements 4096); the
 # roofline's `traffic` scales it by the full launch's items.
-LEAFPARENT_TRAFFIC_PER_ITEM = (438.1e6 + 216.8e6) / 5280796
+LEAFPARENT_TRAFFIC_PER_ITEM = (451.6e6 + 226.6e6) / 5280796
 SVO_C3_DEPTH = 10         # 4096^3
 SVO_C3_EDITS = 65536
 SERVE_DEPTH = 11          # 8192^3

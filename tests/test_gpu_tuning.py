@@ -102,6 +102,6 @@ def test_quick_autotune_writes_settings(cuda, tmp_path):
     for name, value in saved["knobs"].items():
         assert value in vx.tuning_options(name)
     assert vx.tuning() == {"sort.items_u32": 16, "sort.items_u64": 12, "sort.early_counts": 0, "sort.rank_ballots": 1,
-                           "edit.big_item": 32, "edit.blocks_per_sm": 32,
-            "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 8,
+                           "edit.big_item": 16, "edit.blocks_per_sm": 32,
+            "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 4,
             "edit.leafparent_lanes": 4}

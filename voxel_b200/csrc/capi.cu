@@ -178,13 +178,13 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.items_u64", 12, {8, 12}, 2},
     {"sort.early_counts", 0, {0, 1}, 2},
     {"sort.rank_ballots", 1, {0, 1}, 2},
-    {"edit.big_item", 32, {16, 32, 64, 128, 256, 512}, 6},
+    {"edit.big_item", 16, {16, 32, 64, 128, 256, 512}, 6},
     {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
     {"edit.leafparent_blocks", 5, {4, 5, 6}, 3},
-    {"serve.blocks_per_sm", 8, {2, 4, 8, 16, 32}, 5},
+    {"serve.blocks_per_sm", 4, {2, 4, 8, 16, 32}, 5},
     {"edit.leafparent_lanes", 4, {4, 8}, 2},
 };
-std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {32}, {32}, {5}, {8}, {4}};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {16}, {32}, {5}, {4}, {4}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;
