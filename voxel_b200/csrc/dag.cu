@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
           if (k + q < it.pcount) s_pr[grp][q] = x.prims[pairs[it.pstart + k + q]];
           __syncwarp(gmask);
         }
-        const vx_primitive pr = s_pr[grp][k % Lanes];
+        const vx_primitive &pr = s_pr[grp][k % Lanes]; // read in place: fewer registers
         const bool add = vx_prim_op(&pr) == VX_OP_ADD;
 #pragma unroll
         for (uint32_t j = 0; j < kPer; ++j) {
