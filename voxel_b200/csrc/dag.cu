@@ -573,7 +573,7 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
       if (terrain)
         expand_big_kernel<DagTree, true><<<sm_count() * 2, kBlock, 0, s>>>(e, tree, l);
       else
-        expand_big_kernel<DagTree, false><<<sm_count() * 2, kBlock, 0, s>>>(e, tree, l);
+        expand_big_kernel<DagTree, false><<<sm_count(), kBigBlock, 0, s>>>(e, tree, l);
     }
     VX_TRY_CUDA(cudaGetLastError());
   }

@@ -387,12 +387,21 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// Expansion of the long-list items of level l: one block per item.  Three
-// walks over the list: the last fully-covering primitive per child (block
-// max), the partial primitives after it per child (block sum), then an
-// order-preserving block-wide compaction of those into each child's list.
-template <class Policy, bool Terrain>
-__global__ void __launch_bounds__(kBlock)
+// Expansion of the long-list items of level l: one block of Threads
+// threads per item.  Three walks over the list: the last fully-covering
+// primitive per child (block max), the partial primitives after it per child
+// (block sum), then an order-preserving block-wide compaction of those into
+// each child's list.  The root of a batch carries every primitive and is
+// expanded by one block alone, so edits use a wide block (kBigBlock); the
+// terrain generator's classification needs more registers than a wide
+// block leaves a thread, so terrain builds use kBlock.  Lists of up to
+// kBigCache primitives are classified once: walk 1 keeps each primitive's
+// per-child MIXED bits in shared memory for walks 2 and 3.
+constexpr uint32_t kBigBlock = 512;
+constexpr uint32_t kBigCache = 32768;
+
+template <class Policy, bool Terrain, uint32_t Threads = Terrain ? kBlock : kBigBlock>
+__global__ void __launch_bounds__(Threads)
     expand_big_kernel(EditCtx x, Policy pol, uint32_t l) {
   Header *h = x.hdr;
   if (ld_relaxed_u32(&h->status) != kDevOk) return;
@@ -404,38 +413,44 @@ __global__ void __launch_bounds__(kBlock)
   uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
   const int64_t csize = int64_t(4) << (depth - l - 1);
   const uint32_t world_exp = depth + 2;
-  constexpr uint32_t kWarps = kBlock / kWarp;
+  constexpr uint32_t kWarps = Threads / kWarp;
+  static_assert(kWarps <= kWarp, "one warp scans the warps' counts");
   __shared__ int32_t s_last[8];
   __shared__ uint32_t s_cnt[8], s_start[8], s_const[8], s_cm;
-  __shared__ uint32_t s_warp[8][kWarps];
+  __shared__ uint32_t s_warp[8][kWarps], s_total[8];
   __shared__ uint32_t s_item_base, s_pair_base;
   __shared__ bool s_room;
+  __shared__ uint8_t s_mixed[kBigCache];
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
 
   for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
     const uint32_t wi = x.a.big[b];
     const Item it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
+    const bool cached = it.pcount <= kBigCache; // block-uniform
     if (t < 8) {
       s_last[t] = -1;
       s_cnt[t] = 0;
     }
     __syncthreads();
-    // Walk 1: last FULL per child.
+    // Walk 1: last FULL per child (and the MIXED bits, when cached).
     int32_t last[8];
 #pragma unroll
     for (uint32_t c = 0; c < 8; ++c) last[c] = -1;
-    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+    for (uint32_t k = t; k < it.pcount; k += Threads) {
       const uint32_t p = in_pairs[it.pstart + k];
       const vx_primitive pr = x.prims[p];
+      uint32_t mixed = 0;
 #pragma unroll
       for (uint32_t c = 0; c < 8; ++c) {
         const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
         const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
         const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * csize;
-        if (pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, csize) == VX_CELL_FULL)
-          last[c] = max(last[c], static_cast<int32_t>(p));
+        const uint32_t cls = pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, csize);
+        if (cls == VX_CELL_FULL) last[c] = max(last[c], static_cast<int32_t>(p));
+        else if (cls == VX_CELL_MIXED) mixed |= 1u << c;
       }
+      if (cached) s_mixed[k] = static_cast<uint8_t>(mixed);
     }
 #pragma unroll
     for (uint32_t c = 0; c < 8; ++c) {
@@ -447,8 +462,15 @@ __global__ void __launch_bounds__(kBlock)
     for (uint32_t c = 0; c < 8; ++c) last[c] = s_last[c];
     // Walk 2: partial primitives after the last full one.
     uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t k = t; k < it.pcount; k += kBlock) {
+    for (uint32_t k = t; k < it.pcount; k += Threads) {
       const uint32_t p = in_pairs[it.pstart + k];
+      if (cached) { // each thread reads back the bits it wrote in walk 1
+        const uint32_t mixed = s_mixed[k];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c)
+          cnt[c] += (static_cast<int32_t>(p) > last[c] && ((mixed >> c) & 1u)) ? 1u : 0u;
+        continue;
+      }
       const vx_primitive pr = x.prims[p];
 #pragma unroll
       for (uint32_t c = 0; c < 8; ++c) {
@@ -504,14 +526,20 @@ __global__ void __launch_bounds__(kBlock)
       ci.pcount = s_cnt[t];
       x.a.items[next_base + s_item_base + k] = ci;
     }
-    // Walk 3: order-preserving compaction, one 256-pair chunk at a time.
+    // Walk 3: order-preserving compaction, one Threads-pair chunk at a time.
     uint32_t run[8];
 #pragma unroll
     for (uint32_t c = 0; c < 8; ++c) run[c] = s_pair_base + s_start[c];
-    for (uint32_t k0 = 0; k0 < it.pcount && room; k0 += kBlock) {
+    for (uint32_t k0 = 0; k0 < it.pcount && room; k0 += Threads) {
       const uint32_t k = k0 + t;
       uint32_t take = 0, p = 0;
-      if (k < it.pcount) {
+      if (k < it.pcount && cached) {
+        p = in_pairs[it.pstart + k];
+        const uint32_t mixed = s_mixed[k];
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c)
+          if (static_cast<int32_t>(p) > last[c] && ((mixed >> c) & 1u)) take |= 1u << c;
+      } else if (k < it.pcount) {
         p = in_pairs[it.pstart + k];
         const vx_primitive pr = x.prims[p];
 #pragma unroll
@@ -531,17 +559,21 @@ __global__ void __launch_bounds__(kBlock)
         if (lane == 0) s_warp[c][warp] = __popc(ballots[c]);
       }
       __syncthreads();
+      if (warp == 0) { // exclusive offsets of the warps, per child, by shuffles
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) {
+          const uint32_t v = lane < kWarps ? s_warp[c][lane] : 0u;
+          const uint32_t inc = warp_inclusive_sum(v);
+          if (lane < kWarps) s_warp[c][lane] = inc - v;
+          if (lane == kWarp - 1) s_total[c] = inc;
+        }
+      }
+      __syncthreads();
 #pragma unroll
       for (uint32_t c = 0; c < 8; ++c) {
-        uint32_t before = 0, total = 0;
-        for (uint32_t w = 0; w < kWarps; ++w) {
-          const uint32_t v = s_warp[c][w];
-          before += w < warp ? v : 0u;
-          total += v;
-        }
         if ((take >> c) & 1u)
-          out_pairs[run[c] + before + __popc(ballots[c] & lanemask_lt())] = p;
-        run[c] += total;
+          out_pairs[run[c] + s_warp[c][warp] + __popc(ballots[c] & lanemask_lt())] = p;
+        run[c] += s_total[c];
       }
       __syncthreads();
     }

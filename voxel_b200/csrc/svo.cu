@@ -445,7 +445,7 @@ vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_c
     {
       prof::Scope sc("svo_expand_big", s);
       if (terrain) expand_big_kernel<SvoTree, true><<<sm_count() * 2, kBlock, 0, s>>>(e, pol, l);
-      else expand_big_kernel<SvoTree, false><<<sm_count() * 2, kBlock, 0, s>>>(e, pol, l);
+      else expand_big_kernel<SvoTree, false><<<sm_count(), kBigBlock, 0, s>>>(e, pol, l);
     }
     VX_TRY_CUDA(cudaGetLastError());
   }
