@@ -49,8 +49,8 @@ BYTES_SORT_U64 = 200    # 8 passes x (read 12 + write 12) + 8 histogram read
 # Per-launch algorithmic bytes of the dominant kernel (one u64 partition
 # pass: read key 8 + value 4, write key 8 + value 4 per element).
 PART_U64_BYTES = N_SORT * 24
-# DRAM bytes per sort_partition_u64 launch: the ncu capture of a 2^24-key
-# pass (profiles/sort_partition_u64_2p24.md: 202.8 + 158.7 MB) scaled by the
+# DRAM bytes per sort_partition_u64 launch: an ncu capture of one 2^24-key
+# pass (dram__bytes_read 202.8 MB + dram__bytes_write 158.7 MB) scaled by the
 # keys of a launch here (2^28).  At 2^24 part of the input stays in L2, so
 # this is a lower bound for the full size.
 PART_U64_TRAFFIC = round((202.8e6 + 158.7e6) / (1 << 24) * N_SORT)
@@ -61,9 +61,9 @@ DAG_EDITS = 16384
 DAG_MAX_NODES = 1 << 27
 DAG_ARENA = 16 << 30
 PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
-# DRAM bytes per dag_leafparent work item: the ncu capture of the small case
-# (profiles/dag_leafparent_4096cube.md: 451.6 + 226.6 MB) divided by that
-# launch's 5,280,796 items (bench.py --case dag --elements 4096); the
+# DRAM bytes per dag_leafparent work item: an ncu capture of the small case
+# (bench.py --case dag --elements 4096: dram__bytes_read 451.6 MB +
+# dram__bytes_write 226.6 MB) divided by that launch's 5,280,796 items; the
 # roofline's `traffic` scales it by the full launch's items.
 LEAFPARENT_TRAFFIC_PER_ITEM = (451.6e6 + 226.6e6) / 5280796
 SVO_C3_DEPTH = 10         # 4096^3
