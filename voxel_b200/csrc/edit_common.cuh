@@ -303,14 +303,19 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t old_child = have && !big ? pol.child(l, it.old, c) : 0u;
     int32_t last_full = -1;
     uint32_t cnt = 0;
+    // Bit k: the list's k-th primitive cuts this child partially and comes
+    // after every primitive that covers it (kept for lists of up to 32).
+    uint32_t partial = 0;
     for (uint32_t k = 0; k < it.pcount; ++k) {
       const uint32_t p = in_pairs[it.pstart + k];
       const uint32_t cls = pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize);
       if (cls == VX_CELL_FULL) {
         last_full = static_cast<int32_t>(p);
         cnt = 0;
+        partial = 0;
       } else if (cls == VX_CELL_MIXED) {
         ++cnt;
+        if (k < 32u) partial |= 1u << k;
       }
     }
     // Prefix sums over the 8 lanes of the group.
@@ -373,11 +378,18 @@ __global__ void __launch_bounds__(kBlock)
       ci.pcount = cnt;
       x.a.items[next_base + item_off + inc_items - 1] = ci;
       uint32_t j = 0;
-      for (uint32_t k = 0; k < it.pcount && j < cnt; ++k) {
-        const uint32_t p = in_pairs[it.pstart + k];
-        if (static_cast<int32_t>(p) <= last_full) continue;
-        if (pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
-          out_pairs[my_pairs + j++] = p;
+      if (it.pcount <= 32u) {
+        // The child's list is the set bits of `partial`: independent loads
+        // of the pairs, no second classification.
+        for (uint32_t bits = partial; bits != 0u; bits &= bits - 1u)
+          out_pairs[my_pairs + j++] = in_pairs[it.pstart + __ffs(bits) - 1u];
+      } else {
+        for (uint32_t k = 0; k < it.pcount && j < cnt; ++k) {
+          const uint32_t p = in_pairs[it.pstart + k];
+          if (static_cast<int32_t>(p) <= last_full) continue;
+          if (pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize) == VX_CELL_MIXED)
+            out_pairs[my_pairs + j++] = p;
+        }
       }
     }
     if (c == 0) {
