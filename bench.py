@@ -1039,8 +1039,10 @@ def run_case_dag_full(args, torch, vx, dev):
 
 
 def run_case(args):
-    """One operation on a small input, for profiler captures:
-    --case scan|sort_u32|sort_u64 --elements N (runs --steps launches)."""
+    """One operation alone, for profiler captures: --case scan|sort_u32|sort_u64
+    --elements N (runs --steps launches); --case dag --elements E (E spheres
+    on a 4096^3 terrain); --case dag_full (the headline C4 batch, --steps
+    batches, device time per batch and per kernel)."""
     import torch
     import voxel_b200 as vx
     dev = torch.device("cuda:0")
