@@ -34,3 +34,15 @@ def test_set_reject_reset():
 def test_tuning_file_name():
     p = vx.tuning_file("NVIDIA B200")
     assert p.name == "NVIDIA_B200.json" and p.parent.name == "tuning"
+
+
+def test_committed_b200_settings_are_the_defaults():
+    """The autotuner's B200 file holds a valid value for every knob, and the
+    library's compiled defaults are that file's choices (a caller that never
+    loads the file gets the tuned shapes on B200)."""
+    import json
+    saved = json.loads(vx.tuning_file("NVIDIA B200").read_text())["knobs"]
+    assert set(saved) == set(EXPECTED)
+    for name, value in saved.items():
+        assert value in vx.tuning_options(name), name
+    assert saved == EXPECTED
