@@ -110,10 +110,20 @@ vx_status vx_scan_exclusive_sum_u64(uint64_t *data, uint32_t count,
  * in the reference: its scans always take a caller workspace.  The scratch is
  * a 256 KiB array inside this library on each device, so count must be at
  * most 2^28 (larger counts return VX_ERR_CAPACITY and touch nothing); calls
- * that can overlap on the GPU share that array and race; the first call on a
- * device looks up the array's address and should precede any stream capture. */
+ * that can overlap on the GPU share that array and race; the first call in a
+ * CUDA context (again after a device reset) looks up the array's address and
+ * should precede any stream capture.  The call is asynchronous: a look-back
+ * wait that gives up cannot be reported by its return value, so read
+ * vx_scan_noalloc_status afterwards where that matters. */
 vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
                                             vx_stream stream);
+/* Synchronises the stream and returns the device status that the most recent
+ * vx_scan_exclusive_sum_u32_noalloc on the current device left in the shared
+ * scratch: VX_OK, or VX_ERR_TIMEOUT when a bounded look-back wait gave up and
+ * that call's sums are invalid.  Allocates nothing.  No counterpart in the
+ * reference (its scans report through a caller workspace).  With overlapping
+ * calls the word belongs to whichever call wrote it last. */
+vx_status vx_scan_noalloc_status(vx_stream stream);
 
 /* ------------------------------------------------------------------ sort --
  * Stable LSD radix sort ("onesweep": one all-pass digit histogram, then one
@@ -324,6 +334,16 @@ vx_status vx_dag_build_terrain(vx_dag *dag, const vx_terrain *terrain,
  * hash_dag_gpu/query.cuh:12-39). */
 vx_status vx_dag_query(const vx_dag *dag, const vx_voxel *pts, uint32_t count,
                        uint8_t *out, vx_stream stream);
+
+/* Dense read of a box of leaves: out[(z * ny + y) * nx + x] (device memory)
+ * = occupancy mask of the leaf at leaf coordinates (lx0 + x, ly0 + y,
+ * lz0 + z) (voxel coordinates / 4, bit = x + 4y + 16z; 0 outside the world).
+ * The region counterpart of hash_dag_gpu::get_voxel (query.cuh:12-39): one
+ * root-to-leaf walk per leaf instead of per voxel, e.g. to mesh or check a
+ * region.  nx * ny * nz must be below 2^32. */
+vx_status vx_dag_read_leaves(const vx_dag *dag, uint32_t lx0, uint32_t ly0, uint32_t lz0,
+                             uint32_t nx, uint32_t ny, uint32_t nz, uint64_t *out,
+                             vx_stream stream);
 
 /* Canonical dump (host memory, synchronises): DFS from the root, children
  * 0..7, first visit numbers the nodes of each level.  Each inner node is

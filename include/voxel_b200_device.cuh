@@ -85,6 +85,21 @@ __device__ __forceinline__ uint8_t vx_dag_get_voxel(const vx_dag_view &v, uint32
   return (uint8_t)((v.leaves[ref - 2u] >> bit) & 1ull);
 }
 
+/* Occupancy mask of the 4^3 leaf at leaf coordinates (lx, ly, lz) (voxel
+ * coordinates / 4; bit = x + 4y + 16z); 0 outside the world. */
+__device__ __forceinline__ uint64_t vx_dag_get_leaf(const vx_dag_view &v, uint32_t lx,
+                                                    uint32_t ly, uint32_t lz) {
+  if ((lx >> v.depth) | (ly >> v.depth) | (lz >> v.depth)) return 0;
+  uint32_t ref = *v.root;
+  for (uint32_t l = 0; l < v.depth && ref >= 2u; ++l) {
+    const uint32_t s = v.depth - 1 - l;
+    const uint32_t c = ((lx >> s) & 1u) | (((ly >> s) & 1u) << 1) | (((lz >> s) & 1u) << 2);
+    ref = vx_dag_item_child(v.pool[l] + (ref - 2u), c);
+  }
+  if (ref <= 1u) return ref ? ~0ull : 0ull;
+  return v.leaves[ref - 2u];
+}
+
 /* ------------------------------------------------------------------ SVO -- */
 
 /* Value of a child word without a child: material (or 1 without materials)

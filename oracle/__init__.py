@@ -77,9 +77,11 @@ _REF_SIGS = [
     ("ref_dag_edit_box", _I, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _I]),
     ("ref_dag_set_voxel", _I, [_P, _U32, _U32, _U32, _I]),
     ("ref_dag_apply_prim", C.c_longlong, [_P, _I] + [C.c_longlong] * 6 + [_I]),
+    ("ref_dag_apply_prim_clipped", C.c_longlong, [_P, _I] + [C.c_longlong] * 6 + [_I, _P, _P]),
     ("ref_dag_get_voxel", _I, [_P, _U32, _U32, _U32]),
     ("ref_dag_node_count", _U64, [_P]),
     ("ref_dag_export", _I, [_P, C.POINTER(_U32), _P, _P, _U64, _P, _U64]),
+    ("ref_dag_import_region", _I, [_P, _U32, _U32, _U32, _U32, _U32, _P, _P, _P]),
     ("ref_svo_new", _P, [_U32]),
     ("ref_svo_free", None, [_P]),
     ("ref_svo_set_voxel", _I, [_P, _U32, _U32, _U32, _I]),
@@ -145,6 +147,17 @@ _VOXEL_SIGS = [
     ("orc_grid_export_svo", _I, [_P, C.POINTER(_U32), C.POINTER(_U32), _P, _U32,
                                  _P, _P, _U32]),
     ("orc_eval_voxels", None, [_P, _U32, _P, _U64, _P, _U64, _P, _I]),
+    ("orc_sparse_run", _P, [_U32, _P, _P, _U64, _I, _U32, _P, _U32, _I]),
+    ("orc_sparse_free", None, [_P]),
+    ("orc_sparse_export_dag", _I, [_P, C.POINTER(_U32), _P, _P, _U64, _P, _U64]),
+    ("orc_sparse_export_svo", _I, [_P, C.POINTER(_U64), C.POINTER(_U64), _P, _U64, _P, _P,
+                                   _U64]),
+    ("orc_sparse_leaf_block", None, [_P, _P, _P, _P]),
+    ("orc_terrain_leaf_mismatches", _U64, [_P, _P, _U64, _I]),
+    ("orc_terrain_classify_mismatches", _U64, [_P, _P, _U64]),
+    ("orc_generate_primitives", None, [_P, _U64, _U64, _U64, _P]),
+    ("orc_generate_requests", _U64, [_P, _U64, C.c_double, C.c_double, C.c_double, _U32,
+                                     _U64, _P, _P, _U64, _P, C.POINTER(_U64)]),
 ]
 _SIGS.extend(_VOXEL_SIGS)
 
@@ -152,6 +165,63 @@ PRIM_DTYPE = np.dtype([("c", "<i4", 3), ("r", "<u4", 3), ("flags", "<u4"),
                        ("reserved", "<u4")])
 TERRAIN_DTYPE = np.dtype([("seed", "<u4"), ("scale", "<u4"), ("caves", "<u4"),
                           ("world_exp", "<u4")])
+
+
+EDIT_MIX_DTYPE = np.dtype([(k, "<u4") for k in (
+    "world_exp", "sphere_permille", "add_permille", "r_min", "r_max", "log_uniform",
+    "material_min", "material_max")])
+
+
+def _mix(world_exp, sphere_permille, add_permille, r_min, r_max, log_uniform,
+         material_min, material_max) -> np.ndarray:
+    m = np.zeros(1, EDIT_MIX_DTYPE)
+    m[0] = (world_exp, sphere_permille, add_permille, r_min, r_max, int(log_uniform),
+            material_min, material_max)
+    return m
+
+
+def generate_primitives(world_exp: int, count: int, seed: int, *,
+                        sphere_permille: int = 1000, add_permille: int = 500,
+                        r_min: int = 1, r_max: int = 16, log_uniform: bool = False,
+                        material_min: int = 1, material_max: int = 255,
+                        stream: int = 0) -> np.ndarray:
+    """The seeded primitive lists of vx_workload.h (same draws as the
+    library's vx_generate_primitives)."""
+    m = _mix(world_exp, sphere_permille, add_permille, r_min, r_max, log_uniform,
+             material_min, material_max)
+    out = np.zeros(max(count, 1), PRIM_DTYPE)
+    lib().orc_generate_primitives(m.ctypes.data, seed, stream, count, out.ctypes.data)
+    return out[:count]
+
+
+def config_c4_edits(count: int = 16384, seed: int = 7, world_exp: int = 14) -> np.ndarray:
+    """The batched Hash DAG benchmark's spheres: r log-uniform [1, 256], 60 % add."""
+    return generate_primitives(world_exp, count, seed, add_permille=600, r_min=1, r_max=256,
+                               log_uniform=True)
+
+
+def config_c3_edits(count: int = 65536, seed: int = 6, world_exp: int = 12) -> np.ndarray:
+    """The batched SVO benchmark's mix: 70 % spheres / 30 % boxes, r log-uniform [1, 64]."""
+    return generate_primitives(world_exp, count, seed, sphere_permille=700, r_min=1, r_max=64,
+                               log_uniform=True)
+
+
+def generate_requests(world_exp: int, rate: float, seconds: float, seed: int, *,
+                      zipf_s: float = 1.2, max_size: int = 4096, sphere_permille: int = 500,
+                      add_permille: int = 500, r_min: int = 1, r_max: int = 128,
+                      log_uniform: bool = True, max_requests: int = 1 << 40):
+    """A served request stream (arrival_ns, sizes, prims) of vx_workload.h."""
+    m = _mix(world_exp, sphere_permille, add_permille, r_min, r_max, log_uniform, 1, 255)
+    total = C.c_uint64(0)
+    f = lib().orc_generate_requests
+    n = f(m.ctypes.data, seed, rate, seconds, zipf_s, max_size, max_requests, None, None, 0,
+          None, C.byref(total))
+    arr = np.zeros(max(n, 1), np.uint64)
+    sizes = np.zeros(max(n, 1), np.uint32)
+    prims = np.zeros(max(total.value, 1), PRIM_DTYPE)
+    f(m.ctypes.data, seed, rate, seconds, zipf_s, max_size, max_requests, arr.ctypes.data,
+      sizes.ctypes.data, prims.size, prims.ctypes.data, C.byref(total))
+    return arr[:n], sizes[:n], prims[:total.value]
 
 
 def terrain(seed: int, scale: int, caves: bool, world_exp: int = 0) -> np.ndarray:
@@ -283,6 +353,67 @@ def eval_voxels(t, world_exp, prims, xyz, materials=False) -> np.ndarray:
     return out
 
 
+class Sparse:
+    """Sequential editing on a sparse, hash-consed CPU DAG (oracle_sparse.cpp):
+    the terrain of a 4 << depth world (or an empty world), then every
+    primitive in order.  With base > 0 only the cell of that level containing
+    voxel `cell` is built (a region); the work is split into 8^shard_levels
+    shards over `threads` threads.  Dumps use the canonical forms of Grid."""
+
+    def __init__(self, depth: int, terrain_: np.ndarray | None = None, prims=None,
+                 materials: bool = False, base: int = 0, cell=(0, 0, 0),
+                 shard_levels: int = 3, threads: int | None = None):
+        import os
+        self.depth, self.base, self.materials = depth, base, materials
+        p = np.ascontiguousarray(np.zeros(0, PRIM_DTYPE) if prims is None else prims, PRIM_DTYPE)
+        c = np.ascontiguousarray(cell, np.uint32)
+        self._h = lib().orc_sparse_run(depth, None if terrain_ is None else terrain_.ctypes.data,
+                                       p.ctypes.data if p.size else None, p.size, int(materials),
+                                       base, c.ctypes.data, shard_levels,
+                                       threads or os.cpu_count() or 1)
+        assert self._h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_sparse_free(self._h)
+            self._h = None
+
+    def dag(self) -> DagCanon:
+        return _dump_dag(lib().orc_sparse_export_dag, self._h, self.depth - self.base)
+
+    def svo(self) -> SvoCanon:
+        nn, nl = C.c_uint64(0), C.c_uint64(0)
+        f = lib().orc_sparse_export_svo
+        f(self._h, C.byref(nn), C.byref(nl), None, 0, None, None, 0)
+        nodes = np.zeros(max(nn.value * 8, 1), np.uint32)
+        leaves = np.zeros(max(nl.value, 1), np.uint64)
+        mats = np.zeros(max(nl.value * 64, 1), np.uint8) if self.materials else None
+        rc = f(self._h, C.byref(nn), C.byref(nl), nodes.ctypes.data, nn.value,
+               leaves.ctypes.data, None if mats is None else mats.ctypes.data, nl.value)
+        assert rc == 0
+        return SvoCanon(nodes[:nn.value * 8], leaves[:nl.value],
+                        None if mats is None else mats[:nl.value * 64])
+
+    def leaf_block(self, lo, n) -> np.ndarray:
+        """Occupancy masks of the leaves [lo, lo + n) (leaf coordinates), x fastest."""
+        lo_ = np.ascontiguousarray(lo, np.uint32)
+        n_ = np.ascontiguousarray(n, np.uint32)
+        out = np.zeros(int(np.prod(n_.astype(np.uint64))), np.uint64)
+        lib().orc_sparse_leaf_block(self._h, lo_.ctypes.data, n_.ctypes.data, out.ctypes.data)
+        return out
+
+
+def terrain_leaf_mismatches(t: np.ndarray, origins: np.ndarray, materials: bool) -> int:
+    o = np.ascontiguousarray(origins, np.uint32).reshape(-1, 3)
+    return lib().orc_terrain_leaf_mismatches(t.ctypes.data, o.ctypes.data, o.shape[0],
+                                             int(materials))
+
+
+def terrain_classify_mismatches(t: np.ndarray, cubes: np.ndarray) -> int:
+    q = np.ascontiguousarray(cubes, np.uint32).reshape(-1, 4)
+    return lib().orc_terrain_classify_mismatches(t.ctypes.data, q.ctypes.data, q.shape[0])
+
+
 class RefDag:
     """The reference's own CPU HashDAG (algorithm/lib/include/algo/svt/hash_dag.hpp)."""
 
@@ -336,6 +467,20 @@ class RefDag:
 
     def canon(self) -> DagCanon:
         return _dump_dag(ref().ref_dag_export, self._h, self.depth)
+
+    def import_region(self, base: int, cell, dump: DagCanon) -> None:
+        """Load the canonical dump of the cell at level `base` containing voxel
+        `cell` (e.g. Sparse(..., base=base, cell=cell).dag()) into this empty
+        HashDAG with its own find_or_append_node / _leaf; the rest stays empty."""
+        counts = np.ascontiguousarray(dump.counts, np.uint64)
+        nodes = np.ascontiguousarray(dump.nodes, np.uint32)
+        leaves = np.ascontiguousarray(dump.leaves, np.uint64)
+        rc = ref().ref_dag_import_region(self._h, base, *map(int, cell), dump.root,
+                                         counts.ctypes.data,
+                                         nodes.ctypes.data if nodes.size else None,
+                                         leaves.ctypes.data if leaves.size else None)
+        if rc != 0:
+            raise RuntimeError("reference HashDAG bucket capacity exceeded on import")
 
 
 class RefSvo:

@@ -5,7 +5,8 @@
   oracle/_ref/libvxref.so     <- oracle/ref_shim.cpp compiled against the
                                  reference's own headers, read in place from
                                  <reference>/algorithm/lib/include (only when
-                                 that tree is present; nothing is copied)
+                                 that tree is present; nothing is copied);
+                                 <reference> is $VX_REFERENCE or ../reference
 
 Usage: python -m oracle.build [--reference PATH]
 """
@@ -22,7 +23,9 @@ BUILD = HERE / "_build"
 REF_OUT = HERE / "_ref"
 LIB = BUILD / "liboracle.so"
 REF_LIB = REF_OUT / "libvxref.so"
-DEFAULT_REFERENCE = Path("/root/reference")
+# The reference checkout: $VX_REFERENCE, else a "reference" directory beside
+# this repository.
+DEFAULT_REFERENCE = Path(os.environ.get("VX_REFERENCE", str(ROOT.parent / "reference")))
 # -O3 without -march=native: the library may run on a different host CPU.
 CXXFLAGS = ["-O3", "-std=c++20", "-fPIC", "-shared", "-pthread",
             f"-I{ROOT / 'include'}"]
@@ -59,8 +62,7 @@ def build_reference(reference: Path = DEFAULT_REFERENCE,
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get(
-        "VX_REFERENCE", str(DEFAULT_REFERENCE)))
+    ap.add_argument("--reference", default=str(DEFAULT_REFERENCE))
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build_oracle(a.force))

@@ -7,6 +7,7 @@
 // The canonical dumps below read the reference objects' internal node stores,
 // so the shim opens their private members to this translation unit only.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <unordered_map>
@@ -138,33 +139,38 @@ int ref_dag_edit_box(void *h, u32 x0, u32 y0, u32 z0, u32 x1, u32 y1, u32 z1,
 }
 
 // Apply one sphere (|p - c|^2 <= r^2) or box as x-runs of fill_box / clear_box
-// calls, clipped to the world; returns the number of voxels covered (the CPU
-// baseline's unit of work), or -1 on error.
-long long ref_dag_apply_prim(void *h, int shape, long long cx, long long cy,
-                             long long cz, long long r0, long long r1,
-                             long long r2, int fill) {
+// calls, clipped to the box [lo, hi) (the world when lo / hi are null);
+// returns the number of voxels covered (the CPU baseline's unit of work), or
+// -1 on error.
+long long ref_dag_apply_prim_clipped(void *h, int shape, long long cx, long long cy,
+                                     long long cz, long long r0, long long r1, long long r2,
+                                     int fill, const long long *lo, const long long *hi) {
   auto *d = static_cast<HashDAG *>(h);
   const long long world = d->world_voxel_count();
+  const long long b0[3] = {lo ? std::max(0ll, lo[0]) : 0, lo ? std::max(0ll, lo[1]) : 0,
+                           lo ? std::max(0ll, lo[2]) : 0};
+  const long long b1[3] = {hi ? std::min(world, hi[0]) : world, hi ? std::min(world, hi[1]) : world,
+                           hi ? std::min(world, hi[2]) : world};
   long long voxels = 0;
   try {
     if (shape == 1) {
-      const long long x0 = std::max(0ll, cx - r0), x1 = std::min(world, cx + r0 + 1);
-      const long long y0 = std::max(0ll, cy - r1), y1 = std::min(world, cy + r1 + 1);
-      const long long z0 = std::max(0ll, cz - r2), z1 = std::min(world, cz + r2 + 1);
+      const long long x0 = std::max(b0[0], cx - r0), x1 = std::min(b1[0], cx + r0 + 1);
+      const long long y0 = std::max(b0[1], cy - r1), y1 = std::min(b1[1], cy + r1 + 1);
+      const long long z0 = std::max(b0[2], cz - r2), z1 = std::min(b1[2], cz + r2 + 1);
       if (x1 <= x0 || y1 <= y0 || z1 <= z0) return 0;
       HashDAG::Box b{u32(x0), u32(y0), u32(z0), u32(x1), u32(y1), u32(z1)};
       fill ? d->fill_box(b) : d->clear_box(b);
       return (x1 - x0) * (y1 - y0) * (z1 - z0);
     }
     const long long r = r0;
-    for (long long z = std::max(0ll, cz - r); z < std::min(world, cz + r + 1); ++z)
-      for (long long y = std::max(0ll, cy - r); y < std::min(world, cy + r + 1); ++y) {
+    for (long long z = std::max(b0[2], cz - r); z < std::min(b1[2], cz + r + 1); ++z)
+      for (long long y = std::max(b0[1], cy - r); y < std::min(b1[1], cy + r + 1); ++y) {
         const long long rem = r * r - (z - cz) * (z - cz) - (y - cy) * (y - cy);
         if (rem < 0) continue;
         long long dx = static_cast<long long>(std::sqrt(static_cast<double>(rem)));
         while (dx * dx > rem) --dx;
         while ((dx + 1) * (dx + 1) <= rem) ++dx;
-        const long long x0 = std::max(0ll, cx - dx), x1 = std::min(world, cx + dx + 1);
+        const long long x0 = std::max(b0[0], cx - dx), x1 = std::min(b1[0], cx + dx + 1);
         if (x1 <= x0) continue;
         HashDAG::Box b{u32(x0), u32(y), u32(z), u32(x1), u32(y + 1), u32(z + 1)};
         fill ? d->fill_box(b) : d->clear_box(b);
@@ -174,6 +180,11 @@ long long ref_dag_apply_prim(void *h, int shape, long long cx, long long cy,
     return -1;
   }
   return voxels;
+}
+
+long long ref_dag_apply_prim(void *h, int shape, long long cx, long long cy, long long cz,
+                             long long r0, long long r1, long long r2, int fill) {
+  return ref_dag_apply_prim_clipped(h, shape, cx, cy, cz, r0, r1, r2, fill, nullptr, nullptr);
 }
 
 int ref_dag_set_voxel(void *h, u32 x, u32 y, u32 z, int value) {
@@ -218,6 +229,57 @@ int ref_dag_export(void *h, u32 *root, u64 *counts, u32 *nodes, u64 cap_words,
   if (leaves) {
     if (dump.leaves.size() > cap_leaves) return 2;
     for (u64 i = 0; i < dump.leaves.size(); ++i) leaves[i] = dump.leaves[i];
+  }
+  return 0;
+}
+
+// Load the canonical dump (format of ref_dag_export, relative levels
+// 0..depth-base) of the cell at level `base` that contains voxel (cx, cy, cz)
+// into an empty HashDAG: leaves and nodes are inserted bottom-up with the
+// reference's own find_or_append_leaf / find_or_append_node (hash_dag.hpp:
+// 535-560), full subtrees become its full_node_ptrs_ / full_leaf_ptr_, and the
+// rest of the world stays empty.  Returns 0, or 1 when a bucket overflows.
+int ref_dag_import_region(void *h, u32 base, u32 cx, u32 cy, u32 cz, u32 root_id,
+                          const u64 *counts, const u32 *nodes, const u64 *leaves) {
+  HashDAG &d = *static_cast<HashDAG *>(h);
+  const u32 D = d.depth_;
+  if (base > D) return 1;
+  const u32 L = D - base;
+  try {
+    std::vector<u32> leaf_ptr(counts[L]);
+    for (u64 i = 0; i < counts[L]; ++i) leaf_ptr[i] = d.find_or_append_leaf(leaves[i]);
+    std::vector<u64> off(L + 1, 0);
+    for (u32 l = 0; l < L; ++l) off[l + 1] = off[l] + counts[l] * 10;
+    std::vector<std::vector<u32>> ptr(L);
+    auto child_ptr = [&](u32 rl, u32 id) -> u32 {
+      if (id == 0) return 0;
+      if (id == 1) return rl == L ? d.full_leaf_ptr_ : d.full_node_ptrs_[base + rl];
+      return rl == L ? leaf_ptr[id - 2] : ptr[rl][id - 2];
+    };
+    for (u32 rl = L; rl-- > 0;) {
+      ptr[rl].resize(counts[rl]);
+      for (u64 i = 0; i < counts[rl]; ++i) {
+        const u32 *rec = nodes + off[rl] + 10 * i;
+        std::array<u32, 8> children{};
+        u32 mask = 0;
+        for (u32 c = 0; c < 8; ++c) {
+          children[c] = child_ptr(rl + 1, rec[2 + c]);
+          if (children[c] != 0) mask |= 1u << c;
+        }
+        ptr[rl][i] = d.find_or_append_node(base + rl, static_cast<uint8_t>(mask), children);
+      }
+    }
+    u32 sub = child_ptr(0, root_id);
+    for (u32 level = base; level > 0; --level) {
+      const u32 sh = D + 2 - level; // the parent's split bit
+      const u32 c = ((cx >> sh) & 1u) | (((cy >> sh) & 1u) << 1) | (((cz >> sh) & 1u) << 2);
+      std::array<u32, 8> children{};
+      children[c] = sub;
+      sub = sub ? d.find_or_append_node(level - 1, static_cast<uint8_t>(1u << c), children) : 0;
+    }
+    d.root_ = sub;
+  } catch (...) {
+    return 1;
   }
   return 0;
 }

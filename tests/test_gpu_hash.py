@@ -115,3 +115,60 @@ def test_cuckoo_replace_and_overflow(cuda):
     assert (s == vx.HASH_OVERFLOW).sum() == t.dropped() > 0
     found = u32(t.find(dev64(keys, cuda))) != vx.HASH_NOT_FOUND_VALUE
     assert found.sum() <= 64
+
+
+def _mix64(x: int) -> int:
+    m = (1 << 64) - 1
+    x ^= x >> 30
+    x = (x * 0xbf58476d1ce4e5b9) & m
+    x ^= x >> 27
+    x = (x * 0x94d049bb133111eb) & m
+    x ^= x >> 31
+    return x
+
+
+_CUCKOO_SALTS = (0x9e3779b97f4a7c15, 0xc2b2ae3d27d4eb4f, 0x165667b19e3779f9, 0x27d4eb2f165667c5)
+
+
+def _cuckoo_slot(key: int, hid: int, n: int) -> int:
+    return (_mix64(key ^ _CUCKOO_SALTS[hid]) * n) >> 64
+
+
+def _raw_slots(m) -> np.ndarray:
+    """The table's 16-byte slots {key, value | hash id << 32}, copied to the host."""
+    import ctypes
+    v = m.device_view()
+    out = np.empty((v.slot_count, 2), np.uint64)
+    rt = ctypes.CDLL("libcudart.so.12")
+    torch.cuda.synchronize()
+    assert rt.cudaMemcpy(ctypes.c_void_p(out.ctypes.data), ctypes.c_void_p(v.slots),
+                         ctypes.c_size_t(out.nbytes), 2) == 0
+    return out
+
+
+def test_cuckoo_replace_keeps_hash_id_through_later_evictions(cuda):
+    """A replaced entry keeps the hash id that placed it, so the evictions that
+    later move it continue from the right hash function: every stored entry
+    sits at the slot its recorded hash id names, and nothing is dropped."""
+    n_slots = 4096
+    rng = np.random.default_rng(77)
+    keys = unique_keys(rng, 3200)               # final load 0.78
+    vals = np.arange(keys.size, dtype=np.uint32)
+    m = vx.CuckooMap(n_slots, 1000)
+    half = keys.size // 2
+    m.insert(dev64(keys[:half], cuda), torch.from_numpy(vals[:half].view(np.int32)).to(cuda))
+    # replace every entry of the first half (values + 10^6)
+    st = torch.empty(half, dtype=torch.int32, device=cuda)
+    new = vals[:half] + 1_000_000
+    m.insert(dev64(keys[:half], cuda), torch.from_numpy(new.view(np.int32)).to(cuda), st)
+    assert (u32(st) == vx.HASH_REPLACED).all()
+    # the second half evicts many of the replaced entries
+    m.insert(dev64(keys[half:], cuda), torch.from_numpy(vals[half:].view(np.int32)).to(cuda))
+    assert m.dropped() == 0
+    expect = np.concatenate([new, vals[half:]])
+    assert np.array_equal(u32(m.find(dev64(keys, cuda))), expect)
+    raw = _raw_slots(m)
+    empty = np.uint64(0xFFFFFFFFFFFFFFFF)
+    for pos in np.nonzero(raw[:, 0] != empty)[0]:
+        key, word = int(raw[pos, 0]), int(raw[pos, 1])
+        assert _cuckoo_slot(key, word >> 32, n_slots) == pos

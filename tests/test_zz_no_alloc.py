@@ -39,6 +39,8 @@ def test_no_alloc_scan_matches_regular_on_consecutive_calls():
         assert np.array_equal(no_alloc(x, dev), regular(x, dev))
     x = np.full(70_000, 0xFFFFFFFF, np.uint32)  # wrapping sums
     assert np.array_equal(no_alloc(x, dev), regular(x, dev))
+    # the look-back status of the last call is readable without a workspace
+    assert vx.lib().vx_scan_noalloc_status(vx.stream_handle()) == vx.VX_OK
 
 
 def test_no_alloc_scan_rejects_counts_beyond_its_scratch():

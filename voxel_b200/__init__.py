@@ -162,6 +162,7 @@ _SIGS = {
     "vx_scan_inclusive_sum_u32": (_ST, [_P, _U32, _P, _SZ, _P]),
     "vx_scan_exclusive_sum_u64": (_ST, [_P, _U32, _P, _SZ, _P]),
     "vx_scan_exclusive_sum_u32_noalloc": (_ST, [_P, _U32, _P]),
+    "vx_scan_noalloc_status": (_ST, [_P]),
     "vx_sort_workspace_size": (_SZ, [_U32, _U32]),
     "vx_sort_pairs_u32": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_sort_pairs_u64": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
@@ -204,6 +205,7 @@ _SIGS = {
     "vx_dag_status": (_ST, [_P, _P]),
     "vx_dag_build_terrain": (_ST, [_P, C.POINTER(vx_terrain), _P]),
     "vx_dag_query": (_ST, [_P, _P, _U32, _P, _P]),
+    "vx_dag_read_leaves": (_ST, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _P, _P]),
     "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), _P,
                                       _P, _U64, _P, _U64, _P]),
     "vx_dag_get_stats": (_ST, [_P, C.POINTER(vx_dag_stats), _P]),

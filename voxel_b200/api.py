@@ -557,6 +557,17 @@ class HashDag:
               "vx_dag_get_stats")
         return st
 
+    def read_leaves(self, lo, n, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Occupancy masks of the leaf box [lo, lo + n) (leaf coordinates),
+        x fastest, as an int64 device tensor."""
+        count = int(n[0]) * int(n[1]) * int(n[2])
+        if out is None:
+            out = torch.empty(max(count, 1), dtype=torch.int64, device="cuda")
+        check(lib().vx_dag_read_leaves(self._h, int(lo[0]), int(lo[1]), int(lo[2]), int(n[0]),
+                                       int(n[1]), int(n[2]), ptr(out), stream_handle()),
+              "vx_dag_read_leaves")
+        return out[:count]
+
     def canonical(self, at_root: int = 0xFFFFFFFF):
         """(root, counts, nodes, leaves): DFS first-visit canonical dump of the
         current root, or of an earlier root ref still held by the tables."""

@@ -453,6 +453,15 @@ __global__ void query_kernel(vx_dag_view v, const vx_voxel *pts, uint32_t n,
   out[i] = vx_dag_get_voxel(v, p.x, p.y, p.z);
 }
 
+__global__ void read_leaves_kernel(vx_dag_view v, uint32_t lx0, uint32_t ly0, uint32_t lz0,
+                                   uint32_t nx, uint32_t ny, uint32_t n, uint64_t *out) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t x = static_cast<uint32_t>(i % nx), y = static_cast<uint32_t>((i / nx) % ny),
+                 z = static_cast<uint32_t>(i / (uint64_t(nx) * ny));
+  out[i] = vx_dag_get_leaf(v, lx0 + x, ly0 + y, lz0 + z);
+}
+
 // ------------------------------------------------------- plain path prep --
 
 // Voxel -> (leaf key, bit).  The key is the leaf's Morton path, 3 bits per
@@ -898,6 +907,21 @@ vx_status vx_dag_query(const vx_dag *d, const vx_voxel *pts, uint32_t count,
   vx_dag_view view;
   VX_TRY(vx_dag_device_view(d, &view));
   query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, pts, count, out);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_dag_read_leaves(const vx_dag *d, uint32_t lx0, uint32_t ly0, uint32_t lz0,
+                             uint32_t nx, uint32_t ny, uint32_t nz, uint64_t *out,
+                             vx_stream stream) {
+  const uint64_t n = uint64_t(nx) * ny * nz;
+  if (d == nullptr || (out == nullptr && n != 0) || n >= (1ull << 32)) return VX_ERR_INVALID_VALUE;
+  if (n == 0) return VX_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope sc("dag_read_leaves", s);
+  vx_dag_view view;
+  VX_TRY(vx_dag_device_view(d, &view));
+  read_leaves_kernel<<<vx::ceil_div(static_cast<uint32_t>(n), kBlock), kBlock, 0, s>>>(
+      view, lx0, ly0, lz0, nx, ny, static_cast<uint32_t>(n), out);
   return vx::from_cuda(cudaGetLastError());
 }
 

@@ -382,6 +382,22 @@ __device__ __forceinline__ ulonglong2 exch128(ulonglong2 *p, ulonglong2 v) {
   return old;
 }
 
+// 128-bit compare-and-swap of one slot; returns the slot's previous contents.
+__device__ __forceinline__ ulonglong2 cas128(ulonglong2 *p, ulonglong2 expected,
+                                             ulonglong2 desired) {
+  ulonglong2 old;
+  asm volatile(
+      "{\n\t.reg .b128 d, c, b;\n\t"
+      "mov.b128 c, {%2, %3};\n\t"
+      "mov.b128 b, {%4, %5};\n\t"
+      "atom.global.cas.b128 d, [%6], c, b;\n\t"
+      "mov.b128 {%0, %1}, d;\n\t}"
+      : "=l"(old.x), "=l"(old.y)
+      : "l"(expected.x), "l"(expected.y), "l"(desired.x), "l"(desired.y), "l"(p)
+      : "memory");
+  return old;
+}
+
 __device__ __forceinline__ ulonglong2 ld_slot(const ulonglong2 *p) {
   ulonglong2 v;
   asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
@@ -415,6 +431,28 @@ __device__ __forceinline__ bool cuckoo_lookup(const ulonglong2 *slots,
   return false;
 }
 
+// Replace the value stored for key, keeping the slot's hash id (bits 32..63
+// of .y, which the next eviction of this entry continues from).  The swap is
+// a 128-bit CAS on {key, old word}, so an entry that a concurrent eviction
+// moved is looked up again rather than overwritten in its new occupant's
+// slot.  Returns false when the key is not in the table (duplicate keys
+// inside one insert batch are not supported, as in the reference, so a key
+// held in flight by another thread's eviction chain is not expected).
+__device__ __forceinline__ bool cuckoo_replace(ulonglong2 *slots, uint32_t n,
+                                               uint64_t key, uint32_t value) {
+  uint32_t old_value, where;
+  for (uint32_t attempt = 0; attempt < 64; ++attempt) {
+    if (!cuckoo_lookup(slots, n, key, old_value, where)) return false;
+    const ulonglong2 cur = ld_slot(slots + where);
+    if (cur.x != key) continue;
+    const ulonglong2 want =
+        make_ulonglong2(key, (cur.y & 0xffffffff00000000ull) | value);
+    const ulonglong2 seen = cas128(slots + where, cur, want);
+    if (seen.x == cur.x && seen.y == cur.y) return true;
+  }
+  return false;
+}
+
 __global__ void __launch_bounds__(kBlock)
     cuckoo_insert_kernel(ulonglong2 *slots, uint32_t n, uint32_t max_evictions,
                          unsigned long long *dropped,
@@ -426,14 +464,9 @@ __global__ void __launch_bounds__(kBlock)
   const uint64_t key = keys[i];
   const uint32_t value = values ? values[i] : static_cast<uint32_t>(i);
   uint32_t status;
-  uint32_t old_value, where;
   if (key == kEmpty || key == kDeleted) {
     status = VX_HASH_INVALID_KEY;
-  } else if (cuckoo_lookup(slots, n, key, old_value, where)) {
-    // Replace in place (a concurrent eviction may move the slot meanwhile;
-    // duplicate keys inside one batch are not supported, as in the reference).
-    atomicExch(reinterpret_cast<unsigned long long *>(&slots[where].y),
-               static_cast<unsigned long long>(value));
+  } else if (cuckoo_replace(slots, n, key, value)) {
     status = VX_HASH_REPLACED;
   } else {
     ulonglong2 cur = make_ulonglong2(key, value);

@@ -3,6 +3,8 @@
 #include "profile.cuh"
 #include "scan.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace vx {
@@ -269,22 +271,58 @@ constexpr size_t kNoAllocHeader = 256; // tile counter, status word
 static __device__ __align__(256) unsigned char
     g_noalloc_scratch[kNoAllocHeader + size_t(kNoAllocTiles) * sizeof(uint64_t)];
 
-// Device address of g_noalloc_scratch per device (the symbol's name is only a
-// host-side stand-in and must never be handed to a kernel).
+// Unique id of the calling thread's current CUDA context (0 when there is
+// none or the driver entry points are unavailable).  Context ids are never
+// reused within a process, so a context created again after a device reset
+// gets a new id even when its handle value repeats.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  if (get_current == nullptr || get_id == nullptr) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch in the current context (the symbol's
+// name is only a host-side stand-in and must never be handed to a kernel).
+// The address is looked up with cudaGetSymbolAddress once per context and
+// cached under the context's unique id, so a device reset (which unloads the
+// module) is followed by a fresh lookup instead of a dangling address.  When
+// the context id cannot be read, the address is looked up on every call.
 void *noalloc_scratch(cudaError_t *err) {
   static std::mutex mu;
-  static void *addr[64] = {};
-  int dev = 0;
-  *err = cudaGetDevice(&dev);
-  if (*err != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  static unsigned long long cached_ctx = 0;
+  static void *cached_addr = nullptr;
+  *err = cudaSuccess;
+  unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
-    void *p = nullptr;
-    *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (*err != cudaSuccess) return nullptr;
-    addr[dev] = p;
-  }
-  return addr[dev];
+  if (ctx != 0 && ctx == cached_ctx && cached_addr != nullptr) return cached_addr;
+  void *p = nullptr;
+  *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (*err != cudaSuccess) return nullptr;
+  if (ctx == 0) ctx = current_context_id(); // the lookup may have created the context
+  cached_ctx = ctx;
+  cached_addr = ctx != 0 ? p : nullptr;
+  return p;
 }
 
 } // namespace
@@ -295,8 +333,9 @@ extern "C" {
 // Allocation-free exclusive sum (see the block comment above): count must be
 // at most 2^28; every call on a device shares one scratch array, so calls that
 // may overlap on the GPU (different streams without ordering) race.  The
-// first call on each device looks the scratch address up and should come
-// before any stream capture.
+// first call in each CUDA context looks the scratch address up and should
+// come before any stream capture; vx_scan_noalloc_status reads the status
+// word this call leaves behind.
 vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
                                             vx_stream stream) {
   using namespace vx::scan;
@@ -322,6 +361,26 @@ vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
   else
     scan_kernel<uint32_t, false, false><<<tiles, S::kBlock, 0, s>>>(data, count, ws, records);
   return vx::from_cuda(cudaGetLastError());
+}
+
+// Status of the most recent allocation-free scan on the current device:
+// synchronises the stream, then reads the device status word that the scan
+// kernel leaves in the shared scratch (VX_ERR_TIMEOUT when a look-back wait
+// gave up, in which case that call's prefix sums are not valid).  Every call
+// of the allocation-free scan clears the word first, so this reports the last
+// call that ran before the read; with calls that overlap on the GPU the word
+// belongs to whichever wrote it last.
+vx_status vx_scan_noalloc_status(vx_stream stream) {
+  using namespace vx::scan;
+  cudaError_t err = cudaSuccess;
+  char *base = static_cast<char *>(noalloc_scratch(&err));
+  if (base == nullptr) return vx::from_cuda(err);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint32_t code = 0;
+  VX_TRY_CUDA(cudaMemcpyAsync(&code, base + sizeof(uint32_t), sizeof(code),
+                              cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  return vx::status_from_device(code);
 }
 
 } // extern "C"
