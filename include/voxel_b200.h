@@ -144,6 +144,25 @@ vx_status vx_sort_pairs_u64(uint64_t *keys, uint32_t *values, uint32_t count,
                             uint32_t key_bits, void *workspace,
                             size_t workspace_bytes, vx_stream stream);
 
+/* Stable LSD radix sort of multi-word unsigned keys, in place: each key is
+ * `words` 32-bit words (word 0 least significant; the reference's
+ * UIntKey<W>, cuda/sort/uint_key.cuh:15-66, also u32 = 1 word and u64 = 2),
+ * ordered by its low key_bits bits (1 <= key_bits <= 32 * words; the KeyBits
+ * contract of RadixSort, cuda/sort/radix.cuh:55-67).  perm (optional, count
+ * entries) receives, for every output position, the input position of its
+ * key, which orders any number of value arrays of any element size through
+ * vx_gather (the reference's value_arrays, cuda/sort/value_arrays.cuh).
+ * words <= 64; count < 2^30. */
+size_t vx_sort_words_workspace_size(uint32_t count, uint32_t words);
+vx_status vx_sort_words(uint32_t *keys, uint32_t words, uint32_t count, uint32_t key_bits,
+                        uint32_t *perm, void *workspace, size_t workspace_bytes,
+                        vx_stream stream);
+
+/* dst[i] = src[index[i]] for count elements of elem_bytes bytes each (device
+ * memory, dst and src distinct). */
+vx_status vx_gather(void *dst, const void *src, const uint32_t *index, uint32_t count,
+                    uint32_t elem_bytes, vx_stream stream);
+
 /* ----------------------------------------------------------- hash tables --
  * Per-key status codes, identical in value to the reference's
  * kSlabHashStatus* (cuda/hash_table/slab_hash/common.cuh:18-25). */
@@ -335,6 +354,28 @@ vx_status vx_dag_build_terrain(vx_dag *dag, const vx_terrain *terrain,
 vx_status vx_dag_query(const vx_dag *dag, const vx_voxel *pts, uint32_t count,
                        uint8_t *out, vx_stream stream);
 
+/* The voxel engine's leaf edit record (voxel-engine/engine/voxel/src/voxel/
+ * command.rs:8-16, #[repr(C)], 20 bytes): a leaf at leaf coordinates (voxel
+ * coordinates / 4) and a 64-bit voxel mask (bit = x + 4y + 16z) split into
+ * low and high words. */
+typedef struct vx_leaf_command {
+    uint32_t leaf_x, leaf_y, leaf_z;
+    uint32_t voxel_data_low, voxel_data_high;
+} vx_leaf_command;
+
+/* Apply leaf edit commands in one batched edit: the masks of commands that
+ * name the same leaf are OR-merged (LeafEditCommand::merge_commands,
+ * command.rs:30-52), then every named leaf is OR-ed with its mask
+ * (VX_EDIT_PLACE, the engine's OrPolicy) or cleared by it (VX_EDIT_DESTROY,
+ * AndNotPolicy; voxel-engine/engine/voxel/src/shaders/svo/leaf_edit_policy.
+ * slang).  Leaves outside the world are ignored; count 0 is a no-op; the
+ * workspace contract and statuses are those of vx_dag_apply_voxels.  The SVO
+ * form writes `material` (1 when 0) into placed voxels of a material SVO. */
+size_t vx_leaf_command_workspace_size(uint32_t count);
+vx_status vx_dag_apply_leaf_commands(vx_dag *dag, const vx_leaf_command *cmds, uint32_t count,
+                                     uint32_t op, void *workspace, size_t workspace_bytes,
+                                     vx_stream stream);
+
 /* Dense read of a box of leaves: out[(z * ny + y) * nx + x] (device memory)
  * = occupancy mask of the leaf at leaf coordinates (lx0 + x, ly0 + y,
  * lz0 + z) (voxel coordinates / 4, bit = x + 4y + 16z; 0 outside the world).
@@ -456,6 +497,10 @@ vx_status vx_svo_build_terrain(vx_svo *svo, const vx_terrain *terrain,
  * materials) (svt::cuda::get_voxel, svt/cuda/query.cuh:11-35). */
 vx_status vx_svo_query(const vx_svo *svo, const vx_voxel *pts, uint32_t count,
                        uint8_t *out, vx_stream stream);
+/* Leaf edit commands on the SVO (see vx_dag_apply_leaf_commands). */
+vx_status vx_svo_apply_leaf_commands(vx_svo *svo, const vx_leaf_command *cmds, uint32_t count,
+                                     uint32_t op, uint32_t material, void *workspace,
+                                     size_t workspace_bytes, vx_stream stream);
 /* Canonical dump (host, synchronises): DFS first-visit renumbering of nodes
  * and leaves; host_nodes gets 8 words per node with child indices replaced by
  * canonical ones and bits 30/31 (and materials) kept; host_leaves gets the u64

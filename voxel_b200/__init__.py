@@ -166,6 +166,9 @@ _SIGS = {
     "vx_sort_workspace_size": (_SZ, [_U32, _U32]),
     "vx_sort_pairs_u32": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_sort_pairs_u64": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
+    "vx_sort_words_workspace_size": (_SZ, [_U32, _U32]),
+    "vx_sort_words": (_ST, [_P, _U32, _U32, _U32, _P, _P, _SZ, _P]),
+    "vx_gather": (_ST, [_P, _P, _P, _U32, _U32, _P]),
     "vx_slab_set_create": (_ST, [_U32, _U32, C.POINTER(_P)]),
     "vx_slab_set_destroy": (_ST, [_P]),
     "vx_slab_set_clear": (_ST, [_P, _P]),
@@ -205,6 +208,9 @@ _SIGS = {
     "vx_dag_status": (_ST, [_P, _P]),
     "vx_dag_build_terrain": (_ST, [_P, C.POINTER(vx_terrain), _P]),
     "vx_dag_query": (_ST, [_P, _P, _U32, _P, _P]),
+    "vx_leaf_command_workspace_size": (_SZ, [_U32]),
+    "vx_dag_apply_leaf_commands": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
+    "vx_svo_apply_leaf_commands": (_ST, [_P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
     "vx_dag_read_leaves": (_ST, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _P, _P]),
     "vx_dag_export_canonical": (_ST, [_P, C.POINTER(_U32), _P,
                                       _P, _U64, _P, _U64, _P]),

@@ -21,7 +21,7 @@ __all__ = [
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
     "COMPLETION_DTYPE", "TERMINAL_NODE_DTYPE", "TERMINAL_LEAF_DTYPE", "cell_prefix",
     "terminal_nodes", "terminal_leaves", "records_to_device",
-    "tuning", "tuning_options", "set_tuning", "reset_tuning", "Graph",
+    "tuning", "tuning_options", "set_tuning", "reset_tuning", "Graph", "LEAF_COMMAND_DTYPE",
 ]
 
 
@@ -326,6 +326,9 @@ class CuckooMap:
 
 PRIM_DTYPE = np.dtype([("c", "<i4", 3), ("r", "<u4", 3), ("flags", "<u4"),
                        ("reserved", "<u4")])
+# The voxel engine's LeafEditCommand (20 bytes, #[repr(C)]).
+LEAF_COMMAND_DTYPE = np.dtype([("leaf_x", "<u4"), ("leaf_y", "<u4"), ("leaf_z", "<u4"),
+                               ("voxel_data_low", "<u4"), ("voxel_data_high", "<u4")])
 
 
 def make_flags(shape: int, op: int, material: int = 0) -> int:
@@ -557,6 +560,19 @@ class HashDag:
               "vx_dag_get_stats")
         return st
 
+    def apply_leaf_commands(self, cmds: torch.Tensor, op: int,
+                            workspace: torch.Tensor | None = None) -> int:
+        """The voxel engine's leaf edit commands (LEAF_COMMAND_DTYPE records
+        in a device tensor): masks OR-merged per leaf, then placed (op=1) or
+        cleared (op=0).  Returns the status."""
+        n = cmds.numel() * cmds.element_size() // LEAF_COMMAND_DTYPE.itemsize
+        ws = workspace
+        if ws is None:
+            ws = torch.empty(max(lib().vx_leaf_command_workspace_size(n), 1),
+                             dtype=torch.uint8, device=cmds.device)
+        return lib().vx_dag_apply_leaf_commands(self._h, ptr(cmds), n, op, ptr(ws), ws.numel(),
+                                                stream_handle())
+
     def read_leaves(self, lo, n, out: torch.Tensor | None = None) -> torch.Tensor:
         """Occupancy masks of the leaf box [lo, lo + n) (leaf coordinates),
         x fastest, as an int64 device tensor."""
@@ -712,6 +728,18 @@ class Svo:
         t = vx_terrain(seed, scale, int(caves), self.depth + 2)
         check(lib().vx_svo_build_terrain(self._h, C.byref(t), stream_handle()),
               "vx_svo_build_terrain")
+
+    def apply_leaf_commands(self, cmds: torch.Tensor, op: int, material: int = 1,
+                            workspace: torch.Tensor | None = None) -> int:
+        """Leaf edit commands (see HashDag.apply_leaf_commands); placed voxels
+        get `material` in a material SVO.  Returns the status."""
+        n = cmds.numel() * cmds.element_size() // LEAF_COMMAND_DTYPE.itemsize
+        ws = workspace
+        if ws is None:
+            ws = torch.empty(max(lib().vx_leaf_command_workspace_size(n), 1),
+                             dtype=torch.uint8, device=cmds.device)
+        return lib().vx_svo_apply_leaf_commands(self._h, ptr(cmds), n, op, material, ptr(ws),
+                                                ws.numel(), stream_handle())
 
     def query(self, voxels: torch.Tensor) -> torch.Tensor:
         n = voxels.numel() // 3

@@ -496,8 +496,32 @@ __global__ void run_flags_kernel(const uint64_t *keys, uint32_t n, uint32_t dept
   flags[i] = (valid && (i == 0 || keys[i - 1] != keys[i])) ? 1u : 0u;
 }
 
-// Each run start ORs its run's bits into one leaf-mask primitive.
+// Leaf edit command -> (leaf key, command index); leaves outside the world
+// get key 1 << (3 * depth) and are dropped.
+__global__ void pack_leaf_commands_kernel(const vx_leaf_command *c, uint32_t n, uint32_t depth,
+                                          uint64_t *keys, uint32_t *index) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const vx_leaf_command cmd = c[i];
+  index[i] = static_cast<uint32_t>(i);
+  if ((cmd.leaf_x >> depth) | (cmd.leaf_y >> depth) | (cmd.leaf_z >> depth)) {
+    keys[i] = 1ull << (3 * depth);
+    return;
+  }
+  uint64_t key = 0;
+  for (uint32_t l = 0; l < depth; ++l) {
+    const uint32_t s = depth - 1 - l;
+    key = (key << 3) | (((cmd.leaf_x >> s) & 1u) | (((cmd.leaf_y >> s) & 1u) << 1) |
+                        (((cmd.leaf_z >> s) & 1u) << 2));
+  }
+  keys[i] = key;
+}
+
+// Each run start ORs its run's voxel bits (a voxel list) or its commands'
+// masks (leaf edit commands, selected by index) into one leaf-mask primitive.
+template <bool Commands>
 __global__ void reduce_runs_kernel(const uint64_t *keys, const uint32_t *bits,
+                                   const vx_leaf_command *cmds,
                                    const uint32_t *offsets, uint32_t n,
                                    uint32_t depth, uint32_t op, uint32_t material,
                                    vx_primitive *out, uint32_t *out_count) {
@@ -508,7 +532,15 @@ __global__ void reduce_runs_kernel(const uint64_t *keys, const uint32_t *bits,
   const bool start = valid && (i == 0 || keys[i - 1] != key);
   if (start) {
     uint64_t mask = 0;
-    for (uint64_t j = i; j < n && keys[j] == key; ++j) mask |= 1ull << bits[j];
+    for (uint64_t j = i; j < n && keys[j] == key; ++j) {
+      if constexpr (Commands) {
+        const vx_leaf_command &c = cmds[bits[j]];
+        mask |= static_cast<uint64_t>(c.voxel_data_low) |
+                (static_cast<uint64_t>(c.voxel_data_high) << 32);
+      } else {
+        mask |= 1ull << bits[j];
+      }
+    }
     uint32_t lx = 0, ly = 0, lz = 0;
     for (uint32_t l = 0; l < depth; ++l) {
       const uint32_t c = static_cast<uint32_t>(key >> (3 * (depth - 1 - l))) & 7u;
@@ -705,8 +737,43 @@ vx_status prepare(const vx_voxel *edits, uint32_t count, uint32_t depth,
   VX_TRY(vx_scan_exclusive_sum_u32(p.offsets, count, p.scan_ws, p.scan_ws_bytes, s));
   {
     vx::prof::Scope sc("plain_reduce_runs", s);
-    reduce_runs_kernel<<<blocks, kBlock, 0, s>>>(p.keys, p.bits, p.offsets, count,
-                                                 depth, op, material, p.prims, p.count);
+    reduce_runs_kernel<false><<<blocks, kBlock, 0, s>>>(p.keys, p.bits, nullptr, p.offsets,
+                                                        count, depth, op, material, p.prims,
+                                                        p.count);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  *out_prims = p.prims;
+  *out_count = p.count;
+  return VX_OK;
+}
+
+// Leaf edit commands -> one leaf-mask primitive per named leaf, the masks of
+// commands naming the same leaf OR-merged (the engine's merge_commands).
+vx_status prepare_leaf_commands(const vx_leaf_command *cmds, uint32_t count, uint32_t depth,
+                                uint32_t op, uint32_t material, void *workspace,
+                                const vx_primitive **out_prims, const uint32_t **out_count,
+                                cudaStream_t s) {
+  using namespace vx::dag;
+  vx::Carver c(workspace);
+  const PlainLayout p = plain_layout(c, count);
+  const uint32_t blocks = vx::ceil_div(count, kBlock);
+  {
+    vx::prof::Scope sc("plain_pack_leaf_commands", s);
+    pack_leaf_commands_kernel<<<blocks, kBlock, 0, s>>>(cmds, count, depth, p.keys, p.bits);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_sort_pairs_u64(p.keys, p.bits, count, 3 * depth + 1, p.sort_ws,
+                           p.sort_ws_bytes, s));
+  {
+    vx::prof::Scope sc("plain_run_flags", s);
+    run_flags_kernel<<<blocks, kBlock, 0, s>>>(p.keys, count, depth, p.offsets);
+  }
+  VX_TRY_CUDA(cudaGetLastError());
+  VX_TRY(vx_scan_exclusive_sum_u32(p.offsets, count, p.scan_ws, p.scan_ws_bytes, s));
+  {
+    vx::prof::Scope sc("plain_reduce_runs", s);
+    reduce_runs_kernel<true><<<blocks, kBlock, 0, s>>>(p.keys, p.bits, cmds, p.offsets, count,
+                                                       depth, op, material, p.prims, p.count);
   }
   VX_TRY_CUDA(cudaGetLastError());
   *out_prims = p.prims;
@@ -824,6 +891,24 @@ vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
   const vx_primitive *prims = nullptr;
   const uint32_t *n = nullptr;
   VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));
+  VX_TRY(run_pipeline(d, prims, n, count, s));
+  return read_status(d, s, true);
+}
+
+size_t vx_leaf_command_workspace_size(uint32_t count) { return vx::plain::workspace_size(count); }
+
+vx_status vx_dag_apply_leaf_commands(vx_dag *d, const vx_leaf_command *cmds, uint32_t count,
+                                     uint32_t op, void *workspace, size_t workspace_bytes,
+                                     vx_stream stream) {
+  if (d == nullptr || (cmds == nullptr && count != 0) || op > 1) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  if (workspace == nullptr || workspace_bytes < vx_leaf_command_workspace_size(count))
+    return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const vx_primitive *prims = nullptr;
+  const uint32_t *n = nullptr;
+  VX_TRY(vx::plain::prepare_leaf_commands(cmds, count, d->t.depth, op, 0, workspace, &prims, &n,
+                                          s));
   VX_TRY(run_pipeline(d, prims, n, count, s));
   return read_status(d, s, true);
 }

@@ -12,4 +12,8 @@ vx_status prepare(const vx_voxel *edits, uint32_t count, uint32_t depth,
                   uint32_t op, uint32_t material, void *workspace,
                   const vx_primitive **out_prims, const uint32_t **out_count,
                   cudaStream_t s);
+vx_status prepare_leaf_commands(const vx_leaf_command *cmds, uint32_t count, uint32_t depth,
+                                uint32_t op, uint32_t material, void *workspace,
+                                const vx_primitive **out_prims, const uint32_t **out_count,
+                                cudaStream_t s);
 } // namespace vx::plain

@@ -456,9 +456,160 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
   return VX_OK;
 }
 
+// ------------------------------------------------ multi-word keys --
+//
+// Keys of `words` 32-bit words (word 0 least significant, the reference's
+// UIntKey<W>, cuda/sort/uint_key.cuh:15-66) are sorted least significant
+// chunk first: each chunk of up to 64 key bits (words 2c, 2c + 1) is
+// gathered through the permutation built so far and sorted stably together
+// with it by this file's onesweep sort, so the permutation ends up ordering
+// the keys by their low key_bits bits, stably; the keys are then gathered
+// once through it.
+
+__global__ void iota_kernel(uint32_t *p, uint32_t n) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i < n) p[i] = static_cast<uint32_t>(i);
+}
+
+template <class C>
+__global__ void chunk_kernel(const uint32_t *__restrict__ keys, uint32_t words,
+                             const uint32_t *__restrict__ perm, uint32_t first_word,
+                             uint32_t n, C *__restrict__ out) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t *k = keys + static_cast<size_t>(perm[i]) * words + first_word;
+  C v = k[0];
+  if constexpr (sizeof(C) == 8)
+    if (first_word + 1 < words) v |= static_cast<uint64_t>(k[1]) << 32;
+  out[i] = v;
+}
+
+// dst[i] = src[index[i]] for elements of W-byte words x n_words.
+template <class W>
+__global__ void gather_kernel(W *__restrict__ dst, const W *__restrict__ src,
+                              const uint32_t *__restrict__ index, uint32_t count,
+                              uint32_t n_words) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= count) return;
+  const W *s = src + static_cast<size_t>(index[i]) * n_words;
+  W *d = dst + i * n_words;
+  for (uint32_t w = 0; w < n_words; ++w) d[w] = s[w];
+}
+
+namespace {
+
+constexpr size_t kWordsAlign = 256;
+inline size_t align_up(size_t v) { return (v + kWordsAlign - 1) & ~(kWordsAlign - 1); }
+
+struct WordsLayout {
+  size_t sort_ws, perm, chunk, keys, total;
+};
+inline WordsLayout words_layout(uint32_t count, uint32_t words) {
+  WordsLayout l{};
+  l.sort_ws = 0;
+  const size_t sort_bytes = workspace_bytes<uint64_t>(count, kMaxPasses);
+  l.perm = align_up(sort_bytes);
+  l.chunk = l.perm + align_up(sizeof(uint32_t) * size_t(count));
+  l.keys = l.chunk + align_up(sizeof(uint64_t) * size_t(count));
+  l.total = l.keys + align_up(sizeof(uint32_t) * size_t(words) * count);
+  return l;
+}
+
+} // namespace
+
+vx_status gather(void *dst, const void *src, const uint32_t *index, uint32_t count,
+                 uint32_t elem_bytes, cudaStream_t stream) {
+  if (count == 0) return VX_OK;
+  if (dst == nullptr || src == nullptr || index == nullptr || elem_bytes == 0)
+    return VX_ERR_INVALID_VALUE;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src);
+  const uint32_t grid = ceil_div(count, kBlock);
+  prof::Scope scope("sort_gather", stream);
+  if (elem_bytes % 16 == 0 && (a & 15u) == 0)
+    gather_kernel<uint4><<<grid, kBlock, 0, stream>>>(static_cast<uint4 *>(dst),
+                                                      static_cast<const uint4 *>(src), index,
+                                                      count, elem_bytes / 16);
+  else if (elem_bytes % 8 == 0 && (a & 7u) == 0)
+    gather_kernel<uint64_t><<<grid, kBlock, 0, stream>>>(static_cast<uint64_t *>(dst),
+                                                         static_cast<const uint64_t *>(src),
+                                                         index, count, elem_bytes / 8);
+  else if (elem_bytes % 4 == 0 && (a & 3u) == 0)
+    gather_kernel<uint32_t><<<grid, kBlock, 0, stream>>>(static_cast<uint32_t *>(dst),
+                                                         static_cast<const uint32_t *>(src),
+                                                         index, count, elem_bytes / 4);
+  else if (elem_bytes % 2 == 0 && (a & 1u) == 0)
+    gather_kernel<uint16_t><<<grid, kBlock, 0, stream>>>(static_cast<uint16_t *>(dst),
+                                                         static_cast<const uint16_t *>(src),
+                                                         index, count, elem_bytes / 2);
+  else
+    gather_kernel<uint8_t><<<grid, kBlock, 0, stream>>>(static_cast<uint8_t *>(dst),
+                                                        static_cast<const uint8_t *>(src),
+                                                        index, count, elem_bytes);
+  return from_cuda(cudaGetLastError());
+}
+
+vx_status sort_words(uint32_t *keys, uint32_t words, uint32_t count, uint32_t key_bits,
+                     uint32_t *perm_out, void *workspace, size_t ws_bytes,
+                     cudaStream_t stream) {
+  if (words == 0 || words > 64 || key_bits == 0 || key_bits > 32u * words)
+    return VX_ERR_INVALID_VALUE;
+  if (keys == nullptr && count != 0) return VX_ERR_INVALID_VALUE;
+  if (count > kMaxCount) return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  const WordsLayout l = words_layout(count, words);
+  if (workspace == nullptr || ws_bytes < l.total) return VX_ERR_INVALID_VALUE;
+  char *base = static_cast<char *>(workspace);
+  uint32_t *perm = reinterpret_cast<uint32_t *>(base + l.perm);
+  void *chunk = base + l.chunk;
+  const uint32_t grid = ceil_div(count, kBlock);
+  iota_kernel<<<grid, kBlock, 0, stream>>>(perm, count);
+  VX_TRY_CUDA(cudaGetLastError());
+  const size_t sort_bytes = workspace_bytes<uint64_t>(count, kMaxPasses);
+  for (uint32_t lo = 0; lo < key_bits; lo += 64) {
+    const uint32_t bits = key_bits - lo < 64 ? key_bits - lo : 64;
+    const uint32_t first = lo / 32;
+    if (bits <= 32) {
+      auto *c = static_cast<uint32_t *>(chunk);
+      chunk_kernel<uint32_t><<<grid, kBlock, 0, stream>>>(keys, words, perm, first, count, c);
+      VX_TRY_CUDA(cudaGetLastError());
+      VX_TRY(sort_pairs<uint32_t>(c, perm, count, bits, workspace, sort_bytes, stream));
+    } else {
+      auto *c = static_cast<uint64_t *>(chunk);
+      chunk_kernel<uint64_t><<<grid, kBlock, 0, stream>>>(keys, words, perm, first, count, c);
+      VX_TRY_CUDA(cudaGetLastError());
+      VX_TRY(sort_pairs<uint64_t>(c, perm, count, bits, workspace, sort_bytes, stream));
+    }
+  }
+  uint32_t *tmp = reinterpret_cast<uint32_t *>(base + l.keys);
+  VX_TRY(gather(tmp, keys, perm, count, 4u * words, stream));
+  VX_TRY_CUDA(cudaMemcpyAsync(keys, tmp, sizeof(uint32_t) * size_t(words) * count,
+                              cudaMemcpyDeviceToDevice, stream));
+  if (perm_out != nullptr)
+    VX_TRY_CUDA(cudaMemcpyAsync(perm_out, perm, sizeof(uint32_t) * size_t(count),
+                                cudaMemcpyDeviceToDevice, stream));
+  return VX_OK;
+}
+
 } // namespace vx::sort
 
 extern "C" {
+
+size_t vx_sort_words_workspace_size(uint32_t count, uint32_t words) {
+  if (count == 0 || words == 0) return 0;
+  return vx::sort::words_layout(count, words).total;
+}
+
+vx_status vx_sort_words(uint32_t *keys, uint32_t words, uint32_t count, uint32_t key_bits,
+                        uint32_t *perm, void *workspace, size_t workspace_bytes,
+                        vx_stream stream) {
+  return vx::sort::sort_words(keys, words, count, key_bits, perm, workspace, workspace_bytes,
+                              static_cast<cudaStream_t>(stream));
+}
+
+vx_status vx_gather(void *dst, const void *src, const uint32_t *index, uint32_t count,
+                    uint32_t elem_bytes, vx_stream stream) {
+  return vx::sort::gather(dst, src, index, count, elem_bytes, static_cast<cudaStream_t>(stream));
+}
 
 size_t vx_sort_workspace_size(uint32_t count, uint32_t key_bytes) {
   if (count <= 1) return 0;

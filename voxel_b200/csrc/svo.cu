@@ -604,6 +604,24 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
   return read_status(v, s);
 }
 
+vx_status vx_svo_apply_leaf_commands(vx_svo *v, const vx_leaf_command *cmds, uint32_t count,
+                                     uint32_t op, uint32_t material, void *workspace,
+                                     size_t workspace_bytes, vx_stream stream) {
+  if (v == nullptr || (cmds == nullptr && count != 0) || op > 1 || material > 255)
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  if (workspace == nullptr || workspace_bytes < vx_leaf_command_workspace_size(count))
+    return VX_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const vx_primitive *prims = nullptr;
+  const uint32_t *n = nullptr;
+  const uint32_t mat = op == VX_EDIT_PLACE ? (material ? material : 1u) : 0u;
+  VX_TRY(vx::plain::prepare_leaf_commands(cmds, count, v->t.depth, op, mat, workspace, &prims,
+                                          &n, s));
+  VX_TRY(run_pipeline(v, prims, n, count, s, false));
+  return read_status(v, s);
+}
+
 uint32_t vx_svo_depth(const vx_svo *v) { return v ? v->t.depth : 0; }
 
 vx_status vx_svo_device_view(const vx_svo *v, vx_svo_view *out) {
