@@ -459,6 +459,7 @@ def run_dag(args, ws, rank, local, torch, vx, device):
     # the edited DAG (terrain + batch) as a canonical dump in host memory,
     # checked against the CPU oracle after the timed legs
     canon = work.canonical() if rank == 0 else None
+    rays = run_raycast(torch, vx, device, work)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     if ws > 1:
         import torch.distributed as dist
@@ -526,8 +527,50 @@ def run_dag(args, ws, rank, local, torch, vx, device):
         "launches": int(launches), "clocks": clk.summary(),
         "dag_bytes_reserved": int(dag_bytes),
         "graph_ms": g_ms / steps, "graph_kernels": int(graph_kernels),
-        "canon": canon, "prims_np": prims_np,
+        "canon": canon, "prims_np": prims_np, "rays": rays,
     }
+
+
+RAYS = 1 << 20
+RAYS_CHECKED = 20_000
+
+
+def c4_rays(n, seed=13):
+    """Rays over the C4 world: from above the terrain looking down at random
+    angles, and from random points in any direction."""
+    import voxel_b200 as vx
+    rng = np.random.default_rng(seed)
+    world = 4 << DAG_DEPTH
+    r = np.zeros(n, vx.RAY_DTYPE)
+    o = rng.uniform(0, world, (n, 3))
+    down = rng.random(n) < 0.5
+    o[down, 2] = rng.uniform(10240, 12288, down.sum())
+    d = rng.normal(size=(n, 3))
+    d[down, 2] = -np.abs(d[down, 2]) - 0.3
+    r["origin"], r["dir"], r["t_max"] = o, d, 3.0e38
+    return r
+
+
+def run_raycast(torch, vx, device, dag):
+    """Ray casts against the edited C4 DAG: device time of one launch over
+    RAYS rays (inputs resident), and the first RAYS_CHECKED hits for the CPU
+    check."""
+    rays = c4_rays(RAYS)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).to(device)
+    dag.raycast(d_rays)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    reps = 3
+    a.record()
+    for _ in range(reps):
+        hits = dag.raycast(d_rays)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    h = hits.cpu().numpy().view(np.uint32).reshape(-1, 5)
+    return {"ms": ms, "rays": RAYS, "hit_fraction": float((h[:, 3] != 6).mean()),
+            "check_rays": rays[:RAYS_CHECKED], "check_hits": h[:RAYS_CHECKED].copy()}
 
 
 def run_plain_sample(torch, vx, device, work, pristine, prims, counts, prims_np,
@@ -802,6 +845,8 @@ def run_parity(dag, svo, serve, sweep):
     t = time.perf_counter()
     want = oracle.Sparse(DAG_DEPTH, oracle.terrain(DAG_SEED, DAG_SCALE, True), dag["prims_np"])
     out["c4_full_dag"] = want.dag() == oracle.DagCanon(*dag["canon"])
+    rc = dag["rays"]
+    out["c4_raycast"] = bool(np.array_equal(want.raycast(rc["check_rays"]), rc["check_hits"]))
     del want
     secs["c4"] = time.perf_counter() - t
     t = time.perf_counter()
@@ -922,6 +967,9 @@ def run_ours(args, ws, rank, local):
             "batched_graph_ms_per_batch": round(dag["graph_ms"], 3),
             "batched_graph_voxels_per_s": round(dag["voxels_batch"] / (dag["graph_ms"] / 1e3), 1),
             "batched_graph_kernels": dag["graph_kernels"],
+            "raycast_Mrays_per_s": round(dag["rays"]["rays"] / dag["rays"]["ms"] / 1e3, 1),
+            "raycast_ms": round(dag["rays"]["ms"], 3),
+            "raycast_hit_fraction": round(dag["rays"]["hit_fraction"], 3),
             "tuning": vx.tuning(),
             **{k2: v for k2, v in svo.items() if not k2.startswith("_")},
             **{k2: v for k2, v in serve.items() if not k2.startswith("_")},

@@ -354,6 +354,41 @@ vx_status vx_dag_build_terrain(vx_dag *dag, const vx_terrain *terrain,
 vx_status vx_dag_query(const vx_dag *dag, const vx_voxel *pts, uint32_t count,
                        uint8_t *out, vx_stream stream);
 
+/* A ray in the DAG's voxel coordinates (the world is [0, 4 << depth)^3, voxel
+ * (x, y, z) the unit cube at x, y, z): points origin + t * dir for
+ * 0 <= t <= t_max; dir need not be normalised.  32 bytes. */
+typedef struct vx_ray {
+    float origin[3];
+    float dir[3];
+    float t_max;
+    uint32_t reserved;
+} vx_ray;
+
+/* First solid voxel a ray meets: the voxel engine's raycast result words
+ * (voxel-engine/engine/voxel/src/voxel/raycast_data.rs:31-47: voxel x, y, z,
+ * face, distance), 20 bytes.  face is the hit voxel's side the ray entered
+ * through, in the engine's Face order (shaders/svo/face.slang: 0 X+, 1 X-,
+ * 2 Y+, 3 Y-, 4 Z+, 5 Z-), 0 when the ray starts inside the world, and 6 =
+ * VX_FACE_NO_HIT (voxel ~0, t = -1) when nothing solid lies on [0, t_max]
+ * inside the world; t is the ray parameter where it enters the voxel. */
+typedef struct vx_ray_hit {
+    uint32_t voxel[3];
+    uint32_t face;
+    float t;
+} vx_ray_hit;
+#define VX_FACE_NO_HIT 6u
+
+/* Cast rays through the resident DAG: hits[i] for rays[i] (device memory).
+ * A DDA over voxel boundaries that steps over whole empty cells of the DAG
+ * (one root-to-cell walk per step); every floating-point operation is a
+ * correctly rounded single-precision add, multiply, divide or floor, so the
+ * result is reproducible bit for bit (voxel_b200_device.cuh vx_dag_raycast).
+ * The GPU counterpart of the engine's raycast compute pass
+ * (voxel-engine/engine/voxel/src/shaders/svo/raycast_compute_algorithm.slang),
+ * over the Hash DAG and for any number of rays. */
+vx_status vx_dag_raycast(const vx_dag *dag, const vx_ray *rays, uint32_t count,
+                         vx_ray_hit *hits, vx_stream stream);
+
 /* The voxel engine's leaf edit record (voxel-engine/engine/voxel/src/voxel/
  * command.rs:8-16, #[repr(C)], 20 bytes): a leaf at leaf coordinates (voxel
  * coordinates / 4) and a 64-bit voxel mask (bit = x + 4y + 16z) split into

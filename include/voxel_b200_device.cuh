@@ -100,6 +100,113 @@ __device__ __forceinline__ uint64_t vx_dag_get_leaf(const vx_dag_view &v, uint32
   return v.leaves[ref - 2u];
 }
 
+/* First solid voxel along a ray (vx_dag_raycast in voxel_b200.h).  The ray is
+ * clipped to the world box; from the voxel it enters, each step walks the DAG
+ * to the largest uniform cell (or leaf voxel) holding the current voxel: a
+ * full cell or a set leaf bit is the hit, otherwise the ray leaves the cell
+ * through the side with the smallest exit parameter (ties: x, then y, then
+ * z), the next voxel across that side is the next position, and the other
+ * coordinates are floor(origin + t dir) kept inside the cell and never moving
+ * against the ray.  Each step advances one coordinate, so at most
+ * 3 * world steps run. */
+__device__ inline vx_ray_hit vx_dag_raycast(const vx_dag_view &v, const vx_ray &ray) {
+  vx_ray_hit miss;
+  miss.voxel[0] = miss.voxel[1] = miss.voxel[2] = ~0u;
+  miss.face = VX_FACE_NO_HIT;
+  miss.t = -1.0f;
+  const uint32_t D = v.depth;
+  const int32_t W = 4 << D;
+  const float Wf = (float)W;
+  const float o[3] = {ray.origin[0], ray.origin[1], ray.origin[2]};
+  const float d[3] = {ray.dir[0], ray.dir[1], ray.dir[2]};
+  float t0 = 0.0f, t1 = __int_as_float(0x7f800000);
+  int entry = -1;
+  for (int a = 0; a < 3; ++a) {
+    if (d[a] == 0.0f) {
+      if (!(o[a] >= 0.0f && o[a] < Wf)) return miss;
+      continue;
+    }
+    const float ta = __fdiv_rn(__fsub_rn(0.0f, o[a]), d[a]);
+    const float tb = __fdiv_rn(__fsub_rn(Wf, o[a]), d[a]);
+    const float tn = ta < tb ? ta : tb, tf = ta < tb ? tb : ta;
+    if (tn > t0) {
+      t0 = tn;
+      entry = a;
+    }
+    if (tf < t1) t1 = tf;
+  }
+  if (!(t0 < t1) || !(t0 <= ray.t_max)) return miss;
+  int32_t vox[3];
+  for (int a = 0; a < 3; ++a) {
+    if (a == entry) {
+      vox[a] = d[a] > 0.0f ? 0 : W - 1;
+    } else {
+      float f = floorf(__fadd_rn(o[a], __fmul_rn(t0, d[a])));
+      f = f < 0.0f ? 0.0f : (f > Wf - 1.0f ? Wf - 1.0f : f);
+      vox[a] = (int32_t)f;
+    }
+  }
+  uint32_t face = entry < 0 ? 0u : (d[entry] > 0.0f ? 2u * entry + 1u : 2u * entry);
+  float t = t0;
+  const uint32_t root = *v.root;
+  const uint32_t limit = 3u * (uint32_t)W + 8u;
+  for (uint32_t step = 0; step < limit; ++step) {
+    uint32_t ref = root, l = 0;
+    for (; l < D && ref >= 2u; ++l) {
+      const uint32_t sh = D + 1 - l;
+      const uint32_t c = (((uint32_t)vox[0] >> sh) & 1u) | ((((uint32_t)vox[1] >> sh) & 1u) << 1) |
+                         ((((uint32_t)vox[2] >> sh) & 1u) << 2);
+      ref = vx_dag_item_child(v.pool[l] + (ref - 2u), c);
+    }
+    int32_t side;
+    if (ref == 1u) {
+      side = 0;
+    } else if (ref >= 2u) {
+      const uint32_t bit = (vox[0] & 3) + 4u * (vox[1] & 3) + 16u * (vox[2] & 3);
+      side = ((v.leaves[ref - 2u] >> bit) & 1ull) ? 0 : 1;
+    } else {
+      side = 4 << (D - l);
+    }
+    if (side == 0) {
+      vx_ray_hit h;
+      h.voxel[0] = (uint32_t)vox[0];
+      h.voxel[1] = (uint32_t)vox[1];
+      h.voxel[2] = (uint32_t)vox[2];
+      h.face = face;
+      h.t = t;
+      return h;
+    }
+    int32_t cmin[3];
+    for (int a = 0; a < 3; ++a) cmin[a] = vox[a] & ~(side - 1);
+    float tx = 0.0f;
+    int ax = -1;
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] == 0.0f) continue;
+      const float b = (float)(d[a] > 0.0f ? cmin[a] + side : cmin[a]);
+      const float ta = __fdiv_rn(__fsub_rn(b, o[a]), d[a]);
+      if (ax < 0 || ta < tx) {
+        tx = ta;
+        ax = a;
+      }
+    }
+    if (ax < 0 || !(tx <= ray.t_max)) return miss;
+    const int32_t nv = d[ax] > 0.0f ? cmin[ax] + side : cmin[ax] - 1;
+    if (nv < 0 || nv >= W) return miss;
+    for (int b = 0; b < 3; ++b) {
+      if (b == ax || d[b] == 0.0f) continue;
+      const float lo = (float)(d[b] > 0.0f ? vox[b] : cmin[b]);
+      const float hi = (float)(d[b] > 0.0f ? cmin[b] + side - 1 : vox[b]);
+      float f = floorf(__fadd_rn(o[b], __fmul_rn(tx, d[b])));
+      f = f < lo ? lo : (f > hi ? hi : f);
+      vox[b] = (int32_t)f;
+    }
+    vox[ax] = nv;
+    t = tx;
+    face = d[ax] > 0.0f ? 2u * ax + 1u : 2u * ax;
+  }
+  return miss;
+}
+
 /* ------------------------------------------------------------------ SVO -- */
 
 /* Value of a child word without a child: material (or 1 without materials)

@@ -156,6 +156,7 @@ _VOXEL_SIGS = [
     ("orc_terrain_leaf_mismatches", _U64, [_P, _P, _U64, _I]),
     ("orc_terrain_classify_mismatches", _U64, [_P, _P, _U64]),
     ("orc_generate_primitives", None, [_P, _U64, _U64, _U64, _P]),
+    ("orc_sparse_raycast", None, [_P, _P, _U64, _P]),
     ("orc_generate_requests", _U64, [_P, _U64, C.c_double, C.c_double, C.c_double, _U32,
                                      _U64, _P, _P, _U64, _P, C.POINTER(_U64)]),
 ]
@@ -393,6 +394,16 @@ class Sparse:
         assert rc == 0
         return SvoCanon(nodes[:nn.value * 8], leaves[:nl.value],
                         None if mats is None else mats[:nl.value * 64])
+
+    def raycast(self, rays: np.ndarray) -> np.ndarray:
+        """First solid voxel of each ray (records of 8 floats: origin, dir,
+        t_max, unused), as records of 5 words (voxel, face, t bits); the
+        world must be whole (base 0)."""
+        assert self.base == 0
+        r = np.ascontiguousarray(rays).view(np.float32).reshape(-1, 8)
+        out = np.zeros((r.shape[0], 5), np.uint32)
+        lib().orc_sparse_raycast(self._h, r.ctypes.data, r.shape[0], out.ctypes.data)
+        return out
 
     def leaf_block(self, lo, n) -> np.ndarray:
         """Occupancy masks of the leaves [lo, lo + n) (leaf coordinates), x fastest."""

@@ -27,7 +27,9 @@ REF_LIB = REF_OUT / "libvxref.so"
 # this repository.
 DEFAULT_REFERENCE = Path(os.environ.get("VX_REFERENCE", str(ROOT.parent / "reference")))
 # -O3 without -march=native: the library may run on a different host CPU.
-CXXFLAGS = ["-O3", "-std=c++20", "-fPIC", "-shared", "-pthread",
+# -ffp-contract=off: every float operation rounds once, as the GPU code's
+# explicitly rounded intrinsics do (the ray casts are compared bit for bit).
+CXXFLAGS = ["-O3", "-std=c++20", "-ffp-contract=off", "-fPIC", "-shared", "-pthread",
             f"-I{ROOT / 'include'}"]
 
 

@@ -29,7 +29,9 @@
 #include <array>
 #include <atomic>
 #include <cstdint>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <thread>
 #include <type_traits>
@@ -795,9 +797,128 @@ void leaf_block(const World<Mat> &w, const u32 lo[3], const u32 n[3], u64 *out) 
   }
 }
 
+// First solid voxel along a ray (the semantics of vx_dag_raycast, restated
+// over the sparse world): the ray is clipped to the world box, then it steps
+// from cell to cell, each step finding the largest uniform cell (or leaf
+// voxel) that holds the current voxel; a solid one is the hit, otherwise the
+// ray leaves it through the side with the smallest exit parameter (ties x,
+// y, z) into the next voxel, whose other coordinates are floor(o + t d) kept
+// inside the cell and not moving backwards.  Single-precision operations,
+// each rounded once (no contraction), in the order of the GPU code.
+// Output: voxel x, y, z, face (0 X+ .. 5 Z-, 6 no hit), t as float bits.
+template <bool Mat>
+void raycast(const World<Mat> &w, const float *ray, u32 out[5]) {
+  const float *o = ray, *d = ray + 3;
+  const float t_max = ray[6];
+  const u32 no_hit[5] = {~0u, ~0u, ~0u, 6u, 0xbf800000u}; // t = -1.0f
+  std::memcpy(out, no_hit, sizeof(no_hit));
+  const u32 D = w.depth;
+  const int32_t W = 4 << D;
+  const float Wf = static_cast<float>(W);
+  float t0 = 0.0f, t1 = std::numeric_limits<float>::infinity();
+  int entry = -1;
+  for (int a = 0; a < 3; ++a) {
+    if (d[a] == 0.0f) {
+      if (!(o[a] >= 0.0f && o[a] < Wf)) return;
+      continue;
+    }
+    const float ta = (0.0f - o[a]) / d[a];
+    const float tb = (Wf - o[a]) / d[a];
+    const float tn = ta < tb ? ta : tb, tf = ta < tb ? tb : ta;
+    if (tn > t0) {
+      t0 = tn;
+      entry = a;
+    }
+    if (tf < t1) t1 = tf;
+  }
+  if (!(t0 < t1) || !(t0 <= t_max)) return;
+  int32_t vox[3];
+  for (int a = 0; a < 3; ++a) {
+    if (a == entry) {
+      vox[a] = d[a] > 0.0f ? 0 : W - 1;
+    } else {
+      const float prod = t0 * d[a];
+      float f = std::floor(o[a] + prod);
+      f = f < 0.0f ? 0.0f : (f > Wf - 1.0f ? Wf - 1.0f : f);
+      vox[a] = static_cast<int32_t>(f);
+    }
+  }
+  u32 face = entry < 0 ? 0u : (d[entry] > 0.0f ? 2u * entry + 1u : 2u * entry);
+  float t = t0;
+  const u32 limit = 3u * static_cast<u32>(W) + 8u;
+  for (u32 step = 0; step < limit; ++step) {
+    // the largest uniform cell or the leaf holding vox
+    GRef g = w.root;
+    u32 level = 0;
+    bool uniform = g.shard < 0 && g.ref < World<Mat>::kU;
+    while (!uniform && level < D) {
+      const u32 sh = D + 1 - level;
+      const u32 c = ((u32(vox[0]) >> sh) & 1u) | (((u32(vox[1]) >> sh) & 1u) << 1) |
+                    (((u32(vox[2]) >> sh) & 1u) << 2);
+      g = w.children(level, g)[c];
+      ++level;
+      uniform = g.shard < 0 && g.ref < World<Mat>::kU;
+    }
+    int32_t side;
+    if (uniform) {
+      side = g.ref != 0 ? 0 : (4 << (D - level));
+    } else {
+      const u64 m = w.stores[g.shard]->leaf_mask(g.ref);
+      const u32 bit = u32(vox[0] & 3) + 4u * u32(vox[1] & 3) + 16u * u32(vox[2] & 3);
+      side = ((m >> bit) & 1u) ? 0 : 1;
+    }
+    if (side == 0) {
+      out[0] = u32(vox[0]);
+      out[1] = u32(vox[1]);
+      out[2] = u32(vox[2]);
+      out[3] = face;
+      std::memcpy(&out[4], &t, 4);
+      return;
+    }
+    int32_t cmin[3];
+    for (int a = 0; a < 3; ++a) cmin[a] = vox[a] & ~(side - 1);
+    float tx = 0.0f;
+    int ax = -1;
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] == 0.0f) continue;
+      const float b = static_cast<float>(d[a] > 0.0f ? cmin[a] + side : cmin[a]);
+      const float ta = (b - o[a]) / d[a];
+      if (ax < 0 || ta < tx) {
+        tx = ta;
+        ax = a;
+      }
+    }
+    if (ax < 0 || !(tx <= t_max)) return;
+    const int32_t nv = d[ax] > 0.0f ? cmin[ax] + side : cmin[ax] - 1;
+    if (nv < 0 || nv >= W) return;
+    for (int b = 0; b < 3; ++b) {
+      if (b == ax || d[b] == 0.0f) continue;
+      const float lo = static_cast<float>(d[b] > 0.0f ? vox[b] : cmin[b]);
+      const float hi = static_cast<float>(d[b] > 0.0f ? cmin[b] + side - 1 : vox[b]);
+      const float prod = tx * d[b];
+      float f = std::floor(o[b] + prod);
+      f = f < lo ? lo : (f > hi ? hi : f);
+      vox[b] = static_cast<int32_t>(f);
+    }
+    vox[ax] = nv;
+    t = tx;
+    face = d[ax] > 0.0f ? 2u * ax + 1u : 2u * ax;
+  }
+}
+
 } // namespace
 
 extern "C" {
+
+// Rays (8 floats each: origin, dir, t_max, unused) through the whole world
+// (base 0); hits: 5 words each (see raycast above).
+void orc_sparse_raycast(void *hp, const float *rays, u64 n, u32 *hits) {
+  const Handle &h = *static_cast<Handle *>(hp);
+  for (u64 i = 0; i < n; ++i) {
+    if (h.mats) raycast(*h.mat, rays + 8 * i, hits + 5 * i);
+    else raycast(*h.occ, rays + 8 * i, hits + 5 * i);
+  }
+}
 
 // Build the terrain (t may be null: empty world) of a 4 << depth world and
 // apply n primitives in order, restricted to the cell at level `base` that

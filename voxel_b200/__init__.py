@@ -208,6 +208,7 @@ _SIGS = {
     "vx_dag_status": (_ST, [_P, _P]),
     "vx_dag_build_terrain": (_ST, [_P, C.POINTER(vx_terrain), _P]),
     "vx_dag_query": (_ST, [_P, _P, _U32, _P, _P]),
+    "vx_dag_raycast": (_ST, [_P, _P, _U32, _P, _P]),
     "vx_leaf_command_workspace_size": (_SZ, [_U32]),
     "vx_dag_apply_leaf_commands": (_ST, [_P, _P, _U32, _U32, _P, _SZ, _P]),
     "vx_svo_apply_leaf_commands": (_ST, [_P, _P, _U32, _U32, _U32, _P, _SZ, _P]),

@@ -21,7 +21,7 @@ __all__ = [
     "config_c4_edits", "rasterize", "Svo", "Server", "generate_requests",
     "COMPLETION_DTYPE", "TERMINAL_NODE_DTYPE", "TERMINAL_LEAF_DTYPE", "cell_prefix",
     "terminal_nodes", "terminal_leaves", "records_to_device",
-    "tuning", "tuning_options", "set_tuning", "reset_tuning", "Graph", "LEAF_COMMAND_DTYPE",
+    "tuning", "tuning_options", "set_tuning", "reset_tuning", "Graph", "LEAF_COMMAND_DTYPE", "RAY_DTYPE", "HIT_DTYPE",
 ]
 
 
@@ -326,6 +326,10 @@ class CuckooMap:
 
 PRIM_DTYPE = np.dtype([("c", "<i4", 3), ("r", "<u4", 3), ("flags", "<u4"),
                        ("reserved", "<u4")])
+# Rays and hits of vx_dag_raycast (the hit is the engine's raycast result words).
+RAY_DTYPE = np.dtype([("origin", "<f4", 3), ("dir", "<f4", 3), ("t_max", "<f4"),
+                      ("reserved", "<u4")])
+HIT_DTYPE = np.dtype([("voxel", "<u4", 3), ("face", "<u4"), ("t", "<f4")])
 # The voxel engine's LeafEditCommand (20 bytes, #[repr(C)]).
 LEAF_COMMAND_DTYPE = np.dtype([("leaf_x", "<u4"), ("leaf_y", "<u4"), ("leaf_z", "<u4"),
                                ("voxel_data_low", "<u4"), ("voxel_data_high", "<u4")])
@@ -572,6 +576,15 @@ class HashDag:
                              dtype=torch.uint8, device=cmds.device)
         return lib().vx_dag_apply_leaf_commands(self._h, ptr(cmds), n, op, ptr(ws), ws.numel(),
                                                 stream_handle())
+
+    def raycast(self, rays: torch.Tensor) -> torch.Tensor:
+        """First solid voxel of each ray (RAY_DTYPE records in a device tensor):
+        HIT_DTYPE records (voxel, face, t) as a uint8 device tensor."""
+        n = rays.numel() * rays.element_size() // RAY_DTYPE.itemsize
+        out = torch.empty(max(n, 1) * HIT_DTYPE.itemsize, dtype=torch.uint8, device=rays.device)
+        check(lib().vx_dag_raycast(self._h, ptr(rays), n, ptr(out), stream_handle()),
+              "vx_dag_raycast")
+        return out[:n * HIT_DTYPE.itemsize]
 
     def read_leaves(self, lo, n, out: torch.Tensor | None = None) -> torch.Tensor:
         """Occupancy masks of the leaf box [lo, lo + n) (leaf coordinates),

@@ -453,6 +453,13 @@ __global__ void query_kernel(vx_dag_view v, const vx_voxel *pts, uint32_t n,
   out[i] = vx_dag_get_voxel(v, p.x, p.y, p.z);
 }
 
+__global__ void raycast_kernel(vx_dag_view v, const vx_ray *rays, uint32_t n,
+                               vx_ray_hit *hits) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  hits[i] = vx_dag_raycast(v, rays[i]);
+}
+
 __global__ void read_leaves_kernel(vx_dag_view v, uint32_t lx0, uint32_t ly0, uint32_t lz0,
                                    uint32_t nx, uint32_t ny, uint32_t n, uint64_t *out) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
@@ -992,6 +999,19 @@ vx_status vx_dag_query(const vx_dag *d, const vx_voxel *pts, uint32_t count,
   vx_dag_view view;
   VX_TRY(vx_dag_device_view(d, &view));
   query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, pts, count, out);
+  return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_dag_raycast(const vx_dag *d, const vx_ray *rays, uint32_t count,
+                         vx_ray_hit *hits, vx_stream stream) {
+  if (d == nullptr || ((rays == nullptr || hits == nullptr) && count != 0))
+    return VX_ERR_INVALID_VALUE;
+  if (count == 0) return VX_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  vx::prof::Scope sc("dag_raycast", s);
+  vx_dag_view view;
+  VX_TRY(vx_dag_device_view(d, &view));
+  raycast_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, rays, count, hits);
   return vx::from_cuda(cudaGetLastError());
 }
 
