@@ -105,3 +105,37 @@ def test_quick_autotune_writes_settings(cuda, tmp_path):
                            "edit.big_item": 16, "edit.blocks_per_sm": 32,
             "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 4,
             "edit.leafparent_lanes": 4}
+
+
+def test_small_edit_kernel_matches_oracle(cuda):
+    """The single cooperative kernel for small edits (edit.small_*) computes
+    what the multi-launch pipeline does: a primitive batch whose root list
+    takes the block-per-item expansion, and plain voxel lists, on the DAG and
+    the SVO, at every allowed residency."""
+    depth = 6
+    world = 4 << depth
+    rng = np.random.default_rng(33)
+    prims = rand_prims(rng, 300, world, world // 4)
+    vox = rng.integers(0, world, (3000, 3)).astype(np.uint32)
+    t = oracle.terrain(seed=4, scale=1, caves=True)
+    expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
+    expect.apply_voxels(vox, 1)
+    vx.set_tuning("edit.small_max_prims", 4096)
+    vx.set_tuning("edit.small_max_voxels", 16384)
+    try:
+        for blocks in vx.tuning_options("edit.small_blocks_per_sm"):
+            vx.set_tuning("edit.small_blocks_per_sm", blocks)
+            d = vx.HashDag(depth, 1 << 18, 64 << 20)
+            d.build_terrain(4, 1, True)
+            d.apply_primitives(vx.prims_to_device(prims, cuda))
+            assert d.status() == 0
+            assert d.apply_voxels(torch.from_numpy(vox.view(np.int32)).to(cuda), 1) == 0
+            assert oracle.DagCanon(*d.canonical()) == expect.dag(), blocks
+            s = vx.Svo(depth, 1 << 18, 1 << 18, arena_bytes=64 << 20)
+            s.build_terrain(4, 1, True)
+            s.apply_primitives(vx.prims_to_device(prims, cuda))
+            assert s.status() == 0
+            assert s.apply_voxels(torch.from_numpy(vox.view(np.int32)).to(cuda), 1) == 0
+            assert oracle.SvoCanon(*s.canonical()) == expect.svo(), blocks
+    finally:
+        vx.reset_tuning()

@@ -21,6 +21,8 @@
 #include "profile.cuh"
 #include "tuning.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstring>
 #include <cstdio>
@@ -299,13 +301,13 @@ __global__ void mark_pools_kernel(Tables t) {
 // MinBlocks (the knob "edit.leafparent_blocks") trades registers for
 // resident blocks: the kernel is bound by chains of dependent loads, so more
 // items in flight can outweigh a few spilled values.
-template <bool Terrain, int MinBlocks, uint32_t Lanes>
-__global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
+template <bool Terrain, uint32_t Lanes>
+__device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
   static_assert(Lanes == 4 || Lanes == 8, "4 or 8 lanes per item");
   constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
   constexpr uint32_t kGroupBits = (1u << Lanes) - 1u;
   Header *h = x.t.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const uint32_t l = x.t.depth - 1;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
@@ -313,14 +315,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
   const uint32_t world_exp = x.t.depth + 2;
   const uint32_t lane = lane_id();
   const uint64_t total = static_cast<uint64_t>(W) * Lanes;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t stride = static_cast<uint64_t>(blk.count) * blockDim.x;
   // The item's primitives, Lanes at a time: lane q of the group loads the
   // q-th (one parallel load instead of every lane walking the list).
   __shared__ vx_primitive s_pr[kBlock / Lanes][Lanes];
   const uint32_t grp = threadIdx.x / Lanes;
   const uint32_t gbase = lane & ~(Lanes - 1u);
   const uint32_t gmask = kGroupBits << gbase;
-  for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
+  for (uint64_t g0 = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
        g0 < total; g0 += stride) {
     const uint64_t g = g0 + lane;
     const bool have = g < total; // the same for the lanes of a group
@@ -411,14 +413,19 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
   }
 }
 
+template <bool Terrain, int MinBlocks, uint32_t Lanes>
+__global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
+  leafparent_body<Terrain, Lanes>(x, launch_blocks());
+}
+
 // Bottom-up rebuild of level l from its children's results.
-__global__ void __launch_bounds__(kBlock) build_kernel(Ctx x, uint32_t l) {
+__device__ __forceinline__ void build_body(Ctx x, uint32_t l, Blocks blk) {
   Header *h = x.t.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < W; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
     const Item it = x.a.items[base + i];
     const uint32_t cm = it.masks & 0xffu, km = (it.masks >> 8) & 0xffu,
                    kf = (it.masks >> 16) & 0xffu;
@@ -440,9 +447,51 @@ __global__ void __launch_bounds__(kBlock) build_kernel(Ctx x, uint32_t l) {
   }
 }
 
+__global__ void __launch_bounds__(kBlock) build_kernel(Ctx x, uint32_t l) {
+  build_body(x, l, launch_blocks());
+}
+
 __global__ void publish_kernel(Ctx x) {
   Header *h = x.t.hdr;
   if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;
+}
+
+// A whole edit in one cooperative launch, the stages separated by grid-wide
+// barriers instead of kernel boundaries: for small batches, where the ~37
+// launches of the level-synchronous pipeline (and their mostly idle grids)
+// cost more than the work.  The stages are the kernels' own bodies; long
+// primitive lists are expanded block by block with a 256-thread block and a
+// 4 KiB classification cache (lists beyond it are classified again).
+// Requires every block of the grid to be resident (cudaLaunchCooperativeKernel
+// checks it).
+constexpr uint32_t kSmallBigCache = 4096;
+
+template <uint32_t Lanes>
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  const Blocks blk = launch_blocks();
+  const DagTree tree{x.t};
+  init_body(e, kUseHeaderRoot, blk);
+  grid.sync();
+  for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
+    expand_body<DagTree, false>(e, tree, l, blk);
+    grid.sync();
+    expand_big_body<DagTree, false, kBlock, kSmallBigCache>(e, tree, l, blk);
+    grid.sync();
+  }
+  if (blk.id == 0 && threadIdx.x < kMaxDepth)
+    x.t.hdr->pool_mark[threadIdx.x] = x.t.hdr->pool_used[threadIdx.x];
+  grid.sync();
+  leafparent_body<false, Lanes>(x, blk);
+  grid.sync();
+  for (uint32_t r = x.t.depth - 1; r > 0; --r) {
+    build_body(x, r - 1, blk);
+    grid.sync();
+  }
+  if (blk.id == 0 && threadIdx.x == 0) {
+    Header *h = x.t.hdr;
+    if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;
+  }
 }
 
 __global__ void query_kernel(vx_dag_view v, const vx_voxel *pts, uint32_t n,
@@ -589,10 +638,44 @@ inline uint64_t next_pow2(uint64_t v) {
   return p;
 }
 
+// The single cooperative launch of small_edit_kernel, on as many blocks as
+// are resident at once (at most the edit.small_blocks_per_sm knob per SM).
+vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s) {
+  const bool four = tune::get(tune::kEditLeafparentLanes) == 4;
+  void *fn = four ? reinterpret_cast<void *>(&small_edit_kernel<4>)
+                  : reinterpret_cast<void *>(&small_edit_kernel<8>);
+  static int resident[2] = {-1, -1};
+  int &per_sm = resident[four ? 0 : 1];
+  if (per_sm < 0) {
+    int n = 0;
+    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kBlock, 0));
+    per_sm = n;
+  }
+  const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) *
+                        static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
+  if (per_sm < 1) return VX_ERR_INVALID_VALUE;
+  EditCtx ec = e;
+  void *args[] = {&x, &ec};
+  prof::Scope sc("dag_small_edit", s);
+  VX_TRY_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, s));
+  (void)d;
+  return VX_OK;
+}
+
+// Small edits (by the edit.small_max_* knobs) run as one cooperative kernel:
+// a batch of primitives by its count, a voxel list or leaf commands (one
+// leaf-mask primitive per touched leaf) by its length.
+inline bool small_batch(uint32_t n, bool voxel_list) {
+  return n <= static_cast<uint32_t>(tune::get(voxel_list ? tune::kEditSmallMaxVoxels
+                                                         : tune::kEditSmallMaxPrims));
+}
+
 vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
                        const uint32_t *d_count, uint32_t host_count,
                        cudaStream_t s, bool terrain = false,
-                       uint32_t blocks_per_sm = 0 /* 0: the edit.blocks_per_sm knob */) {
+                       uint32_t blocks_per_sm = 0 /* 0: the edit.blocks_per_sm knob */,
+                       int small = -1 /* -1: by host_count as a primitive batch */) {
   Ctx x{d->t, d->a, prims, d_count, host_count};
   const EditCtx e{d->t.hdr, d->a, prims, d_count, host_count, d->t.depth,
                   static_cast<uint32_t>(tune::get(tune::kEditBigItem))};
@@ -600,6 +683,8 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         (blocks_per_sm ? blocks_per_sm
                                        : static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm)));
+  if (!terrain && (small < 0 ? small_batch(host_count, false) : small != 0))
+    return run_small(d, x, e, s);
   {
     prof::Scope sc("dag_init", s);
     init_kernel<<<std::min<uint32_t>(grid, ceil_div(std::max(host_count, 1u), kBlock) + 1),
@@ -898,7 +983,7 @@ vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
   const vx_primitive *prims = nullptr;
   const uint32_t *n = nullptr;
   VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));
-  VX_TRY(run_pipeline(d, prims, n, count, s));
+  VX_TRY(run_pipeline(d, prims, n, count, s, false, 0, small_batch(count, true)));
   return read_status(d, s, true);
 }
 
@@ -916,7 +1001,7 @@ vx_status vx_dag_apply_leaf_commands(vx_dag *d, const vx_leaf_command *cmds, uin
   const uint32_t *n = nullptr;
   VX_TRY(vx::plain::prepare_leaf_commands(cmds, count, d->t.depth, op, 0, workspace, &prims, &n,
                                           s));
-  VX_TRY(run_pipeline(d, prims, n, count, s));
+  VX_TRY(run_pipeline(d, prims, n, count, s, false, 0, small_batch(count, true)));
   return read_status(d, s, true);
 }
 
@@ -964,7 +1049,7 @@ vx_status vx_dag_graph_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count, 
         const vx_primitive *prims = nullptr;
         const uint32_t *n = nullptr;
         VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));
-        return run_pipeline(d, prims, n, count, s);
+        return run_pipeline(d, prims, n, count, s, false, 0, small_batch(count, true));
       },
       out);
 }

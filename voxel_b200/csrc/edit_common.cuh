@@ -215,16 +215,31 @@ struct EditCtx {
 //   replaced(l, old, c)                   - child c of `old` is overwritten
 //       by a fully covering primitive (its subtree is dropped).
 
-static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
+// The blocks a pipeline stage runs on: its own launch (blockIdx / gridDim), or
+// the whole grid of the single cooperative kernel that runs every stage of a
+// small edit in a row.
+struct Blocks {
+  uint32_t id, count;
+};
+__device__ __forceinline__ Blocks launch_blocks() { return Blocks{blockIdx.x, gridDim.x}; }
+
+// True on every thread of the block when the edit's status is no longer ok.
+// Block-uniform, so a stage that returns on it never leaves part of a block
+// at a barrier.
+__device__ __forceinline__ bool edit_failed(const Header *h) {
+  return __syncthreads_or(ld_relaxed_u32(&h->status) != kDevOk) != 0;
+}
+
+__device__ __forceinline__ void init_body(EditCtx x, uint32_t root_old, Blocks blk) {
   Header *h = x.hdr;
   // With a device-side count, host_prim_count is the capacity of the list.
   const uint32_t dn = x.d_prim_count ? *x.d_prim_count : 0u;
   if (x.d_prim_count && dn > x.host_prim_count) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) set_status(&h->status, kDevInvalid);
+    if (blk.id == 0 && threadIdx.x == 0) set_status(&h->status, kDevInvalid);
     return;
   }
   const uint32_t n = x.d_prim_count ? dn : x.host_prim_count;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blk.id == 0 && threadIdx.x == 0) {
     for (uint32_t l = 0; l < 16; ++l) {
       h->item_off[l] = 0;
       h->item_count[l] = 0;
@@ -246,9 +261,13 @@ static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
     }
   }
   if (n > x.a.pair_cap) return;
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < n; i += static_cast<uint64_t>(blk.count) * blockDim.x)
     x.a.pairs[0][i] = static_cast<uint32_t>(i);
+}
+
+static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
+  init_body(x, root_old, launch_blocks());
 }
 
 // Top-down expansion of level l into level l + 1 (l + 1 < depth).  Eight
@@ -258,15 +277,14 @@ static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
 // partial ones after it; a second walk writes those to the child's list.
 // Output space for a block's 32 items is taken with one atomicAdd per counter.
 template <class Policy, bool Terrain>
-__global__ void __launch_bounds__(kBlock)
-    expand_kernel(EditCtx x, Policy pol, uint32_t l) {
+__device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const uint32_t depth = x.depth;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
   const uint32_t next_base = base + W;
-  if (blockIdx.x == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
+  if (blk.id == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
   const uint32_t *in_pairs = x.a.pairs[l & 1u];
   uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
   const int64_t csize = int64_t(4) << (depth - l - 1); // child cell size
@@ -279,7 +297,7 @@ __global__ void __launch_bounds__(kBlock)
   const uint32_t group = threadIdx.x >> 3, c = threadIdx.x & 7u;
   const uint32_t gshift = (lane_id() >> 3) * 8u; // this group's byte in a ballot
 
-  for (uint64_t tile = blockIdx.x; tile * kGroups < W; tile += gridDim.x) {
+  for (uint64_t tile = blk.id; tile * kGroups < W; tile += blk.count) {
     const uint32_t wi = static_cast<uint32_t>(tile * kGroups) + group;
     const bool have = wi < W;
     Item it{};
@@ -399,6 +417,12 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+template <class Policy, bool Terrain>
+__global__ void __launch_bounds__(kBlock)
+    expand_kernel(EditCtx x, Policy pol, uint32_t l) {
+  expand_body<Policy, Terrain>(x, pol, l, launch_blocks());
+}
+
 // Expansion of the long-list items of level l: one block of Threads
 // threads per item.  Three walks over the list: the last fully-covering
 // primitive per child (block max), the partial primitives after it per child
@@ -412,11 +436,10 @@ __global__ void __launch_bounds__(kBlock)
 constexpr uint32_t kBigBlock = 512;
 constexpr uint32_t kBigCache = 32768;
 
-template <class Policy, bool Terrain, uint32_t Threads = Terrain ? kBlock : kBigBlock>
-__global__ void __launch_bounds__(Threads)
-    expand_big_kernel(EditCtx x, Policy pol, uint32_t l) {
+template <class Policy, bool Terrain, uint32_t Threads, uint32_t Cache>
+__device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const uint32_t nbig = min(h->big_count[l], x.a.big_cap);
   const uint32_t depth = x.depth;
   const uint32_t base = h->item_off[l];
@@ -432,14 +455,14 @@ __global__ void __launch_bounds__(Threads)
   __shared__ uint32_t s_warp[8][kWarps], s_total[8];
   __shared__ uint32_t s_item_base, s_pair_base;
   __shared__ bool s_room;
-  __shared__ uint8_t s_mixed[kBigCache];
+  __shared__ uint8_t s_mixed[Cache];
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
 
-  for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
+  for (uint32_t b = blk.id; b < nbig; b += blk.count) {
     const uint32_t wi = x.a.big[b];
     const Item it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
-    const bool cached = it.pcount <= kBigCache; // block-uniform
+    const bool cached = it.pcount <= Cache; // block-uniform
     if (t < 8) {
       s_last[t] = -1;
       s_cnt[t] = 0;
@@ -591,6 +614,12 @@ __global__ void __launch_bounds__(Threads)
     }
     __syncthreads();
   }
+}
+
+template <class Policy, bool Terrain, uint32_t Threads = Terrain ? kBlock : kBigBlock>
+__global__ void __launch_bounds__(Threads)
+    expand_big_kernel(EditCtx x, Policy pol, uint32_t l) {
+  expand_big_body<Policy, Terrain, Threads, kBigCache>(x, pol, l, launch_blocks());
 }
 
 } // namespace vx::edit

@@ -21,6 +21,8 @@
 // reclaimed by a reachability pass that rebuilds the free lists.  Before any
 // write the edit checks that the worst-case allocation fits; if not it
 // reports VX_ERR_CAPACITY and changes nothing.
+#include <cooperative_groups.h>
+
 #include "edit_common.cuh"
 #include "voxel_b200_device.cuh"
 #include "plain.cuh"
@@ -144,7 +146,7 @@ __device__ uint32_t finish_node(const Tables &t, uint32_t old, const uint32_t (&
   return kChild | idx | (old & kFilled);
 }
 
-__global__ void begin_kernel(Tables t) {
+__device__ __forceinline__ void begin_body(Tables t) {
   Counters *c = t.ctr;
   c->base_node_count = c->node_count;
   c->base_leaf_count = c->leaf_count;
@@ -153,10 +155,11 @@ __global__ void begin_kernel(Tables t) {
   c->taken_nodes = 0;
   c->taken_leaves = 0;
 }
+__global__ void begin_kernel(Tables t) { begin_body(t); }
 
 // Worst case before any write: every item below the root may need a node and
 // every leaf child of the last level a leaf.
-__global__ void check_capacity_kernel(Tables t) {
+__device__ __forceinline__ void check_capacity_body(Tables t) {
   Header *h = t.hdr;
   if (h->status != kDevOk) return;
   uint64_t nodes = 0;
@@ -167,11 +170,12 @@ __global__ void check_capacity_kernel(Tables t) {
   const uint64_t avail_leaves = c->base_free_leaves + uint64_t(t.max_leaves - c->base_leaf_count);
   if (nodes > avail_nodes || leaves > avail_leaves) h->status = kDevCapacity;
 }
+__global__ void check_capacity_kernel(Tables t) { check_capacity_body(t); }
 
 template <bool Terrain>
-__global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t) {
+__device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk) {
   Header *h = x.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const SvoTree pol{t};
   const uint32_t l = t.depth - 1;
   const uint32_t W = h->item_count[l];
@@ -181,8 +185,8 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t)
   const bool mats = t.materials != 0;
   const uint32_t lane = lane_id();
   const uint64_t total = static_cast<uint64_t>(W) * 8u;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t g0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
+  const uint64_t stride = static_cast<uint64_t>(blk.count) * blockDim.x;
+  for (uint64_t g0 = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
        g0 < total; g0 += stride) {
     const uint64_t g = g0 + lane;
     const bool have = g < total;
@@ -284,13 +288,18 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t)
   }
 }
 
-__global__ void __launch_bounds__(kBlock) build_kernel(EditCtx x, Tables t, uint32_t l) {
+template <bool Terrain>
+__global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t) {
+  leafparent_body<Terrain>(x, t, launch_blocks());
+}
+
+__device__ __forceinline__ void build_body(EditCtx x, Tables t, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
-  if (ld_relaxed_u32(&h->status) != kDevOk) return;
+  if (edit_failed(h)) return;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < W; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
     const Item it = x.a.items[base + i];
     const uint32_t cm = it.masks & 0xffu;
     uint32_t child[8];
@@ -311,7 +320,11 @@ __global__ void __launch_bounds__(kBlock) build_kernel(EditCtx x, Tables t, uint
   }
 }
 
-__global__ void finalize_kernel(Tables t) {
+__global__ void __launch_bounds__(kBlock) build_kernel(EditCtx x, Tables t, uint32_t l) {
+  build_body(x, t, l, launch_blocks());
+}
+
+__device__ __forceinline__ void finalize_body(Tables t) {
   Counters *c = t.ctr;
   if (t.hdr->status != kDevOk) return;
   const uint32_t tn = c->taken_nodes, tl = c->taken_leaves;
@@ -328,33 +341,35 @@ __global__ void finalize_kernel(Tables t) {
     c->leaf_count = c->base_leaf_count + (tl - c->base_free_leaves);
   }
 }
+__global__ void finalize_kernel(Tables t) { finalize_body(t); }
 
 // ------------------------------------------------------------------- GC --
 
-__global__ void gc_clear_kernel(Tables t) {
+__device__ __forceinline__ void gc_clear_body(Tables t, Blocks blk) {
   Counters *c = t.ctr;
   if (!c->detached) return;
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < c->node_count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < c->node_count; i += static_cast<uint64_t>(blk.count) * blockDim.x)
     t.node_mark[i] = 0;
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < c->leaf_count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+       i < c->leaf_count; i += static_cast<uint64_t>(blk.count) * blockDim.x)
     t.leaf_mark[i] = 0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blk.id == 0 && threadIdx.x == 0) {
     for (uint32_t l = 0; l <= kMaxDepth; ++l) c->gc_count[l] = 0;
     c->gc_count[0] = 1;
     t.front[0][0] = 0; // the root
   }
 }
+__global__ void gc_clear_kernel(Tables t) { gc_clear_body(t, launch_blocks()); }
 
-__global__ void gc_level_kernel(Tables t, uint32_t l) {
+__device__ __forceinline__ void gc_level_body(Tables t, uint32_t l, Blocks blk) {
   Counters *c = t.ctr;
   if (!c->detached) return;
   const uint32_t n = c->gc_count[l];
   const uint32_t *front = t.front[l & 1u];
   uint32_t *next = t.front[(l + 1) & 1u];
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x) {
     const uint32_t node = front[i];
     t.node_mark[node] = 1;
     for (uint32_t k = 0; k < 8; ++k) {
@@ -365,27 +380,75 @@ __global__ void gc_level_kernel(Tables t, uint32_t l) {
     }
   }
 }
+__global__ void gc_level_kernel(Tables t, uint32_t l) { gc_level_body(t, l, launch_blocks()); }
 
-__global__ void gc_zero_free_kernel(Tables t) {
+__device__ __forceinline__ void gc_zero_free_body(Tables t) {
   Counters *c = t.ctr;
   if (!c->detached) return;
   c->free_node_count = 0;
   c->free_leaf_count = 0;
 }
+__global__ void gc_zero_free_kernel(Tables t) { gc_zero_free_body(t); }
 
-__global__ void gc_rebuild_kernel(Tables t) {
+__device__ __forceinline__ void gc_rebuild_body(Tables t, Blocks blk) {
   Counters *c = t.ctr;
   if (!c->detached) return;
   const uint32_t nn = c->node_count, nl = c->leaf_count;
-  for (uint64_t i = 1 + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nn;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+  for (uint64_t i = 1 + blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nn;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x)
     if (!t.node_mark[i]) t.free_nodes[atomicAdd(&c->free_node_count, 1u)] = static_cast<uint32_t>(i);
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nl;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nl;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x)
     if (!t.leaf_mark[i]) t.free_leaves[atomicAdd(&c->free_leaf_count, 1u)] = static_cast<uint32_t>(i);
 }
+__global__ void gc_rebuild_kernel(Tables t) { gc_rebuild_body(t, launch_blocks()); }
 
 __global__ void gc_end_kernel(Tables t) { t.ctr->detached = 0; }
+
+// A whole edit, collection included, in one cooperative launch: the stages
+// of run_pipeline separated by grid-wide barriers instead of kernel
+// boundaries, for small batches, where ~30 launches cost more than the work
+// (the plain per-call path).  Long primitive lists are expanded with a
+// 256-thread block and a 4 KiB classification cache.  Requires every block of
+// the grid to be resident (cudaLaunchCooperativeKernel checks it).
+constexpr uint32_t kSmallBigCache = 4096;
+
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  const Blocks blk = launch_blocks();
+  const SvoTree pol{t};
+  const bool lead = blk.id == 0 && threadIdx.x == 0;
+  if (lead) begin_body(t);
+  init_body(e, kChild, blk);
+  grid.sync();
+  for (uint32_t l = 0; l + 1 < t.depth; ++l) {
+    expand_body<SvoTree, false>(e, pol, l, blk);
+    grid.sync();
+    expand_big_body<SvoTree, false, kBlock, kSmallBigCache>(e, pol, l, blk);
+    grid.sync();
+  }
+  if (lead) check_capacity_body(t);
+  grid.sync();
+  leafparent_body<false>(e, t, blk);
+  grid.sync();
+  for (uint32_t r = t.depth - 1; r > 0; --r) {
+    build_body(e, t, r - 1, blk);
+    grid.sync();
+  }
+  if (lead) finalize_body(t);
+  grid.sync();
+  gc_clear_body(t, blk);
+  grid.sync();
+  for (uint32_t l = 0; l < t.depth; ++l) {
+    gc_level_body(t, l, blk);
+    grid.sync();
+  }
+  if (lead) gc_zero_free_body(t);
+  grid.sync();
+  gc_rebuild_body(t, blk);
+  grid.sync();
+  if (lead) t.ctr->detached = 0;
+}
 
 __global__ void reset_kernel(Tables t) {
 #pragma unroll
@@ -419,8 +482,40 @@ struct vx_svo {
 
 namespace vx::svo {
 
+// The single cooperative launch of small_edit_kernel, on as many blocks as
+// are resident at once (at most the edit.small_blocks_per_sm knob per SM).
+vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s) {
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    int n = 0;
+    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, reinterpret_cast<const void *>(&small_edit_kernel), kBlock, 0));
+    per_sm = n;
+  }
+  if (per_sm < 1) return VX_ERR_INVALID_VALUE;
+  const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
+  const uint32_t grid = static_cast<uint32_t>(sm_count()) *
+                        static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
+  EditCtx ec = e;
+  Tables tc = t;
+  void *args[] = {&ec, &tc};
+  prof::Scope sc("svo_small_edit", s);
+  VX_TRY_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(&small_edit_kernel),
+                                          dim3(grid), dim3(kBlock), args, 0, s));
+  return VX_OK;
+}
+
+// Small edits (by the edit.small_max_* knobs) run as one cooperative kernel:
+// a batch of primitives by its count, a voxel list or leaf commands by its
+// length.
+inline bool small_batch(uint32_t n, bool voxel_list) {
+  return n <= static_cast<uint32_t>(tune::get(voxel_list ? tune::kEditSmallMaxVoxels
+                                                         : tune::kEditSmallMaxPrims));
+}
+
 vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_count,
-                       uint32_t host_count, cudaStream_t s, bool terrain) {
+                       uint32_t host_count, cudaStream_t s, bool terrain,
+                       int small = -1 /* -1: by host_count as a primitive batch */) {
   const Tables &t = v->t;
   const EditCtx e{t.hdr, v->a, prims, d_count, host_count, t.depth,
                   static_cast<uint32_t>(tune::get(tune::kEditBigItem))};
@@ -428,6 +523,8 @@ vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_c
   const uint32_t depth = t.depth;
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(tune::get(tune::kEditBlocksPerSm));
+  if (!terrain && (small < 0 ? small_batch(host_count, false) : small != 0))
+    return run_small(e, t, s);
   {
     prof::Scope sc("svo_init", s);
     begin_kernel<<<1, 1, 0, s>>>(t);
@@ -600,7 +697,7 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
   const uint32_t *n = nullptr;
   const uint32_t mat = op == VX_EDIT_PLACE ? (material ? material : 1u) : 0u;
   VX_TRY(vx::plain::prepare(edits, count, v->t.depth, op, mat, workspace, &prims, &n, s));
-  VX_TRY(run_pipeline(v, prims, n, count, s, false));
+  VX_TRY(run_pipeline(v, prims, n, count, s, false, small_batch(count, true)));
   return read_status(v, s);
 }
 
@@ -618,7 +715,7 @@ vx_status vx_svo_apply_leaf_commands(vx_svo *v, const vx_leaf_command *cmds, uin
   const uint32_t mat = op == VX_EDIT_PLACE ? (material ? material : 1u) : 0u;
   VX_TRY(vx::plain::prepare_leaf_commands(cmds, count, v->t.depth, op, mat, workspace, &prims,
                                           &n, s));
-  VX_TRY(run_pipeline(v, prims, n, count, s, false));
+  VX_TRY(run_pipeline(v, prims, n, count, s, false, small_batch(count, true)));
   return read_status(v, s);
 }
 

@@ -17,6 +17,9 @@ enum Id : uint32_t {
   kEditLeafparentBlocks, // resident blocks the DAG leaf-parent kernel is built for
   kServeBlocksPerSm, // grid of the serving loop's edit graphs, in blocks per SM
   kEditLeafparentLanes, // threads per item in the DAG leaf-parent kernel: 4 or 8
+  kEditSmallMaxPrims, // batches of at most this many primitives run as one cooperative kernel
+  kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
+  kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
   kKnobCount
 };
 
