@@ -731,7 +731,7 @@ def run_serve(args, ws, rank, local, torch, vx, device):
     dag = vx.HashDag(SERVE_DEPTH, SERVE_MAX_NODES, SERVE_ARENA)
     dag.build_terrain(8, 32, True)
     assert dag.status() == 0
-    srv = vx.Server(dag, max_batch_prims=1 << 16, compact_at_fill=0.5)
+    srv = vx.Server(dag, max_batch_prims=1 << 16, compact_at_fill=0.9)
     t0 = srv.now_ns() + 200_000_000  # first arrival 0.2 s from now
 
     def submitter():
@@ -1268,11 +1268,44 @@ def run_case_dag_full(args, torch, vx, dev):
                       "kernel_ms_per_batch": kern, "tuning": vx.tuning()}))
 
 
+def run_case_hash(args, torch, vx, dev):
+    """--case slab|cuckoo --elements N: N u64 keys inserted at load factor
+    0.8, then N lookups at 50 % hits, --steps times; device time per insert
+    and per lookup launch (for profiling the hash tables alone)."""
+    n = args.elements
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    keys = torch.randint(-2**63, 2**63 - 2, (n,), dtype=torch.int64, device=dev, generator=g)
+    fresh = torch.randint(-2**63, 2**63 - 2, (n // 2,), dtype=torch.int64, device=dev, generator=g)
+    q = torch.cat([keys[torch.randperm(n, device=dev, generator=g)[:n // 2]], fresh])
+    q = q[torch.randperm(n, device=dev, generator=g)].contiguous()
+    out = torch.empty(n, dtype=torch.int32, device=dev)
+    if args.case == "slab":
+        t = vx.SlabHashSet(int(n / (HASH_LOAD * 15)) + 1, n // 30)
+        ins, look = (lambda: t.insert(keys)), (lambda: t.contains(q, out))
+    else:
+        t = vx.CuckooMap(int(n / HASH_LOAD) + 1, 2000)
+        ins, look = (lambda: t.insert(keys)), (lambda: t.find(q, out))
+    res = {"insert_ms": [], "lookup_ms": []}
+    for _ in range(args.steps):
+        t.clear()
+        for name, fn in (("insert_ms", ins), ("lookup_ms", look)):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            res[name].append(round(a.elapsed_time(b), 3))
+    print(json.dumps({"case": args.case, "elements": n, **res}))
+
+
 def run_case(args):
     """One operation alone, for profiler captures: --case scan|sort_u32|sort_u64
     --elements N (runs --steps launches); --case dag --elements E (E spheres
     on a 4096^3 terrain); --case dag_full (the headline C4 batch, --steps
-    batches, device time per batch and per kernel)."""
+    batches, device time per batch and per kernel); --case slab|cuckoo
+    --elements N (insert and look up N u64 keys)."""
     import torch
     import voxel_b200 as vx
     dev = torch.device("cuda:0")
@@ -1280,6 +1313,8 @@ def run_case(args):
     ms = []
     if args.case == "dag_full":
         return run_case_dag_full(args, torch, vx, dev)
+    if args.case in ("slab", "cuckoo"):
+        return run_case_hash(args, torch, vx, dev)
     for _ in range(args.steps):
         if args.case == "scan":
             x = torch.randint(0, 256, (n,), dtype=torch.int32, device=dev)
@@ -1328,7 +1363,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64", "dag", "dag_full"],
+    ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64", "dag", "dag_full",
+                                       "slab", "cuckoo"],
                     default=None)
     ap.add_argument("--elements", type=int, default=1 << 24)
     ap.add_argument("--serve-seconds", type=float, default=SERVE_SECONDS,

@@ -679,8 +679,12 @@ vx_status vx_dag_apply_terminal(vx_dag *dag, const vx_terminal_node *nodes,
  * A request loop over a resident Hash DAG with continuous batching: submitted
  * requests (lists of primitives) are applied in submission order; queued
  * requests are coalesced into one batched edit per launch, up to two launches
- * are in flight, and the DAG is compacted when a table passes
- * compact_at_fill (admission by memory headroom).  Completions report the
+ * are in flight.  Admission is by the memory a request needs: each request's
+ * new nodes per level are estimated from its primitives' surfaces, and a
+ * request joins a batch only while the tables' use plus the estimates of the
+ * batches in flight and of the batch stay within compact_at_fill of every
+ * table's room; when not even the next request fits, the DAG is compacted
+ * first.  Completions report the
  * commit time (host clock of vx_serve_now_ns, when the batch's completion was
  * observed) and the root the batch published.  The server owns the DAG's
  * stream while it runs.  No counterpart in the reference (no serving path). */
@@ -689,7 +693,8 @@ typedef struct vx_server vx_server;
 typedef struct vx_serve_config {
     uint32_t max_batch_prims;    /* primitives per launch (0 = 65536) */
     uint32_t max_batch_requests; /* requests per launch (0 = unlimited, 1 = one each) */
-    double compact_at_fill;      /* compact above this table fill (0 = 0.5) */
+    double compact_at_fill;      /* fill limit of admission (0 = 0.9; above 1 never compacts
+                                    before a batch overflows) */
     uint32_t max_inflight;       /* launches in flight, 1 or 2 (0 = 2) */
     uint32_t launch_mode;        /* 0 = one CUDA graph launch per batch,
                                     1 = the pipeline's kernels one by one */

@@ -105,3 +105,20 @@ def test_graph_and_direct_launches_agree(cuda):
     b = fresh_dag()
     run(b, arr, sizes, prims, graphs=False)
     assert canon(a) == canon(b)
+
+
+def test_admission_by_need_compacts_before_the_tables_fill(cuda):
+    """A small DAG (32 Ki nodes per table) under a stream that creates far
+    more nodes than that: admission by each request's estimated need compacts
+    before a batch can overflow, so no batch fails and is recovered, and the
+    final state is still sequential application."""
+    arr, sizes, prims = stream(n_seconds=0.3, seed=29)
+    dag = vx.HashDag(DEPTH, max_nodes=1 << 15, arena_bytes=64 << 20)
+    dag.build_terrain(5, 1, True)
+    assert dag.status() == 0
+    done, stats = run(dag, arr, sizes, prims)
+    assert (done["status"] == 0).all()
+    assert stats.compactions > 0
+    assert stats.recoveries == 0
+    t = oracle.terrain(5, 1, True)
+    assert canon(dag) == oracle.Grid(DEPTH).terrain(t).apply_prims(prims).dag()

@@ -2067,6 +2067,27 @@ size_t header_bytes() { return sizeof(vx::edit::Header); }
 uint32_t header_root(const void *hh) { return static_cast<const vx::edit::Header *>(hh)->root; }
 uint32_t header_status(const void *hh) { return static_cast<const vx::edit::Header *>(hh)->status; }
 
+TableRoom table_room(const vx_dag *d, const void *hh) {
+  const auto *h = static_cast<const vx::edit::Header *>(hh);
+  TableRoom r{};
+  r.depth = d->t.depth;
+  for (uint32_t l = 0; l < d->t.depth; ++l) {
+    r.node_cap[l] = d->index_slots[l] / 2;
+    r.word_cap[l] = d->t.pool_cap[l];
+    r.nodes[l] = h->node_count[l];
+    r.words[l] = h->pool_used[l];
+  }
+  r.node_cap[d->t.depth] = d->leaf_slots / 2;
+  r.nodes[d->t.depth] = h->node_count[d->t.depth];
+  return r;
+}
+
+vx_status read_header(const vx_dag *d, void *host, cudaStream_t s) {
+  VX_TRY_CUDA(cudaMemcpyAsync(host, d->t.hdr, sizeof(vx::edit::Header), cudaMemcpyDeviceToHost, s));
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  return VX_OK;
+}
+
 double fill_fraction(const vx_dag *d, const void *hh) {
   const auto *h = static_cast<const vx::edit::Header *>(hh);
   double f = 0.0;

@@ -15,21 +15,28 @@
 // order, so the DAG always equals sequential application of the committed
 // requests in arrival order.
 //
-// Admission by memory headroom: edits are copy-on-write, so superseded nodes
-// accumulate; before a batch is launched the worker checks the fill of every
-// node table (from the header copy of the last completed batch) and, above
-// compact_at_fill, waits for the in-flight batches and compacts the DAG.  A
-// batch that still runs out of room (status VX_ERR_CAPACITY) is recovered:
-// the in-flight batches are drained, their requests requeued in order, the
-// DAG compacted and the batch size halved until it fits (a single request
-// that cannot fit is reported with its status).
+// Admission by the memory a request needs: edits are copy-on-write, so every
+// batch adds nodes to the tables (superseded ones stay until a compaction).
+// Each request carries an estimate, per level, of the nodes its primitives
+// can create there (the cells their surfaces cross, see estimate_need), and a
+// request joins a batch only while the tables' use (exact, from the header of
+// the last completed batch) plus the estimates of the batches in flight, of
+// the batch so far and of the request stay within compact_at_fill of every
+// table's room (index, pool, leaf set).  When not even the first queued
+// request fits, the worker waits for the in-flight batches and compacts the
+// DAG.  A batch that still runs out of room (status VX_ERR_CAPACITY) is
+// recovered: the in-flight batches are drained, their requests requeued in
+// order, the DAG compacted and the batch size halved until it fits (a single
+// request that cannot fit is reported with its status).
 #include "common.cuh"
 #include "dag_internal.cuh"
 #include "profile.cuh"
 #include "tuning.cuh"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -46,10 +53,49 @@ uint64_t now_ns() {
                                    .count());
 }
 
+// Estimated new nodes per level (index depth = leaves).
+using Need = std::array<double, 16>;
+
+// Upper estimate of the nodes the primitives can create at each level: a
+// level-l node is rebuilt only where a primitive cuts its cell partially, and
+// those cells lie in the shell of thickness side * sqrt(3) around a sphere's
+// surface, or in a box's bounding cells minus its interior ones; each level
+// is also capped by the primitive's bounding cells and the level's cell
+// count.
+Need estimate_need(const vx_primitive *p, size_t n, uint32_t depth) {
+  Need need{};
+  for (size_t i = 0; i < n; ++i) {
+    const uint32_t shape = vx_prim_shape(&p[i]);
+    double ext[3];
+    for (int a = 0; a < 3; ++a)
+      ext[a] = shape == VX_SHAPE_AABB ? double(p[i].r[a])
+                                      : 2.0 * double(shape == VX_SHAPE_SPHERE ? p[i].r[0] : p[i].r[a]) + 1.0;
+    for (uint32_t l = 1; l <= depth; ++l) {
+      const double side = double(4u << (depth - std::min(l, depth)));
+      double bbox = 1.0, inner = 1.0;
+      for (int a = 0; a < 3; ++a) {
+        bbox *= ext[a] / side + 2.0;
+        inner *= std::max(0.0, ext[a] / side - 2.0);
+      }
+      double cells = bbox - inner;
+      if (shape == VX_SHAPE_SPHERE) {
+        const double r = p[i].r[0], w = side * 1.7320508075688772;
+        const double shell = 4.18879020478639 * (std::pow(r + w, 3) - std::pow(std::max(0.0, r - w), 3)) /
+                             (side * side * side);
+        cells = std::min(bbox, shell);
+      }
+      need[l] += std::min(cells, std::ldexp(1.0, static_cast<int>(std::min(3 * l, 60u))));
+    }
+  }
+  need[0] = 1.0;
+  return need;
+}
+
 struct Request {
   uint64_t id;
   uint64_t arrival_ns;
   std::vector<vx_primitive> prims;
+  Need need{};
 };
 
 struct Batch {
@@ -57,6 +103,7 @@ struct Batch {
   uint32_t nprims = 0;
   int slot = -1;
   cudaEvent_t done = nullptr;
+  Need need{};
 };
 
 } // namespace
@@ -81,6 +128,7 @@ struct vx_server {
   bool slot_busy[2] = {false, false};
   std::vector<unsigned char> last_hdr; // header copy of the last completed batch
   bool have_hdr = false;
+  uint32_t depth = 0;
 
   std::mutex mu;
   std::condition_variable cv;
@@ -89,6 +137,7 @@ struct vx_server {
   std::vector<vx_serve_completion> done;
   bool stop = false;
   bool recovering = false;
+  bool compacted_for_head = false; // the head request got its compaction
   uint32_t batch_cap = 0; // current primitive cap (halved on failures)
   uint32_t hard_cap = 0;  // capacity of the upload buffers
   bool worker_done = false;
@@ -100,17 +149,42 @@ struct vx_server {
 
 namespace {
 
-// Compact the DAG on the server stream (worker thread; nothing in flight).
+// Compact the DAG on the server stream (worker or completion thread; nothing
+// in flight), then take a fresh copy of its header for admission.
 vx_status compact(vx_server *s) {
   const uint64_t t0 = now_ns();
   vx_status st = vx_dag_status(s->dag, s->stream); // clears a sticky error
   (void)st;
   st = vx_dag_compact(s->dag, s->stream);
+  std::vector<unsigned char> hdr(vx::dag::header_bytes());
+  const vx_status hs = vx::dag::read_header(s->dag, hdr.data(), s->stream);
   std::lock_guard<std::mutex> lock(s->mu);
   s->stats.compactions += 1;
   s->stats.compact_ms += (now_ns() - t0) * 1e-6;
-  s->have_hdr = false;
+  s->have_hdr = hs == VX_OK;
+  if (s->have_hdr) s->last_hdr.swap(hdr);
   return st;
+}
+
+// Whether a batch of estimated need `add` fits in the tables' room on top of
+// their use in the last header and the batches in flight (caller holds mu).
+bool fits(const vx_server *s, const Need &add) {
+  if (!s->have_hdr) return true;
+  const vx::dag::TableRoom r = vx::dag::table_room(s->dag, s->last_hdr.data());
+  const double f = s->cfg.compact_at_fill;
+  for (uint32_t l = 0; l <= r.depth; ++l) {
+    double inflight = 0.0;
+    for (const Batch &b : s->inflight) inflight += b.need[l];
+    const double level_cells = std::ldexp(1.0, static_cast<int>(std::min(3 * l, 60u)));
+    const double add_l = std::min(add[l] + inflight, level_cells * (1.0 + s->inflight.size()));
+    if (double(r.nodes[l]) + add_l > f * double(r.node_cap[l])) return false;
+    if (r.word_cap[l] != 0) {
+      // words per new item: the level's average so far, plus one
+      const double wpi = (r.nodes[l] ? double(r.words[l]) / double(r.nodes[l]) : 9.0) + 1.0;
+      if (double(r.words[l]) + add_l * wpi > f * double(r.word_cap[l])) return false;
+    }
+  }
+  return true;
 }
 
 void worker_loop(vx_server *s) {
@@ -130,22 +204,31 @@ void worker_loop(vx_server *s) {
         s->worker_done = true;
         break;
       }
-      if (s->have_hdr && vx::dag::fill_fraction(s->dag, s->last_hdr.data()) > s->cfg.compact_at_fill) {
-        // Headroom is low: wait for the in-flight batches, then compact.
+      if (!fits(s, s->queue.front().need) && !s->compacted_for_head) {
+        // Not even the next request fits: wait for the in-flight batches,
+        // then compact (once per head request; if it still does not fit it
+        // runs alone and the overflow recovery takes over).
         s->cv.wait(lock, [&] { return s->inflight.empty(); });
         need_compact = true;
+        s->compacted_for_head = true;
       } else {
-        // Coalesce queued requests in arrival order.
+        // Coalesce queued requests in arrival order while they fit.
         while (!s->queue.empty()) {
           Request &r = s->queue.front();
           const uint32_t n = static_cast<uint32_t>(r.prims.size());
-          if (!b.reqs.empty() && (b.nprims + n > s->batch_cap ||
-                                  b.reqs.size() >= s->cfg.max_batch_requests))
-            break;
+          if (!b.reqs.empty()) {
+            if (b.nprims + n > s->batch_cap || b.reqs.size() >= s->cfg.max_batch_requests)
+              break;
+            Need sum = b.need;
+            for (uint32_t l = 0; l < 16; ++l) sum[l] += r.need[l];
+            if (!fits(s, sum)) break;
+          }
           b.nprims += n;
+          for (uint32_t l = 0; l < 16; ++l) b.need[l] += r.need[l];
           b.reqs.push_back(std::move(r));
           s->queue.pop_front();
         }
+        s->compacted_for_head = false;
         b.slot = s->slot_busy[0] ? 1 : 0;
         s->slot_busy[b.slot] = true;
       }
@@ -296,7 +379,7 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
   if (cfg) s->cfg = *cfg;
   if (s->cfg.max_batch_prims == 0) s->cfg.max_batch_prims = 1u << 16;
   if (s->cfg.max_batch_requests == 0) s->cfg.max_batch_requests = 0xffffffffu;
-  if (s->cfg.compact_at_fill <= 0.0) s->cfg.compact_at_fill = 0.5;
+  if (s->cfg.compact_at_fill <= 0.0) s->cfg.compact_at_fill = 0.9;
   if (s->cfg.max_inflight == 0 || s->cfg.max_inflight > 2) s->cfg.max_inflight = 2;
   // the upload buffers also hold a single request larger than the batch cap
   s->hard_cap = std::max<uint32_t>(s->cfg.max_batch_prims, 1u << 16);
@@ -317,6 +400,15 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
     vx_serve_destroy(s);
     return vx::from_cuda(e);
   }
+  // the tables' current use, for admission
+  s->last_hdr.resize(vx::dag::header_bytes());
+  const vx_status hs = vx::dag::read_header(dag, s->last_hdr.data(), s->stream);
+  if (hs != VX_OK) {
+    vx_serve_destroy(s);
+    return hs;
+  }
+  s->have_hdr = true;
+  s->depth = vx::dag::table_room(dag, s->last_hdr.data()).depth;
   if (s->cfg.launch_mode == 0) {
     for (int k = 0; k < 2; ++k) {
       const vx_status st = vx::dag::graph_primitives_grid(
@@ -341,6 +433,7 @@ vx_status vx_serve_submit(vx_server *s, uint64_t request_id, const vx_primitive 
   r.id = request_id;
   r.arrival_ns = arrival_ns;
   r.prims.assign(host_prims, host_prims + count);
+  r.need = estimate_need(host_prims, count, s->depth);
   {
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stop) return VX_ERR_INVALID_VALUE;
