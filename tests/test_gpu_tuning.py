@@ -76,7 +76,7 @@ def test_edit_settings_match_oracle(cuda):
     t = oracle.terrain(seed=4, scale=1, caves=True)
     expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
     for big, bps, lpb, lanes in [(16, 2, 4, 4), (64, 8, 5, 8), (512, 16, 6, 4), (32, 32, 4, 8),
-                                 (32, 32, 5, 4)]:
+                                 (32, 32, 5, 4), (16, 32, 4, 2), (32, 16, 5, 2), (16, 8, 6, 2)]:
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)

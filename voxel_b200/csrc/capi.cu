@@ -182,7 +182,7 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
     {"edit.leafparent_blocks", 5, {4, 5, 6}, 3},
     {"serve.blocks_per_sm", 4, {2, 4, 8, 16, 32}, 5},
-    {"edit.leafparent_lanes", 4, {4, 8}, 2},
+    {"edit.leafparent_lanes", 4, {2, 4, 8}, 3},
     {"edit.small_max_prims", 256, {0, 64, 256, 1024, 4096}, 5},
     {"edit.small_blocks_per_sm", 2, {1, 2, 4}, 3},
     {"edit.small_max_voxels", 16384, {0, 4096, 16384, 65536}, 4},

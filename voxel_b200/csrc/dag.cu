@@ -303,7 +303,7 @@ __global__ void mark_pools_kernel(Tables t) {
 // items in flight can outweigh a few spilled values.
 template <bool Terrain, uint32_t Lanes>
 __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
-  static_assert(Lanes == 4 || Lanes == 8, "4 or 8 lanes per item");
+  static_assert(Lanes == 2 || Lanes == 4 || Lanes == 8, "2, 4 or 8 lanes per item");
   constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
   constexpr uint32_t kGroupBits = (1u << Lanes) - 1u;
   Header *h = x.t.hdr;
@@ -640,17 +640,31 @@ inline uint64_t next_pow2(uint64_t v) {
 
 // The single cooperative launch of small_edit_kernel, on as many blocks as
 // are resident at once (at most the edit.small_blocks_per_sm knob per SM).
-vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s) {
-  const bool four = tune::get(tune::kEditLeafparentLanes) == 4;
-  void *fn = four ? reinterpret_cast<void *>(&small_edit_kernel<4>)
-                  : reinterpret_cast<void *>(&small_edit_kernel<8>);
-  static int resident[2] = {-1, -1};
-  int &per_sm = resident[four ? 0 : 1];
-  if (per_sm < 0) {
+// Resident blocks per SM of small_edit_kernel<2 / 4 / 8 lanes>, queried once
+// (at DAG creation, so never first inside a stream capture).
+void *small_kernel(int64_t lanes) {
+  return lanes == 2   ? reinterpret_cast<void *>(&small_edit_kernel<2>)
+         : lanes == 4 ? reinterpret_cast<void *>(&small_edit_kernel<4>)
+                      : reinterpret_cast<void *>(&small_edit_kernel<8>);
+}
+int g_small_resident[3] = {-1, -1, -1};
+vx_status query_small_residency() {
+  const int64_t lanes[3] = {2, 4, 8};
+  for (int i = 0; i < 3; ++i) {
+    if (g_small_resident[i] >= 0) continue;
     int n = 0;
-    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kBlock, 0));
-    per_sm = n;
+    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, small_kernel(lanes[i]),
+                                                              kBlock, 0));
+    g_small_resident[i] = n;
   }
+  return VX_OK;
+}
+
+vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s) {
+  const int64_t lanes = tune::get(tune::kEditLeafparentLanes);
+  void *fn = small_kernel(lanes);
+  VX_TRY(query_small_residency());
+  const int per_sm = g_small_resident[lanes == 2 ? 0 : (lanes == 4 ? 1 : 2)];
   const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
@@ -718,9 +732,16 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   {
     prof::Scope sc("dag_leafparent", s);
     const int64_t lb = tune::get(tune::kEditLeafparentBlocks);
-    const bool four = tune::get(tune::kEditLeafparentLanes) == 4;
+    const int64_t lanes = tune::get(tune::kEditLeafparentLanes);
+    const bool four = lanes == 4;
     if (terrain)
       leafparent_kernel<true, 4, 8><<<grid, kBlock, 0, s>>>(x);
+    else if (lanes == 2 && lb == 6)
+      leafparent_kernel<false, 6, 2><<<grid, kBlock, 0, s>>>(x);
+    else if (lanes == 2 && lb == 5)
+      leafparent_kernel<false, 5, 2><<<grid, kBlock, 0, s>>>(x);
+    else if (lanes == 2)
+      leafparent_kernel<false, 4, 2><<<grid, kBlock, 0, s>>>(x);
     else if (four && lb == 6)
       leafparent_kernel<false, 6, 4><<<grid, kBlock, 0, s>>>(x);
     else if (four && lb == 5)
@@ -916,6 +937,10 @@ vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
   if ((e = cudaMalloc(&d->t.hdr, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&d->tmp_prim, sizeof(vx_primitive))) != cudaSuccess) return fail(e);
   d->bytes += d->leaf_slots * 8;
+  if (vx_status qs = vx::dag::query_small_residency(); qs != VX_OK) {
+    vx_dag_destroy(d);
+    return qs;
+  }
   const uint64_t arena = cfg->arena_bytes ? cfg->arena_bytes : (512ull << 20);
   if ((e = cudaMalloc(&d->arena_mem, arena)) != cudaSuccess) return fail(e);
   d->bytes += arena;

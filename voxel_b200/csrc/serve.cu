@@ -7,7 +7,8 @@
 // from pinned host memory and launches the batched edit on the server's
 // stream (one CUDA graph per upload slot, captured at creation, which reads
 // the batch size from device memory, so a batch is two copies and one
-// launch; the copies run on a second stream and overlap the previous edit); up to max_inflight batches are in flight, so requests that arrive
+// launch; batches within the small-edit threshold replay a second graph that
+// holds the edit as one cooperative kernel); the copies run on a second stream and overlap the previous edit); up to max_inflight batches are in flight, so requests that arrive
 // while the GPU works on one batch are admitted into the next as soon as a
 // slot frees, and their upload overlaps the running edit.  A completion
 // thread waits for each batch's event, stamps every request of the batch with
@@ -120,6 +121,10 @@ struct vx_server {
   uint32_t *h_count = nullptr; // pinned, one word per slot
   uint32_t *d_count = nullptr; // one word per slot
   vx_graph *graph[2] = {nullptr, nullptr};
+  // per slot: the same edit for batches of at most small_cap primitives,
+  // captured as the single cooperative kernel of small edits
+  vx_graph *graph_small[2] = {nullptr, nullptr};
+  uint32_t small_cap = 0;
   // uploads run on their own stream, so a batch's copy overlaps the edit
   // of the batch before it; the edit waits on the slot's upload event
   cudaStream_t copy_stream = nullptr;
@@ -269,7 +274,9 @@ void worker_loop(vx_server *s) {
                     cudaMemcpyHostToDevice, s->copy_stream);
     cudaEventRecord(s->uploaded[b.slot], s->copy_stream);
     cudaStreamWaitEvent(s->stream, s->uploaded[b.slot], 0);
-    if (s->graph[b.slot] != nullptr) {
+    if (s->graph_small[b.slot] != nullptr && b.nprims <= s->small_cap) {
+      vx_graph_launch(s->graph_small[b.slot], s->stream);
+    } else if (s->graph[b.slot] != nullptr) {
       vx_graph_launch(s->graph[b.slot], s->stream);
     } else if (b.nprims) {
       vx_dag_apply_primitives(s->dag, s->d_buf[b.slot], b.nprims, s->stream);
@@ -410,10 +417,15 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
   s->have_hdr = true;
   s->depth = vx::dag::table_room(dag, s->last_hdr.data()).depth;
   if (s->cfg.launch_mode == 0) {
+    s->small_cap = std::min<uint32_t>(
+        s->hard_cap, static_cast<uint32_t>(vx::tune::get(vx::tune::kEditSmallMaxPrims)));
     for (int k = 0; k < 2; ++k) {
-      const vx_status st = vx::dag::graph_primitives_grid(
+      vx_status st = vx::dag::graph_primitives_grid(
           dag, s->d_buf[k], s->d_count + k, s->hard_cap,
           static_cast<uint32_t>(vx::tune::get(vx::tune::kServeBlocksPerSm)), &s->graph[k]);
+      if (st == VX_OK && s->small_cap > 0)
+        st = vx::dag::graph_primitives_grid(dag, s->d_buf[k], s->d_count + k, s->small_cap, 0,
+                                            &s->graph_small[k]);
       if (st != VX_OK) {
         vx_serve_destroy(s);
         return st;
@@ -488,6 +500,7 @@ vx_status vx_serve_destroy(vx_server *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (int k = 0; k < 2; ++k) {
     if (s->graph[k]) vx_graph_destroy(s->graph[k]);
+    if (s->graph_small[k]) vx_graph_destroy(s->graph_small[k]);
     if (s->h_buf[k]) cudaFreeHost(s->h_buf[k]);
     if (s->d_buf[k]) cudaFree(s->d_buf[k]);
     if (s->h_hdr[k]) cudaFreeHost(s->h_hdr[k]);

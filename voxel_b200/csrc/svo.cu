@@ -484,14 +484,21 @@ namespace vx::svo {
 
 // The single cooperative launch of small_edit_kernel, on as many blocks as
 // are resident at once (at most the edit.small_blocks_per_sm knob per SM).
+// Resident blocks per SM of small_edit_kernel, queried once (at SVO
+// creation, so never first inside a stream capture).
+int g_small_resident = -1;
+vx_status query_small_residency() {
+  if (g_small_resident >= 0) return VX_OK;
+  int n = 0;
+  VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &n, reinterpret_cast<const void *>(&small_edit_kernel), kBlock, 0));
+  g_small_resident = n;
+  return VX_OK;
+}
+
 vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s) {
-  static int per_sm = -1;
-  if (per_sm < 0) {
-    int n = 0;
-    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &n, reinterpret_cast<const void *>(&small_edit_kernel), kBlock, 0));
-    per_sm = n;
-  }
+  VX_TRY(query_small_residency());
+  const int per_sm = g_small_resident;
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
@@ -613,6 +620,10 @@ vx_status vx_svo_create(const vx_svo_config *cfg, vx_svo **out) {
     return vx::from_cuda(e);
   };
   cudaError_t e;
+  if (vx_status qs = vx::svo::query_small_residency(); qs != VX_OK) {
+    vx_svo_destroy(v);
+    return qs;
+  }
   const size_t nn = cfg->max_nodes, nl = cfg->max_leaves;
   if ((e = cudaMalloc(&t.nodes, nn * 32)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&t.leaves, nl * 8)) != cudaSuccess) return fail(e);

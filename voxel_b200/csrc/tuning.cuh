@@ -16,7 +16,7 @@ enum Id : uint32_t {
   kEditBlocksPerSm, // grid of the edit pipelines' item kernels, in blocks per SM
   kEditLeafparentBlocks, // resident blocks the DAG leaf-parent kernel is built for
   kServeBlocksPerSm, // grid of the serving loop's edit graphs, in blocks per SM
-  kEditLeafparentLanes, // threads per item in the DAG leaf-parent kernel: 4 or 8
+  kEditLeafparentLanes, // threads per item in the DAG leaf-parent kernel: 2, 4 or 8
   kEditSmallMaxPrims, // batches of at most this many primitives run as one cooperative kernel
   kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
   kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
