@@ -466,11 +466,22 @@ __global__ void publish_kernel(Ctx x) {
 // checks it).
 constexpr uint32_t kSmallBigCache = 4096;
 
-template <uint32_t Lanes>
-__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e) {
+// With Plain, the edit's input is a voxel list (one op): the first stages
+// turn it into leaf-mask primitives (PlainPrep) in place of the sort-based
+// preparation of the multi-launch path.
+template <uint32_t Lanes, bool Plain>
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, PlainPrep prep) {
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const Blocks blk = launch_blocks();
   const DagTree tree{x.t};
+  if (Plain) {
+    plain_prep_clear(prep, blk);
+    grid.sync();
+    plain_prep_aggregate(prep, x.t.depth, blk);
+    grid.sync();
+    plain_prep_emit(prep, blk);
+    grid.sync();
+  }
   init_body(e, kUseHeaderRoot, blk);
   grid.sync();
   for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
@@ -640,37 +651,49 @@ inline uint64_t next_pow2(uint64_t v) {
 
 // The single cooperative launch of small_edit_kernel, on as many blocks as
 // are resident at once (at most the edit.small_blocks_per_sm knob per SM).
-// Resident blocks per SM of small_edit_kernel<2 / 4 / 8 lanes>, queried once
-// (at DAG creation, so never first inside a stream capture).
-void *small_kernel(int64_t lanes) {
-  return lanes == 2   ? reinterpret_cast<void *>(&small_edit_kernel<2>)
-         : lanes == 4 ? reinterpret_cast<void *>(&small_edit_kernel<4>)
-                      : reinterpret_cast<void *>(&small_edit_kernel<8>);
+// Resident blocks per SM of small_edit_kernel<2 / 4 / 8 lanes, plain or
+// not>, queried once (at DAG creation, so never first inside a stream
+// capture).
+void *small_kernel(int64_t lanes, bool plain) {
+  if (plain)
+    return lanes == 2   ? reinterpret_cast<void *>(&small_edit_kernel<2, true>)
+           : lanes == 4 ? reinterpret_cast<void *>(&small_edit_kernel<4, true>)
+                        : reinterpret_cast<void *>(&small_edit_kernel<8, true>);
+  return lanes == 2   ? reinterpret_cast<void *>(&small_edit_kernel<2, false>)
+         : lanes == 4 ? reinterpret_cast<void *>(&small_edit_kernel<4, false>)
+                      : reinterpret_cast<void *>(&small_edit_kernel<8, false>);
 }
-int g_small_resident[3] = {-1, -1, -1};
+int g_small_resident[6] = {-1, -1, -1, -1, -1, -1};
+inline int small_slot(int64_t lanes, bool plain) {
+  return (lanes == 2 ? 0 : (lanes == 4 ? 1 : 2)) + (plain ? 3 : 0);
+}
 vx_status query_small_residency() {
   const int64_t lanes[3] = {2, 4, 8};
-  for (int i = 0; i < 3; ++i) {
-    if (g_small_resident[i] >= 0) continue;
-    int n = 0;
-    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, small_kernel(lanes[i]),
-                                                              kBlock, 0));
-    g_small_resident[i] = n;
-  }
+  for (int plain = 0; plain < 2; ++plain)
+    for (int i = 0; i < 3; ++i) {
+      int &slot = g_small_resident[small_slot(lanes[i], plain != 0)];
+      if (slot >= 0) continue;
+      int n = 0;
+      VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, small_kernel(lanes[i], plain != 0), kBlock, 0));
+      slot = n;
+    }
   return VX_OK;
 }
 
-vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s) {
+vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s,
+                    const PlainPrep *prep = nullptr) {
   const int64_t lanes = tune::get(tune::kEditLeafparentLanes);
-  void *fn = small_kernel(lanes);
+  void *fn = small_kernel(lanes, prep != nullptr);
   VX_TRY(query_small_residency());
-  const int per_sm = g_small_resident[lanes == 2 ? 0 : (lanes == 4 ? 1 : 2)];
+  const int per_sm = g_small_resident[small_slot(lanes, prep != nullptr)];
   const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   EditCtx ec = e;
-  void *args[] = {&x, &ec};
+  PlainPrep pp = prep ? *prep : PlainPrep{};
+  void *args[] = {&x, &ec, &pp};
   prof::Scope sc("dag_small_edit", s);
   VX_TRY_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, s));
   (void)d;
@@ -1005,6 +1028,16 @@ vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
   if (workspace == nullptr || workspace_bytes < vx_dag_voxel_workspace_size(count))
     return VX_ERR_INVALID_VALUE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PlainPrep prep;
+  if (small_batch(count, true) &&
+      plain_prep_layout(workspace, workspace_bytes, edits, count, op, 0, &prep)) {
+    // one cooperative launch: voxels -> leaf masks -> the edit
+    Ctx x{d->t, d->a, prep.prims, prep.nprims, count};
+    const EditCtx e{d->t.hdr, d->a, prep.prims, prep.nprims, count, d->t.depth,
+                    static_cast<uint32_t>(vx::tune::get(vx::tune::kEditBigItem))};
+    VX_TRY(run_small(d, x, e, s, &prep));
+    return read_status(d, s, true);
+  }
   const vx_primitive *prims = nullptr;
   const uint32_t *n = nullptr;
   VX_TRY(vx::plain::prepare(edits, count, d->t.depth, op, 0, workspace, &prims, &n, s));

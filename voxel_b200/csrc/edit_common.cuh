@@ -14,6 +14,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "voxel_b200_device.cuh"
 
 namespace vx::edit {
 
@@ -268,6 +269,91 @@ __device__ __forceinline__ void init_body(EditCtx x, uint32_t root_old, Blocks b
 
 static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
   init_body(x, root_old, launch_blocks());
+}
+
+// ------------------------------------------- plain voxel lists, small edits --
+//
+// Inside the single cooperative kernel of a small edit, a voxel list (one op
+// for every voxel) becomes its leaf-mask primitives without a sort: voxels
+// are aggregated into a hash table of {leaf key + 1, mask} slots (atomicCAS
+// claims a slot, atomicOr sets the voxel's bit), then every used slot is
+// appended to the primitive list.  One op for all voxels makes the order of
+// the primitives irrelevant.  Stages: clear, aggregate, emit, each followed
+// by a grid-wide barrier.
+struct PlainPrep {
+  const vx_voxel *edits;
+  uint32_t count;       // voxels
+  uint32_t op, material;
+  ulonglong2 *slots;    // {packed leaf coordinates + 1 (0 = free), mask}
+  uint32_t nslots;
+  vx_primitive *prims;  // out: one leaf-mask primitive per touched leaf
+  uint32_t *nprims;     // out: their number (the edit's device-side count)
+};
+
+// The prep's table and primitive list carved from a plain-path workspace;
+// false when they do not fit it.
+inline bool plain_prep_layout(void *ws, size_t ws_bytes, const vx_voxel *edits, uint32_t count,
+                              uint32_t op, uint32_t material, PlainPrep *out) {
+  Carver c(ws);
+  PlainPrep p{};
+  p.edits = edits;
+  p.count = count;
+  p.op = op;
+  p.material = material;
+  p.nslots = count + count / 2u + 1u; // distinct leaves <= count: load <= 2/3
+  p.slots = c.take<ulonglong2>(p.nslots);
+  p.prims = c.take<vx_primitive>(count);
+  p.nprims = c.take<uint32_t>(1);
+  if (c.offset > ws_bytes) return false;
+  *out = p;
+  return true;
+}
+
+__device__ __forceinline__ void plain_prep_clear(const PlainPrep &p, Blocks blk) {
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < p.nslots;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x)
+    p.slots[i] = make_ulonglong2(0ull, 0ull);
+  if (blk.id == 0 && threadIdx.x == 0) *p.nprims = 0;
+}
+
+__device__ __forceinline__ void plain_prep_aggregate(const PlainPrep &p, uint32_t depth,
+                                                     Blocks blk) {
+  const uint32_t side_exp = depth + 2;
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < p.count;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x) {
+    const vx_voxel v = p.edits[i];
+    if ((v.x >> side_exp) | (v.y >> side_exp) | (v.z >> side_exp)) continue; // outside: ignored
+    const uint64_t key = (static_cast<uint64_t>(v.x >> 2) | (static_cast<uint64_t>(v.y >> 2) << 21) |
+                          (static_cast<uint64_t>(v.z >> 2) << 42)) + 1ull;
+    const uint64_t bit = 1ull << ((v.x & 3u) + 4u * (v.y & 3u) + 16u * (v.z & 3u));
+    uint32_t pos = vx_reduce_hash(vx_mix64(key), p.nslots);
+    for (uint32_t probe = 0; probe < p.nslots; ++probe) {
+      const unsigned long long old =
+          atomicCAS(reinterpret_cast<unsigned long long *>(&p.slots[pos].x), 0ull, key);
+      if (old == 0ull || old == key) {
+        atomicOr(reinterpret_cast<unsigned long long *>(&p.slots[pos].y), bit);
+        break;
+      }
+      pos = pos + 1u == p.nslots ? 0u : pos + 1u;
+    }
+  }
+}
+
+__device__ __forceinline__ void plain_prep_emit(const PlainPrep &p, Blocks blk) {
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < p.nslots;
+       i += static_cast<uint64_t>(blk.count) * blockDim.x) {
+    const ulonglong2 e = p.slots[i];
+    if (e.x == 0ull) continue;
+    const uint64_t k = e.x - 1ull;
+    vx_primitive pr{};
+    pr.c[0] = static_cast<int32_t>((k & 0x1fffffull) * 4u);
+    pr.c[1] = static_cast<int32_t>(((k >> 21) & 0x1fffffull) * 4u);
+    pr.c[2] = static_cast<int32_t>(((k >> 42) & 0x1fffffull) * 4u);
+    pr.r[0] = static_cast<uint32_t>(e.y);
+    pr.r[1] = static_cast<uint32_t>(e.y >> 32);
+    pr.flags = vx_make_flags(kShapeLeafMask, p.op, p.material);
+    p.prims[atomicAdd(p.nprims, 1u)] = pr;
+  }
 }
 
 // Top-down expansion of level l into level l + 1 (l + 1 < depth).  Eight

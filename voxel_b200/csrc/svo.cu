@@ -413,11 +413,23 @@ __global__ void gc_end_kernel(Tables t) { t.ctr->detached = 0; }
 // the grid to be resident (cudaLaunchCooperativeKernel checks it).
 constexpr uint32_t kSmallBigCache = 4096;
 
-__global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t) {
+// With Plain, the edit's input is a voxel list (one op and material): the
+// first stages turn it into leaf-mask primitives (PlainPrep) in place of the
+// sort-based preparation of the multi-launch path.
+template <bool Plain>
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t, PlainPrep prep) {
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const Blocks blk = launch_blocks();
   const SvoTree pol{t};
   const bool lead = blk.id == 0 && threadIdx.x == 0;
+  if (Plain) {
+    plain_prep_clear(prep, blk);
+    grid.sync();
+    plain_prep_aggregate(prep, t.depth, blk);
+    grid.sync();
+    plain_prep_emit(prep, blk);
+    grid.sync();
+  }
   if (lead) begin_body(t);
   init_body(e, kChild, blk);
   grid.sync();
@@ -484,31 +496,39 @@ namespace vx::svo {
 
 // The single cooperative launch of small_edit_kernel, on as many blocks as
 // are resident at once (at most the edit.small_blocks_per_sm knob per SM).
-// Resident blocks per SM of small_edit_kernel, queried once (at SVO
-// creation, so never first inside a stream capture).
-int g_small_resident = -1;
+// Resident blocks per SM of small_edit_kernel<plain or not>, queried once
+// (at SVO creation, so never first inside a stream capture).
+int g_small_resident[2] = {-1, -1};
+inline const void *small_kernel(bool plain) {
+  return plain ? reinterpret_cast<const void *>(&small_edit_kernel<true>)
+               : reinterpret_cast<const void *>(&small_edit_kernel<false>);
+}
 vx_status query_small_residency() {
-  if (g_small_resident >= 0) return VX_OK;
-  int n = 0;
-  VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &n, reinterpret_cast<const void *>(&small_edit_kernel), kBlock, 0));
-  g_small_resident = n;
+  for (int plain = 0; plain < 2; ++plain) {
+    if (g_small_resident[plain] >= 0) continue;
+    int n = 0;
+    VX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, small_kernel(plain != 0),
+                                                              kBlock, 0));
+    g_small_resident[plain] = n;
+  }
   return VX_OK;
 }
 
-vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s) {
+vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s,
+                    const PlainPrep *prep = nullptr) {
   VX_TRY(query_small_residency());
-  const int per_sm = g_small_resident;
+  const int per_sm = g_small_resident[prep ? 1 : 0];
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   const int want = static_cast<int>(tune::get(tune::kEditSmallBlocksPerSm));
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   EditCtx ec = e;
   Tables tc = t;
-  void *args[] = {&ec, &tc};
+  PlainPrep pp = prep ? *prep : PlainPrep{};
+  void *args[] = {&ec, &tc, &pp};
   prof::Scope sc("svo_small_edit", s);
-  VX_TRY_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(&small_edit_kernel),
-                                          dim3(grid), dim3(kBlock), args, 0, s));
+  VX_TRY_CUDA(cudaLaunchCooperativeKernel(small_kernel(prep != nullptr), dim3(grid),
+                                          dim3(kBlock), args, 0, s));
   return VX_OK;
 }
 
@@ -707,6 +727,15 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
   const vx_primitive *prims = nullptr;
   const uint32_t *n = nullptr;
   const uint32_t mat = op == VX_EDIT_PLACE ? (material ? material : 1u) : 0u;
+  PlainPrep prep;
+  if (small_batch(count, true) &&
+      plain_prep_layout(workspace, workspace_bytes, edits, count, op, mat, &prep)) {
+    // one cooperative launch: voxels -> leaf masks -> the edit and collection
+    const EditCtx e{v->t.hdr, v->a, prep.prims, prep.nprims, count, v->t.depth,
+                    static_cast<uint32_t>(vx::tune::get(vx::tune::kEditBigItem))};
+    VX_TRY(run_small(e, v->t, s, &prep));
+    return read_status(v, s);
+  }
   VX_TRY(vx::plain::prepare(edits, count, v->t.depth, op, mat, workspace, &prims, &n, s));
   VX_TRY(run_pipeline(v, prims, n, count, s, false, small_batch(count, true)));
   return read_status(v, s);
