@@ -41,13 +41,11 @@ __device__ __forceinline__ uint32_t vx_reduce_hash(uint64_t h, uint32_t n) {
   return (uint32_t)__umul64hi(h, (uint64_t)n);
 }
 
-/* Slot of key under cuckoo hash function hid (0..3) in a table of n slots. */
-__device__ __forceinline__ uint32_t vx_cuckoo_slot(uint64_t key, uint32_t hid, uint32_t n) {
-  const uint64_t salt = hid == 0 ? 0x9e3779b97f4a7c15ull
-                      : hid == 1 ? 0xc2b2ae3d27d4eb4full
-                      : hid == 2 ? 0x165667b19e3779f9ull
-                                 : 0x27d4eb2f165667c5ull;
-  return vx_reduce_hash(vx_mix64(key ^ salt), n);
+/* Bucket of key under choice c (0 or 1) in a cuckoo table of `buckets`
+ * buckets of two 16-byte slots (one 32-byte sector each). */
+__device__ __forceinline__ uint32_t vx_cuckoo_bucket(uint64_t key, uint32_t c, uint32_t buckets) {
+  const uint64_t salt = c == 0 ? 0x9e3779b97f4a7c15ull : 0xc2b2ae3d27d4eb4full;
+  return vx_reduce_hash(vx_mix64(key ^ salt), buckets);
 }
 
 __device__ __forceinline__ uint64_t vx_ld_relaxed_u64(const uint64_t *p) {
@@ -237,24 +235,28 @@ __device__ __forceinline__ uint8_t vx_svo_get_voxel(const vx_svo_view &v, uint32
 
 /* ---------------------------------------------------------- hash tables -- */
 
-/* Cuckoo find: true and *value if key is present. */
+/* Cuckoo find: true and *value if key is present.  Both candidate buckets
+ * (two 32-byte sectors) are loaded at once. */
 __device__ __forceinline__ bool vx_cuckoo_find(const vx_cuckoo_view &v, uint64_t key,
                                                uint32_t *value) {
   if (key == VX_HASH_EMPTY_KEY || key == VX_HASH_DELETED_KEY) return false;
   const ulonglong2 *slots = (const ulonglong2 *)v.slots;
+  const uint32_t nb = v.slot_count / 2u;
+  const ulonglong2 *b[2] = {slots + 2ull * vx_cuckoo_bucket(key, 0, nb),
+                            slots + 2ull * vx_cuckoo_bucket(key, 1, nb)};
+  ulonglong2 e[4];
 #pragma unroll
-  for (uint32_t h = 0; h < 4; ++h) {
-    const uint32_t s = vx_cuckoo_slot(key, h, v.slot_count);
-    ulonglong2 e;
+  for (uint32_t i = 0; i < 4; ++i)
     asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
-                 : "=l"(e.x), "=l"(e.y)
-                 : "l"(slots + s)
+                 : "=l"(e[i].x), "=l"(e[i].y)
+                 : "l"(b[i >> 1] + (i & 1u))
                  : "memory");
-    if (e.x == key) {
-      *value = (uint32_t)e.y;
+#pragma unroll
+  for (uint32_t i = 0; i < 4; ++i)
+    if (e[i].x == key) {
+      *value = (uint32_t)e[i].y;
       return true;
     }
-  }
   return false;
 }
 

@@ -127,11 +127,11 @@ def _mix64(x: int) -> int:
     return x
 
 
-_CUCKOO_SALTS = (0x9e3779b97f4a7c15, 0xc2b2ae3d27d4eb4f, 0x165667b19e3779f9, 0x27d4eb2f165667c5)
+_CUCKOO_SALTS = (0x9e3779b97f4a7c15, 0xc2b2ae3d27d4eb4f)
 
 
-def _cuckoo_slot(key: int, hid: int, n: int) -> int:
-    return (_mix64(key ^ _CUCKOO_SALTS[hid]) * n) >> 64
+def _cuckoo_bucket(key: int, choice: int, buckets: int) -> int:
+    return (_mix64(key ^ _CUCKOO_SALTS[choice]) * buckets) >> 64
 
 
 def _raw_slots(m) -> np.ndarray:
@@ -147,9 +147,9 @@ def _raw_slots(m) -> np.ndarray:
 
 
 def test_cuckoo_replace_keeps_hash_id_through_later_evictions(cuda):
-    """A replaced entry keeps the hash id that placed it, so the evictions that
-    later move it continue from the right hash function: every stored entry
-    sits at the slot its recorded hash id names, and nothing is dropped."""
+    """A replaced entry keeps the choice bits that placed it, so the evictions
+    that later move it go to its other bucket: every stored entry sits in the
+    bucket (two slots) its recorded choice names, and nothing is dropped."""
     n_slots = 4096
     rng = np.random.default_rng(77)
     keys = unique_keys(rng, 3200)               # final load 0.78
@@ -171,4 +171,4 @@ def test_cuckoo_replace_keeps_hash_id_through_later_evictions(cuda):
     empty = np.uint64(0xFFFFFFFFFFFFFFFF)
     for pos in np.nonzero(raw[:, 0] != empty)[0]:
         key, word = int(raw[pos, 0]), int(raw[pos, 1])
-        assert _cuckoo_slot(key, word >> 32, n_slots) == pos
+        assert _cuckoo_bucket(key, word >> 32, n_slots // 2) == pos // 2

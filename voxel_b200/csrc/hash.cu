@@ -3,26 +3,31 @@
 // Slab hash set: the u64 widening of the reference's BasicSlabHashSetU32
 // (cuda/hash_table/slab_hash/set/host.cuh:13-121, device.cuh:31-315).  A slab
 // is one 128-byte line: 15 u64 key slots and a u64 link to the next slab of
-// the bucket's chain.  Sixteen lanes read a slab with one coalesced request,
-// so each warp works on two keys at once (one per half-warp), where the
-// reference's u32 slab needs the whole warp per key.  Inserts CAS an empty or
-// deleted slot; full chains grow from a pool of overflow slabs taken with a
-// bump counter.  Statuses are the reference's kSlabHashStatus* values.  Every
-// retry loop is bounded (the reference's kSlabHashMaxContentionRetries).
+// the bucket's chain.  Where the reference's warp serves one key at a time,
+// here every thread walks its own key: a slab is read one 32-byte sector at a
+// time starting at the key's home sector, and the walk ends at the first
+// empty slot (inserts take the first free slot in that order), so most
+// lookups read one sector and a warp has 32 keys in flight.  Inserts CAS an
+// empty or deleted slot; full chains grow from a pool of overflow slabs taken
+// with a bump counter.  Statuses are the reference's kSlabHashStatus*
+// values.  Every retry loop is bounded (the reference's
+// kSlabHashMaxContentionRetries).
 //
 // Slab map: u32 -> u32, the reference's SlabHashMapU32 (below).
 //
 // Cuckoo map: the u64-keyed widening of cuckoo_insert / cuckoo_find
-// (cuda/cuckoo_hash.cuh:54-120).  Four hash functions address one array of
-// 16-byte slots {key, value | hash id << 32}; an eviction moves a whole slot
-// with one 128-bit atomic exchange (atom.exch.b128, sm_90+), so key and value
-// never separate.  Eviction chains are bounded by max_evictions (the
-// reference's insertion_attempts); a chain that runs out drops the key in
-// hand, reports VX_HASH_OVERFLOW and counts it.
+// (cuda/cuckoo_hash.cuh:54-120), bucketed: two hash functions each name a
+// bucket of two 16-byte slots {key, value | choice << 32} (one 32-byte
+// sector), so a lookup is two independent sector loads; an eviction moves a
+// whole slot with one 128-bit atomic exchange (atom.exch.b128, sm_90+), so
+// key and value never separate.  Eviction chains are bounded by
+// max_evictions (the reference's insertion_attempts); a chain that runs out
+// drops the key in hand, reports VX_HASH_OVERFLOW and counts it.
 #include "common.cuh"
 #include "profile.cuh"
 #include "voxel_b200_device.cuh"
 
+#include <algorithm>
 #include <new>
 
 namespace vx::hash {
@@ -87,124 +92,139 @@ __global__ void slab_init_kernel(SetView t, uint64_t words) {
 
 enum class SetOp { Insert, Contains, Erase };
 
-// One key per half-warp at a time.  All 32 lanes call this; each half-warp
-// drains its own queue of active lanes.
+// Probe order of a key inside every slab of its chain: its home sector (32
+// bytes: 4 key slots; the last sector has 3 and the link) first, then the
+// next ones cyclically.  An insert takes the first free slot (empty or
+// deleted) in that order, so a key present in the chain always lies before
+// the first empty slot of its order: a lookup reads one sector at a time and
+// stops at the first empty slot, which for most keys is in the home sector.
+__device__ __forceinline__ uint32_t home_sector(uint64_t h) { return static_cast<uint32_t>(h) & 3u; }
+
+__device__ __forceinline__ ulonglong2 ld_relaxed_u64x2(const uint64_t *p) {
+  ulonglong2 v;
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+               : "=l"(v.x), "=l"(v.y)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+
+// Sector j of a slab: words 4j .. 4j + 3 (two 16-byte relaxed loads, one
+// 32-byte sector).
+__device__ __forceinline__ void ld_sector(const Slab *slab, uint32_t j, uint64_t w[4]) {
+  const ulonglong2 a = ld_relaxed_u64x2(&slab->w[4 * j]);
+  const ulonglong2 b = ld_relaxed_u64x2(&slab->w[4 * j + 2]);
+  w[0] = a.x;
+  w[1] = a.y;
+  w[2] = b.x;
+  w[3] = b.y;
+}
+
+// One key per thread: every lane walks its own key's chain (no warp
+// cooperation), so a warp has 32 keys in flight.
 template <SetOp Op>
 __global__ void __launch_bounds__(kBlock)
     slab_set_kernel(SetView t, const uint64_t *__restrict__ keys,
                     uint32_t count, uint32_t *contains, uint32_t *statuses) {
-  const uint32_t lane = lane_id();
-  const uint32_t sub = lane & 15u;
-  const uint32_t half = lane >> 4;
-  const uint32_t hmask = half ? 0xffff0000u : 0x0000ffffu;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  // Every lane of a warp iterates the same number of rounds.
-  const uint64_t warp_first = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) - lane;
-  for (uint64_t base = warp_first; base < count; base += stride) {
-    const uint64_t idx = base + lane;
-    bool active = idx < count;
-    uint64_t key = active ? keys[idx] : 0;
-    uint32_t status = VX_HASH_NOT_FOUND, found = 0;
-    if (active && (key == kEmpty || key == kDeleted)) {
-      status = VX_HASH_INVALID_KEY;
-      active = false;
-    }
-    uint32_t queue = __ballot_sync(hmask, active) & hmask;
-    while (queue) {
-      const uint32_t src = __ffs(queue) - 1u;
-      const uint64_t k = __shfl_sync(hmask, key, src);
-      Slab *slab = &t.slabs[reduce(mix64(k), t.bucket_count)];
-      uint32_t result = VX_HASH_OVERFLOW;
-      const uint64_t max_steps =
-          Op == SetOp::Contains
-              ? t.capacity + 1ull
-              : (t.capacity + 1ull) * static_cast<uint64_t>(kMaxContentionRetries);
-      for (uint64_t step = 0; step < max_steps; ++step) {
-        const uint64_t w = ld_relaxed_u64(&slab->w[sub]);
-        const bool key_slot = sub < kSlotsPerSlab;
-        const uint32_t hit = __ballot_sync(hmask, key_slot && w == k) & hmask;
-        if (hit) {
-          if (Op == SetOp::Erase) {
-            const uint32_t dst = __ffs(hit) - 1u;
-            unsigned long long old = 0;
-            if (lane == dst)
-              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]),
-                              k, kDeleted);
-            old = __shfl_sync(hmask, old, dst);
-            if (old != k) continue; // lost a race: re-read this slab
-            result = VX_HASH_ERASED;
-          } else {
-            result = Op == SetOp::Insert ? VX_HASH_ALREADY_PRESENT : VX_HASH_FOUND;
+  for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < count;
+       idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t k = keys[idx];
+    uint32_t result;
+    if (k == kEmpty || k == kDeleted) {
+      result = VX_HASH_INVALID_KEY;
+    } else {
+      const uint64_t h = mix64(k);
+      const uint32_t home = home_sector(h);
+      Slab *const first = &t.slabs[reduce(h, t.bucket_count)];
+      result = VX_HASH_OVERFLOW;
+      // a chain is at most the pool long; a lost CAS restarts the walk
+      const uint64_t max_steps = (t.capacity + 1ull) * 4ull;
+      uint32_t restarts = 0;
+      bool restart = true;
+      while (restart && restarts++ < kMaxContentionRetries) {
+        restart = false;
+        Slab *slab = first;
+        uint64_t *free_slot = nullptr; // first free slot of the walk (insert)
+        uint64_t free_old = 0;
+        bool done = false;
+        for (uint64_t step = 0; step < max_steps && !done;) {
+          uint64_t link = kNullLink;
+          bool ended = false; // met an empty slot: the key is not further on
+          for (uint32_t q = 0; q < 4 && !done && !ended; ++q, ++step) {
+            const uint32_t j = (home + q) & 3u;
+            uint64_t w[4];
+            ld_sector(slab, j, w);
+            const uint32_t slots = j == 3 ? 3u : 4u;
+            if (j == 3) link = w[3];
+            for (uint32_t i = 0; i < slots; ++i) {
+              if (w[i] == k) {
+                if (Op == SetOp::Erase) {
+                  const unsigned long long old = atomicCAS(
+                      reinterpret_cast<unsigned long long *>(&slab->w[4 * j + i]), k, kDeleted);
+                  if (old == k) result = VX_HASH_ERASED;
+                  else restart = true; // changed meanwhile: walk again
+                } else {
+                  result = Op == SetOp::Insert ? VX_HASH_ALREADY_PRESENT : VX_HASH_FOUND;
+                }
+                done = true;
+                break;
+              }
+              if (Op == SetOp::Insert && free_slot == nullptr && (w[i] == kEmpty || w[i] == kDeleted)) {
+                free_slot = &slab->w[4 * j + i];
+                free_old = w[i];
+              }
+              if (w[i] == kEmpty) {
+                ended = true;
+                break;
+              }
+            }
           }
-          break;
-        }
-        if (Op == SetOp::Insert) {
-          const uint32_t free_mask =
-              __ballot_sync(hmask, key_slot && (w == kEmpty || w == kDeleted)) & hmask;
-          if (free_mask) {
-            const uint32_t dst = __ffs(free_mask) - 1u;
-            const uint64_t expect = __shfl_sync(hmask, w, dst);
-            unsigned long long old = 0;
-            if (lane == dst)
-              old = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[sub]),
-                              expect, k);
-            old = __shfl_sync(hmask, old, dst);
-            if (old == expect) {
-              result = VX_HASH_INSERTED;
+          if (done) break;
+          if (ended || link == kNullLink) {
+            if (Op != SetOp::Insert) {
+              result = VX_HASH_NOT_FOUND;
+              done = true;
               break;
             }
-            continue; // slot taken meanwhile: re-read this slab
-          }
-        }
-        const uint64_t link = __shfl_sync(hmask, w, (half << 4) + 15u);
-        if (link != kNullLink) {
-          slab = &t.slabs[link];
-          continue;
-        }
-        if (Op != SetOp::Insert) {
-          result = VX_HASH_NOT_FOUND;
-          break;
-        }
-        // Grow the chain: take a pool slab, initialise it, link it with CAS.
-        uint32_t ord = 0;
-        if (sub == 0) ord = atomicAdd(t.alloc, 1u);
-        ord = __shfl_sync(hmask, ord, half << 4);
-        if (ord >= t.capacity) {
-          // Pool exhausted; another half-warp may have linked a slab since.
-          uint64_t again = 0;
-          if (sub == 15u) again = ld_relaxed_u64(&slab->w[15]);
-          again = __shfl_sync(hmask, again, (half << 4) + 15u);
-          if (again != kNullLink) {
-            slab = &t.slabs[again];
+            if (free_slot != nullptr) {
+              const unsigned long long old = atomicCAS(
+                  reinterpret_cast<unsigned long long *>(free_slot), free_old, k);
+              if (old == free_old) result = VX_HASH_INSERTED;
+              else restart = true;
+              done = true;
+              break;
+            }
+            // Full chain: take a pool slab, initialise it, link it with CAS.
+            const uint32_t ord = atomicAdd(t.alloc, 1u);
+            if (ord >= t.capacity) {
+              // pool exhausted; another thread may have linked a slab since
+              const uint64_t again = ld_relaxed_u64(&slab->w[15]);
+              if (again != kNullLink) {
+                slab = &t.slabs[again];
+                continue;
+              }
+              result = VX_HASH_OVERFLOW;
+              done = true;
+              break;
+            }
+            Slab *fresh = &t.slabs[t.bucket_count + ord];
+            for (uint32_t i = 0; i < 15; ++i) fresh->w[i] = kEmpty;
+            fresh->w[15] = kNullLink;
+            __threadfence();
+            const unsigned long long observed = atomicCAS(
+                reinterpret_cast<unsigned long long *>(&slab->w[15]), kNullLink,
+                t.bucket_count + ord);
+            // either our slab was linked or another thread's was: follow it
+            // (a pool slab that lost the race stays unused)
+            slab = &t.slabs[observed == kNullLink ? t.bucket_count + ord : observed];
             continue;
           }
-          result = VX_HASH_OVERFLOW;
-          break;
+          slab = &t.slabs[link];
         }
-        Slab *fresh = &t.slabs[t.bucket_count + ord];
-        fresh->w[sub] = sub == 15u ? kNullLink : kEmpty;
-        __threadfence();
-        __syncwarp(hmask);
-        unsigned long long observed = 0;
-        if (sub == 15u)
-          observed = atomicCAS(reinterpret_cast<unsigned long long *>(&slab->w[15]),
-                               kNullLink, t.bucket_count + ord);
-        observed = __shfl_sync(hmask, observed, (half << 4) + 15u);
-        // Either our slab was linked or another warp's was; follow the link.
-        // (A pool slab that lost the race stays unused.)
-        slab = &t.slabs[observed == kNullLink ? t.bucket_count + ord : observed];
       }
-      if (lane == src) {
-        status = result;
-        found = (result == VX_HASH_FOUND) ? 1u : 0u;
-        active = false;
-      }
-      queue = __ballot_sync(hmask, active) & hmask;
     }
-    if (idx < count) {
-      if (statuses) statuses[idx] = status;
-      if (Op == SetOp::Contains && contains) contains[idx] = found;
-    }
+    if (statuses) statuses[idx] = result;
+    if (Op == SetOp::Contains && contains) contains[idx] = result == VX_HASH_FOUND ? 1u : 0u;
   }
 }
 
@@ -361,13 +381,15 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ------------------------------------------------------------ cuckoo --
-
-constexpr uint32_t kCuckooHashes = 4;
-
-__device__ __forceinline__ uint32_t cuckoo_slot(uint64_t key, uint32_t hid,
-                                                uint32_t n) {
-  return vx_cuckoo_slot(key, hid, n);
-}
+//
+// Two-choice bucketed cuckoo: a bucket is one 32-byte sector holding two
+// 16-byte slots {key, value | choice << 32}, and a key lives in one of its
+// two buckets (vx_cuckoo_bucket).  A lookup loads both sectors at once (one
+// round trip, two sectors).  An insert first replaces the value of a present
+// key (128-bit CAS, keeping its choice), else claims a free slot of either
+// bucket (128-bit CAS from empty), else evicts a slot of one of the buckets
+// with a 128-bit exchange and carries the evicted entry to its other bucket,
+// for at most max_evictions moves.
 
 __device__ __forceinline__ ulonglong2 exch128(ulonglong2 *p, ulonglong2 v) {
   ulonglong2 old;
@@ -415,40 +437,48 @@ __global__ void cuckoo_init_kernel(ulonglong2 *slots, uint32_t n,
   if (blockIdx.x == 0 && threadIdx.x == 0) *dropped = 0;
 }
 
-__device__ __forceinline__ bool cuckoo_lookup(const ulonglong2 *slots,
-                                              uint32_t n, uint64_t key,
-                                              uint32_t &value, uint32_t &where) {
+__device__ __forceinline__ uint64_t with_choice(uint64_t key_value_word, uint32_t choice) {
+  return (key_value_word & 0xffffffffull) | (static_cast<uint64_t>(choice) << 32);
+}
+
+// Replace the value stored for key, keeping the slot's choice bits (the
+// bucket the next eviction of this entry moves it from).  The swap is a
+// 128-bit CAS on {key, old word}, so an entry that a concurrent eviction
+// moved is looked up again rather than overwritten in its new occupant's
+// slot.  Returns false when the key is not in the table (duplicate keys
+// inside one insert batch are not supported, as in the reference).
+__device__ __forceinline__ bool cuckoo_replace(ulonglong2 *slots, uint32_t nb, uint64_t key,
+                                               uint32_t value) {
+  for (uint32_t attempt = 0; attempt < 64; ++attempt) {
+    ulonglong2 *b0 = slots + 2ull * vx_cuckoo_bucket(key, 0, nb);
+    ulonglong2 *b1 = slots + 2ull * vx_cuckoo_bucket(key, 1, nb);
+    ulonglong2 *where = nullptr;
+    ulonglong2 cur{};
+    ulonglong2 *cand[4] = {b0, b0 + 1, b1, b1 + 1};
+    ulonglong2 v[4];
 #pragma unroll
-  for (uint32_t h = 0; h < kCuckooHashes; ++h) {
-    const uint32_t s = cuckoo_slot(key, h, n);
-    const ulonglong2 v = ld_slot(slots + s);
-    if (v.x == key) {
-      value = static_cast<uint32_t>(v.y);
-      where = s;
-      return true;
-    }
+    for (int i = 0; i < 4; ++i) v[i] = ld_slot(cand[i]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (where == nullptr && v[i].x == key) {
+        where = cand[i];
+        cur = v[i];
+      }
+    if (where == nullptr) return false;
+    const ulonglong2 want = make_ulonglong2(key, (cur.y & 0xffffffff00000000ull) | value);
+    const ulonglong2 seen = cas128(where, cur, want);
+    if (seen.x == cur.x && seen.y == cur.y) return true;
   }
   return false;
 }
 
-// Replace the value stored for key, keeping the slot's hash id (bits 32..63
-// of .y, which the next eviction of this entry continues from).  The swap is
-// a 128-bit CAS on {key, old word}, so an entry that a concurrent eviction
-// moved is looked up again rather than overwritten in its new occupant's
-// slot.  Returns false when the key is not in the table (duplicate keys
-// inside one insert batch are not supported, as in the reference, so a key
-// held in flight by another thread's eviction chain is not expected).
-__device__ __forceinline__ bool cuckoo_replace(ulonglong2 *slots, uint32_t n,
-                                               uint64_t key, uint32_t value) {
-  uint32_t old_value, where;
-  for (uint32_t attempt = 0; attempt < 64; ++attempt) {
-    if (!cuckoo_lookup(slots, n, key, old_value, where)) return false;
-    const ulonglong2 cur = ld_slot(slots + where);
-    if (cur.x != key) continue;
-    const ulonglong2 want =
-        make_ulonglong2(key, (cur.y & 0xffffffff00000000ull) | value);
-    const ulonglong2 seen = cas128(slots + where, cur, want);
-    if (seen.x == cur.x && seen.y == cur.y) return true;
+// Claim a free slot of bucket b for entry e (choice c); true on success.
+__device__ __forceinline__ bool cuckoo_claim(ulonglong2 *bucket, ulonglong2 e, uint32_t c) {
+  const ulonglong2 want = make_ulonglong2(e.x, with_choice(e.y, c));
+  for (int i = 0; i < 2; ++i) {
+    if (ld_slot(bucket + i).x != kEmpty) continue;
+    const ulonglong2 seen = cas128(bucket + i, make_ulonglong2(kEmpty, 0ull), want);
+    if (seen.x == kEmpty && seen.y == 0ull) return true;
   }
   return false;
 }
@@ -461,30 +491,48 @@ __global__ void __launch_bounds__(kBlock)
                          uint32_t *statuses) {
   const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (i >= count) return;
+  const uint32_t nb = n / 2u;
   const uint64_t key = keys[i];
   const uint32_t value = values ? values[i] : static_cast<uint32_t>(i);
   uint32_t status;
   if (key == kEmpty || key == kDeleted) {
     status = VX_HASH_INVALID_KEY;
-  } else if (cuckoo_replace(slots, n, key, value)) {
+  } else if (cuckoo_replace(slots, nb, key, value)) {
     status = VX_HASH_REPLACED;
   } else {
     ulonglong2 cur = make_ulonglong2(key, value);
-    uint32_t hid = 0;
     status = VX_HASH_OVERFLOW;
+    // a new key may go to either bucket; an evicted one to its other bucket
+    int from = -1;
+    uint64_t rnd = mix64(key ^ 0x5851f42d4c957f2dull);
     for (uint32_t a = 0; a <= max_evictions; ++a) {
-      cur.y = (cur.y & 0xffffffffull) | (static_cast<uint64_t>(hid) << 32);
-      const ulonglong2 prev = exch128(slots + cuckoo_slot(cur.x, hid, n), cur);
-      if (prev.x == kEmpty) {
+      bool placed = false;
+      uint32_t target;
+      if (from < 0) {
+        const uint32_t first = static_cast<uint32_t>(rnd >> 63);
+        placed = cuckoo_claim(slots + 2ull * vx_cuckoo_bucket(cur.x, first, nb), cur, first) ||
+                 cuckoo_claim(slots + 2ull * vx_cuckoo_bucket(cur.x, 1u - first, nb), cur,
+                              1u - first);
+        target = first;
+      } else {
+        target = 1u - static_cast<uint32_t>(from);
+        placed = cuckoo_claim(slots + 2ull * vx_cuckoo_bucket(cur.x, target, nb), cur, target);
+      }
+      if (placed) {
         status = VX_HASH_INSERTED;
         break;
       }
-      if (prev.x == cur.x) { // same key displaced: keep the newer value
+      // evict one of the target bucket's two slots
+      rnd = mix64(rnd + a);
+      ulonglong2 *victim = slots + 2ull * vx_cuckoo_bucket(cur.x, target, nb) + (rnd & 1u);
+      const ulonglong2 prev =
+          exch128(victim, make_ulonglong2(cur.x, with_choice(cur.y, target)));
+      if (prev.x == kEmpty || prev.x == cur.x) { // a free slot, or the same key
         status = VX_HASH_INSERTED;
         break;
       }
       cur = prev;
-      hid = (static_cast<uint32_t>(prev.y >> 32) + 1u) % kCuckooHashes;
+      from = static_cast<int>(prev.y >> 32) & 1;
     }
     if (status == VX_HASH_OVERFLOW) atomicAdd(dropped, 1ull);
   }
@@ -701,10 +749,10 @@ size_t vx_slab_set_bytes(const vx_slab_set *s) {
 
 vx_status vx_cuckoo_create(uint32_t slot_count, uint32_t max_evictions,
                            vx_cuckoo **out) {
-  if (out == nullptr || slot_count == 0) return VX_ERR_INVALID_VALUE;
+  if (out == nullptr || slot_count == 0 || slot_count > 0xfffffffeu) return VX_ERR_INVALID_VALUE;
   auto *c = new (std::nothrow) vx_cuckoo;
   if (c == nullptr) return VX_ERR_MEMORY_ALLOCATION;
-  c->slot_count = slot_count;
+  c->slot_count = std::max<uint32_t>(2u, (slot_count + 1u) & ~1u); // whole two-slot buckets
   c->max_evictions = max_evictions;
   cudaError_t e = cudaMalloc(&c->slots, sizeof(ulonglong2) * slot_count);
   if (e == cudaSuccess) e = cudaMalloc(&c->dropped, sizeof(unsigned long long));
