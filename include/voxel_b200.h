@@ -590,7 +590,7 @@ typedef struct vx_slab_set_view {
 } vx_slab_set_view;
 
 typedef struct vx_cuckoo_view {
-    const void *slots;       /* 16-byte slots {key, value | hash id << 32} */
+    const void *slots;       /* buckets of two 16-byte slots {key, value | choice << 32} */
     uint32_t slot_count;
     uint32_t reserved;
 } vx_cuckoo_view;

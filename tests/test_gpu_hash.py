@@ -135,7 +135,7 @@ def _cuckoo_bucket(key: int, choice: int, buckets: int) -> int:
 
 
 def _raw_slots(m) -> np.ndarray:
-    """The table's 16-byte slots {key, value | hash id << 32}, copied to the host."""
+    """The table's 16-byte slots {key, value | choice << 32}, copied to the host."""
     import ctypes
     v = m.device_view()
     out = np.empty((v.slot_count, 2), np.uint64)
