@@ -24,18 +24,21 @@ def rand_prims(rng, n, world, rmax):
     return p
 
 
-def test_dag_graph_with_device_count(cuda):
+@pytest.mark.parametrize("cap", [256, 512])
+def test_dag_graph_with_device_count(cuda, cap):
     depth = 6
     world = 4 << depth
     rng = np.random.default_rng(31)
     batches = [rand_prims(rng, n, world, world // 5) for n in (120, 7, 200, 0)]
-    cap = 256
     buf = torch.zeros((cap, 8), dtype=torch.int32, device=cuda)
     cnt = torch.zeros(1, dtype=torch.int32, device=cuda)
     dag = vx.HashDag(depth, 1 << 18, 64 << 20)
     dag.build_terrain(3, 1, True)
     g = dag.graph_primitives(buf, cnt, cap)
-    assert g.kernels > depth
+    # within the small-edit threshold the graph holds the single cooperative
+    # kernel; above it, the level-by-level launches
+    small = cap <= vx.tuning()["edit.small_max_prims"]
+    assert g.kernels == 1 if small else g.kernels > depth
     t = oracle.terrain(seed=3, scale=1, caves=True)
     grid = oracle.Grid(depth).terrain(t)
     for b in batches:
