@@ -337,6 +337,22 @@ def run_sweep(args, ws, rank, local, torch, vx, device):
     value = ws * bytes_step * steps / (total_ms / 1e3) / 1e9
     del bufs
     torch.cuda.empty_cache()
+    # A library sort beside ours, for context: torch.sort (CUB radix sort),
+    # stable, on the same 2^28 32-bit keys (it returns int64 indices, so it
+    # writes more than our u32 payload).
+    ks = base_k32.clone()
+    torch.cuda.synchronize()
+    cub_ms = []
+    for _ in range(3):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        torch.sort(ks, stable=True)
+        b.record()
+        torch.cuda.synchronize()
+        cub_ms.append(a.elapsed_time(b))
+    del ks
+    torch.cuda.empty_cache()
     e2e = run_e2e(torch, vx, device, base_scan, base_k32, base_k64, vals,
                   ws_scan, ws_sort, max(1, min(steps, 3)), ws,
                   (slab, cuckoo, hkeys, hq))
@@ -353,6 +369,8 @@ def run_sweep(args, ws, rank, local, torch, vx, device):
         "sort_u32_ms": round(s32_ms / steps, 3),
         "sort_u64_ms": round(s64_ms / steps, 3),
         "sort_u32_Gkeys_per_s": round(N_SORT * steps / s32_ms / 1e6, 3),
+        "library_sort_u32_ms": round(min(cub_ms), 3),
+        "library_sort": "torch.sort (CUB radix sort), stable, 2^28 int32 keys -> values + int64 indices",
         "sort_u64_Gkeys_per_s": round(N_SORT * steps / s64_ms / 1e6, 3),
         "slab_insert_GBps": round(N_HASH * BYTES_HASH_INSERT * steps / slab_ins_ms / 1e6, 1),
         "slab_lookup_GBps": round(N_HASH * BYTES_HASH_LOOKUP * steps / slab_q_ms / 1e6, 1),
@@ -1300,6 +1318,31 @@ def run_case_hash(args, torch, vx, dev):
     print(json.dumps({"case": args.case, "elements": n, **res}))
 
 
+def run_case_gather(args, torch, dev):
+    """--case gather --elements N: N random 8-byte reads from a 2 GiB table
+    (torch.take, a library gather), each touching one 32-byte sector: the rate
+    of random sectors the hash tables' lookups are bound by."""
+    n = args.elements
+    table = torch.zeros(1 << 28, dtype=torch.int64, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(9)
+    idx = torch.randint(0, 1 << 28, (n,), dtype=torch.int64, device=dev, generator=g)
+    torch.take(table, idx)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        torch.take(table, idx)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    best = min(ms)
+    print(json.dumps({"case": "gather", "elements": n, "ms": [round(x, 3) for x in ms],
+                      "G_sectors_per_s": round(n / best / 1e6, 2)}))
+
+
 def run_case(args):
     """One operation alone, for profiler captures: --case scan|sort_u32|sort_u64
     --elements N (runs --steps launches); --case dag --elements E (E spheres
@@ -1315,6 +1358,8 @@ def run_case(args):
         return run_case_dag_full(args, torch, vx, dev)
     if args.case in ("slab", "cuckoo"):
         return run_case_hash(args, torch, vx, dev)
+    if args.case == "gather":
+        return run_case_gather(args, torch, dev)
     for _ in range(args.steps):
         if args.case == "scan":
             x = torch.randint(0, 256, (n,), dtype=torch.int32, device=dev)
@@ -1364,7 +1409,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--case", choices=["scan", "sort_u32", "sort_u64", "dag", "dag_full",
-                                       "slab", "cuckoo"],
+                                       "slab", "cuckoo", "gather"],
                     default=None)
     ap.add_argument("--elements", type=int, default=1 << 24)
     ap.add_argument("--serve-seconds", type=float, default=SERVE_SECONDS,
