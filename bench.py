@@ -1004,6 +1004,10 @@ def run_ours(args, ws, rank, local):
             "frac": round(lp_achieved / hbm, 4) if lp_achieved else None,
             "traffic": (round(LEAFPARENT_TRAFFIC_PER_ITEM * lp_items)
                         if LEAFPARENT_TRAFFIC_PER_ITEM else None),
+            # the DRAM bytes ncu counted per item, over the measured launch time
+            "dram_frac": (round(LEAFPARENT_TRAFFIC_PER_ITEM * lp_items / (lp_ms / lp_n / 1e3)
+                                / 1e9 / hbm, 4)
+                          if LEAFPARENT_TRAFFIC_PER_ITEM and lp_n else None),
             "algorithmic_bytes_per_launch": lp_bytes,
             "launches": lp_n,
             "avg_launch_ms": round(lp_ms / lp_n, 3) if lp_n else None,

@@ -186,10 +186,10 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"edit.small_max_prims", 256, {0, 64, 256, 1024, 4096}, 5},
     {"edit.small_blocks_per_sm", 2, {1, 2, 4}, 3},
     {"edit.small_max_voxels", 16384, {0, 4096, 16384, 65536}, 4},
-    {"sort.persistent", 1, {0, 1}, 2},
+    {"sort.lookback_window", 8, {8, 16, 32}, 3},
 };
 std::atomic<int64_t> g_values[kKnobCount] = {{16}, {12}, {0}, {1}, {16}, {32}, {5}, {4}, {4},
-                                             {256}, {2}, {16384}, {1}};
+                                             {256}, {2}, {16384}, {8}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

@@ -4,8 +4,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "../../include/voxel_b200.h"
 
 namespace vx {
@@ -144,13 +142,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     if (global_ns() - t0 > kWaitLimitNs) return false;
   return true;
 }
-// Orders the calling thread's earlier shared-memory accesses (generic proxy)
-// before bulk copies into shared memory issued after it (async proxy): a
-// buffer that threads wrote is refilled by copy only after each writer fenced
-// and a block barrier followed.
-__device__ __forceinline__ void fence_proxy_async_shared() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
 // Global -> shared bulk copy; src, dst 16-byte aligned, bytes a multiple of 16.
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
                                           uint64_t *bar) {
@@ -221,36 +212,6 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Number of SMs of the current device (cached per process).
 int sm_count();
-
-// Resident blocks per SM of a persistent kernel launched with Block threads
-// and Smem bytes of dynamic shared memory, queried once per process after
-// raising the kernel's dynamic shared-memory limit; 0 with *err set when
-// either call fails.  Call it outside stream capture first (the graph
-// capture helper does, through prepare_persistent_kernels).
-template <auto Kernel, int Block, int Smem> uint32_t resident_blocks(cudaError_t *err) {
-  static uint32_t cached = 0;
-  static cudaError_t cached_err = cudaSuccess;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    int n = 0;
-    cached_err = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem);
-    if (cached_err == cudaSuccess)
-      cached_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, Kernel, Block, Smem);
-    if (cached_err == cudaSuccess && n <= 0) cached_err = cudaErrorInvalidConfiguration;
-    if (cached_err == cudaSuccess) cached = static_cast<uint32_t>(n);
-  });
-  *err = cached_err;
-  return cached;
-}
-
-namespace scan {
-// Runs the one-time launch setup of every persistent scan kernel.
-cudaError_t prepare_persistent_kernels();
-}
-namespace sort {
-// Runs the one-time launch setup of every persistent partition kernel.
-cudaError_t prepare_persistent_kernels();
-}
 
 // Carves typed sub-buffers out of one caller-owned workspace, 256-B aligned.
 struct Carver {

@@ -12,10 +12,6 @@ namespace vx::graph {
 vx_status capture(const std::function<vx_status(cudaStream_t)> &body, vx_graph **out) {
   if (out == nullptr) return VX_ERR_INVALID_VALUE;
   *out = nullptr;
-  // Kernel attributes and occupancy queries are set up before the capture,
-  // so that nothing but stream work happens inside it.
-  VX_TRY_CUDA(scan::prepare_persistent_kernels());
-  VX_TRY_CUDA(sort::prepare_persistent_kernels());
   cudaStream_t s = nullptr;
   VX_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   const uint64_t before = prof::launch_count();

@@ -36,146 +36,114 @@ template <class T> typename RecordsFor<T>::type make_records(const ScanLayout &w
   return r;
 }
 
-// A persistent kernel: one block per resident slot, each taking tiles in the
-// order of a global counter (a tile only waits on tiles already taken by
-// running blocks, and every block works on its tiles in increasing order, so
-// the lowest unfinished tile can always proceed).  Two tile buffers per
-// block: while a tile is scanned, the next one the block has taken is already
-// arriving by bulk copy, so the copy's latency hides behind the scan, the
-// look-back and the stores.  A full, aligned tile arrives by one bulk copy;
-// the last, partial tile and unaligned data use guarded loads.  Pass 1 reads
-// the rows from shared memory for per-row warp totals, warp 0 scans the block
-// and looks back, pass 2 re-reads the rows, recomputes each thread's offset
-// inside its warp and writes the prefix sums straight to global memory.
+// One tile per block, tiles taken in the order of a global counter (a tile
+// only waits on tiles already taken by running blocks).  A full, aligned tile
+// arrives by one bulk copy; the last, partial tile and unaligned data use
+// guarded loads.  Pass 1 reads the rows from shared memory for per-row warp
+// totals, warp 0 scans the block and looks back, pass 2 re-reads the rows,
+// recomputes each thread's offset inside its warp (cheaper than holding it in
+// registers, which bound the resident blocks) and writes the prefix sums
+// straight to global memory.
 template <class T, bool Inclusive, bool Vectorised>
 __global__ void __launch_bounds__(TileShape<T>::kBlock, TileShape<T>::kMinBlocks)
     scan_kernel(T *__restrict__ data, uint32_t count, ScanLayout ws,
                 typename RecordsFor<T>::type records) {
   using S = TileShape<T>;
   constexpr uint32_t kTileBytes = S::kTile * sizeof(T);
-  extern __shared__ __align__(128) unsigned char s_dyn[];
-  T *const s_buf = reinterpret_cast<T *>(s_dyn); // two tiles
-  __shared__ uint64_t s_bar[2];
-  __shared__ uint32_t s_next;
+  __shared__ __align__(128) T s_data[S::kTile];
+  __shared__ uint64_t s_bar;
+  __shared__ uint32_t s_tile;
   __shared__ T s_warp[S::kWarps][S::kRows];
   __shared__ T s_row_off[S::kRows];
   __shared__ T s_prefix;
 
-  const uint32_t tiles =
-      static_cast<uint32_t>((static_cast<uint64_t>(count) + S::kTile - 1) / S::kTile);
   const uint32_t t = threadIdx.x;
   const uint32_t lane = lane_id();
   const uint32_t warp = t / kWarp;
-  auto by_copy = [&](uint32_t tile) {
-    return Vectorised && static_cast<uint64_t>(tile + 1) * S::kTile <= count;
-  };
-  // Thread 0: take the next tile and, when it arrives by copy, start the copy
-  // into buffer b (free: its last reader has passed a block barrier).
-  auto take = [&](uint32_t b) {
-    const uint32_t tile = atomicAdd(ws.tile_counter, 1u);
-    if (tile < tiles && by_copy(tile)) {
-      fence_proxy_async_shared();
-      mbar_arrive_expect_tx(&s_bar[b], kTileBytes);
-      bulk_load(s_buf + b * S::kTile, data + static_cast<uint64_t>(tile) * S::kTile,
-                kTileBytes, &s_bar[b]);
-    }
-    return tile;
-  };
   if (t == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    fence_proxy_async_shared(); // the inits, before the copy engine uses them
-    s_next = take(0);
+    const uint32_t tile = atomicAdd(ws.tile_counter, 1u);
+    s_tile = tile;
+    if (Vectorised && static_cast<uint64_t>(tile + 1) * S::kTile <= count) {
+      mbar_init(&s_bar, 1);
+      mbar_arrive_expect_tx(&s_bar, kTileBytes);
+      bulk_load(s_data, data + static_cast<uint64_t>(tile) * S::kTile, kTileBytes, &s_bar);
+    }
   }
   __syncthreads();
-  uint32_t tile = s_next;
-  uint32_t cur = 0, parity = 0; // bit b: parity of buffer b's next completion
-  while (tile < tiles) {
-    __syncthreads(); // every thread has read s_next
-    if (t == 0) s_next = take(cur ^ 1u);
-    T *const s_data = s_buf + cur * S::kTile;
-    const uint64_t base = static_cast<uint64_t>(tile) * S::kTile;
-    const bool bulk = by_copy(tile);
-    if (bulk) {
-      const uint32_t ph = (parity >> cur) & 1u;
-      parity ^= 1u << cur;
-      const bool ok = mbar_wait(&s_bar[cur], ph);
-      if (!__syncthreads_and(ok)) {
-        // Never expected: report, let the copies in flight land, stop.
-        if (t == 0) set_status(ws.status, kDevTimeout);
-        if (!ok) mbar_wait(&s_bar[cur], ph);
-        const uint32_t next = s_next;
-        if (next < tiles && by_copy(next)) mbar_wait(&s_bar[cur ^ 1u], (parity >> (cur ^ 1u)) & 1u);
-        return;
-      }
-    } else {
-      for (uint32_t i = t; i < S::kTile; i += S::kBlock)
-        s_data[i] = base + i < count ? data[base + i] : T(0);
-      __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t base = static_cast<uint64_t>(tile) * S::kTile;
+  const bool bulk = Vectorised && base + S::kTile <= count;
+  if (bulk) {
+    if (!mbar_wait(&s_bar, 0)) {
+      // Never expected: report, let the copy land, give up on this tile.
+      if (t == 0) set_status(ws.status, kDevTimeout);
+      mbar_wait(&s_bar, 0);
+      return;
     }
-    const uint4 *rows = reinterpret_cast<const uint4 *>(s_data);
-
-    // Pass 1: per-row warp totals.
-#pragma unroll 4
-    for (uint32_t r = 0; r < S::kRows; ++r) {
-      const uint4 q = rows[r * S::kBlock + t];
-      const T *qt = reinterpret_cast<const T *>(&q);
-      T sum = 0;
-#pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
-      sum = warp_sum<T>(sum);
-      if (lane == 0) s_warp[warp][r] = sum;
-    }
+  } else {
+    for (uint32_t i = t; i < S::kTile; i += S::kBlock)
+      s_data[i] = base + i < count ? data[base + i] : T(0);
     __syncthreads();
-    const uint32_t next = s_next;
+  }
+  const uint4 *rows = reinterpret_cast<const uint4 *>(s_data);
 
-    if (warp == 0) {
-      T acc = 0;
-#pragma unroll
-      for (uint32_t r = 0; r < S::kRows; ++r) {
-        const T w = lane < S::kWarps ? s_warp[lane][r] : T(0);
-        const T wi = warp_inclusive_sum<T>(w);
-        if (lane < S::kWarps) s_warp[lane][r] = wi - w; // exclusive warp offset
-        if (lane == 0) s_row_off[r] = acc;
-        acc += __shfl_sync(kFullMask, wi, S::kWarps - 1);
-      }
-      const T prefix = warp_lookback<T>(records, tile, acc, ws.status);
-      if (lane == 0) s_prefix = prefix;
-    }
-    __syncthreads();
-
-    // Pass 2: prefix sums, written straight to global memory.
-    const T tile_prefix = s_prefix;
+  // Pass 1: per-row warp totals.
 #pragma unroll 4
+  for (uint32_t r = 0; r < S::kRows; ++r) {
+    const uint4 q = rows[r * S::kBlock + t];
+    const T *qt = reinterpret_cast<const T *>(&q);
+    T sum = 0;
+#pragma unroll
+    for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
+    sum = warp_sum<T>(sum);
+    if (lane == 0) s_warp[warp][r] = sum;
+  }
+  __syncthreads();
+
+  if (warp == 0) {
+    T acc = 0;
+#pragma unroll
     for (uint32_t r = 0; r < S::kRows; ++r) {
-      uint4 q = rows[r * S::kBlock + t];
-      T *qt = reinterpret_cast<T *>(&q);
-      T sum = 0;
+      const T w = lane < S::kWarps ? s_warp[lane][r] : T(0);
+      const T wi = warp_inclusive_sum<T>(w);
+      if (lane < S::kWarps) s_warp[lane][r] = wi - w; // exclusive warp offset
+      if (lane == 0) s_row_off[r] = acc;
+      acc += __shfl_sync(kFullMask, wi, S::kWarps - 1);
+    }
+    const T prefix = warp_lookback<T>(records, tile, acc, ws.status);
+    if (lane == 0) s_prefix = prefix;
+  }
+  __syncthreads();
+
+  // Pass 2: prefix sums, written straight to global memory.
+  const T tile_prefix = s_prefix;
+#pragma unroll 4
+  for (uint32_t r = 0; r < S::kRows; ++r) {
+    uint4 q = rows[r * S::kBlock + t];
+    T *qt = reinterpret_cast<T *>(&q);
+    T sum = 0;
 #pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
-      T run = tile_prefix + s_row_off[r] + s_warp[warp][r] + (warp_inclusive_sum<T>(sum) - sum);
+    for (uint32_t e = 0; e < S::kPerVec; ++e) sum += qt[e];
+    T run = tile_prefix + s_row_off[r] + s_warp[warp][r] + (warp_inclusive_sum<T>(sum) - sum);
 #pragma unroll
-      for (uint32_t e = 0; e < S::kPerVec; ++e) {
-        const T x = qt[e];
-        if (Inclusive) {
-          run += x;
-          qt[e] = run;
-        } else {
-          qt[e] = run;
-          run += x;
-        }
-      }
-      if (bulk) {
-        reinterpret_cast<uint4 *>(data + base)[r * S::kBlock + t] = q;
+    for (uint32_t e = 0; e < S::kPerVec; ++e) {
+      const T x = qt[e];
+      if (Inclusive) {
+        run += x;
+        qt[e] = run;
       } else {
-        const uint64_t i0 = base + (static_cast<uint64_t>(r) * S::kBlock + t) * S::kPerVec;
-#pragma unroll
-        for (uint32_t e = 0; e < S::kPerVec; ++e)
-          if (i0 + e < count) data[i0 + e] = qt[e];
+        qt[e] = run;
+        run += x;
       }
     }
-    tile = next;
-    cur ^= 1u;
+    if (bulk) {
+      reinterpret_cast<uint4 *>(data + base)[r * S::kBlock + t] = q;
+    } else {
+      const uint64_t i0 = base + (static_cast<uint64_t>(r) * S::kBlock + t) * S::kPerVec;
+#pragma unroll
+      for (uint32_t e = 0; e < S::kPerVec; ++e)
+        if (i0 + e < count) data[i0 + e] = qt[e];
+    }
   }
 }
 
@@ -184,38 +152,7 @@ uint32_t max_tiles(uint32_t count) {
   return ceil_div(count, TileShape<uint64_t>::kTile) + 1;
 }
 
-template <class T, bool Inclusive, bool Vectorised>
-vx_status launch_scan(T *data, uint32_t count, const ScanLayout &ws,
-                      typename RecordsFor<T>::type records, cudaStream_t stream) {
-  using S = TileShape<T>;
-  constexpr int kSmem = 2 * S::kTile * sizeof(T); // two tile buffers
-  cudaError_t err = cudaSuccess;
-  const uint32_t per_sm =
-      resident_blocks<scan_kernel<T, Inclusive, Vectorised>, S::kBlock, kSmem>(&err);
-  if (per_sm == 0) return from_cuda(err);
-  const uint32_t tiles = ceil_div(count, S::kTile);
-  const uint32_t grid = std::min<uint32_t>(tiles, per_sm * sm_count());
-  scan_kernel<T, Inclusive, Vectorised><<<grid, S::kBlock, kSmem, stream>>>(data, count, ws, records);
-  return from_cuda(cudaGetLastError());
-}
-
-template <class T> cudaError_t prepare_type() {
-  using S = TileShape<T>;
-  constexpr int kSmem = 2 * S::kTile * sizeof(T);
-  cudaError_t e = cudaSuccess;
-  resident_blocks<scan_kernel<T, true, true>, S::kBlock, kSmem>(&e);
-  if (e == cudaSuccess) resident_blocks<scan_kernel<T, true, false>, S::kBlock, kSmem>(&e);
-  if (e == cudaSuccess) resident_blocks<scan_kernel<T, false, true>, S::kBlock, kSmem>(&e);
-  if (e == cudaSuccess) resident_blocks<scan_kernel<T, false, false>, S::kBlock, kSmem>(&e);
-  return e;
-}
-
 } // namespace
-
-cudaError_t prepare_persistent_kernels() {
-  const cudaError_t e = prepare_type<uint32_t>();
-  return e != cudaSuccess ? e : prepare_type<uint64_t>();
-}
 
 size_t workspace_size(uint32_t count) {
   if (count == 0) return 0;
@@ -251,16 +188,25 @@ vx_status scan_launch(T *data, uint32_t count, bool inclusive, void *workspace,
   if (count == 0) return VX_OK;
   if (workspace == nullptr || workspace_bytes < workspace_size(count))
     return VX_ERR_INVALID_VALUE;
+  using S = TileShape<T>;
   const ScanLayout ws = carve(workspace, count, sizeof(T));
   VX_TRY_CUDA(cudaMemsetAsync(workspace, 0, ws.clear_bytes, stream));
+  const uint32_t tiles = ceil_div(count, S::kTile);
   const bool vec = (reinterpret_cast<uintptr_t>(data) & 15u) == 0;
   const auto records = make_records<T>(ws);
   prof::Scope scope(sizeof(T) == 4 ? "scan_u32" : "scan_u64", stream);
-  if (inclusive)
-    return vec ? launch_scan<T, true, true>(data, count, ws, records, stream)
-               : launch_scan<T, true, false>(data, count, ws, records, stream);
-  return vec ? launch_scan<T, false, true>(data, count, ws, records, stream)
-             : launch_scan<T, false, false>(data, count, ws, records, stream);
+  if (inclusive) {
+    if (vec)
+      scan_kernel<T, true, true><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+    else
+      scan_kernel<T, true, false><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+  } else {
+    if (vec)
+      scan_kernel<T, false, true><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+    else
+      scan_kernel<T, false, false><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+  }
+  return from_cuda(cudaGetLastError());
 }
 
 template vx_status scan_launch<uint32_t>(uint32_t *, uint32_t, bool, void *,
@@ -410,9 +356,11 @@ vx_status vx_scan_exclusive_sum_u32_noalloc(uint32_t *data, uint32_t count,
   VX_TRY_CUDA(cudaMemsetAsync(base, 0, kNoAllocHeader + size_t(tiles) * sizeof(uint64_t), s));
   PackedRecords32 records{ws.rec_a};
   vx::prof::Scope scope("scan_u32_noalloc", s);
-  return (reinterpret_cast<uintptr_t>(data) & 15u) == 0
-             ? launch_scan<uint32_t, false, true>(data, count, ws, records, s)
-             : launch_scan<uint32_t, false, false>(data, count, ws, records, s);
+  if ((reinterpret_cast<uintptr_t>(data) & 15u) == 0)
+    scan_kernel<uint32_t, false, true><<<tiles, S::kBlock, 0, s>>>(data, count, ws, records);
+  else
+    scan_kernel<uint32_t, false, false><<<tiles, S::kBlock, 0, s>>>(data, count, ws, records);
+  return vx::from_cuda(cudaGetLastError());
 }
 
 // Status of the most recent allocation-free scan on the current device:

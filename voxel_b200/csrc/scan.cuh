@@ -147,7 +147,7 @@ __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
 template <class T> struct TileShape {
   static constexpr uint32_t kBlock = 256;
   static constexpr uint32_t kRows = 8;
-  static constexpr uint32_t kMinBlocks = 3; // two 32 KB tile buffers per block
+  static constexpr uint32_t kMinBlocks = 6;
   static constexpr uint32_t kPerVec = 16 / sizeof(T);
   static constexpr uint32_t kTile = kBlock * kRows * kPerVec;
   static constexpr uint32_t kWarps = kBlock / kWarp;

@@ -177,10 +177,10 @@ __device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
 // that one has not published its count (bounded by the GPU timer); then it
 // publishes this tile's inclusive count.  Returns the digit's count over all
 // earlier tiles.
+template <uint32_t kWindow>
 __device__ __forceinline__ uint32_t digit_lookback(uint32_t *records, uint32_t tile, uint32_t t,
                                                    uint32_t tile_count, uint32_t *status) {
   if (tile == 0) return 0;
-  constexpr uint32_t kWindow = 8;
   uint32_t exclusive = 0;
   const uint64_t t0 = global_ns();
   int64_t pred = static_cast<int64_t>(tile) - 1;
@@ -228,7 +228,7 @@ __device__ __forceinline__ uint32_t digit_lookback(uint32_t *records, uint32_t t
 // with one ballot per digit bit (warp-level multi-split, Adinets & Merrill)
 // instead of __match_any_sync, which executes on a narrow pipe and bounds
 // the pass when every key is ranked with it.
-template <class K, bool HasValues, uint32_t kItems, bool Early, bool Ballots>
+template <class K, bool HasValues, uint32_t kItems, bool Early, bool Ballots, uint32_t kWindow>
 __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     partition_kernel(const K *__restrict__ in_keys,
                      const uint32_t *__restrict__ in_vals,
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
   const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
   s_digit_off[t] = digit_off;
 
-  const uint32_t exclusive = digit_lookback(records, tile, t, tile_count, status);
+  const uint32_t exclusive = digit_lookback<kWindow>(records, tile, t, tile_count, status);
   s_global[t] = global_start + exclusive - digit_off;
   __syncthreads();
 
@@ -380,245 +380,6 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     out_keys[dst] = k;
     if (HasValues) out_vals[dst] = s_vals[j];
   }
-}
-
-// Persistent form of the partition pass: one block per resident slot, tiles
-// taken in the order of a global counter and processed in increasing order
-// by each block (so the lowest unfinished tile can always proceed).  Each
-// block holds two tile buffers: while one tile is ranked, looked back and
-// written out, the next tile the block has taken arrives by bulk copy into
-// the other buffer, so the copy's latency (the largest part of a tile's
-// lifetime in the one-tile-per-block form) overlaps the work.  The digit
-// starts of the pass are scanned once per block, not once per tile.
-template <class K> struct PersistentShape;
-// 30 KB of keys and payloads per buffer, three blocks per SM.
-template <> struct PersistentShape<uint32_t> { static constexpr uint32_t kItems = 15; };
-template <> struct PersistentShape<uint64_t> { static constexpr uint32_t kItems = 10; };
-
-template <class K, bool HasValues> constexpr uint32_t persistent_buffer_bytes() {
-  constexpr uint32_t tile = kBlock * PersistentShape<K>::kItems;
-  return tile * sizeof(K) + (HasValues ? tile * 4u : 0u);
-}
-
-template <class K, bool HasValues, bool Early, bool Ballots>
-__global__ void __launch_bounds__(kBlock, 3)
-    partition_persistent_kernel(const K *__restrict__ in_keys,
-                                const uint32_t *__restrict__ in_vals,
-                                K *__restrict__ out_keys, uint32_t *__restrict__ out_vals,
-                                uint32_t count, uint32_t shift, uint32_t mask,
-                                const uint32_t *__restrict__ pass_hist,
-                                uint32_t *records, uint32_t *tile_counter,
-                                uint32_t *status, bool aligned) {
-  constexpr uint32_t kItems = PersistentShape<K>::kItems;
-  constexpr uint32_t kTile = kBlock * kItems;
-  constexpr uint32_t kKeyBytes = kTile * sizeof(K);
-  constexpr uint32_t kValBytes = HasValues ? kTile * 4u : 0u;
-  constexpr uint32_t kBufBytes = persistent_buffer_bytes<K, HasValues>();
-  static_assert(kKeyBytes % 128 == 0 && kBufBytes % 128 == 0, "buffers stay 128-byte aligned");
-  extern __shared__ __align__(128) unsigned char s_dyn[]; // two buffers: keys, then payloads
-  __shared__ uint64_t s_bar[2];
-  __shared__ uint32_t s_next;
-  __shared__ uint32_t s_warp_hist[kWarps][kBins];
-  __shared__ uint32_t s_count[Early ? kBins : 1];
-  __shared__ uint32_t s_digit_off[kBins];
-  __shared__ uint32_t s_global[kBins];
-  __shared__ uint32_t s_tmp[kWarps];
-
-  const uint32_t tiles =
-      static_cast<uint32_t>((static_cast<uint64_t>(count) + kTile - 1) / kTile);
-  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
-  auto keys_of = [&](uint32_t b) { return reinterpret_cast<K *>(s_dyn + b * kBufBytes); };
-  auto vals_of = [&](uint32_t b) {
-    return reinterpret_cast<uint32_t *>(s_dyn + b * kBufBytes + kKeyBytes);
-  };
-  auto by_copy = [&](uint32_t tile) {
-    return aligned && static_cast<uint64_t>(tile + 1) * kTile <= count;
-  };
-  // Thread 0: take the next tile and, when it arrives by copy, start its
-  // copies into buffer b (free: its last reader has passed a block barrier).
-  auto take = [&](uint32_t b) {
-    const uint32_t tile = atomicAdd(tile_counter, 1u);
-    if (tile < tiles && by_copy(tile)) {
-      const uint64_t first = static_cast<uint64_t>(tile) * kTile;
-      fence_proxy_async_shared();
-      mbar_arrive_expect_tx(&s_bar[b], kKeyBytes + kValBytes);
-      bulk_load(keys_of(b), in_keys + first, kKeyBytes, &s_bar[b]);
-      if (HasValues) bulk_load(vals_of(b), in_vals + first, kValBytes, &s_bar[b]);
-    }
-    return tile;
-  };
-  if (t == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    fence_proxy_async_shared(); // the inits, before the copy engine uses them
-    s_next = take(0);
-  }
-  // Where each digit's run of this pass starts (the same for every tile).
-  const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
-  uint32_t tile = s_next;
-  uint32_t cur = 0, parity = 0; // bit b: parity of buffer b's next completion
-  while (tile < tiles) {
-    __syncthreads(); // s_next read by all; the previous tile's buffers released
-    if (t == 0) s_next = take(cur ^ 1u);
-#pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) s_warp_hist[w][t] = 0;
-    if (Early) s_count[t] = 0;
-    K *const s_keys = keys_of(cur);
-    uint32_t *const s_vals = vals_of(cur);
-    const uint64_t tile_base = static_cast<uint64_t>(tile) * kTile;
-    const uint32_t valid_in_tile =
-        count - tile_base < kTile ? static_cast<uint32_t>(count - tile_base) : kTile;
-    if (by_copy(tile)) {
-      const uint32_t ph = (parity >> cur) & 1u;
-      parity ^= 1u << cur;
-      const bool ok = mbar_wait(&s_bar[cur], ph);
-      if (!__syncthreads_and(ok)) {
-        // Never expected: report, let the copies in flight land, stop.
-        if (t == 0) set_status(status, kDevTimeout);
-        if (!ok) mbar_wait(&s_bar[cur], ph);
-        const uint32_t next = s_next;
-        if (next < tiles && by_copy(next))
-          mbar_wait(&s_bar[cur ^ 1u], (parity >> (cur ^ 1u)) & 1u);
-        return;
-      }
-    } else {
-      for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
-        s_keys[j] = in_keys[tile_base + j];
-        if (HasValues) s_vals[j] = in_vals[tile_base + j];
-      }
-      __syncthreads();
-    }
-    const uint32_t warp_first = warp * kWarp * kItems; // tile-local index of item 0
-    const uint64_t warp_base = tile_base + warp_first;
-
-    K key[kItems];
-    uint32_t val[kItems];
-    uint32_t rank2[(kItems + 1) / 2]; // two 16-bit ranks per register
-#pragma unroll
-    for (uint32_t i = 0; i < kItems; ++i) {
-      const uint32_t j = warp_first + i * kWarp + lane;
-      key[i] = j < valid_in_tile ? s_keys[j] : K(0);
-      val[i] = HasValues && j < valid_in_tile ? s_vals[j] : 0u;
-    }
-
-    uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
-    if (Early) {
-#pragma unroll
-      for (uint32_t i = 0; i < kItems; ++i)
-        if (warp_base + i * kWarp + lane < count)
-          atomicAdd(&s_count[digit_of(key[i], shift, mask)], 1u);
-      __syncthreads();
-      st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | s_count[t]);
-    }
-
-    // Warp-level multi-split: rank each key among the warp's keys of its digit.
-#pragma unroll
-    for (uint32_t i = 0; i < kItems; ++i) {
-      const uint64_t idx = warp_base + i * kWarp + lane;
-      const bool valid = idx < count;
-      const uint32_t d = valid ? digit_of(key[i], shift, mask) : kBins;
-      uint32_t peers;
-      if (Ballots) {
-        const uint32_t vb = __ballot_sync(kFullMask, valid);
-        peers = valid ? vb : ~vb;
-#pragma unroll
-        for (uint32_t b = 0; b < kRadixBits; ++b) {
-          const bool bit = (d >> b) & 1u;
-          const uint32_t bb = __ballot_sync(kFullMask, bit);
-          peers &= bit ? bb : ~bb;
-        }
-      } else {
-        peers = __match_any_sync(kFullMask, d);
-      }
-      const uint32_t below = __popc(peers & lanemask_lt());
-      const uint32_t leader = 31u - __clz(peers);
-      uint32_t pre = 0;
-      if (valid) pre = s_warp_hist[warp][d];
-      const uint32_t rk = pre + below;
-      if (i & 1u) rank2[i / 2] |= rk << 16;
-      else rank2[i / 2] = rk;
-      __syncwarp();
-      if (valid && lane == leader) s_warp_hist[warp][d] = pre + __popc(peers);
-      __syncwarp();
-    }
-    __syncthreads();
-
-    // Thread t owns digit t: warp offsets, tile count, tile-local digit offset.
-    uint32_t tile_count = 0;
-#pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) {
-      const uint32_t c = s_warp_hist[w][t];
-      s_warp_hist[w][t] = tile_count;
-      tile_count += c;
-    }
-    if (!Early) st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | tile_count);
-    const uint32_t digit_off = block_exclusive_256(tile_count, s_tmp);
-    s_digit_off[t] = digit_off;
-    const uint32_t next = s_next; // written before the barriers above
-
-    const uint32_t exclusive = digit_lookback(records, tile, t, tile_count, status);
-    s_global[t] = global_start + exclusive - digit_off;
-    __syncthreads();
-
-    // Sort the tile in shared memory (its input copy is in registers now).
-#pragma unroll
-    for (uint32_t i = 0; i < kItems; ++i) {
-      const uint64_t idx = warp_base + i * kWarp + lane;
-      if (idx < count) {
-        const uint32_t d = digit_of(key[i], shift, mask);
-        const uint32_t rk = (i & 1u) ? (rank2[i / 2] >> 16) : (rank2[i / 2] & 0xffffu);
-        const uint32_t pos = s_digit_off[d] + s_warp_hist[warp][d] + rk;
-        s_keys[pos] = key[i];
-        if (HasValues) s_vals[pos] = val[i];
-      }
-    }
-    __syncthreads();
-
-    // Write the tile's runs out in order.
-#pragma unroll 4
-    for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
-      const K k = s_keys[j];
-      const uint32_t dst = s_global[digit_of(k, shift, mask)] + j;
-      if (dst >= count) continue; // only reachable after a look-back timeout
-      out_keys[dst] = k;
-      if (HasValues) out_vals[dst] = s_vals[j];
-    }
-    fence_proxy_async_shared(); // this buffer is refilled by copy next
-    tile = next;
-    cur ^= 1u;
-  }
-}
-
-// One persistent partition instantiation and its dynamic shared memory.
-template <class K, bool HV, bool Early, bool Ballots> struct Persistent {
-  static constexpr auto kernel = partition_persistent_kernel<K, HV, Early, Ballots>;
-  static constexpr int kSmem = 2 * persistent_buffer_bytes<K, HV>();
-};
-static_assert(PersistentShape<uint32_t>::kItems >= Shape<uint32_t>::kSmall &&
-                  PersistentShape<uint64_t>::kItems >= Shape<uint64_t>::kSmall,
-              "the workspace's look-back records cover the persistent tiles");
-
-template <class K, bool HV> cudaError_t prepare_persistent() {
-  cudaError_t e = cudaSuccess;
-  resident_blocks<Persistent<K, HV, true, true>::kernel, kBlock, Persistent<K, HV, true, true>::kSmem>(&e);
-  if (e == cudaSuccess)
-    resident_blocks<Persistent<K, HV, true, false>::kernel, kBlock,
-                    Persistent<K, HV, true, false>::kSmem>(&e);
-  if (e == cudaSuccess)
-    resident_blocks<Persistent<K, HV, false, true>::kernel, kBlock,
-                    Persistent<K, HV, false, true>::kSmem>(&e);
-  if (e == cudaSuccess)
-    resident_blocks<Persistent<K, HV, false, false>::kernel, kBlock,
-                    Persistent<K, HV, false, false>::kSmem>(&e);
-  return e;
-}
-
-cudaError_t prepare_persistent_kernels() {
-  cudaError_t e = prepare_persistent<uint32_t, true>();
-  if (e == cudaSuccess) e = prepare_persistent<uint32_t, false>();
-  if (e == cudaSuccess) e = prepare_persistent<uint64_t, true>();
-  if (e == cudaSuccess) e = prepare_persistent<uint64_t, false>();
-  return e;
 }
 
 template <class K>
@@ -653,13 +414,12 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
   }
   VX_TRY_CUDA(cudaGetLastError());
 
-  const bool persistent = tune::get(tune::kSortPersistent) != 0;
   const bool large = tune::get(sizeof(K) == 4 ? tune::kSortItemsU32 : tune::kSortItemsU64) ==
                      static_cast<int64_t>(Shape<K>::kLarge);
   const bool early = tune::get(tune::kSortEarlyCounts) != 0;
   const bool ballots = tune::get(tune::kSortRankBallots) != 0;
-  const uint32_t items = persistent ? PersistentShape<K>::kItems
-                                    : large ? Shape<K>::kLarge : Shape<K>::kSmall;
+  const uint32_t window = static_cast<uint32_t>(tune::get(tune::kSortLookbackWindow));
+  const uint32_t items = large ? Shape<K>::kLarge : Shape<K>::kSmall;
   const uint32_t tiles = ceil_div(count, kBlock * items);
   K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
   uint32_t *src_v = values, *dst_v = l.tmp_vals;
@@ -668,43 +428,33 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
     uint32_t *rec = l.records + static_cast<size_t>(p) * tiles * kBins;
     prof::Scope scope(sizeof(K) == 4 ? "sort_partition_u32" : "sort_partition_u64", stream);
     const bool aligned = aligned16(src_k) && (values == nullptr || aligned16(src_v));
-    auto launch = [&](auto kernel, uint32_t grid = 0, int smem = 0) {
-      kernel<<<grid ? grid : tiles, kBlock, smem, stream>>>(
-          src_k, src_v, dst_k, dst_v, count, info.shift[p], info.mask[p], l.hist + p * kBins, rec,
-          l.counters + 2 + p, l.counters + 1, aligned);
+    auto launch = [&](auto kernel) {
+      kernel<<<tiles, kBlock, 0, stream>>>(src_k, src_v, dst_k, dst_v, count, info.shift[p],
+                                           info.mask[p], l.hist + p * kBins, rec,
+                                           l.counters + 2 + p, l.counters + 1, aligned);
     };
-    // Persistent form: as many blocks as fit on the GPU at once.
-    cudaError_t setup = cudaSuccess;
-    auto launch_persistent = [&](auto tag) {
-      using Kernel = decltype(tag);
-      const uint32_t per_sm = resident_blocks<Kernel::kernel, kBlock, Kernel::kSmem>(&setup);
-      if (per_sm != 0)
-        launch(Kernel::kernel, std::min<uint32_t>(tiles, per_sm * sm_count()), Kernel::kSmem);
+    // (values, items, early, ballots, window) -> one of 48 instantiations
+    auto by_window = [&](auto hv, auto it, auto ea, auto ba) {
+      constexpr bool HV = decltype(hv)::value, E = decltype(ea)::value, B = decltype(ba)::value;
+      constexpr uint32_t I = decltype(it)::value;
+      if (window == 32) launch(partition_kernel<K, HV, I, E, B, 32>);
+      else if (window == 16) launch(partition_kernel<K, HV, I, E, B, 16>);
+      else launch(partition_kernel<K, HV, I, E, B, 8>);
     };
-    constexpr uint32_t S = Shape<K>::kSmall, L = Shape<K>::kLarge;
-    // (values, persistent / items, early, ballots) -> one of 24 instantiations
-    auto pick = [&](auto hv) {
-      constexpr bool HV = decltype(hv)::value;
-      if (persistent) {
-        if (early) ballots ? launch_persistent(Persistent<K, HV, true, true>{})
-                           : launch_persistent(Persistent<K, HV, true, false>{});
-        else ballots ? launch_persistent(Persistent<K, HV, false, true>{})
-                     : launch_persistent(Persistent<K, HV, false, false>{});
-      } else if (large) {
-        if (early) ballots ? launch(partition_kernel<K, HV, L, true, true>)
-                           : launch(partition_kernel<K, HV, L, true, false>);
-        else ballots ? launch(partition_kernel<K, HV, L, false, true>)
-                     : launch(partition_kernel<K, HV, L, false, false>);
-      } else {
-        if (early) ballots ? launch(partition_kernel<K, HV, S, true, true>)
-                           : launch(partition_kernel<K, HV, S, true, false>);
-        else ballots ? launch(partition_kernel<K, HV, S, false, true>)
-                     : launch(partition_kernel<K, HV, S, false, false>);
-      }
+    auto by_ballots = [&](auto hv, auto it, auto ea) {
+      if (ballots) by_window(hv, it, ea, std::true_type{});
+      else by_window(hv, it, ea, std::false_type{});
     };
-    if (values != nullptr) pick(std::true_type{});
-    else pick(std::false_type{});
-    VX_TRY_CUDA(setup);
+    auto by_early = [&](auto hv, auto it) {
+      if (early) by_ballots(hv, it, std::true_type{});
+      else by_ballots(hv, it, std::false_type{});
+    };
+    auto by_items = [&](auto hv) {
+      if (large) by_early(hv, std::integral_constant<uint32_t, Shape<K>::kLarge>{});
+      else by_early(hv, std::integral_constant<uint32_t, Shape<K>::kSmall>{});
+    };
+    if (values != nullptr) by_items(std::true_type{});
+    else by_items(std::false_type{});
     VX_TRY_CUDA(cudaGetLastError());
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);

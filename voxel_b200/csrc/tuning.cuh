@@ -20,7 +20,7 @@ enum Id : uint32_t {
   kEditSmallMaxPrims, // batches of at most this many primitives run as one cooperative kernel
   kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
   kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
-  kSortPersistent,  // partition passes as persistent double-buffered kernels (1) or one tile per block (0)
+  kSortLookbackWindow, // predecessor tiles a partition look-back reads per round trip: 8, 16 or 32
   kKnobCount
 };
 
