@@ -548,6 +548,19 @@ vx_status vx_svo_export_canonical(const vx_svo *svo, uint32_t *host_node_count,
                                   uint8_t *host_materials,
                                   uint32_t leaves_capacity, vx_stream stream);
 
+/* Garbage collection.  A subtree that an edit overwrites with a uniform
+ * region becomes unreachable; its nodes and leaves go back to the free lists
+ * when a collection runs (mark from the root, then rebuild the free lists).
+ * Edits collect lazily: only when one would not fit in the room left (free
+ * lists plus the never-used tail) does the collection run, inside that edit
+ * and before it allocates anything; the edit fails with VX_ERR_CAPACITY only
+ * if it still does not fit.  vx_svo_collect runs a collection now (stream
+ * ordered; nothing runs when no subtree was detached since the last one), so
+ * that the counters below count only reachable storage.  The reference frees
+ * a collapsed node's storage as part of each edit (svt/cuda/voxel/detail/
+ * collapse/pipeline.cuh:55-110). */
+vx_status vx_svo_collect(vx_svo *svo, vx_stream stream);
+
 /* Counters (GpuSvoCounters, svt/cuda/device_view.cuh:24-29). */
 typedef struct vx_svo_counters {
     uint32_t node_count;

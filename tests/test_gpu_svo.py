@@ -74,7 +74,8 @@ def test_terrain_then_batches_queries_and_gc(cuda, mats):
     expect[inside] = oracle.eval_voxels(t, depth + 2, np.concatenate(all_prims), pts[inside],
                                         materials=mats)
     assert np.array_equal(got, expect)
-    # live structure = counters minus free lists
+    # after a collection, live structure = counters minus free lists
+    s.collect()
     c = s.counters()
     nodes, leaves, _ = s.canonical()
     assert c.node_count - c.free_node_count == nodes.size // 8
@@ -126,6 +127,51 @@ def test_capacity_overflow_changes_nothing(cuda):
     many = np.random.default_rng(2).integers(0, 4 << depth, (3000, 3)).astype(np.uint32)
     assert s.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE) == vx.VX_ERR_CAPACITY
     assert canon(s) == before
+
+
+@pytest.mark.parametrize("small_max_prims", [256, 0])
+def test_lazy_collection_reclaims_detached_subtrees(cuda, small_max_prims):
+    """Edits collect garbage only when they would not fit otherwise: a cycle
+    of (carve a sphere, fill the world) detaches every carved subtree, so 30
+    cycles need about 30 spheres' storage without collection; in room for
+    three they all succeed, through the single cooperative kernel (256) and
+    the level-by-level launches (0), and the content stays the oracle's."""
+    vx.set_tuning("edit.small_max_prims", small_max_prims)
+    try:
+        depth = 5
+        world = 4 << depth
+        rng = np.random.default_rng(44)
+
+        def sphere(c):
+            p = np.zeros(1, oracle.PRIM_DTYPE)
+            p[0] = (c, (20, 0, 0), 0, 0)  # remove a sphere of radius 20
+            return p
+
+        fill = np.zeros(1, oracle.PRIM_DTYPE)
+        fill[0] = ((0, 0, 0), (world, world, world), 4 | (1 << 8) | (1 << 16), 0)  # whole world
+        probe = vx.Svo(depth, 1 << 16, 1 << 16)
+        probe.apply_primitives(vx.prims_to_device(fill, cuda))
+        probe.apply_primitives(vx.prims_to_device(sphere((64, 64, 64)), cuda))
+        assert probe.status() == 0
+        used = probe.counters()
+        s = vx.Svo(depth, 3 * used.node_count + 8, 3 * used.leaf_count + 8)
+        g = oracle.Grid(depth)
+        for i in range(30):
+            c = tuple(int(v) for v in rng.integers(24, world - 24, 3))
+            for prims in (fill, sphere(c)):
+                s.apply_primitives(vx.prims_to_device(prims, cuda))
+                g.apply_prims(prims)
+                assert s.status() == 0, i
+            assert canon(s) == g.svo()
+        c = s.counters()
+        assert c.node_count <= 3 * used.node_count + 8
+        s.collect()
+        c = s.counters()
+        nodes, leaves, _ = s.canonical()
+        assert c.node_count - c.free_node_count == nodes.size // 8
+        assert c.leaf_count - c.free_leaf_count == leaves.size
+    finally:
+        vx.reset_tuning()
 
 
 def test_config_c1_full_size_plain_and_batched_bit_exact(cuda):

@@ -242,6 +242,7 @@ _SIGS = {
     "vx_svo_export_canonical": (_ST, [_P, C.POINTER(_U32), C.POINTER(_U32),
                                       _P, _U32, _P, _P, _U32, _P]),
     "vx_svo_get_counters": (_ST, [_P, C.POINTER(vx_svo_counters), _P]),
+    "vx_svo_collect": (_ST, [_P, _P]),
     "vx_svo_depth": (_U32, [_P]),
     "vx_terminal_workspace_size": (_SZ, [_U32, _U32]),
     "vx_svo_apply_terminal": (_ST, [_P, _P, _U32, _P, _U32, _U32, _U32, _P, _SZ, _P]),

@@ -768,6 +768,11 @@ class Svo:
               "vx_svo_get_counters")
         return c
 
+    def collect(self) -> None:
+        """Return the storage of every unreachable subtree to the free lists
+        now (edits collect only when they would not fit otherwise)."""
+        check(lib().vx_svo_collect(self._h, stream_handle()), "vx_svo_collect")
+
     def canonical(self):
         """(nodes [8 words each], leaves, materials or None): DFS pre-order."""
         nn, nl = C.c_uint32(0), C.c_uint32(0)

@@ -45,7 +45,8 @@ struct Counters {
   uint32_t node_count, leaf_count, free_node_count, free_leaf_count;
   uint32_t base_node_count, base_leaf_count, base_free_nodes, base_free_leaves;
   uint32_t taken_nodes, taken_leaves;
-  uint32_t detached;
+  uint32_t detached;   // some subtree became unreachable since the last collection
+  uint32_t gc_needed;  // the collection stages run (gate read by every block)
   uint32_t gc_count[kMaxDepth + 1];
 };
 
@@ -92,7 +93,7 @@ struct SvoTree {
     return old; // a uniform region's children hold the same value
   }
   // A materialised child overwritten by a covering primitive leaves its
-  // subtree unreachable: flag it for the end-of-edit collection.
+  // subtree unreachable: flag it for a later collection.
   __device__ void replaced(uint32_t l, uint32_t old, uint32_t c) const {
     if ((old & kChild) && (child(l, old, c) & kChild)) atomicOr(&t.ctr->detached, 1u);
   }
@@ -159,16 +160,33 @@ __global__ void begin_kernel(Tables t) { begin_body(t); }
 
 // Worst case before any write: every item below the root may need a node and
 // every leaf child of the last level a leaf.
-__device__ __forceinline__ void check_capacity_body(Tables t) {
-  Header *h = t.hdr;
-  if (h->status != kDevOk) return;
+// Nodes and leaves the edit may need (every item below the root a node, 8
+// leaves per leaf-parent item) against what the free lists and the unused
+// tail hold.
+__device__ __forceinline__ bool edit_fits(const Tables &t) {
+  const Header *h = t.hdr;
   uint64_t nodes = 0;
   for (uint32_t l = 1; l < t.depth; ++l) nodes += h->item_count[l];
   const uint64_t leaves = 8ull * h->item_count[t.depth - 1];
   const Counters *c = t.ctr;
   const uint64_t avail_nodes = c->base_free_nodes + uint64_t(t.max_nodes - c->base_node_count);
   const uint64_t avail_leaves = c->base_free_leaves + uint64_t(t.max_leaves - c->base_leaf_count);
-  if (nodes > avail_nodes || leaves > avail_leaves) h->status = kDevCapacity;
+  return nodes <= avail_nodes && leaves <= avail_leaves;
+}
+
+// Garbage is collected lazily: only when an edit would not fit in the room
+// left does the collection run, before the edit allocates anything (the
+// edit has only read the tree so far, so marking from the current root
+// keeps everything it reads).  A capacity error follows only if the edit
+// still does not fit after it.
+__device__ __forceinline__ void check_capacity_body(Tables t) {
+  Header *h = t.hdr;
+  t.ctr->gc_needed = 0;
+  if (h->status != kDevOk) return;
+  if (!edit_fits(t)) {
+    if (t.ctr->detached) t.ctr->gc_needed = 1;
+    else h->status = kDevCapacity;
+  }
 }
 __global__ void check_capacity_kernel(Tables t) { check_capacity_body(t); }
 
@@ -347,7 +365,7 @@ __global__ void finalize_kernel(Tables t) { finalize_body(t); }
 
 __device__ __forceinline__ void gc_clear_body(Tables t, Blocks blk) {
   Counters *c = t.ctr;
-  if (!c->detached) return;
+  if (!c->gc_needed) return;
   for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
        i < c->node_count; i += static_cast<uint64_t>(blk.count) * blockDim.x)
     t.node_mark[i] = 0;
@@ -364,7 +382,7 @@ __global__ void gc_clear_kernel(Tables t) { gc_clear_body(t, launch_blocks()); }
 
 __device__ __forceinline__ void gc_level_body(Tables t, uint32_t l, Blocks blk) {
   Counters *c = t.ctr;
-  if (!c->detached) return;
+  if (!c->gc_needed) return;
   const uint32_t n = c->gc_count[l];
   const uint32_t *front = t.front[l & 1u];
   uint32_t *next = t.front[(l + 1) & 1u];
@@ -384,7 +402,7 @@ __global__ void gc_level_kernel(Tables t, uint32_t l) { gc_level_body(t, l, laun
 
 __device__ __forceinline__ void gc_zero_free_body(Tables t) {
   Counters *c = t.ctr;
-  if (!c->detached) return;
+  if (!c->gc_needed) return;
   c->free_node_count = 0;
   c->free_leaf_count = 0;
 }
@@ -392,7 +410,7 @@ __global__ void gc_zero_free_kernel(Tables t) { gc_zero_free_body(t); }
 
 __device__ __forceinline__ void gc_rebuild_body(Tables t, Blocks blk) {
   Counters *c = t.ctr;
-  if (!c->detached) return;
+  if (!c->gc_needed) return;
   const uint32_t nn = c->node_count, nl = c->leaf_count;
   for (uint64_t i = 1 + blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nn;
        i += static_cast<uint64_t>(blk.count) * blockDim.x)
@@ -403,7 +421,25 @@ __device__ __forceinline__ void gc_rebuild_body(Tables t, Blocks blk) {
 }
 __global__ void gc_rebuild_kernel(Tables t) { gc_rebuild_body(t, launch_blocks()); }
 
-__global__ void gc_end_kernel(Tables t) { t.ctr->detached = 0; }
+// After a collection inside an edit: the free lists are the edit's starting
+// point; the edit fails only if it still does not fit.
+__device__ __forceinline__ void gc_recheck_body(Tables t) {
+  Counters *c = t.ctr;
+  if (!c->gc_needed) return;
+  c->gc_needed = 0;
+  c->detached = 0;
+  c->base_free_nodes = c->free_node_count;
+  c->base_free_leaves = c->free_leaf_count;
+  if (t.hdr->status == kDevOk && !edit_fits(t)) t.hdr->status = kDevCapacity;
+}
+__global__ void gc_recheck_kernel(Tables t) { gc_recheck_body(t); }
+
+// vx_svo_collect: a collection on request, between edits.
+__global__ void gc_request_kernel(Tables t) { t.ctr->gc_needed = t.ctr->detached; }
+__global__ void gc_end_kernel(Tables t) {
+  if (t.ctr->gc_needed) t.ctr->detached = 0;
+  t.ctr->gc_needed = 0;
+}
 
 // A whole edit, collection included, in one cooperative launch: the stages
 // of run_pipeline separated by grid-wide barriers instead of kernel
@@ -441,6 +477,20 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
   }
   if (lead) check_capacity_body(t);
   grid.sync();
+  if (t.ctr->gc_needed) { // the same in every block: written before the barrier
+    gc_clear_body(t, blk);
+    grid.sync();
+    for (uint32_t l = 0; l < t.depth; ++l) {
+      gc_level_body(t, l, blk);
+      grid.sync();
+    }
+    if (lead) gc_zero_free_body(t);
+    grid.sync();
+    gc_rebuild_body(t, blk);
+    grid.sync();
+    if (lead) gc_recheck_body(t);
+    grid.sync();
+  }
   leafparent_body<false>(e, t, blk);
   grid.sync();
   for (uint32_t r = t.depth - 1; r > 0; --r) {
@@ -448,18 +498,6 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
     grid.sync();
   }
   if (lead) finalize_body(t);
-  grid.sync();
-  gc_clear_body(t, blk);
-  grid.sync();
-  for (uint32_t l = 0; l < t.depth; ++l) {
-    gc_level_body(t, l, blk);
-    grid.sync();
-  }
-  if (lead) gc_zero_free_body(t);
-  grid.sync();
-  gc_rebuild_body(t, blk);
-  grid.sync();
-  if (lead) t.ctr->detached = 0;
 }
 
 __global__ void reset_kernel(Tables t) {
@@ -471,6 +509,7 @@ __global__ void reset_kernel(Tables t) {
   c->free_node_count = 0;
   c->free_leaf_count = 0;
   c->detached = 0;
+  c->gc_needed = 0;
   t.hdr->status = kDevOk;
 }
 
@@ -540,6 +579,21 @@ inline bool small_batch(uint32_t n, bool voxel_list) {
                                                          : tune::kEditSmallMaxPrims));
 }
 
+// The collection stages as kernels, each leaving at once unless gc_needed is
+// set: by the capacity check inside an edit (ended by gc_recheck_kernel), or
+// by gc_request_kernel when a caller asks (ended by gc_end_kernel).
+vx_status launch_collection(const Tables &t, uint32_t grid, cudaStream_t s, bool on_request) {
+  prof::Scope sc("svo_gc", s);
+  if (on_request) gc_request_kernel<<<1, 1, 0, s>>>(t);
+  gc_clear_kernel<<<grid, kBlock, 0, s>>>(t);
+  for (uint32_t l = 0; l < t.depth; ++l) gc_level_kernel<<<grid, kBlock, 0, s>>>(t, l);
+  gc_zero_free_kernel<<<1, 1, 0, s>>>(t);
+  gc_rebuild_kernel<<<grid, kBlock, 0, s>>>(t);
+  if (on_request) gc_end_kernel<<<1, 1, 0, s>>>(t);
+  else gc_recheck_kernel<<<1, 1, 0, s>>>(t);
+  return from_cuda(cudaGetLastError());
+}
+
 vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_count,
                        uint32_t host_count, cudaStream_t s, bool terrain,
                        int small = -1 /* -1: by host_count as a primitive batch */) {
@@ -577,6 +631,7 @@ vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_c
     prof::Scope sc("svo_check_capacity", s);
     check_capacity_kernel<<<1, 1, 0, s>>>(t);
   }
+  VX_TRY(launch_collection(t, grid, s, false));
   {
     prof::Scope sc("svo_leafparent", s);
     if (terrain) leafparent_kernel<true><<<grid, kBlock, 0, s>>>(e, t);
@@ -591,14 +646,6 @@ vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_c
   {
     prof::Scope sc("svo_finalize", s);
     finalize_kernel<<<1, 1, 0, s>>>(t);
-  }
-  {
-    prof::Scope sc("svo_gc", s);
-    gc_clear_kernel<<<grid, kBlock, 0, s>>>(t);
-    for (uint32_t l = 0; l < depth; ++l) gc_level_kernel<<<grid, kBlock, 0, s>>>(t, l);
-    gc_zero_free_kernel<<<1, 1, 0, s>>>(t);
-    gc_rebuild_kernel<<<grid, kBlock, 0, s>>>(t);
-    gc_end_kernel<<<1, 1, 0, s>>>(t);
   }
   return from_cuda(cudaGetLastError());
 }
@@ -814,6 +861,13 @@ vx_status vx_svo_query(const vx_svo *v, const vx_voxel *pts, uint32_t count,
   VX_TRY(vx_svo_device_view(v, &view));
   query_kernel<<<vx::ceil_div(count, kBlock), kBlock, 0, s>>>(view, pts, count, out);
   return vx::from_cuda(cudaGetLastError());
+}
+
+vx_status vx_svo_collect(vx_svo *v, vx_stream stream) {
+  if (v == nullptr) return VX_ERR_INVALID_VALUE;
+  const uint32_t grid = static_cast<uint32_t>(vx::sm_count()) *
+                        static_cast<uint32_t>(vx::tune::get(vx::tune::kEditBlocksPerSm));
+  return launch_collection(v->t, grid, static_cast<cudaStream_t>(stream), true);
 }
 
 vx_status vx_svo_get_counters(const vx_svo *v, vx_svo_counters *host, vx_stream stream) {
