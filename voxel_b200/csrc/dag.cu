@@ -483,16 +483,20 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, Pl
     grid.sync();
   }
   init_body(e, kUseHeaderRoot, blk);
+  // pool_mark: nothing is inserted before the leaf-parent level
+  if (blk.id == 0 && threadIdx.x < kMaxDepth)
+    x.t.hdr->pool_mark[threadIdx.x] = x.t.hdr->pool_used[threadIdx.x];
   grid.sync();
   for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
     expand_body<DagTree, false>(e, tree, l, blk);
     grid.sync();
-    expand_big_body<DagTree, false, kBlock, kSmallBigCache>(e, tree, l, blk);
-    grid.sync();
+    // The block-per-item stage only when it has items: the count is final
+    // at the barrier, so every block skips it (and its barrier) alike.
+    if (x.t.hdr->big_count[l] != 0) {
+      expand_big_body<DagTree, false, kBlock, kSmallBigCache>(e, tree, l, blk);
+      grid.sync();
+    }
   }
-  if (blk.id == 0 && threadIdx.x < kMaxDepth)
-    x.t.hdr->pool_mark[threadIdx.x] = x.t.hdr->pool_used[threadIdx.x];
-  grid.sync();
   leafparent_body<false, Lanes>(x, blk);
   grid.sync();
   for (uint32_t r = x.t.depth - 1; r > 0; --r) {

@@ -472,8 +472,12 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
   for (uint32_t l = 0; l + 1 < t.depth; ++l) {
     expand_body<SvoTree, false>(e, pol, l, blk);
     grid.sync();
-    expand_big_body<SvoTree, false, kBlock, kSmallBigCache>(e, pol, l, blk);
-    grid.sync();
+    // The block-per-item stage only when it has items: the count is final
+    // at the barrier, so every block skips it (and its barrier) alike.
+    if (t.hdr->big_count[l] != 0) {
+      expand_big_body<SvoTree, false, kBlock, kSmallBigCache>(e, pol, l, blk);
+      grid.sync();
+    }
   }
   if (lead) check_capacity_body(t);
   grid.sync();
