@@ -38,8 +38,16 @@ def svo():
     return vx.Svo(D, 256, 64, arena_bytes=32 << 20)
 
 
+def counters(s):
+    """Counters after a collection: the reference frees a replaced subtree
+    within the edit; this library collects lazily (when an edit would not fit
+    otherwise, or on request), so free-list deltas are read after one."""
+    s.collect()
+    return s.counters()
+
+
 def live(s):
-    c = s.counters()
+    c = counters(s)
     return c.node_count - c.free_node_count, c.leaf_count - c.free_leaf_count
 
 
@@ -84,10 +92,10 @@ def test_reference_destroy_and_collapse_cases(cuda):
     # AllocatesLeafWhenEditingUniformTerminalLeaf
     s = svo()
     place(s, nodes=[(10, 0, 0, 0, 0)])
-    before = s.counters()
+    before = counters(s)
     assert before.free_leaf_count == 0
     destroy(s, leaves=[(0, 1, 0, 0, 0)])
-    after = s.counters()
+    after = counters(s)
     assert after.leaf_count == before.leaf_count + 1 and after.free_leaf_count == 0
     assert query(s, [(0, 0, 0), (1, 0, 0)]) == [0, 1]
 
@@ -111,27 +119,27 @@ def test_reference_release_cases(cuda):
     materialised subtree frees exactly its nodes and leaves."""
     s = svo()
     place(s, leaves=[(0, 1, 0, 0, 0)])
-    b = s.counters()
+    b = counters(s)
     assert b.free_leaf_count == 0 and b.free_node_count == 0
     place(s, nodes=[(9, 0, 0, 0, 0)])
-    a = s.counters()
+    a = counters(s)
     assert (a.free_leaf_count - b.free_leaf_count, a.free_node_count - b.free_node_count) == (1, 1)
     assert query(s, [(0, 0, 0), (7, 7, 7), (8, 0, 0)]) == [1, 1, 0]
 
     s = svo()
     place(s, nodes=[(9, 0, 0, 0, 0)])
-    b = s.counters()
+    b = counters(s)
     place(s, nodes=[(8, 0, 0, 0, 0)])
-    a = s.counters()
+    a = counters(s)
     assert (a.free_leaf_count - b.free_leaf_count, a.free_node_count - b.free_node_count) == (0, 1)
     assert query(s, [(0, 0, 0), (15, 15, 15), (16, 0, 0)]) == [1, 1, 0]
 
     s = svo()
     place(s, leaves=[(key(0, 0, 0), 1, 0, 0, 0), (key(16, 0, 0), 1, 0, 0, 0)])
-    b = s.counters()
+    b = counters(s)
     assert b.free_leaf_count == 0 and b.free_node_count == 0
     place(s, nodes=[(5, 0, 0, 0, 0)])
-    a = s.counters()
+    a = counters(s)
     assert (a.free_leaf_count - b.free_leaf_count, a.free_node_count - b.free_node_count) == (2, 9)
     assert query(s, [(0, 0, 0), (64, 0, 0), (127, 127, 127), (128, 0, 0)]) == [1, 1, 1, 0]
 
