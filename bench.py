@@ -817,6 +817,8 @@ def run_serve(args, ws, rank, local, torch, vx, device):
         "serve_batches": int(st.batches),
         "serve_compactions": int(st.compactions),
         "serve_compact_ms_total": round(st.compact_ms, 1),
+        "serve_compact_share": round(st.compact_ms / 1e3 / span_s, 4),
+        "serve_p999_ms": round(float(np.percentile(lat_ms, 99.9)), 3),
         "serve_query_mismatches_vs_sequential": mism,
         "_c5": {"regions": regions, "blocks": blocks, "prims": prims, "offs": offs,
                 "committed": committed},

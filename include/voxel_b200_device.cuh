@@ -146,15 +146,21 @@ __device__ inline vx_ray_hit vx_dag_raycast(const vx_dag_view &v, const vx_ray &
   }
   uint32_t face = entry < 0 ? 0u : (d[entry] > 0.0f ? 2u * entry + 1u : 2u * entry);
   float t = t0;
-  const uint32_t root = *v.root;
+  /* path[k] = ref of the level-k cell holding the current voxel, valid for
+   * k <= l; a step keeps the cells that still hold the next voxel, so the
+   * walk resumes below the deepest common cell instead of at the root. */
+  uint32_t path[15]; /* depth <= 14 */
+  path[0] = *v.root;
+  uint32_t l = 0;
   const uint32_t limit = 3u * (uint32_t)W + 8u;
   for (uint32_t step = 0; step < limit; ++step) {
-    uint32_t ref = root, l = 0;
+    uint32_t ref = path[l];
     for (; l < D && ref >= 2u; ++l) {
       const uint32_t sh = D + 1 - l;
       const uint32_t c = (((uint32_t)vox[0] >> sh) & 1u) | ((((uint32_t)vox[1] >> sh) & 1u) << 1) |
                          ((((uint32_t)vox[2] >> sh) & 1u) << 2);
       ref = vx_dag_item_child(v.pool[l] + (ref - 2u), c);
+      path[l + 1] = ref;
     }
     int32_t side;
     if (ref == 1u) {
@@ -190,15 +196,21 @@ __device__ inline vx_ray_hit vx_dag_raycast(const vx_dag_view &v, const vx_ray &
     if (ax < 0 || !(tx <= ray.t_max)) return miss;
     const int32_t nv = d[ax] > 0.0f ? cmin[ax] + side : cmin[ax] - 1;
     if (nv < 0 || nv >= W) return miss;
+    uint32_t moved = (uint32_t)(vox[ax] ^ nv);
     for (int b = 0; b < 3; ++b) {
       if (b == ax || d[b] == 0.0f) continue;
       const float lo = (float)(d[b] > 0.0f ? vox[b] : cmin[b]);
       const float hi = (float)(d[b] > 0.0f ? cmin[b] + side - 1 : vox[b]);
       float f = floorf(__fadd_rn(o[b], __fmul_rn(tx, d[b])));
       f = f < lo ? lo : (f > hi ? hi : f);
+      moved |= (uint32_t)(vox[b] ^ (int32_t)f);
       vox[b] = (int32_t)f;
     }
     vox[ax] = nv;
+    /* The level-k cell (side 2^(D+2-k)) still holds the voxel iff no
+     * coordinate bit at or above D + 2 - k changed. */
+    const uint32_t keep = D + 1u - (31u - (uint32_t)__clz((int)moved));
+    if (keep < l) l = keep;
     t = tx;
     face = d[ax] > 0.0f ? 2u * ax + 1u : 2u * ax;
   }
