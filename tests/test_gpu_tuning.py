@@ -30,7 +30,7 @@ def to_dev(a, device):
 
 @pytest.mark.parametrize("key_bytes,key_bits,n,offset", [
     (4, 32, 1_000_003, 0), (4, 32, 100_000, 1), (4, 20, 3072 * 5, 0),
-    (8, 60, 700_001, 0), (8, 64, 65_537, 1), (8, 40, 2048 * 7, 0)])
+    (8, 60, 700_001, 0), (8, 64, 65_537, 1), (8, 40, 2048 * 7, 0), (8, 40, 2560 * 7, 0)])
 def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
     rng = np.random.default_rng(n + key_bits)
     dt = np.uint64 if key_bytes == 8 else np.uint32
@@ -39,10 +39,9 @@ def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
     vals = np.arange(n, dtype=np.uint32)
     ek, ev = oracle.stable_sort_pairs(keys, vals, key_bits)
     knob = "sort.items_u32" if key_bytes == 4 else "sort.items_u64"
-    for items, early, ballots, window in itertools.product(
-            vx.tuning_options(knob), vx.tuning_options("sort.early_counts"),
-            vx.tuning_options("sort.rank_ballots"), vx.tuning_options("sort.lookback_window")):
-        vx.set_tuning("sort.lookback_window", window)
+    for items, early, ballots in itertools.product(vx.tuning_options(knob),
+                                                   vx.tuning_options("sort.early_counts"),
+                                                   vx.tuning_options("sort.rank_ballots")):
         vx.set_tuning(knob, items)
         vx.set_tuning("sort.early_counts", early)
         vx.set_tuning("sort.rank_ballots", ballots)
@@ -51,11 +50,11 @@ def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
         vbuf = to_dev(np.concatenate([np.zeros(offset, np.uint32), vals]), cuda)
         dk, dv = kbuf[offset:], vbuf[offset:]
         vx.sort_pairs(dk, dv, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, window)
-        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early, ballots, window)
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots)
+        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early, ballots)
         dk = to_dev(keys.copy(), cuda)
         vx.sort_pairs(dk, None, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, window, "keys only")
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, "keys only")
 
 
 def rand_prims(rng, n, world, rmax):

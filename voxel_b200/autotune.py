@@ -6,11 +6,11 @@ Times every allowed value of each knob on a representative workload on the
 current GPU and writes the fastest settings to voxel_b200/tuning/<device>.json,
 which the library applies when it is first loaded on that kind of device:
 
-  * sort.items_u32 / sort.items_u64 / sort.early_counts / sort.rank_ballots /
-    sort.lookback_window: radix-sort partition tile size (items per thread,
-    hence blocks per SM), the predecessor tiles one look-back round trip reads,
+  * sort.items_u32 / sort.items_u64 / sort.early_counts / sort.rank_ballots:
+    radix-sort partition tile size (items per thread, hence blocks per SM),
     whether a tile publishes its digit counts before or after ranking, and
-    whether keys are ranked with per-bit ballots or match_any; timed on 2^26
+    whether keys are ranked with per-bit ballots or a shared-memory atomic
+    OR per digit; timed on 2^26
     u32 and 2^25 60-bit u64 key/value pairs;
   * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks /
     edit.leafparent_lanes: the primitive-list length above which a work item
@@ -81,44 +81,40 @@ def tune_sort(n32: int, n64: int, reps: int, log) -> tuple[dict, dict]:
         restore()
         vx.sort_pairs(k, v, bits, ws)
         ref_k, ref_v = k.clone(), v.clone()
-        for items, early, ballots, window in itertools.product(
+        for items, early, ballots in itertools.product(
                 vx.tuning_options(knob), vx.tuning_options("sort.early_counts"),
-                vx.tuning_options("sort.rank_ballots"), vx.tuning_options("sort.lookback_window")):
+                vx.tuning_options("sort.rank_ballots")):
             vx.set_tuning(knob, items)
             vx.set_tuning("sort.early_counts", early)
             vx.set_tuning("sort.rank_ballots", ballots)
-            vx.set_tuning("sort.lookback_window", window)
             restore()
             vx.sort_pairs(k, v, bits, ws)
             same = bool(torch.equal(k, ref_k) and torch.equal(v, ref_v))
             ms = _time(lambda: vx.sort_pairs(k, v, bits, ws), reps, restore) if same else None
-            times[(label, items, early, ballots, window)] = ms
-            log(f"  sort {label} items={items} early={early} ballots={ballots} "
-                f"window={window}: " + (f"{ms:.3f} ms" if same else "DIFFERENT OUTPUT (not used)"))
+            times[(label, items, early, ballots)] = ms
+            log(f"  sort {label} items={items} early={early} ballots={ballots}: "
+                + (f"{ms:.3f} ms" if same else "DIFFERENT OUTPUT (not used)"))
     vx.reset_tuning()
-    # early / ballots / window are shared by both key widths: pick the triple
-    # with the least total time (each width at its best items); then items
-    # per width.
+    # early / ballots are shared by both key widths: pick the pair with the
+    # least total time (each width at its best items); then items per width.
     best: dict = {}
     score = {}
-    for early, ballots, window in itertools.product(vx.tuning_options("sort.early_counts"),
-                                                    vx.tuning_options("sort.rank_ballots"),
-                                                    vx.tuning_options("sort.lookback_window")):
+    for early, ballots in itertools.product(vx.tuning_options("sort.early_counts"),
+                                            vx.tuning_options("sort.rank_ballots")):
         tot = 0.0
         for label, (_, _, knob) in cases.items():
-            cand = [times[(label, i, early, ballots, window)] for i in vx.tuning_options(knob)]
+            cand = [times[(label, i, early, ballots)] for i in vx.tuning_options(knob)]
             cand = [c for c in cand if c is not None]
             tot = tot + min(cand) if cand else float("inf")
-        score[(early, ballots, window)] = tot
-    early, ballots, window = min(score, key=score.get)
+        score[(early, ballots)] = tot
+    early, ballots = min(score, key=score.get)
     best["sort.early_counts"], best["sort.rank_ballots"] = early, ballots
-    best["sort.lookback_window"] = window
     for label, (_, _, knob) in cases.items():
-        opts = {i: times[(label, i, early, ballots, window)] for i in vx.tuning_options(knob)}
+        opts = {i: times[(label, i, early, ballots)] for i in vx.tuning_options(knob)}
         opts = {i: t for i, t in opts.items() if t is not None}
         best[knob] = min(opts, key=opts.get)
-    return best, {f"{l} items={i} early={e} ballots={b} window={w}": t
-                  for (l, i, e, b, w), t in times.items()}
+    return best, {f"{l} items={i} early={e} ballots={b}": t
+                  for (l, i, e, b), t in times.items()}
 
 
 def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int,

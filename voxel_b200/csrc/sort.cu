@@ -50,7 +50,7 @@ template <> struct Shape<uint32_t> {
   static constexpr uint32_t kSmall = 12, kLarge = 16;
 };
 template <> struct Shape<uint64_t> {
-  static constexpr uint32_t kSmall = 8, kLarge = 12;
+  static constexpr uint32_t kSmall = 8, kLarge = 10;
 };
 template <uint32_t Items, class K> constexpr uint32_t min_blocks() {
   return Items == Shape<K>::kSmall ? 4u : 3u;
@@ -177,10 +177,10 @@ __device__ __forceinline__ uint32_t block_exclusive_256(uint32_t v,
 // that one has not published its count (bounded by the GPU timer); then it
 // publishes this tile's inclusive count.  Returns the digit's count over all
 // earlier tiles.
-template <uint32_t kWindow>
 __device__ __forceinline__ uint32_t digit_lookback(uint32_t *records, uint32_t tile, uint32_t t,
                                                    uint32_t tile_count, uint32_t *status) {
   if (tile == 0) return 0;
+  constexpr uint32_t kWindow = 8;
   uint32_t exclusive = 0;
   const uint64_t t0 = global_ns();
   int64_t pred = static_cast<int64_t>(tile) - 1;
@@ -225,10 +225,16 @@ __device__ __forceinline__ uint32_t digit_lookback(uint32_t *records, uint32_t t
 // before ranking, so later tiles' look-backs wait less; otherwise they are
 // published after ranking, from the per-warp counts.
 // Ballots = find a key's peers (the lanes of its warp with the same digit)
-// with one ballot per digit bit (warp-level multi-split, Adinets & Merrill)
-// instead of __match_any_sync, which executes on a narrow pipe and bounds
-// the pass when every key is ranked with it.
-template <class K, bool HasValues, uint32_t kItems, bool Early, bool Ballots, uint32_t kWindow>
+// with one ballot per digit bit (warp-level multi-split, Adinets & Merrill);
+// otherwise every lane ORs its bit into a per-warp, per-digit word in shared
+// memory and reads the word back (three shared-memory operations per key in
+// place of eight ballots and their selects).
+//
+// The pass is bound by instruction issue, so the per-key work is kept short:
+// a full tile (every tile but the last) runs without validity tests, 32-bit
+// indices throughout, two ranks share a register, and one table gives each
+// (warp, digit) its tile-local base.
+template <class K, bool HasValues, uint32_t kItems, bool Early, bool Ballots>
 __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     partition_kernel(const K *__restrict__ in_keys,
                      const uint32_t *__restrict__ in_vals,
@@ -240,11 +246,13 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
   constexpr uint32_t kTile = kBlock * kItems;
   constexpr uint32_t kKeyBytes = kTile * sizeof(K);
   constexpr uint32_t kValBytes = HasValues ? kTile * 4u : 0u;
+  static_assert(kTile <= 0xffffu, "ranks are 16-bit");
   __shared__ uint64_t s_bar;
   __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_warp_hist[kWarps][kBins];
+  // per (warp, digit): the warp's count, then its tile-local base
+  __shared__ uint16_t s_warp_base[kWarps][kBins];
+  __shared__ uint32_t s_match[Ballots ? 1 : kWarps][Ballots ? 1 : kBins];
   __shared__ uint32_t s_count[Early ? kBins : 1];
-  __shared__ uint32_t s_digit_off[kBins];
   __shared__ uint32_t s_global[kBins];
   __shared__ uint32_t s_tmp[kWarps];
   // The tile arrives here (input order), and later holds it sorted by digit.
@@ -263,15 +271,21 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
       if (HasValues) bulk_load(s_vals, in_vals + b, kValBytes, &s_bar);
     }
   }
+  // Where each digit's run of this pass starts (independent of the tile).
+  const uint32_t hist_t = pass_hist[t];
 #pragma unroll
-  for (uint32_t w = 0; w < kWarps; ++w) s_warp_hist[w][t] = 0;
+  for (uint32_t w = 0; w < kWarps; ++w) s_warp_base[w][t] = 0;
+  if (!Ballots) {
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) s_match[w][t] = 0;
+  }
   if (Early) s_count[t] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const uint64_t tile_base = static_cast<uint64_t>(tile) * kTile;
-  const uint32_t valid_in_tile =
-      count - tile_base < kTile ? static_cast<uint32_t>(count - tile_base) : kTile;
-  if (aligned && valid_in_tile == kTile) {
+  const uint32_t tile_base = tile * kTile; // count < 2^30
+  const uint32_t valid_in_tile = count - tile_base < kTile ? count - tile_base : kTile;
+  const bool full = valid_in_tile == kTile;
+  if (aligned && full) {
     if (!mbar_wait(&s_bar, 0)) {
       // Never expected: report, let the copies land, give up on this tile.
       if (t == 0) set_status(status, kDevTimeout);
@@ -286,38 +300,42 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
     __syncthreads();
   }
   const uint32_t warp_first = warp * kWarp * kItems; // tile-local index of item 0
-  const uint64_t warp_base = tile_base + warp_first;
+  // Item i of this lane is tile-local key warp_first + i * 32 + lane; a lane
+  // past the end of a partial tile holds no key (digit kBins).
+  auto valid = [&](uint32_t i) { return full || warp_first + i * kWarp + lane < valid_in_tile; };
 
   K key[kItems];
   uint32_t val[kItems];
-  uint32_t rank2[(kItems + 1) / 2]; // two 16-bit ranks per register
+  uint32_t rank2[(kItems + 1) / 2]; // ranks within the warp's keys of a digit, 16 bits each
 #pragma unroll
   for (uint32_t i = 0; i < kItems; ++i) {
     const uint32_t j = warp_first + i * kWarp + lane;
-    key[i] = j < valid_in_tile ? s_keys[j] : K(0);
-    val[i] = HasValues && j < valid_in_tile ? s_vals[j] : 0u;
+    key[i] = valid(i) ? s_keys[j] : K(0);
+    val[i] = HasValues && valid(i) ? s_vals[j] : 0u;
   }
 
   uint32_t *rec = records + static_cast<size_t>(tile) * kBins + t;
   if (Early) {
 #pragma unroll
     for (uint32_t i = 0; i < kItems; ++i)
-      if (warp_base + i * kWarp + lane < count)
-        atomicAdd(&s_count[digit_of(key[i], shift, mask)], 1u);
+      if (valid(i)) atomicAdd(&s_count[digit_of(key[i], shift, mask)], 1u);
     __syncthreads();
     st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | s_count[t]);
   }
 
-  // Warp-level multi-split: rank each key among the warp's keys of its digit.
+  // Rank each key among the warp's earlier keys of its digit (stable: the
+  // order of items, then of lanes).
 #pragma unroll
   for (uint32_t i = 0; i < kItems; ++i) {
-    const uint64_t idx = warp_base + i * kWarp + lane;
-    const bool valid = idx < count;
-    const uint32_t d = valid ? digit_of(key[i], shift, mask) : kBins;
+    const bool v = valid(i);
+    const uint32_t d = v ? digit_of(key[i], shift, mask) : kBins;
     uint32_t peers;
     if (Ballots) {
-      const uint32_t vb = __ballot_sync(kFullMask, valid);
-      peers = valid ? vb : ~vb;
+      peers = kFullMask;
+      if (!full) { // lanes without a key form their own group
+        const uint32_t vb = __ballot_sync(kFullMask, v);
+        peers = v ? vb : ~vb;
+      }
 #pragma unroll
       for (uint32_t b = 0; b < kRadixBits; ++b) {
         const bool bit = (d >> b) & 1u;
@@ -325,58 +343,67 @@ __global__ void __launch_bounds__(kBlock, (min_blocks<kItems, K>()))
         peers &= bit ? bb : ~bb;
       }
     } else {
-      peers = __match_any_sync(kFullMask, d);
+      if (v) atomicOr(&s_match[warp][d], 1u << lane);
+      __syncwarp();
+      peers = v ? s_match[warp][d] : 0u;
     }
-    const uint32_t below = __popc(peers & lanemask_lt());
-    const uint32_t leader = 31u - __clz(peers);
     uint32_t pre = 0;
-    if (valid) pre = s_warp_hist[warp][d];
-    const uint32_t rk = pre + below;
+    if (v) pre = s_warp_base[warp][d];
+    __syncwarp();
+    if (v && lane == 31u - __clz(peers)) { // the digit's last lane
+      s_warp_base[warp][d] = static_cast<uint16_t>(pre + __popc(peers));
+      if (!Ballots) s_match[warp][d] = 0u;
+    }
+    __syncwarp();
+    const uint32_t rk = pre + __popc(peers & lanemask_lt());
     if (i & 1u) rank2[i / 2] |= rk << 16;
     else rank2[i / 2] = rk;
-    __syncwarp();
-    if (valid && lane == leader) s_warp_hist[warp][d] = pre + __popc(peers);
-    __syncwarp();
   }
   __syncthreads();
 
-  // Thread t owns digit t: warp offsets, tile count, tile-local digit offset.
-  uint32_t tile_count = 0;
+  // Thread t owns digit t: the warps' counts become tile-local bases.
+  uint32_t wc[kWarps], tile_count = 0;
 #pragma unroll
   for (uint32_t w = 0; w < kWarps; ++w) {
-    const uint32_t c = s_warp_hist[w][t];
-    s_warp_hist[w][t] = tile_count;
-    tile_count += c;
+    wc[w] = s_warp_base[w][t];
+    tile_count += wc[w];
   }
   if (!Early) st_relaxed_u32(rec, (tile == 0 ? kRecInc : kRecAgg) | tile_count);
   const uint32_t digit_off = block_exclusive_256(tile_count, s_tmp);
-  const uint32_t global_start = block_exclusive_256(pass_hist[t], s_tmp);
-  s_digit_off[t] = digit_off;
-
-  const uint32_t exclusive = digit_lookback<kWindow>(records, tile, t, tile_count, status);
+  {
+    uint32_t run = digit_off;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) {
+      s_warp_base[w][t] = static_cast<uint16_t>(run);
+      run += wc[w];
+    }
+  }
+  const uint32_t global_start = block_exclusive_256(hist_t, s_tmp);
+  const uint32_t exclusive = digit_lookback(records, tile, t, tile_count, status);
   s_global[t] = global_start + exclusive - digit_off;
   __syncthreads();
 
-  // Sort the tile in shared memory.
+  // Sort the tile in shared memory (its input copy is in registers now).
 #pragma unroll
   for (uint32_t i = 0; i < kItems; ++i) {
-    const uint64_t idx = warp_base + i * kWarp + lane;
-    if (idx < count) {
-      const uint32_t d = digit_of(key[i], shift, mask);
-      const uint32_t rk = (i & 1u) ? (rank2[i / 2] >> 16) : (rank2[i / 2] & 0xffffu);
-      const uint32_t pos = s_digit_off[d] + s_warp_hist[warp][d] + rk;
-      s_keys[pos] = key[i];
-      if (HasValues) s_vals[pos] = val[i];
-    }
+    if (!valid(i)) continue;
+    const uint32_t d = digit_of(key[i], shift, mask);
+    const uint32_t rk = (i & 1u) ? (rank2[i / 2] >> 16) : (rank2[i / 2] & 0xffffu);
+    const uint32_t pos = s_warp_base[warp][d] + rk;
+    s_keys[pos] = key[i];
+    if (HasValues) s_vals[pos] = val[i];
   }
   __syncthreads();
 
-  // Write the tile's runs out in order.
-#pragma unroll 4
-  for (uint32_t j = t; j < valid_in_tile; j += kBlock) {
+  // Write the tile's runs out in order: consecutive threads, consecutive
+  // addresses of each run.  dst stays below count even after a look-back
+  // timeout (a partial prefix is a lower bound of the true one).
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t j = r * kBlock + t;
+    if (!full && j >= valid_in_tile) break;
     const K k = s_keys[j];
     const uint32_t dst = s_global[digit_of(k, shift, mask)] + j;
-    if (dst >= count) continue; // only reachable after a look-back timeout
     out_keys[dst] = k;
     if (HasValues) out_vals[dst] = s_vals[j];
   }
@@ -418,7 +445,6 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
                      static_cast<int64_t>(Shape<K>::kLarge);
   const bool early = tune::get(tune::kSortEarlyCounts) != 0;
   const bool ballots = tune::get(tune::kSortRankBallots) != 0;
-  const uint32_t window = static_cast<uint32_t>(tune::get(tune::kSortLookbackWindow));
   const uint32_t items = large ? Shape<K>::kLarge : Shape<K>::kSmall;
   const uint32_t tiles = ceil_div(count, kBlock * items);
   K *src_k = keys, *dst_k = static_cast<K *>(l.tmp_keys);
@@ -433,17 +459,12 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
                                            info.mask[p], l.hist + p * kBins, rec,
                                            l.counters + 2 + p, l.counters + 1, aligned);
     };
-    // (values, items, early, ballots, window) -> one of 48 instantiations
-    auto by_window = [&](auto hv, auto it, auto ea, auto ba) {
-      constexpr bool HV = decltype(hv)::value, E = decltype(ea)::value, B = decltype(ba)::value;
-      constexpr uint32_t I = decltype(it)::value;
-      if (window == 32) launch(partition_kernel<K, HV, I, E, B, 32>);
-      else if (window == 16) launch(partition_kernel<K, HV, I, E, B, 16>);
-      else launch(partition_kernel<K, HV, I, E, B, 8>);
-    };
+    // (values, items, early, ballots) -> one of 16 instantiations
     auto by_ballots = [&](auto hv, auto it, auto ea) {
-      if (ballots) by_window(hv, it, ea, std::true_type{});
-      else by_window(hv, it, ea, std::false_type{});
+      constexpr bool HV = decltype(hv)::value, E = decltype(ea)::value;
+      constexpr uint32_t I = decltype(it)::value;
+      if (ballots) launch(partition_kernel<K, HV, I, E, true>);
+      else launch(partition_kernel<K, HV, I, E, false>);
     };
     auto by_early = [&](auto hv, auto it) {
       if (early) by_ballots(hv, it, std::true_type{});

@@ -9,9 +9,9 @@ namespace vx::tune {
 
 enum Id : uint32_t {
   kSortItemsU32,    // partition items per thread, u32 keys: 12 or 16
-  kSortItemsU64,    // partition items per thread, u64 keys: 8 or 12
+  kSortItemsU64,    // partition items per thread, u64 keys: 8 or 10
   kSortEarlyCounts, // publish tile digit counts before ranking: 0 or 1
-  kSortRankBallots, // rank keys with per-bit ballots (1) or match_any (0)
+  kSortRankBallots, // rank keys with per-bit ballots (1) or shared-memory atomic OR (0)
   kEditBigItem,     // items with more primitives go to the block-per-item expansion
   kEditBlocksPerSm, // grid of the edit pipelines' item kernels, in blocks per SM
   kEditLeafparentBlocks, // resident blocks the DAG leaf-parent kernel is built for
@@ -20,7 +20,6 @@ enum Id : uint32_t {
   kEditSmallMaxPrims, // batches of at most this many primitives run as one cooperative kernel
   kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
   kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
-  kSortLookbackWindow, // predecessor tiles a partition look-back reads per round trip: 8, 16 or 32
   kKnobCount
 };
 
