@@ -38,6 +38,25 @@ def test_batched_primitives_match_oracle(cuda, depth, n, seed):
     assert canon(dag) == oracle.Grid(depth).apply_prims(prims).dag()
 
 
+def test_large_spheres_match_sparse_oracle(cuda):
+    """Sphere leaf masks take single precision up to radius 1024 and 32-bit
+    integers above: radii on both sides of the switch (and near the world's
+    size), adds and removes, against the sparse CPU oracle at 4096^3."""
+    depth = 10
+    world = 4 << depth
+    rng = np.random.default_rng(77)
+    radii = [1, 2, 3, 700, 1020, 1023, 1024, 1025, 1026, 1100, 1500, 2047, 3000]
+    p = np.zeros(len(radii), oracle.PRIM_DTYPE)
+    for i, r in enumerate(radii):
+        c = rng.integers(-r // 2, world + r // 2, 3)
+        op = int(i % 3 != 2)
+        p[i] = (c, (r, 0, 0), (op << 8), 0)
+    dag = vx.HashDag(depth, max_nodes=1 << 22, arena_bytes=1 << 30)
+    dag.apply_primitives(vx.prims_to_device(p, cuda))
+    assert dag.status() == 0
+    assert canon(dag) == oracle.Sparse(depth, None, p).dag()
+
+
 @pytest.mark.parametrize("depth,caves", [(4, False), (5, True), (7, True)])
 def test_terrain_build_matches_oracle(cuda, depth, caves):
     t = oracle.terrain(seed=1, scale=1 if depth <= 6 else 2, caves=caves)

@@ -50,21 +50,25 @@ __host__ __device__ __forceinline__ uint64_t child_cell(uint64_t p, uint32_t c) 
 // definitions of vx_workload.h; both give identical results.
 constexpr int64_t kFastRadius = int64_t(1) << 14;
 
+// Cells lie in [0, 2^16] per axis (depth <= 14); a centre clamped to
+// [-2^16, 2^18] keeps every outcome (a clamped centre is still more than
+// 2^14 > r away from every cell), so the differences fit in 32 bits.
 __device__ __forceinline__ uint32_t sphere_classify32(const vx_primitive &p, int64_t ox,
                                                       int64_t oy, int64_t oz, int64_t n) {
-  const int64_t r = p.r[0];
-  const int64_t lo[3] = {ox, oy, oz};
+  const int32_t r = static_cast<int32_t>(p.r[0]);
+  const int32_t lo[3] = {static_cast<int32_t>(ox), static_cast<int32_t>(oy),
+                         static_cast<int32_t>(oz)};
+  const int32_t n1 = static_cast<int32_t>(n) - 1;
   uint32_t near2 = 0, far2 = 0;
   bool far_in = true;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int64_t c = p.c[a], a0 = lo[a], a1 = lo[a] + n - 1;
-    const int64_t d = c < a0 ? a0 - c : (c > a1 ? c - a1 : 0);
+    const int32_t c = max(-(1 << 16), min(1 << 18, p.c[a]));
+    const int32_t a0 = lo[a], a1 = lo[a] + n1;
+    const int32_t d = c < a0 ? a0 - c : (c > a1 ? c - a1 : 0);
     if (d > r) return VX_CELL_EMPTY;
     near2 += static_cast<uint32_t>(d) * static_cast<uint32_t>(d);
-    const int64_t f0 = c - a0 > 0 ? c - a0 : a0 - c;
-    const int64_t f1 = c - a1 > 0 ? c - a1 : a1 - c;
-    const int64_t f = f0 > f1 ? f0 : f1;
+    const int32_t f = max(abs(c - a0), abs(c - a1));
     if (f > r) far_in = false;
     else far2 += static_cast<uint32_t>(f) * static_cast<uint32_t>(f);
   }
@@ -101,6 +105,49 @@ __device__ __forceinline__ uint64_t sphere_leaf_mask32(const vx_primitive &p, in
     }
   }
   return m;
+}
+
+// The same mask for radii up to kFloatMaskRadius, in single precision: the
+// caller has classified the leaf MIXED, so every coordinate difference is at
+// most r + 3 and every value below is an integer under 2^22 in magnitude,
+// which each single-precision operation (contracted or not) keeps exact.  A
+// voxel is inside when sx <= r^2 - sy - sz, i.e. when sx - (r^2 + 1 - sy -
+// sz) is negative; an exact zero is +0, so the sign bit is the voxel's bit.
+// The sign bits of a row's four voxels are gathered by byte permutes and one
+// multiply (bits 7, 15, 23, 31 land in bits 28-31 with no carries into
+// them), which moves most of the work off the integer pipe.
+constexpr uint32_t kFloatMaskRadius = 1024;
+
+__device__ __forceinline__ uint64_t sphere_leaf_mask_f32(const vx_primitive &p, int64_t ox,
+                                                        int64_t oy, int64_t oz) {
+  const float r = static_cast<float>(p.r[0]);
+  const float fx = static_cast<float>(static_cast<int32_t>(ox - p.c[0]));
+  const float fy = static_cast<float>(static_cast<int32_t>(oy - p.c[1]));
+  const float fz = static_cast<float>(static_cast<int32_t>(oz - p.c[2]));
+  float sx[4], sy[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float a = fx + static_cast<float>(i), b = fy + static_cast<float>(i);
+    sx[i] = a * a;
+    sy[i] = b * b;
+  }
+  const float r2p1 = r * r + 1.0f;
+  uint32_t half[2] = {0u, 0u};
+#pragma unroll
+  for (int z = 0; z < 4; ++z) {
+    const float c = fz + static_cast<float>(z);
+    const float tz = r2p1 - c * c;
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      const float t = tz - sy[y];
+      const uint32_t d01 = __byte_perm(__float_as_uint(sx[0] - t), __float_as_uint(sx[1] - t), 0x0073);
+      const uint32_t d23 = __byte_perm(__float_as_uint(sx[2] - t), __float_as_uint(sx[3] - t), 0x0073);
+      const uint32_t w = __byte_perm(d01, d23, 0x5410); // byte x = the top byte of voxel x's value
+      const uint32_t row = ((w & 0x80808080u) * 0x00204081u) >> 28;
+      half[z >> 1] |= row << (4 * y + 16 * (z & 1));
+    }
+  }
+  return (static_cast<uint64_t>(half[1]) << 32) | half[0];
 }
 
 // Classify primitive p against the voxel cube [o, o + n)^3.  Kernels that
@@ -146,6 +193,8 @@ __device__ __forceinline__ uint64_t leaf_mask(const vx_primitive &p,
     if (p.c[0] != ox || p.c[1] != oy || p.c[2] != oz) return 0;
     return static_cast<uint64_t>(p.r[0]) | (static_cast<uint64_t>(p.r[1]) << 32);
   }
+  if (shape == VX_SHAPE_SPHERE && p.r[0] <= kFloatMaskRadius)
+    return sphere_leaf_mask_f32(p, ox, oy, oz);
   if (shape == VX_SHAPE_SPHERE && p.r[0] < kFastRadius)
     return sphere_leaf_mask32(p, ox, oy, oz);
   return vx_prim_leaf_mask(&p, ox, oy, oz);
