@@ -319,7 +319,11 @@ __global__ void mark_pools_kernel(Tables t) {
 // MinBlocks (the knob "edit.leafparent_blocks") trades registers for
 // resident blocks: the kernel is bound by chains of dependent loads, so more
 // items in flight can outweigh a few spilled values.
-template <bool Terrain, uint32_t Lanes>
+__device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l);
+
+// Climb: after storing an item's result, finish its ancestors (the single
+// cooperative kernel's bottom-up build, without level barriers).
+template <bool Terrain, uint32_t Lanes, bool Climb = false>
 __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
   static_assert(Lanes == 2 || Lanes == 4 || Lanes == 8, "2, 4 or 8 lanes per item");
   constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
@@ -457,6 +461,7 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
         r = node_find_or_insert<HashedChildWords, false>(x.t, l, HashedChildWords{{header, child}, h});
       }
       x.a.items[base + wi].result = r;
+      if (Climb) finish_upwards(x, it.result, l); // it.result: the parent's index
     }
   }
 }
@@ -467,31 +472,68 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
 }
 
 // Bottom-up rebuild of level l from its children's results.
+// The rebuilt ref of one item at inner level l from its children's results.
+__device__ __forceinline__ uint32_t build_item(const Ctx &x, uint32_t l, const Item &it) {
+  const uint32_t cm = it.masks & 0xffu, km = (it.masks >> 8) & 0xffu,
+                 kf = (it.masks >> 16) & 0xffu;
+  uint32_t child[8];
+  uint32_t k = 0;
+#pragma unroll
+  for (uint32_t c = 0; c < 8; ++c) {
+    const uint32_t bit = 1u << c;
+    if (cm & bit) child[c] = x.a.items[it.child_base + k++].result;
+    else if (km & bit) child[c] = (kf & bit) ? kFullRef : kEmptyRef;
+    else child[c] = child_ref(x.t, l, it.old, c);
+  }
+  // Every child kept its ref: the node is the old one (refs are canonical).
+  bool same = true;
+#pragma unroll
+  for (uint32_t c = 0; c < 8; ++c)
+    if ((cm | km) & (1u << c)) same = same && child[c] == child_ref(x.t, l, it.old, c);
+  return same ? it.old : canon_node(x.t, l, child);
+}
+
 __device__ __forceinline__ void build_body(Ctx x, uint32_t l, Blocks blk) {
   Header *h = x.t.hdr;
   if (edit_failed(h)) return;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
   for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
-    const Item it = x.a.items[base + i];
-    const uint32_t cm = it.masks & 0xffu, km = (it.masks >> 8) & 0xffu,
-                   kf = (it.masks >> 16) & 0xffu;
-    uint32_t child[8];
-    uint32_t k = 0;
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      const uint32_t bit = 1u << c;
-      if (cm & bit) child[c] = x.a.items[it.child_base + k++].result;
-      else if (km & bit) child[c] = (kf & bit) ? kFullRef : kEmptyRef;
-      else child[c] = child_ref(x.t, l, it.old, c);
+       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x)
+    x.a.items[base + i].result = build_item(x, l, x.a.items[base + i]);
+}
+
+// Bottom-up without level barriers: an item at level l has just stored its
+// result; count it off its parent's pending children (a release), and when
+// it was the last one rebuild the parent (after an acquire) and go on up.
+__device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l) {
+  while (parent != kNoParent) {
+    __threadfence();
+    if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
+    __threadfence();
+    --l;
+    const Item it = x.a.items[parent];
+    x.a.items[parent].result = build_item(x, l, it);
+    parent = it.result; // the grandparent, stored there until now
+  }
+}
+
+// Items below the leaf-parent level with no child items (every child
+// unchanged or uniform) have nothing to wait for: they rebuild at once and
+// start their own climb.
+__device__ __forceinline__ void rebuild_childless_body(Ctx x, Blocks blk) {
+  Header *h = x.t.hdr;
+  if (edit_failed(h)) return;
+  for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
+    const uint32_t W = h->item_count[l];
+    const uint32_t base = h->item_off[l];
+    for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
+      const Item it = x.a.items[base + i];
+      if (it.masks & 0xffu) continue;
+      x.a.items[base + i].result = build_item(x, l, it);
+      finish_upwards(x, it.result, l);
     }
-    // Every child kept its ref: the node is the old one (refs are canonical).
-    bool same = true;
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c)
-      if ((cm | km) & (1u << c)) same = same && child[c] == child_ref(x.t, l, it.old, c);
-    x.a.items[base + i].result = same ? it.old : canon_node(x.t, l, child);
   }
 }
 
@@ -545,12 +587,12 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, Pl
       grid.sync();
     }
   }
-  leafparent_body<false, Lanes>(x, blk);
+  // The bottom-up build without level barriers: the leaf-parent items and
+  // the childless items of the levels above finish their ancestors, each
+  // item rebuilt by the last of its children to finish.
+  leafparent_body<false, Lanes, true>(x, blk);
+  rebuild_childless_body(x, blk);
   grid.sync();
-  for (uint32_t r = x.t.depth - 1; r > 0; --r) {
-    build_body(x, r - 1, blk);
-    grid.sync();
-  }
   if (blk.id == 0 && threadIdx.x == 0) {
     Header *h = x.t.hdr;
     if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;

@@ -200,16 +200,22 @@ __device__ __forceinline__ uint64_t leaf_mask(const vx_primitive &p,
   return vx_prim_leaf_mask(&p, ox, oy, oz);
 }
 
-// One work item of the top-down expansion (32 bytes).
+// One work item of the top-down expansion (32 bytes).  Two fields change
+// meaning over an edit: `pstart`, once the item is expanded, counts its child
+// items that have not finished yet, and `result`, until the item is rebuilt,
+// holds its parent's item index (kNoParent for the root), so that a
+// bottom-up build can run without level barriers: the last child to finish
+// rebuilds its parent.
 struct Item {
   uint64_t cell;
   uint32_t old;        // ref (DAG) or slot word (SVO) of the previous content
-  uint32_t pstart;     // first pair of this item in its level's pair array
+  uint32_t pstart;     // first pair of this item in its level's pair array; then pending children
   uint32_t pcount;     // number of pairs
   uint32_t child_base; // first child item at the next level
   uint32_t masks;      // child_mask | const_mask << 8 | const_full << 16
-  uint32_t result;     // rebuilt ref / slot word
+  uint32_t result;     // parent index until rebuilt, then the rebuilt ref / slot word
 };
+constexpr uint32_t kNoParent = 0xffffffffu;
 static_assert(sizeof(Item) == 32, "Item is 32 bytes");
 
 // Per-edit device bookkeeping (one per structure).
@@ -307,6 +313,7 @@ __device__ __forceinline__ void init_body(EditCtx x, uint32_t root_old, Blocks b
       it.old = root_old == kUseHeaderRoot ? h->root : root_old;
       it.pstart = 0;
       it.pcount = n;
+      it.result = kNoParent;
       x.a.items[0] = it;
     }
   }
@@ -529,6 +536,7 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
       ci.old = last_full >= 0 ? const_val : old_child;
       ci.pstart = my_pairs;
       ci.pcount = cnt;
+      ci.result = static_cast<uint32_t>(base + wi);
       x.a.items[next_base + item_off + inc_items - 1] = ci;
       uint32_t j = 0;
       if (it.pcount <= 32u) {
@@ -548,6 +556,7 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
     if (c == 0) {
       x.a.items[base + wi].child_base = next_base + item_off;
       x.a.items[base + wi].masks = child_mask | (const_mask << 8) | (const_full << 16);
+      x.a.items[base + wi].pstart = __popc(child_mask); // the pairs were read above
     }
   }
 }
@@ -682,6 +691,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
         set_status(&h->status, kDevCapacity);
       x.a.items[base + wi].child_base = next_base + s_item_base;
       x.a.items[base + wi].masks = cm | (km << 8) | (kf << 16);
+      x.a.items[base + wi].pstart = __popc(cm); // every thread holds its own copy of it
       s_room = ld_relaxed_u32(&h->status) == kDevOk;
     }
     __syncthreads();
@@ -694,6 +704,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
       ci.old = s_last[t] >= 0 ? s_const[t] : pol.child(l, it.old, t);
       ci.pstart = s_pair_base + s_start[t];
       ci.pcount = s_cnt[t];
+      ci.result = static_cast<uint32_t>(base + wi);
       x.a.items[next_base + s_item_base + k] = ci;
     }
     // Walk 3: order-preserving compaction, one Threads-pair chunk at a time.

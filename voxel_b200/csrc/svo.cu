@@ -190,7 +190,11 @@ __device__ __forceinline__ void check_capacity_body(Tables t) {
 }
 __global__ void check_capacity_kernel(Tables t) { check_capacity_body(t); }
 
-template <bool Terrain>
+__device__ void finish_upwards(const EditCtx &x, const Tables &t, uint32_t parent, uint32_t l);
+
+// Climb: after storing an item's word, finish its ancestors (the single
+// cooperative kernel's bottom-up build, without level barriers).
+template <bool Terrain, bool Climb = false>
 __device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk) {
   Header *h = x.hdr;
   if (edit_failed(h)) return;
@@ -301,8 +305,10 @@ __device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk)
 #pragma unroll
     for (uint32_t k = 0; k < 8; ++k)
       child[k] = __shfl_sync(kFullMask, result, (lane & ~7u) + k);
-    if (have && c == 0)
+    if (have && c == 0) {
       x.a.items[base + wi].result = finish_node(t, it.old, child, l == 0);
+      if (Climb) finish_upwards(x, t, it.result, l); // it.result: the parent's index
+    }
   }
 }
 
@@ -311,30 +317,69 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t)
   leafparent_body<Terrain>(x, t, launch_blocks());
 }
 
+// The rebuilt word of one item at inner level l from its children's results.
+__device__ __forceinline__ uint32_t build_item(const EditCtx &x, const Tables &t, uint32_t l,
+                                               const Item &it) {
+  const uint32_t cm = it.masks & 0xffu;
+  uint32_t child[8];
+  if (it.old & kChild) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(t.nodes + static_cast<size_t>(it.old & kIndex) * 8u);
+    const uint4 a = src[0], b = src[1];
+    child[0] = a.x; child[1] = a.y; child[2] = a.z; child[3] = a.w;
+    child[4] = b.x; child[5] = b.y; child[6] = b.z; child[7] = b.w;
+  } else {
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) child[c] = it.old;
+  }
+  uint32_t k = 0;
+#pragma unroll
+  for (uint32_t c = 0; c < 8; ++c)
+    if (cm & (1u << c)) child[c] = x.a.items[it.child_base + k++].result;
+  return finish_node(t, it.old, child, l == 0);
+}
+
 __device__ __forceinline__ void build_body(EditCtx x, Tables t, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
   if (edit_failed(h)) return;
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
   for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
-    const Item it = x.a.items[base + i];
-    const uint32_t cm = it.masks & 0xffu;
-    uint32_t child[8];
-    if (it.old & kChild) {
-      const uint4 *src = reinterpret_cast<const uint4 *>(t.nodes + static_cast<size_t>(it.old & kIndex) * 8u);
-      const uint4 a = src[0], b = src[1];
-      child[0] = a.x; child[1] = a.y; child[2] = a.z; child[3] = a.w;
-      child[4] = b.x; child[5] = b.y; child[6] = b.z; child[7] = b.w;
-    } else {
-#pragma unroll
-      for (uint32_t c = 0; c < 8; ++c) child[c] = it.old;
+       i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x)
+    x.a.items[base + i].result = build_item(x, t, l, x.a.items[base + i]);
+}
+
+// Bottom-up without level barriers (the single cooperative kernel): an item
+// at level l has just stored its word; count it off its parent's pending
+// children (a release), and when it was the last one rebuild the parent
+// (after an acquire) and go on up.  A node is rewritten in place only when
+// all of its children are done, as in the level-by-level build.
+__device__ void finish_upwards(const EditCtx &x, const Tables &t, uint32_t parent, uint32_t l) {
+  while (parent != kNoParent) {
+    __threadfence();
+    if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
+    __threadfence();
+    --l;
+    const Item it = x.a.items[parent];
+    x.a.items[parent].result = build_item(x, t, l, it);
+    parent = it.result; // the grandparent, stored there until now
+  }
+}
+
+// Items below the leaf-parent level with no child items rebuild at once and
+// start their own climb.
+__device__ __forceinline__ void rebuild_childless_body(EditCtx x, Tables t, Blocks blk) {
+  Header *h = x.hdr;
+  if (edit_failed(h)) return;
+  for (uint32_t l = 0; l + 1 < t.depth; ++l) {
+    const uint32_t W = h->item_count[l];
+    const uint32_t base = h->item_off[l];
+    for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
+      const Item it = x.a.items[base + i];
+      if (it.masks & 0xffu) continue;
+      x.a.items[base + i].result = build_item(x, t, l, it);
+      finish_upwards(x, t, it.result, l);
     }
-    uint32_t k = 0;
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c)
-      if (cm & (1u << c)) child[c] = x.a.items[it.child_base + k++].result;
-    x.a.items[base + i].result = finish_node(t, it.old, child, l == 0);
   }
 }
 
@@ -495,12 +540,12 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
     if (lead) gc_recheck_body(t);
     grid.sync();
   }
-  leafparent_body<false>(e, t, blk);
+  // The bottom-up build without level barriers: the leaf-parent items and
+  // the childless items of the levels above finish their ancestors, each
+  // item rebuilt by the last of its children to finish.
+  leafparent_body<false, true>(e, t, blk);
+  rebuild_childless_body(e, t, blk);
   grid.sync();
-  for (uint32_t r = t.depth - 1; r > 0; --r) {
-    build_body(e, t, r - 1, blk);
-    grid.sync();
-  }
   if (lead) finalize_body(t);
 }
 
