@@ -1031,6 +1031,11 @@ def run_ours(args, ws, rank, local):
                                    if result["cpu_baseline"]["value"] else None),
             "parity_all": parity["all"],
         }
+        # the same verdicts right after the headline keys too, for readers that
+        # keep only the start of the line
+        head = ("metric", "value", "unit")
+        result = {**{k: result[k] for k in head}, "headline": result["summary"],
+                  **{k: v for k, v in result.items() if k not in head}}
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
