@@ -473,6 +473,12 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
 
 // Bottom-up rebuild of level l from its children's results.
 // The rebuilt ref of one item at inner level l from its children's results.
+// WarpCounters: the pool and node counters are bumped once per warp, which
+// needs every active lane of the warp at the same level (true for the
+// level-by-level build, not for climbs, where lanes may be at any level).
+// Climb: the children's results come from L2 (other SMs wrote them in this
+// launch); the level-by-level build reads them in a later launch.
+template <bool WarpCounters = true, bool Climb = false>
 __device__ __forceinline__ uint32_t build_item(const Ctx &x, uint32_t l, const Item &it) {
   const uint32_t cm = it.masks & 0xffu, km = (it.masks >> 8) & 0xffu,
                  kf = (it.masks >> 16) & 0xffu;
@@ -481,8 +487,12 @@ __device__ __forceinline__ uint32_t build_item(const Ctx &x, uint32_t l, const I
 #pragma unroll
   for (uint32_t c = 0; c < 8; ++c) {
     const uint32_t bit = 1u << c;
-    if (cm & bit) child[c] = x.a.items[it.child_base + k++].result;
-    else if (km & bit) child[c] = (kf & bit) ? kFullRef : kEmptyRef;
+    if (cm & bit) {
+      const uint32_t *r = &x.a.items[it.child_base + k++].result;
+      child[c] = Climb ? __ldcg(r) : *r;
+    } else if (km & bit) {
+      child[c] = (kf & bit) ? kFullRef : kEmptyRef;
+    }
     else child[c] = child_ref(x.t, l, it.old, c);
   }
   // Every child kept its ref: the node is the old one (refs are canonical).
@@ -490,7 +500,7 @@ __device__ __forceinline__ uint32_t build_item(const Ctx &x, uint32_t l, const I
 #pragma unroll
   for (uint32_t c = 0; c < 8; ++c)
     if ((cm | km) & (1u << c)) same = same && child[c] == child_ref(x.t, l, it.old, c);
-  return same ? it.old : canon_node(x.t, l, child);
+  return same ? it.old : canon_node<WarpCounters>(x.t, l, child);
 }
 
 __device__ __forceinline__ void build_body(Ctx x, uint32_t l, Blocks blk) {
@@ -512,8 +522,8 @@ __device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l) {
     if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
     __threadfence();
     --l;
-    const Item it = x.a.items[parent];
-    x.a.items[parent].result = build_item(x, l, it);
+    const Item it = load_item_l2(&x.a.items[parent]);
+    x.a.items[parent].result = build_item<false, true>(x, l, it);
     parent = it.result; // the grandparent, stored there until now
   }
 }
@@ -531,7 +541,7 @@ __device__ __forceinline__ void rebuild_childless_body(Ctx x, Blocks blk) {
          i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
       const Item it = x.a.items[base + i];
       if (it.masks & 0xffu) continue;
-      x.a.items[base + i].result = build_item(x, l, it);
+      x.a.items[base + i].result = build_item<false, true>(x, l, it);
       finish_upwards(x, it.result, l);
     }
   }

@@ -216,6 +216,22 @@ struct Item {
   uint32_t result;     // parent index until rebuilt, then the rebuilt ref / slot word
 };
 constexpr uint32_t kNoParent = 0xffffffffu;
+
+// Item reads on a climb (another SM wrote the item or its children's
+// results in this launch): from L2, never from this SM's L1.
+__device__ __forceinline__ Item load_item_l2(const Item *p) {
+  const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
+  const uint4 b = __ldcg(reinterpret_cast<const uint4 *>(p) + 1);
+  Item it;
+  it.cell = static_cast<uint64_t>(a.x) | (static_cast<uint64_t>(a.y) << 32);
+  it.old = a.z;
+  it.pstart = a.w;
+  it.pcount = b.x;
+  it.child_base = b.y;
+  it.masks = b.z;
+  it.result = b.w;
+  return it;
+}
 static_assert(sizeof(Item) == 32, "Item is 32 bytes");
 
 // Per-edit device bookkeeping (one per structure).

@@ -317,7 +317,9 @@ __global__ void __launch_bounds__(kBlock) leafparent_kernel(EditCtx x, Tables t)
   leafparent_body<Terrain>(x, t, launch_blocks());
 }
 
-// The rebuilt word of one item at inner level l from its children's results.
+// The rebuilt word of one item at inner level l from its children's results
+// (Climb: read from L2, other SMs wrote them in this launch).
+template <bool Climb = false>
 __device__ __forceinline__ uint32_t build_item(const EditCtx &x, const Tables &t, uint32_t l,
                                                const Item &it) {
   const uint32_t cm = it.masks & 0xffu;
@@ -334,7 +336,10 @@ __device__ __forceinline__ uint32_t build_item(const EditCtx &x, const Tables &t
   uint32_t k = 0;
 #pragma unroll
   for (uint32_t c = 0; c < 8; ++c)
-    if (cm & (1u << c)) child[c] = x.a.items[it.child_base + k++].result;
+    if (cm & (1u << c)) {
+      const uint32_t *r = &x.a.items[it.child_base + k++].result;
+      child[c] = Climb ? __ldcg(r) : *r;
+    }
   return finish_node(t, it.old, child, l == 0);
 }
 
@@ -359,8 +364,8 @@ __device__ void finish_upwards(const EditCtx &x, const Tables &t, uint32_t paren
     if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
     __threadfence();
     --l;
-    const Item it = x.a.items[parent];
-    x.a.items[parent].result = build_item(x, t, l, it);
+    const Item it = load_item_l2(&x.a.items[parent]);
+    x.a.items[parent].result = build_item<true>(x, t, l, it);
     parent = it.result; // the grandparent, stored there until now
   }
 }
@@ -377,7 +382,7 @@ __device__ __forceinline__ void rebuild_childless_body(EditCtx x, Tables t, Bloc
          i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
       const Item it = x.a.items[base + i];
       if (it.masks & 0xffu) continue;
-      x.a.items[base + i].result = build_item(x, t, l, it);
+      x.a.items[base + i].result = build_item<true>(x, t, l, it);
       finish_upwards(x, t, it.result, l);
     }
   }
