@@ -180,11 +180,11 @@ __device__ uint32_t leaf_find_or_insert(const Tables &t, uint64_t mask) {
 }
 
 // Probes use relaxed loads.  An item found through a published entry is
-// read after an acquire load of that entry only when it was inserted by this
-// edit (its offset is at or above pool_mark, the pool use when the edit's
-// inserts began): items from earlier launches are visible without one, and
-// most matches of an edit are such pre-existing subtrees.  Inserts publish
-// with a release store.
+// read after an acquire fence only when it was inserted by this edit (its
+// offset is at or above pool_mark, the pool use when the edit's inserts
+// began): items from earlier launches are visible without one, and most
+// matches of an edit are such pre-existing subtrees.  Inserts publish with a
+// release store.
 // WarpCounters: bump the level's pool and node counters with one atomic per
 // warp (warp_atomic_add_small), for kernels whose lanes insert side by side;
 // a kernel with a few inserting lanes per warp does better with plain ones.
@@ -238,12 +238,7 @@ __device__ uint32_t node_find_or_insert(const Tables &t, uint32_t l, const Words
         }
       }
       if (r >= 2u) {
-        // Inserted by this edit: read it after an acquire load of its
-        // published entry (a second load of the same, final value), which
-        // pairs with the inserter's release store at the cost of one more
-        // L2 round trip instead of a fence that also waits for this
-        // thread's own outstanding stores.
-        if (r - 2u >= mark) (void)ld_acquire_u64(idx + pos);
+        if (r - 2u >= mark) fence_acq_rel_gpu(); // inserted by this edit
         if (w.equals(pool + (r - 2u))) return r;
       }
     }
