@@ -189,12 +189,6 @@ __device__ __forceinline__ void warp_count_u64(unsigned long long *ctr) {
   if (lane_id() == __ffs(am) - 1u) atomicAdd(ctr, static_cast<unsigned long long>(__popc(am)));
 }
 
-__device__ __forceinline__ uint64_t shfl_xor_u64(uint64_t v, uint32_t lane_mask) {
-  const uint32_t lo = __shfl_xor_sync(kFullMask, static_cast<uint32_t>(v), lane_mask);
-  const uint32_t hi = __shfl_xor_sync(kFullMask, static_cast<uint32_t>(v >> 32), lane_mask);
-  return (static_cast<uint64_t>(hi) << 32) | lo;
-}
-
 template <class T> __device__ __forceinline__ T warp_inclusive_sum(T v) {
 #pragma unroll
   for (uint32_t d = 1; d < kWarp; d <<= 1) {

@@ -59,23 +59,17 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
   return x;
 }
 
-// Hash of an item's n words: the sum over positions k of a term mixing word
-// k with its position (an xor with a position constant, a multiply by an odd
-// 64-bit constant and an xor-shift), then splitmix64's finaliser.  The terms
-// are independent, so the lanes sharing a leaf-parent item each add the
-// terms of their own children and a shuffle sums them; the position inside
-// each term keeps the hash order-dependent.
-__device__ __forceinline__ uint64_t word_term(uint32_t w, uint32_t k) {
-  const uint64_t x = static_cast<uint64_t>(w ^ (k * 0x9e3779b9u)) * 0xd6e8feb86659fd93ull;
-  return x ^ (x >> 29);
-}
-__device__ __forceinline__ uint64_t hash_seed(uint32_t n) { return 0x243f6a8885a308d3ull ^ n; }
-
+// Hash of an item's n words, fed one word at a time: each word is folded in
+// by an xor, a multiply by an odd constant and a rotation (a bijection of
+// the state for every word, so items that differ in one word never
+// collide), and splitmix64's finaliser spreads the state over all 64 bits.
 struct WordHash {
   uint64_t h;
-  uint32_t k = 0;
-  __device__ __forceinline__ explicit WordHash(uint32_t n) : h(hash_seed(n)) {}
-  __device__ __forceinline__ void add(uint32_t w) { h += word_term(w, k++); }
+  __device__ __forceinline__ explicit WordHash(uint32_t n) : h(0x243f6a8885a308d3ull ^ n) {}
+  __device__ __forceinline__ void add(uint32_t w) {
+    const uint64_t x = (h ^ w) * 0x9fb21c651e98df25ull;
+    h = (x << 29) | (x >> 35);
+  }
   __device__ __forceinline__ uint64_t finish() const { return mix64(h); }
 };
 
@@ -132,13 +126,6 @@ struct ChildWords {
     for (uint32_t c = 0; c < 8; ++c)
       if (header & (1u << c)) dst[k++] = child[c];
   }
-};
-
-// ChildWords whose hash the caller computed (the leaf-parent level sums the
-// terms across the lanes of an item).
-struct HashedChildWords : ChildWords {
-  uint64_t h;
-  __device__ __forceinline__ uint64_t hash() const { return h; }
 };
 
 // ------------------------------------------------------------- reading --
@@ -424,38 +411,9 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
 #pragma unroll
       for (uint32_t k = 0; k < Lanes; ++k)
         child[k + Lanes * j] = __shfl_sync(kFullMask, result[j], gbase + k);
-    // The item's child and fill masks by ballots, and its hash as the sum of
-    // the group's lanes' terms (child c = q + Lanes * j sits at word 1 +
-    // popc(cm below c)); the same value WordHash gives for these words.
-    uint32_t cm = 0, fm = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < kPer; ++j) {
-      const uint32_t bn = __ballot_sync(kFullMask, result[j] >= 2u);
-      const uint32_t bf = __ballot_sync(kFullMask, result[j] == kFullRef);
-      cm |= ((bn >> gbase) & kGroupBits) << (Lanes * j);
-      fm |= ((bf >> gbase) & kGroupBits) << (Lanes * j);
-    }
-    uint64_t part = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < kPer; ++j) {
-      const uint32_t c = q + Lanes * j;
-      if (result[j] >= 2u) part += word_term(result[j], 1u + __popc(cm & ((1u << c) - 1u)));
-    }
-#pragma unroll
-    for (uint32_t o = 1; o < Lanes; o <<= 1) part += shfl_xor_u64(part, o);
     // At most 32 / Lanes lanes of a warp insert a node here: plain counters.
     if (have && q == 0) {
-      uint32_t r;
-      if (same) {
-        r = it.old;
-      } else if (cm == 0 && (fm == 0u || fm == 0xffu)) {
-        r = fm ? kFullRef : kEmptyRef; // uniform: a sentinel
-      } else {
-        const uint32_t header = cm | (fm << 8);
-        const uint64_t h = mix64(hash_seed(1u + __popc(cm)) + word_term(header, 0) + part);
-        r = node_find_or_insert<HashedChildWords, false>(x.t, l, HashedChildWords{{header, child}, h});
-      }
-      x.a.items[base + wi].result = r;
+      x.a.items[base + wi].result = same ? it.old : canon_node<false>(x.t, l, child);
       if (Climb) finish_upwards(x, it.result, l); // it.result: the parent's index
     }
   }
@@ -466,7 +424,6 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
   leafparent_body<Terrain, Lanes>(x, launch_blocks());
 }
 
-// Bottom-up rebuild of level l from its children's results.
 // The rebuilt ref of one item at inner level l from its children's results.
 // WarpCounters: the pool and node counters are bumped once per warp, which
 // needs every active lane of the warp at the same level (true for the
