@@ -695,6 +695,7 @@ struct vx_dag {
   void *arena_mem = nullptr;
   size_t bytes = 0;
   vx_primitive *tmp_prim = nullptr; // one terrain primitive
+  uint32_t *host_status = nullptr;  // pinned word for status reads (allocated on first use)
 };
 
 namespace vx::dag {
@@ -847,15 +848,26 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
   return from_cuda(cudaGetLastError());
 }
 
+// The device status, read through a pinned word (a copy into pageable
+// memory goes through a staging buffer); a failed status is cleared.
 vx_status read_status(vx_dag *d, cudaStream_t s, bool clear) {
-  uint32_t code = 0;
-  VX_TRY_CUDA(cudaMemcpyAsync(&code, &d->t.hdr->status, sizeof(code),
+  if (d->host_status == nullptr &&
+      cudaHostAlloc(reinterpret_cast<void **>(&d->host_status), sizeof(uint32_t),
+                    cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError(); // not fatal: read through a stack word instead
+    d->host_status = nullptr;
+  }
+  uint32_t stack_code = 0;
+  uint32_t *code = d->host_status ? d->host_status : &stack_code;
+  VX_TRY_CUDA(cudaMemcpyAsync(code, &d->t.hdr->status, sizeof(uint32_t),
                               cudaMemcpyDeviceToHost, s));
   VX_TRY_CUDA(cudaStreamSynchronize(s));
-  if (clear && code != kDevOk)
+  const uint32_t c = *code;
+  if (clear && c != kDevOk) {
     VX_TRY_CUDA(cudaMemsetAsync(&d->t.hdr->status, 0, sizeof(uint32_t), s));
-  if (clear) VX_TRY_CUDA(cudaStreamSynchronize(s));
-  return status_from_device(code);
+    VX_TRY_CUDA(cudaStreamSynchronize(s));
+  }
+  return status_from_device(c);
 }
 
 struct PlainLayout {
@@ -1055,6 +1067,7 @@ vx_status vx_dag_destroy(vx_dag *d) {
   cudaFree(d->t.hdr);
   cudaFree(d->arena_mem);
   cudaFree(d->tmp_prim);
+  if (d->host_status) cudaFreeHost(d->host_status);
   delete d;
   return VX_OK;
 }

@@ -424,7 +424,7 @@ __device__ __forceinline__ void plain_prep_emit(const PlainPrep &p, Blocks blk) 
     pr.r[0] = static_cast<uint32_t>(e.y);
     pr.r[1] = static_cast<uint32_t>(e.y >> 32);
     pr.flags = vx_make_flags(kShapeLeafMask, p.op, p.material);
-    p.prims[atomicAdd(p.nprims, 1u)] = pr;
+    p.prims[warp_atomic_add_small(p.nprims, 1u)] = pr; // one atomic per warp
   }
 }
 

@@ -583,6 +583,7 @@ struct vx_svo {
   vx::edit::Arena a{};
   void *arena_mem = nullptr;
   vx_primitive *tmp_prim = nullptr;
+  uint32_t *host_status = nullptr; // pinned word for status reads (allocated on first use)
 };
 
 namespace vx::svo {
@@ -704,16 +705,26 @@ vx_status run_pipeline(vx_svo *v, const vx_primitive *prims, const uint32_t *d_c
   return from_cuda(cudaGetLastError());
 }
 
+// The device status, read through a pinned word (a copy into pageable
+// memory goes through a staging buffer); a failed status is cleared.
 vx_status read_status(vx_svo *v, cudaStream_t s) {
-  uint32_t code = 0;
-  VX_TRY_CUDA(cudaMemcpyAsync(&code, &v->t.hdr->status, sizeof(code),
+  if (v->host_status == nullptr &&
+      cudaHostAlloc(reinterpret_cast<void **>(&v->host_status), sizeof(uint32_t),
+                    cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError(); // not fatal: read through a stack word instead
+    v->host_status = nullptr;
+  }
+  uint32_t stack_code = 0;
+  uint32_t *code = v->host_status ? v->host_status : &stack_code;
+  VX_TRY_CUDA(cudaMemcpyAsync(code, &v->t.hdr->status, sizeof(uint32_t),
                               cudaMemcpyDeviceToHost, s));
   VX_TRY_CUDA(cudaStreamSynchronize(s));
-  if (code != kDevOk) {
+  const uint32_t c = *code;
+  if (c != kDevOk) {
     VX_TRY_CUDA(cudaMemsetAsync(&v->t.hdr->status, 0, sizeof(uint32_t), s));
     VX_TRY_CUDA(cudaStreamSynchronize(s));
   }
-  return status_from_device(code);
+  return status_from_device(c);
 }
 
 } // namespace vx::svo
@@ -798,6 +809,7 @@ vx_status vx_svo_destroy(vx_svo *v) {
   cudaFree(t.ctr);
   cudaFree(t.hdr);
   cudaFree(v->tmp_prim);
+  if (v->host_status) cudaFreeHost(v->host_status);
   cudaFree(v->arena_mem);
   delete v;
   return VX_OK;
