@@ -93,6 +93,19 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// atomicSub with acquire-release semantics at GPU scope: this thread's earlier
+// stores are visible to whoever observes the new value, and the stores that
+// earlier releases of the same word published are visible to this thread's
+// later loads.  Returns the old value.
+__device__ __forceinline__ uint32_t atomic_sub_acq_rel(uint32_t *p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+               : "=r"(old)
+               : "l"(p), "r"(0u - v)
+               : "memory");
+  return old;
+}
+
 // Acquire / release fence at GPU scope: after a relaxed load that observed a
 // release store, it makes the writer's earlier stores visible.
 __device__ __forceinline__ void fence_acq_rel_gpu() {

@@ -466,13 +466,13 @@ __device__ __forceinline__ void build_body(Ctx x, uint32_t l, Blocks blk) {
 }
 
 // Bottom-up without level barriers: an item at level l has just stored its
-// result; count it off its parent's pending children (a release), and when
-// it was the last one rebuild the parent (after an acquire) and go on up.
+// result; count it off its parent's pending children with one
+// acquire-release decrement (its result store is published, and the last
+// child sees every sibling's), and when it was the last one rebuild the parent
+// and go on up.
 __device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l) {
   while (parent != kNoParent) {
-    __threadfence();
-    if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
-    __threadfence();
+    if (atomic_sub_acq_rel(&x.a.items[parent].pstart, 1u) != 1u) return;
     --l;
     const Item it = load_item_l2(&x.a.items[parent]);
     x.a.items[parent].result = build_item<false, true>(x, l, it);
@@ -749,6 +749,7 @@ vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s,
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   EditCtx ec = e;
+  ec.big_item = std::max(ec.big_item, kSmallBigItem);
   PlainPrep pp = prep ? *prep : PlainPrep{};
   void *args[] = {&x, &ec, &pp};
   prof::Scope sc("dag_small_edit", s);

@@ -355,14 +355,12 @@ __device__ __forceinline__ void build_body(EditCtx x, Tables t, uint32_t l, Bloc
 
 // Bottom-up without level barriers (the single cooperative kernel): an item
 // at level l has just stored its word; count it off its parent's pending
-// children (a release), and when it was the last one rebuild the parent
-// (after an acquire) and go on up.  A node is rewritten in place only when
+// children with one acquire-release decrement, and when it was the last one
+// rebuild the parent and go on up.  A node is rewritten in place only when
 // all of its children are done, as in the level-by-level build.
 __device__ void finish_upwards(const EditCtx &x, const Tables &t, uint32_t parent, uint32_t l) {
   while (parent != kNoParent) {
-    __threadfence();
-    if (atomicSub(&x.a.items[parent].pstart, 1u) != 1u) return;
-    __threadfence();
+    if (atomic_sub_acq_rel(&x.a.items[parent].pstart, 1u) != 1u) return;
     --l;
     const Item it = load_item_l2(&x.a.items[parent]);
     x.a.items[parent].result = build_item<true>(x, t, l, it);
@@ -617,6 +615,7 @@ vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s,
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   EditCtx ec = e;
+  ec.big_item = std::max(ec.big_item, kSmallBigItem);
   Tables tc = t;
   PlainPrep pp = prep ? *prep : PlainPrep{};
   void *args[] = {&ec, &tc, &pp};
