@@ -749,7 +749,6 @@ vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s,
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   EditCtx ec = e;
-  ec.big_item = std::max(ec.big_item, kSmallBigItem);
   PlainPrep pp = prep ? *prep : PlainPrep{};
   void *args[] = {&x, &ec, &pp};
   prof::Scope sc("dag_small_edit", s);

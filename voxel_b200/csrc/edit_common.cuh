@@ -594,10 +594,6 @@ __global__ void __launch_bounds__(kBlock)
 // kBigCache primitives are classified once: walk 1 keeps each primitive's
 // per-child MIXED bits in shared memory for walks 2 and 3.
 constexpr uint32_t kBigBlock = 512;
-// Inside the single cooperative kernel of a small edit, a level's
-// block-per-item stage costs a grid barrier plus its three walks; lists of
-// up to this many primitives are walked faster by the item's own 8 lanes.
-constexpr uint32_t kSmallBigItem = 64;
 constexpr uint32_t kBigCache = 32768;
 
 template <class Policy, bool Terrain, uint32_t Threads, uint32_t Cache>

@@ -615,7 +615,6 @@ vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s,
   const uint32_t grid = static_cast<uint32_t>(sm_count()) *
                         static_cast<uint32_t>(std::max(1, std::min(per_sm, want)));
   EditCtx ec = e;
-  ec.big_item = std::max(ec.big_item, kSmallBigItem);
   Tables tc = t;
   PlainPrep pp = prep ? *prep : PlainPrep{};
   void *args[] = {&ec, &tc, &pp};
