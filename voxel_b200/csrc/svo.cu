@@ -360,9 +360,12 @@ __device__ __forceinline__ void build_body(EditCtx x, Tables t, uint32_t l, Bloc
 // all of its children are done, as in the level-by-level build.
 __device__ void finish_upwards(const EditCtx &x, const Tables &t, uint32_t parent, uint32_t l) {
   while (parent != kNoParent) {
+    // The parent's own fields were written by its expansion, stages ago:
+    // read them while the decrement is in flight (only the children's
+    // results need its acquire).
+    const Item it = load_item_l2(&x.a.items[parent]);
     if (atomic_sub_acq_rel(&x.a.items[parent].pstart, 1u) != 1u) return;
     --l;
-    const Item it = load_item_l2(&x.a.items[parent]);
     x.a.items[parent].result = build_item<true>(x, t, l, it);
     parent = it.result; // the grandparent, stored there until now
   }
