@@ -1461,8 +1461,9 @@ namespace vx::dag {
 // an old one is new_refs[rank(old)].  Nothing is sized on the host except by
 // upper bounds, so the whole pass is stream-ordered.
 struct LevelMarks {
-  uint32_t *bits;   // mark bitmap
-  uint32_t *prefix; // exclusive prefix of popcount(bits[w])
+  uint32_t *bits;   // mark bitmap word w at bits[2w]; bits[2w + 1] holds prefix[w]
+                    // once ranked, so that a rank costs one 8-byte load
+  uint32_t *prefix; // exclusive prefix of popcount(bits[2w]) (the scan's array)
   uint32_t *refs;   // live old refs in ascending order (rank order)
   uint32_t *new_refs;
   uint32_t *live;   // device count of live refs
@@ -1472,7 +1473,8 @@ struct LevelMarks {
 
 __device__ __forceinline__ uint32_t rank_of(const LevelMarks &m, uint32_t ref) {
   const uint32_t b = ref - 2u;
-  return m.prefix[b >> 5] + __popc(m.bits[b >> 5] & ((1u << (b & 31u)) - 1u));
+  const uint2 w = reinterpret_cast<const uint2 *>(m.bits)[b >> 5]; // {bits, prefix}
+  return w.y + __popc(w.x & ((1u << (b & 31u)) - 1u));
 }
 
 // Marks the children of level l's live items in level l+1's bitmap.
@@ -1485,7 +1487,8 @@ __global__ void mark_children_kernel(Tables t, uint32_t l, LevelMarks m, LevelMa
     for (uint32_t k = 0; k < static_cast<uint32_t>(__popc(cm)); ++k) {
       const uint32_t b = item[1 + k] - 2u;
       const uint32_t bit = 1u << (b & 31u);
-      if (!(ld_relaxed_u32(next.bits + (b >> 5)) & bit)) atomicOr(next.bits + (b >> 5), bit);
+      uint32_t *word = next.bits + 2u * (b >> 5);
+      if (!(ld_relaxed_u32(word) & bit)) atomicOr(word, bit);
     }
   }
 }
@@ -1493,7 +1496,7 @@ __global__ void mark_children_kernel(Tables t, uint32_t l, LevelMarks m, LevelMa
 __global__ void popcount_kernel(LevelMarks m) {
   for (uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; w < m.words;
        w += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-    m.prefix[w] = __popc(m.bits[w]);
+    m.prefix[w] = __popc(m.bits[2 * w]);
 }
 
 // After the scan: the live count and the rank-ordered list of live refs.
@@ -1502,13 +1505,14 @@ __global__ void list_kernel(Tables t, LevelMarks m) {
   const uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (first == 0) {
     const uint64_t last = m.words - 1;
-    const uint32_t total = m.prefix[last] + __popc(m.bits[last]);
+    const uint32_t total = m.prefix[last] + __popc(m.bits[2 * last]);
     if (total > m.cap) set_status(&t.hdr->status, kDevCapacity);
     *m.live = min(total, m.cap);
   }
   for (uint64_t w = first; w < m.words; w += stride) {
-    uint32_t bits = m.bits[w];
+    uint32_t bits = m.bits[2 * w];
     uint32_t at = m.prefix[w];
+    m.bits[2 * w + 1] = at; // beside the bitmap word, for rank_of
     while (bits) {
       const uint32_t b = __ffs(bits) - 1u;
       bits &= bits - 1u;
@@ -2070,7 +2074,7 @@ vx_status vx_dag_compact(vx_dag *d, vx_stream stream) {
     scan_ws = c.template take<unsigned char>(scan_bytes);
     for (uint32_t l = 0; l <= D; ++l) {
       m[l].live = counts + l;
-      m[l].bits = c.template take<uint32_t>(m[l].words);
+      m[l].bits = c.template take<uint32_t>(2 * m[l].words);
       m[l].prefix = c.template take<uint32_t>(m[l].words);
       m[l].refs = c.template take<uint32_t>(m[l].cap);
       m[l].new_refs = c.template take<uint32_t>(m[l].cap);
@@ -2092,7 +2096,7 @@ vx_status vx_dag_compact(vx_dag *d, vx_stream stream) {
   vx::Carver carver(marks_base);
   carve_marks(carver);
   for (uint32_t l = 1; l <= D; ++l)
-    VX_TRY_CUDA(cudaMemsetAsync(m[l].bits, 0, m[l].words * 4, s));
+    VX_TRY_CUDA(cudaMemsetAsync(m[l].bits, 0, m[l].words * 8, s));
   {
     vx::prof::Scope sc("dag_compact_mark", s);
     seed_root_kernel<<<1, 1, 0, s>>>(m[0], h.root);
