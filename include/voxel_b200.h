@@ -700,7 +700,9 @@ vx_status vx_dag_apply_terminal(vx_dag *dag, const vx_terminal_node *nodes,
  * first.  Completions report the
  * commit time (host clock of vx_serve_now_ns, when the batch's completion was
  * observed) and the root the batch published.  The server owns the DAG's
- * stream while it runs.  No counterpart in the reference (no serving path). */
+ * stream while it runs.  Creation compacts the DAG once (synchronously), which
+ * also loads the compaction kernels before the first request.  No
+ * counterpart in the reference (no serving path). */
 typedef struct vx_server vx_server;
 
 typedef struct vx_serve_config {

@@ -137,6 +137,7 @@ class SlabHashSet:
         check(lib().vx_slab_set_create(bucket_count, slab_capacity, C.byref(h)),
               "vx_slab_set_create")
         self._h = h
+        self._free = lib().vx_slab_set_destroy
         self.bucket_count = bucket_count
         self.slab_capacity = slab_capacity
 
@@ -148,10 +149,12 @@ class SlabHashSet:
         return v
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_slab_set_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     @property
     def nbytes(self) -> int:
@@ -191,12 +194,15 @@ class SlabHashMap:
         check(lib().vx_slab_map_create(bucket_count, slab_capacity, C.byref(h)),
               "vx_slab_map_create")
         self._h = h
+        self._free = lib().vx_slab_map_destroy
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_slab_map_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     @property
     def nbytes(self) -> int:
@@ -234,13 +240,16 @@ class ItemSet:
         h = C.c_void_p()
         check(lib().vx_itemset_create(width, max_items, C.byref(h)), "vx_itemset_create")
         self._h = h
+        self._free = lib().vx_itemset_destroy
         self.width = width
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_itemset_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     def _op(self, fn, items, name):
         n = items.numel() // self.width
@@ -281,6 +290,7 @@ class CuckooMap:
         check(lib().vx_cuckoo_create(slot_count, max_evictions, C.byref(h)),
               "vx_cuckoo_create")
         self._h = h
+        self._free = lib().vx_cuckoo_destroy
         self.slot_count = slot_count
 
     def device_view(self):
@@ -291,10 +301,12 @@ class CuckooMap:
         return v
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_cuckoo_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     @property
     def nbytes(self) -> int:
@@ -451,6 +463,7 @@ class HashDag:
         h = C.c_void_p()
         check(lib().vx_dag_create(C.byref(cfg), C.byref(h)), "vx_dag_create")
         self._h = h
+        self._free = lib().vx_dag_destroy
         self.depth = depth
 
     def device_view(self):
@@ -461,10 +474,12 @@ class HashDag:
         return v
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_dag_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     @property
     def world(self) -> int:
@@ -679,6 +694,7 @@ class Svo:
         h = C.c_void_p()
         check(lib().vx_svo_create(C.byref(cfg), C.byref(h)), "vx_svo_create")
         self._h = h
+        self._free = lib().vx_svo_destroy
         self.depth = depth
         self.materials = materials
 
@@ -690,10 +706,12 @@ class Svo:
         return v
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().vx_svo_destroy(h)
-            self._h = None
+        # the destroy function bound at creation: at interpreter exit the
+        # module's globals may already be gone
+        h, free = getattr(self, "_h", None), getattr(self, "_free", None)
+        if h is not None and h.value and free is not None:
+            free(h)
+        self._h = None
 
     @property
     def world(self) -> int:

@@ -407,6 +407,17 @@ vx_status vx_serve_create(vx_dag *dag, const vx_serve_config *cfg, vx_server **o
     vx_serve_destroy(s);
     return vx::from_cuda(e);
   }
+  // A compaction before the first request: its kernels are loaded now (the
+  // first launch of a kernel loads its code, a cost no request should wait
+  // for), and the tables start without garbage.  An arena too small for it
+  // changes nothing and is reported by the first compaction under load.
+  {
+    const vx_status cs = vx_dag_compact(dag, s->stream);
+    if (cs != VX_OK && cs != VX_ERR_CAPACITY) {
+      vx_serve_destroy(s);
+      return cs;
+    }
+  }
   // the tables' current use, for admission
   s->last_hdr.resize(vx::dag::header_bytes());
   const vx_status hs = vx::dag::read_header(dag, s->last_hdr.data(), s->stream);
