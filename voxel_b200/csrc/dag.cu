@@ -543,14 +543,15 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, Pl
     x.t.hdr->pool_mark[threadIdx.x] = x.t.hdr->pool_used[threadIdx.x];
   grid.sync();
   for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
+    // Short and long lists of level l side by side, one barrier per level:
+    // the long ones were listed when level l was emitted (their count is
+    // final at the barrier before, the same in every block) and go to the
+    // blocks from the last one down, the short ones from block 0 up.
     expand_body<DagTree, false>(e, tree, l, blk);
+    if (x.t.hdr->big_count[l] != 0)
+      expand_big_body<DagTree, false, kBlock, kSmallBigCache>(e, tree, l,
+                                                          Blocks{blk.count - 1u - blk.id, blk.count});
     grid.sync();
-    // The block-per-item stage only when it has items: the count is final
-    // at the barrier, so every block skips it (and its barrier) alike.
-    if (x.t.hdr->big_count[l] != 0) {
-      expand_big_body<DagTree, false, kBlock, kSmallBigCache>(e, tree, l, blk);
-      grid.sync();
-    }
   }
   // The bottom-up build without level barriers: the leaf-parent items and
   // the childless items of the levels above finish their ancestors, each

@@ -259,7 +259,14 @@ struct Arena {
 };
 
 // Items with more primitives than EditCtx::big_item (the tuning knob
-// "edit.big_item", 32 by default) are expanded by a whole block.
+// "edit.big_item", 32 by default) are expanded by a whole block.  They are
+// listed when they are emitted (the level above's expansion, or the init of
+// the root), so that a level's short and long lists can be expanded side by
+// side; the big buffer's two halves alternate by level, so level l + 1's
+// list fills while level l's is read.
+__device__ __forceinline__ uint32_t *big_list(const Arena &a, uint32_t l) {
+  return a.big + (l & 1u) * (a.big_cap / 2u);
+}
 
 
 // init_kernel's root_old value meaning "the root stored in the header".
@@ -275,6 +282,17 @@ struct EditCtx {
   uint32_t depth;
   uint32_t big_item; // longer primitive lists go to expand_big_kernel
 };
+
+// List item `idx` of level l (its index within the level) for the
+// block-per-item expansion when its primitive list is long and level l is
+// expanded at all (levels below depth - 1).
+__device__ __forceinline__ void note_big(const EditCtx &x, uint32_t l, uint32_t idx,
+                                         uint32_t pcount) {
+  if (pcount <= x.big_item || l + 1 >= x.depth) return;
+  const uint32_t slot = atomicAdd(&x.hdr->big_count[l], 1u);
+  if (slot < x.a.big_cap / 2u) big_list(x.a, l)[slot] = idx;
+  else set_status(&x.hdr->status, kDevCapacity);
+}
 
 // A tree Policy supplies:
 //   static constexpr bool kItemsForConst  - also create a (primitive-free)
@@ -331,6 +349,7 @@ __device__ __forceinline__ void init_body(EditCtx x, uint32_t root_old, Blocks b
       it.pcount = n;
       it.result = kNoParent;
       x.a.items[0] = it;
+      note_big(x, 0, 0, n);
     }
   }
   if (n > x.a.pair_cap) return;
@@ -460,16 +479,10 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
     const bool have = wi < W;
     Item it{};
     if (have) it = x.a.items[base + wi];
+    // Long lists were listed for expand_big (one block per item) when the
+    // item was emitted.
     const bool big = have && it.pcount > x.big_item;
-    if (big) {
-      // Long lists go to expand_big_kernel (one block per item).
-      if (c == 0) {
-        const uint32_t slot = atomicAdd(&h->big_count[l], 1u);
-        if (slot < x.a.big_cap) x.a.big[slot] = wi;
-        else set_status(&h->status, kDevCapacity);
-      }
-      it.pcount = 0;
-    }
+    if (big) it.pcount = 0;
     const Cell cell = unpack_cell(it.cell);
     const int64_t ox = int64_t(2 * cell.x + (c & 1u)) * csize;
     const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * csize;
@@ -554,6 +567,7 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
       ci.pcount = cnt;
       ci.result = static_cast<uint32_t>(base + wi);
       x.a.items[next_base + item_off + inc_items - 1] = ci;
+      note_big(x, l + 1, item_off + inc_items - 1, cnt);
       uint32_t j = 0;
       if (it.pcount <= 32u) {
         // The child's list is the set bits of `partial`: independent loads
@@ -600,7 +614,8 @@ template <class Policy, bool Terrain, uint32_t Threads, uint32_t Cache>
 __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
   if (edit_failed(h)) return;
-  const uint32_t nbig = min(h->big_count[l], x.a.big_cap);
+  const uint32_t nbig = min(h->big_count[l], x.a.big_cap / 2u);
+  const uint32_t *bigs = big_list(x.a, l);
   const uint32_t depth = x.depth;
   const uint32_t base = h->item_off[l];
   const uint32_t next_base = base + h->item_count[l];
@@ -619,7 +634,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
 
   for (uint32_t b = blk.id; b < nbig; b += blk.count) {
-    const uint32_t wi = x.a.big[b];
+    const uint32_t wi = bigs[b];
     const Item it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
     const bool cached = it.pcount <= Cache; // block-uniform
@@ -722,6 +737,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
       ci.pcount = s_cnt[t];
       ci.result = static_cast<uint32_t>(base + wi);
       x.a.items[next_base + s_item_base + k] = ci;
+      note_big(x, l + 1, s_item_base + k, s_cnt[t]);
     }
     // Walk 3: order-preserving compaction, one Threads-pair chunk at a time.
     uint32_t run[8];

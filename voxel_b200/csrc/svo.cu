@@ -521,18 +521,29 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
   init_body(e, kChild, blk);
   grid.sync();
   for (uint32_t l = 0; l + 1 < t.depth; ++l) {
+    // Short and long lists of level l side by side, one barrier per level:
+    // the long ones were listed when level l was emitted (their count is
+    // final at the barrier before, the same in every block) and go to the
+    // blocks from the last one down, the short ones from block 0 up.
     expand_body<SvoTree, false>(e, pol, l, blk);
+    if (t.hdr->big_count[l] != 0)
+      expand_big_body<SvoTree, false, kBlock, kSmallBigCache>(e, pol, l,
+                                                          Blocks{blk.count - 1u - blk.id, blk.count});
     grid.sync();
-    // The block-per-item stage only when it has items: the count is final
-    // at the barrier, so every block skips it (and its barrier) alike.
-    if (t.hdr->big_count[l] != 0) {
-      expand_big_body<SvoTree, false, kBlock, kSmallBigCache>(e, pol, l, blk);
-      grid.sync();
-    }
   }
-  if (lead) check_capacity_body(t);
-  grid.sync();
-  if (t.ctr->gc_needed) { // the same in every block: written before the barrier
+  // Every block reaches the capacity verdict of check_capacity_body from the
+  // same final counts, so the common case (the edit fits) needs no barrier.
+  __shared__ uint32_t s_verdict; // 0 fits, 1 collect first, 2 no room
+  if (threadIdx.x == 0) {
+    uint32_t v = 0;
+    if (t.hdr->status == kDevOk && !edit_fits(t)) v = t.ctr->detached ? 1u : 2u;
+    s_verdict = v;
+  }
+  __syncthreads();
+  const uint32_t verdict = s_verdict;
+  if (lead) t.ctr->gc_needed = verdict == 1u; // no other block reads it before a barrier
+  if (verdict == 1u) {
+    grid.sync(); // gc_needed, read by every collection stage
     gc_clear_body(t, blk);
     grid.sync();
     for (uint32_t l = 0; l < t.depth; ++l) {
@@ -549,10 +560,16 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
   // The bottom-up build without level barriers: the leaf-parent items and
   // the childless items of the levels above finish their ancestors, each
   // item rebuilt by the last of its children to finish.
-  leafparent_body<false, true>(e, t, blk);
-  rebuild_childless_body(e, t, blk);
+  if (verdict != 2u) {
+    leafparent_body<false, true>(e, t, blk);
+    rebuild_childless_body(e, t, blk);
+  }
   grid.sync();
-  if (lead) finalize_body(t);
+  if (lead) {
+    // written after the barrier: every block has read the status by then
+    if (verdict == 2u) t.hdr->status = kDevCapacity;
+    finalize_body(t);
+  }
 }
 
 __global__ void reset_kernel(Tables t) {
