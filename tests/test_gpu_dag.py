@@ -197,6 +197,9 @@ def test_capacity_overflow_keeps_previous_root(cuda):
     st = dag.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE)
     assert st == vx.VX_ERR_CAPACITY
     assert canon(dag) == before
+    # the error was reported once: the next edit starts from a clear status
+    assert dag.apply_voxels(vx.voxels_to_device(small, cuda), vx.EDIT_PLACE) == 0
+    assert canon(dag) == before
 
 
 def test_rasterize_matches_voxel_definition(cuda):

@@ -127,6 +127,9 @@ def test_capacity_overflow_changes_nothing(cuda):
     many = np.random.default_rng(2).integers(0, 4 << depth, (3000, 3)).astype(np.uint32)
     assert s.apply_voxels(vx.voxels_to_device(many, cuda), vx.EDIT_PLACE) == vx.VX_ERR_CAPACITY
     assert canon(s) == before
+    # the error was reported once: the next edit starts from a clear status
+    assert s.apply_voxels(vx.voxels_to_device(small, cuda), vx.EDIT_PLACE) == 0
+    assert canon(s) == before
 
 
 @pytest.mark.parametrize("small_max_prims", [256, 0])

@@ -53,7 +53,15 @@ def reset_tuning() -> None:
     check(lib().vx_tuning_reset(), "vx_tuning_reset")
 
 
+# The current stream's raw handle without building a torch.cuda.Stream object
+# (a few microseconds per call, which per-call edits feel).
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_device = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    if stream is None and _raw_stream is not None and _cur_device is not None:
+        return _raw_stream(_cur_device())
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream
 

@@ -525,7 +525,8 @@ constexpr uint32_t kSmallBigCache = 4096;
 // turn it into leaf-mask primitives (PlainPrep) in place of the sort-based
 // preparation of the multi-launch path.
 template <uint32_t Lanes, bool Plain>
-__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, PlainPrep prep) {
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, PlainPrep prep,
+                                                            uint32_t *status_out) {
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const Blocks blk = launch_blocks();
   const DagTree tree{x.t};
@@ -562,6 +563,7 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, Pl
   if (blk.id == 0 && threadIdx.x == 0) {
     Header *h = x.t.hdr;
     if (h->status == kDevOk && h->item_count[0] == 1) h->root = x.a.items[0].result;
+    if (status_out) *status_out = h->status; // the caller's mapped host word
   }
 }
 
@@ -700,6 +702,7 @@ struct vx_dag {
   size_t bytes = 0;
   vx_primitive *tmp_prim = nullptr; // one terrain primitive
   uint32_t *host_status = nullptr;  // pinned word for status reads (allocated on first use)
+  uint32_t *status_alias = nullptr; // its device address, when mapped at creation
 };
 
 namespace vx::dag {
@@ -742,8 +745,9 @@ vx_status query_small_residency() {
   return VX_OK;
 }
 
+// status_out: a mapped host word the kernel's last act writes the status to.
 vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s,
-                    const PlainPrep *prep = nullptr) {
+                    const PlainPrep *prep = nullptr, uint32_t *status_out = nullptr) {
   const int64_t lanes = tune::get(tune::kEditLeafparentLanes);
   void *fn = small_kernel(lanes, prep != nullptr);
   VX_TRY(query_small_residency());
@@ -754,7 +758,7 @@ vx_status run_small(vx_dag *d, Ctx &x, const EditCtx &e, cudaStream_t s,
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
   EditCtx ec = e;
   PlainPrep pp = prep ? *prep : PlainPrep{};
-  void *args[] = {&x, &ec, &pp};
+  void *args[] = {&x, &ec, &pp, &status_out};
   prof::Scope sc("dag_small_edit", s);
   VX_TRY_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, s));
   (void)d;
@@ -868,6 +872,21 @@ vx_status read_status(vx_dag *d, cudaStream_t s, bool clear) {
   VX_TRY_CUDA(cudaStreamSynchronize(s));
   const uint32_t c = *code;
   if (clear && c != kDevOk) {
+    VX_TRY_CUDA(cudaMemsetAsync(&d->t.hdr->status, 0, sizeof(uint32_t), s));
+    VX_TRY_CUDA(cudaStreamSynchronize(s));
+  }
+  return status_from_device(c);
+}
+
+// The status a small kernel wrote into the mapped host word (set to
+// kStatusUnset before the launch): after the kernel there is no copy to
+// wait for.  A word the kernel did not write falls back to read_status.
+constexpr uint32_t kStatusUnset = 0xffffffffu;
+vx_status read_written_status(vx_dag *d, cudaStream_t s) {
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  const uint32_t c = *reinterpret_cast<volatile uint32_t *>(d->host_status);
+  if (c == kStatusUnset) return read_status(d, s, true);
+  if (c != kDevOk) {
     VX_TRY_CUDA(cudaMemsetAsync(&d->t.hdr->status, 0, sizeof(uint32_t), s));
     VX_TRY_CUDA(cudaStreamSynchronize(s));
   }
@@ -1030,6 +1049,14 @@ vx_status vx_dag_create(const vx_dag_config *cfg, vx_dag **out) {
   d->t.leaf_mask = d->leaf_slots - 1;
   if ((e = cudaMalloc(&d->t.leaves, d->leaf_slots * 8)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&d->t.hdr, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
+  // the status word, mapped so that a small kernel can write it directly
+  if (cudaHostAlloc(reinterpret_cast<void **>(&d->host_status), sizeof(uint32_t),
+                    cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void **>(&d->status_alias), d->host_status,
+                               0) != cudaSuccess) {
+    cudaGetLastError(); // not fatal: statuses are then copied
+    d->status_alias = nullptr;
+  }
   if ((e = cudaMalloc(&d->tmp_prim, sizeof(vx_primitive))) != cudaSuccess) return fail(e);
   d->bytes += d->leaf_slots * 8;
   if (vx_status qs = vx::dag::query_small_residency(); qs != VX_OK) {
@@ -1108,8 +1135,13 @@ vx_status vx_dag_apply_voxels(vx_dag *d, const vx_voxel *edits, uint32_t count,
     Ctx x{d->t, d->a, prep.prims, prep.nprims, count};
     const EditCtx e{d->t.hdr, d->a, prep.prims, prep.nprims, count, d->t.depth,
                     static_cast<uint32_t>(vx::tune::get(vx::tune::kEditBigItem))};
-    VX_TRY(run_small(d, x, e, s, &prep));
-    return read_status(d, s, true);
+    if (d->status_alias == nullptr) {
+      VX_TRY(run_small(d, x, e, s, &prep));
+      return read_status(d, s, true);
+    }
+    *reinterpret_cast<volatile uint32_t *>(d->host_status) = kStatusUnset;
+    VX_TRY(run_small(d, x, e, s, &prep, d->status_alias));
+    return read_written_status(d, s);
   }
   const vx_primitive *prims = nullptr;
   const uint32_t *n = nullptr;

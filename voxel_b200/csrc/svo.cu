@@ -504,7 +504,8 @@ constexpr uint32_t kSmallBigCache = 4096;
 // first stages turn it into leaf-mask primitives (PlainPrep) in place of the
 // sort-based preparation of the multi-launch path.
 template <bool Plain>
-__global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t, PlainPrep prep) {
+__global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t, PlainPrep prep,
+                                                            uint32_t *status_out) {
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const Blocks blk = launch_blocks();
   const SvoTree pol{t};
@@ -569,6 +570,7 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
     // written after the barrier: every block has read the status by then
     if (verdict == 2u) t.hdr->status = kDevCapacity;
     finalize_body(t);
+    if (status_out) *status_out = t.hdr->status; // the caller's mapped host word
   }
 }
 
@@ -602,6 +604,7 @@ struct vx_svo {
   void *arena_mem = nullptr;
   vx_primitive *tmp_prim = nullptr;
   uint32_t *host_status = nullptr; // pinned word for status reads (allocated on first use)
+  uint32_t *status_alias = nullptr; // its device address, when mapped at creation
 };
 
 namespace vx::svo {
@@ -626,8 +629,9 @@ vx_status query_small_residency() {
   return VX_OK;
 }
 
+// status_out: a mapped host word the kernel's last act writes the status to.
 vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s,
-                    const PlainPrep *prep = nullptr) {
+                    const PlainPrep *prep = nullptr, uint32_t *status_out = nullptr) {
   VX_TRY(query_small_residency());
   const int per_sm = g_small_resident[prep ? 1 : 0];
   if (per_sm < 1) return VX_ERR_INVALID_VALUE;
@@ -637,7 +641,7 @@ vx_status run_small(const EditCtx &e, const Tables &t, cudaStream_t s,
   EditCtx ec = e;
   Tables tc = t;
   PlainPrep pp = prep ? *prep : PlainPrep{};
-  void *args[] = {&ec, &tc, &pp};
+  void *args[] = {&ec, &tc, &pp, &status_out};
   prof::Scope sc("svo_small_edit", s);
   VX_TRY_CUDA(cudaLaunchCooperativeKernel(small_kernel(prep != nullptr), dim3(grid),
                                           dim3(kBlock), args, 0, s));
@@ -745,6 +749,21 @@ vx_status read_status(vx_svo *v, cudaStream_t s) {
   return status_from_device(c);
 }
 
+// The status a small kernel wrote into the mapped host word (set to
+// kStatusUnset before the launch): after the kernel there is no copy to
+// wait for.  A word the kernel did not write falls back to read_status.
+constexpr uint32_t kStatusUnset = 0xffffffffu;
+vx_status read_written_status(vx_svo *v, cudaStream_t s) {
+  VX_TRY_CUDA(cudaStreamSynchronize(s));
+  const uint32_t c = *reinterpret_cast<volatile uint32_t *>(v->host_status);
+  if (c == kStatusUnset) return read_status(v, s);
+  if (c != kDevOk) {
+    VX_TRY_CUDA(cudaMemsetAsync(&v->t.hdr->status, 0, sizeof(uint32_t), s));
+    VX_TRY_CUDA(cudaStreamSynchronize(s));
+  }
+  return status_from_device(c);
+}
+
 } // namespace vx::svo
 
 using namespace vx::svo;
@@ -786,6 +805,14 @@ vx_status vx_svo_create(const vx_svo_config *cfg, vx_svo **out) {
   if ((e = cudaMalloc(&t.front[1], nn * 4)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&t.ctr, sizeof(Counters))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&t.hdr, sizeof(vx::edit::Header))) != cudaSuccess) return fail(e);
+  // the status word, mapped so that a small kernel can write it directly
+  if (cudaHostAlloc(reinterpret_cast<void **>(&v->host_status), sizeof(uint32_t),
+                    cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void **>(&v->status_alias), v->host_status,
+                               0) != cudaSuccess) {
+    cudaGetLastError(); // not fatal: statuses are then copied
+    v->status_alias = nullptr;
+  }
   if ((e = cudaMalloc(&v->tmp_prim, sizeof(vx_primitive))) != cudaSuccess) return fail(e);
   const uint64_t arena = cfg->arena_bytes ? cfg->arena_bytes : (256ull << 20);
   if ((e = cudaMalloc(&v->arena_mem, arena)) != cudaSuccess) return fail(e);
@@ -864,8 +891,13 @@ vx_status vx_svo_apply_voxels(vx_svo *v, const vx_voxel *edits, uint32_t count,
     // one cooperative launch: voxels -> leaf masks -> the edit and collection
     const EditCtx e{v->t.hdr, v->a, prep.prims, prep.nprims, count, v->t.depth,
                     static_cast<uint32_t>(vx::tune::get(vx::tune::kEditBigItem))};
-    VX_TRY(run_small(e, v->t, s, &prep));
-    return read_status(v, s);
+    if (v->status_alias == nullptr) {
+      VX_TRY(run_small(e, v->t, s, &prep));
+      return read_status(v, s);
+    }
+    *reinterpret_cast<volatile uint32_t *>(v->host_status) = kStatusUnset;
+    VX_TRY(run_small(e, v->t, s, &prep, v->status_alias));
+    return read_written_status(v, s);
   }
   VX_TRY(vx::plain::prepare(edits, count, v->t.depth, op, mat, workspace, &prims, &n, s));
   VX_TRY(run_pipeline(v, prims, n, count, s, false, small_batch(count, true)));
