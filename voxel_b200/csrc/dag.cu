@@ -535,8 +535,7 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, Pl
     grid.sync();
     plain_prep_aggregate(prep, x.t.depth, blk);
     grid.sync();
-    plain_prep_emit(prep, blk);
-    grid.sync();
+    plain_prep_fill(prep, blk); // beside init: both need only the final count
   }
   init_body(e, kUseHeaderRoot, blk);
   // pool_mark: nothing is inserted before the leaf-parent level

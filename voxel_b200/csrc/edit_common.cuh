@@ -367,16 +367,18 @@ static __global__ void init_kernel(EditCtx x, uint32_t root_old) {
 // Inside the single cooperative kernel of a small edit, a voxel list (one op
 // for every voxel) becomes its leaf-mask primitives without a sort: voxels
 // are aggregated into a hash table of {leaf key + 1, mask} slots (atomicCAS
-// claims a slot, atomicOr sets the voxel's bit), then every used slot is
-// appended to the primitive list.  One op for all voxels makes the order of
-// the primitives irrelevant.  Stages: clear, aggregate, emit, each followed
-// by a grid-wide barrier.
+// claims a slot and lists it, atomicOr sets the voxel's bit), then primitive
+// i is written from the i-th listed slot.  One op for all voxels makes the
+// order of the primitives irrelevant.  Stages: clear, aggregate, fill (the
+// last beside the edit's init, which only needs the count), each followed by
+// a grid-wide barrier.
 struct PlainPrep {
   const vx_voxel *edits;
   uint32_t count;       // voxels
   uint32_t op, material;
   ulonglong2 *slots;    // {packed leaf coordinates + 1 (0 = free), mask}
   uint32_t nslots;
+  uint32_t *order;      // used slots in the order they were claimed
   vx_primitive *prims;  // out: one leaf-mask primitive per touched leaf
   uint32_t *nprims;     // out: their number (the edit's device-side count)
 };
@@ -393,6 +395,7 @@ inline bool plain_prep_layout(void *ws, size_t ws_bytes, const vx_voxel *edits, 
   p.material = material;
   p.nslots = count + count / 2u + 1u; // distinct leaves <= count: load <= 2/3
   p.slots = c.take<ulonglong2>(p.nslots);
+  p.order = c.take<uint32_t>(count);
   p.prims = c.take<vx_primitive>(count);
   p.nprims = c.take<uint32_t>(1);
   if (c.offset > ws_bytes) return false;
@@ -422,6 +425,7 @@ __device__ __forceinline__ void plain_prep_aggregate(const PlainPrep &p, uint32_
       const unsigned long long old =
           atomicCAS(reinterpret_cast<unsigned long long *>(&p.slots[pos].x), 0ull, key);
       if (old == 0ull || old == key) {
+        if (old == 0ull) p.order[atomicAdd(p.nprims, 1u)] = pos; // distinct leaves <= count
         atomicOr(reinterpret_cast<unsigned long long *>(&p.slots[pos].y), bit);
         break;
       }
@@ -430,11 +434,11 @@ __device__ __forceinline__ void plain_prep_aggregate(const PlainPrep &p, uint32_
   }
 }
 
-__device__ __forceinline__ void plain_prep_emit(const PlainPrep &p, Blocks blk) {
-  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < p.nslots;
+__device__ __forceinline__ void plain_prep_fill(const PlainPrep &p, Blocks blk) {
+  const uint32_t n = *p.nprims;
+  for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<uint64_t>(blk.count) * blockDim.x) {
-    const ulonglong2 e = p.slots[i];
-    if (e.x == 0ull) continue;
+    const ulonglong2 e = p.slots[p.order[i]];
     const uint64_t k = e.x - 1ull;
     vx_primitive pr{};
     pr.c[0] = static_cast<int32_t>((k & 0x1fffffull) * 4u);
@@ -443,7 +447,7 @@ __device__ __forceinline__ void plain_prep_emit(const PlainPrep &p, Blocks blk) 
     pr.r[0] = static_cast<uint32_t>(e.y);
     pr.r[1] = static_cast<uint32_t>(e.y >> 32);
     pr.flags = vx_make_flags(kShapeLeafMask, p.op, p.material);
-    p.prims[warp_atomic_add_small(p.nprims, 1u)] = pr; // one atomic per warp
+    p.prims[i] = pr;
   }
 }
 
@@ -471,8 +475,13 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
 
   __shared__ uint32_t s_items[kGroups], s_pairs[kGroups];
   __shared__ uint32_t s_item_base, s_pair_base;
+  __shared__ bool s_room;
+  // the group's current chunk of its item's list: pair values and primitives
+  __shared__ uint32_t s_pidx[kGroups][8];
+  __shared__ vx_primitive s_prim[kGroups][8];
   const uint32_t group = threadIdx.x >> 3, c = threadIdx.x & 7u;
   const uint32_t gshift = (lane_id() >> 3) * 8u; // this group's byte in a ballot
+  const uint32_t gmask = 0xffu << gshift;        // this group's lanes
 
   for (uint64_t tile = blk.id; tile * kGroups < W; tile += blk.count) {
     const uint32_t wi = static_cast<uint32_t>(tile * kGroups) + group;
@@ -495,7 +504,13 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
     // Bit k: the list's k-th primitive cuts this child partially and comes
     // after every primitive that covers it (kept for lists of up to 32).
     uint32_t partial = 0;
-    for (uint32_t k = 0; k < it.pcount; ++k) {
+    // Eight primitives at a time: each lane of the group loads one pair and
+    // its primitive (two rounds of independent loads per chunk instead of two
+    // dependent loads per primitive), then every lane walks the chunk for its
+    // own child.  pcount is the same on the group's lanes, so they pass the
+    // group barriers together.
+    // (A terrain build's items hold its one primitive: walked in place.)
+    for (uint32_t k = 0; Terrain && k < it.pcount; ++k) {
       const uint32_t p = in_pairs[it.pstart + k];
       const uint32_t cls = pol.template classify<Terrain>(x.prims[p], world_exp, ox, oy, oz, csize);
       if (cls == VX_CELL_FULL) {
@@ -506,6 +521,29 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
         ++cnt;
         if (k < 32u) partial |= 1u << k;
       }
+    }
+    for (uint32_t k0 = 0; !Terrain && k0 < it.pcount; k0 += 8) {
+      if (k0 + c < it.pcount) {
+        const uint32_t p = in_pairs[it.pstart + k0 + c];
+        s_pidx[group][c] = p;
+        s_prim[group][c] = x.prims[p];
+      }
+      __syncwarp(gmask);
+      const uint32_t m = min(8u, it.pcount - k0);
+      for (uint32_t j = 0; j < m; ++j) {
+        const uint32_t k = k0 + j;
+        const uint32_t cls =
+            pol.template classify<Terrain>(s_prim[group][j], world_exp, ox, oy, oz, csize);
+        if (cls == VX_CELL_FULL) {
+          last_full = static_cast<int32_t>(s_pidx[group][j]);
+          cnt = 0;
+          partial = 0;
+        } else if (cls == VX_CELL_MIXED) {
+          ++cnt;
+          if (k < 32u) partial |= 1u << k;
+        }
+      }
+      __syncwarp(gmask); // the chunk is overwritten next
     }
     // Prefix sums over the 8 lanes of the group.
     uint32_t inc_items =
@@ -544,14 +582,17 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
       if (threadIdx.x == 0) {
         s_item_base = ti ? atomicAdd(&h->item_count[l + 1], ti) : 0;
         s_pair_base = tp ? atomicAdd(&h->pair_count[l + 1], tp) : 0;
-        if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap)
-          set_status(&h->status, kDevCapacity);
-        if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap)
-          set_status(&h->status, kDevCapacity);
+        // this tile's own room (an overflow elsewhere fails the edit at the
+        // next stage; writing within the buffers meanwhile is harmless)
+        bool room = true;
+        if (ti && static_cast<uint64_t>(next_base) + s_item_base + ti > x.a.item_cap) room = false;
+        if (tp && static_cast<uint64_t>(s_pair_base) + tp > x.a.pair_cap) room = false;
+        if (!room) set_status(&h->status, kDevCapacity);
+        s_room = room;
       }
     }
     __syncthreads();
-    const bool room = ld_relaxed_u32(&h->status) == kDevOk;
+    const bool room = s_room;
     const uint32_t item_off = s_item_base + s_items[group];
     const uint32_t pair_off = s_pair_base + s_pairs[group];
     __syncthreads(); // s_* are reused by the next tile
@@ -638,6 +679,9 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
     const Item it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
     const bool cached = it.pcount <= Cache; // block-uniform
+    // child t's previous content, loaded beside the walks (used unless a
+    // primitive covers the child)
+    const uint32_t old_child = t < 8 ? pol.child(l, it.old, t) : 0u;
     if (t < 8) {
       s_last[t] = -1;
       s_cnt[t] = 0;
@@ -716,14 +760,16 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
       s_cm = cm;
       s_item_base = ni ? atomicAdd(&h->item_count[l + 1], ni) : 0;
       s_pair_base = np ? atomicAdd(&h->pair_count[l + 1], np) : 0;
-      if (ni && static_cast<uint64_t>(next_base) + s_item_base + ni > x.a.item_cap)
-        set_status(&h->status, kDevCapacity);
-      if (np && static_cast<uint64_t>(s_pair_base) + np > x.a.pair_cap)
-        set_status(&h->status, kDevCapacity);
+      // this item's own room (an overflow elsewhere fails the edit at the
+      // next stage; writing within the buffers meanwhile is harmless)
+      bool room = true;
+      if (ni && static_cast<uint64_t>(next_base) + s_item_base + ni > x.a.item_cap) room = false;
+      if (np && static_cast<uint64_t>(s_pair_base) + np > x.a.pair_cap) room = false;
+      if (!room) set_status(&h->status, kDevCapacity);
       x.a.items[base + wi].child_base = next_base + s_item_base;
       x.a.items[base + wi].masks = cm | (km << 8) | (kf << 16);
       x.a.items[base + wi].pstart = __popc(cm); // every thread holds its own copy of it
-      s_room = ld_relaxed_u32(&h->status) == kDevOk;
+      s_room = room;
     }
     __syncthreads();
     const bool room = s_room; // block-uniform: it guards barriers below
@@ -732,7 +778,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
       const uint32_t k = __popc(s_cm & ((1u << t) - 1u));
       Item ci{};
       ci.cell = child_cell(it.cell, t);
-      ci.old = s_last[t] >= 0 ? s_const[t] : pol.child(l, it.old, t);
+      ci.old = s_last[t] >= 0 ? s_const[t] : old_child;
       ci.pstart = s_pair_base + s_start[t];
       ci.pcount = s_cnt[t];
       ci.result = static_cast<uint32_t>(base + wi);

@@ -515,8 +515,7 @@ __global__ void __launch_bounds__(kBlock) small_edit_kernel(EditCtx e, Tables t,
     grid.sync();
     plain_prep_aggregate(prep, t.depth, blk);
     grid.sync();
-    plain_prep_emit(prep, blk);
-    grid.sync();
+    plain_prep_fill(prep, blk); // beside init: both need only the final count
   }
   if (lead) begin_body(t);
   init_body(e, kChild, blk);
