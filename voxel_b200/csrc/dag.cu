@@ -311,10 +311,10 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
   constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
   constexpr uint32_t kGroupBits = (1u << Lanes) - 1u;
   Header *h = x.t.hdr;
-  if (edit_failed(h)) return;
   const uint32_t l = x.t.depth - 1;
-  const uint32_t W = h->item_count[l];
+  const uint32_t W = h->item_count[l]; // loaded beside the status
   const uint32_t base = h->item_off[l];
+  if (edit_failed(h)) return;
   const uint32_t *pairs = x.a.pairs[l & 1u];
   const uint32_t world_exp = x.t.depth + 2;
   const uint32_t lane = lane_id();
@@ -457,9 +457,9 @@ __device__ __forceinline__ uint32_t build_item(const Ctx &x, uint32_t l, const I
 
 __device__ __forceinline__ void build_body(Ctx x, uint32_t l, Blocks blk) {
   Header *h = x.t.hdr;
-  if (edit_failed(h)) return;
-  const uint32_t W = h->item_count[l];
+  const uint32_t W = h->item_count[l]; // loaded beside the status
   const uint32_t base = h->item_off[l];
+  if (edit_failed(h)) return;
   for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
        i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x)
     x.a.items[base + i].result = build_item(x, l, x.a.items[base + i]);
@@ -488,10 +488,16 @@ __device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l) {
 // start their own climb.
 __device__ __forceinline__ void rebuild_childless_body(Ctx x, Blocks blk) {
   Header *h = x.t.hdr;
-  if (edit_failed(h)) return;
+  // every level's counts in one round trip
+  __shared__ uint32_t s_w[kMaxDepth], s_base[kMaxDepth];
+  if (threadIdx.x < kMaxDepth) {
+    s_w[threadIdx.x] = h->item_count[threadIdx.x];
+    s_base[threadIdx.x] = h->item_off[threadIdx.x];
+  }
+  if (edit_failed(h)) return; // (its barrier also publishes s_w, s_base)
   for (uint32_t l = 0; l + 1 < x.t.depth; ++l) {
-    const uint32_t W = h->item_count[l];
-    const uint32_t base = h->item_off[l];
+    const uint32_t W = s_w[l];
+    const uint32_t base = s_base[l];
     for (uint64_t i = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
          i < W; i += static_cast<uint64_t>(blk.count) * blockDim.x) {
       const Item it = x.a.items[base + i];
@@ -524,8 +530,10 @@ constexpr uint32_t kSmallBigCache = 4096;
 // With Plain, the edit's input is a voxel list (one op): the first stages
 // turn it into leaf-mask primitives (PlainPrep) in place of the sort-based
 // preparation of the multi-launch path.
+// One block per SM runs it, so it may take up to 255 registers (the
+// default cap for 256-thread blocks, 128, made it spill).
 template <uint32_t Lanes, bool Plain>
-__global__ void __launch_bounds__(kBlock) small_edit_kernel(Ctx x, EditCtx e, PlainPrep prep,
+__global__ void __maxnreg__(255) small_edit_kernel(Ctx x, EditCtx e, PlainPrep prep,
                                                             uint32_t *status_out) {
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const Blocks blk = launch_blocks();

@@ -460,10 +460,11 @@ __device__ __forceinline__ void plain_prep_fill(const PlainPrep &p, Blocks blk) 
 template <class Policy, bool Terrain>
 __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
-  if (edit_failed(h)) return;
-  const uint32_t depth = x.depth;
+  // the level's counts load beside the status (one round trip, not two)
   const uint32_t W = h->item_count[l];
   const uint32_t base = h->item_off[l];
+  if (edit_failed(h)) return;
+  const uint32_t depth = x.depth;
   const uint32_t next_base = base + W;
   if (blk.id == 0 && threadIdx.x == 0) h->item_off[l + 1] = next_base;
   const uint32_t *in_pairs = x.a.pairs[l & 1u];
@@ -654,12 +655,15 @@ constexpr uint32_t kBigCache = 32768;
 template <class Policy, bool Terrain, uint32_t Threads, uint32_t Cache>
 __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
-  if (edit_failed(h)) return;
+  // the level's counts and this block's first listed item load beside the
+  // status (the list is read past its count only within its buffer)
   const uint32_t nbig = min(h->big_count[l], x.a.big_cap / 2u);
   const uint32_t *bigs = big_list(x.a, l);
-  const uint32_t depth = x.depth;
   const uint32_t base = h->item_off[l];
   const uint32_t next_base = base + h->item_count[l];
+  uint32_t first_wi = blk.id < x.a.big_cap / 2u ? bigs[blk.id] : 0u;
+  if (edit_failed(h)) return;
+  const uint32_t depth = x.depth;
   const uint32_t *in_pairs = x.a.pairs[l & 1u];
   uint32_t *out_pairs = x.a.pairs[(l + 1) & 1u];
   const int64_t csize = int64_t(4) << (depth - l - 1);
@@ -675,7 +679,7 @@ __device__ __forceinline__ void expand_big_body(EditCtx x, Policy pol, uint32_t 
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t / kWarp;
 
   for (uint32_t b = blk.id; b < nbig; b += blk.count) {
-    const uint32_t wi = bigs[b];
+    const uint32_t wi = b == blk.id ? first_wi : bigs[b];
     const Item it = x.a.items[base + wi];
     const Cell cell = unpack_cell(it.cell);
     const bool cached = it.pcount <= Cache; // block-uniform
