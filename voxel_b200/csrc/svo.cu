@@ -206,6 +206,10 @@ __device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk)
   const uint32_t world_exp = t.depth + 2;
   const bool mats = t.materials != 0;
   const uint32_t lane = lane_id();
+  // one item per 8 lanes: its group's chunk of primitives
+  __shared__ vx_primitive s_prim[kBlock / 8][8];
+  const uint32_t group = threadIdx.x >> 3;
+  const uint32_t gmask = 0xffu << (lane & ~7u);
   const uint64_t total = static_cast<uint64_t>(W) * 8u;
   const uint64_t stride = static_cast<uint64_t>(blk.count) * blockDim.x;
   for (uint64_t g0 = blk.id * static_cast<uint64_t>(blockDim.x) + threadIdx.x - lane;
@@ -222,37 +226,43 @@ __device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk)
       const int64_t oy = int64_t(2 * cell.y + ((c >> 1) & 1u)) * 4;
       const int64_t oz = int64_t(2 * cell.z + ((c >> 2) & 1u)) * 4;
       const uint32_t oc = pol.child(l, it.old, c);
+      // The leaf's previous content: for edits loaded beside the primitives
+      // (a covering primitive overwrites all of it, so loading it in any case
+      // changes nothing); a terrain build, whose classification needs the
+      // registers, loads it at its first partial primitive.
       uint64_t mask = 0;
       uint32_t v[16]; // 64 material bytes, 4 per word; word w holds z = w >> 2
-      bool loaded = false, touched = false;
-      for (uint32_t k = 0; k < it.pcount; ++k) {
-        const vx_primitive pr = x.prims[pairs[it.pstart + k]];
-        const uint32_t cls = pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
-        if (cls == VX_CELL_EMPTY) continue;
-        const bool add = vx_prim_op(&pr) == VX_OP_ADD;
-        if (!loaded && cls == VX_CELL_MIXED) {
-          if (oc & kChild) {
-            const uint32_t li = oc & kIndex;
-            mask = t.leaves[li];
-            if (mats) {
-              const uint4 *src = reinterpret_cast<const uint4 *>(t.mats + static_cast<size_t>(li) * 64u);
+      auto load_old = [&]() {
+        if (oc & kChild) {
+          const uint32_t li = oc & kIndex;
+          mask = t.leaves[li];
+          if (mats) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(t.mats + static_cast<size_t>(li) * 64u);
 #pragma unroll
-              for (uint32_t q = 0; q < 4; ++q) {
-                const uint4 u = src[q];
-                v[4 * q] = u.x;
-                v[4 * q + 1] = u.y;
-                v[4 * q + 2] = u.z;
-                v[4 * q + 3] = u.w;
-              }
+            for (uint32_t q = 0; q < 4; ++q) {
+              const uint4 u = src[q];
+              v[4 * q] = u.x;
+              v[4 * q + 1] = u.y;
+              v[4 * q + 2] = u.z;
+              v[4 * q + 3] = u.w;
             }
-          } else {
-            const uint32_t val = word_value(oc, mats);
-            mask = val ? ~0ull : 0ull;
-            if (mats)
-#pragma unroll
-              for (uint32_t w = 0; w < 16; ++w) v[w] = val * 0x01010101u;
           }
+        } else {
+          const uint32_t val = word_value(oc, mats);
+          mask = val ? ~0ull : 0ull;
+          if (mats)
+#pragma unroll
+            for (uint32_t w = 0; w < 16; ++w) v[w] = val * 0x01010101u;
         }
+      };
+      if (!Terrain) load_old();
+      bool loaded = !Terrain, touched = false;
+      // One primitive's effect on this lane's leaf.
+      auto apply = [&](const vx_primitive &pr) {
+        const uint32_t cls = pol.template classify<Terrain>(pr, world_exp, ox, oy, oz, 4);
+        if (cls == VX_CELL_EMPTY) return;
+        const bool add = vx_prim_op(&pr) == VX_OP_ADD;
+        if (!loaded && cls == VX_CELL_MIXED) load_old();
         loaded = true;
         touched = true;
         const uint64_t m = cls == VX_CELL_FULL ? ~0ull : leaf_mask<Terrain>(pr, world_exp, ox, oy, oz);
@@ -269,6 +279,18 @@ __device__ __forceinline__ void leafparent_body(EditCtx x, Tables t, Blocks blk)
             v[w] = (v[w] & ~bm) | ((val * 0x01010101u) & bm);
           }
         }
+      };
+      // A terrain build's items hold its single primitive, read in place; an
+      // edit's primitives come eight at a time, staged in shared memory by the
+      // item's eight lanes (independent loads, not two dependent ones per
+      // primitive).
+      for (uint32_t k = 0; Terrain && k < it.pcount; ++k) apply(x.prims[pairs[it.pstart + k]]);
+      for (uint32_t k0 = 0; !Terrain && k0 < it.pcount; k0 += 8) {
+        if (k0 + c < it.pcount) s_prim[group][c] = x.prims[pairs[it.pstart + k0 + c]];
+        __syncwarp(gmask);
+        const uint32_t m = min(8u, it.pcount - k0);
+        for (uint32_t j = 0; j < m; ++j) apply(s_prim[group][j]);
+        __syncwarp(gmask); // the chunk is overwritten next
       }
       if (!touched) {
         result = oc;
