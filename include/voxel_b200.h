@@ -127,7 +127,9 @@ vx_status vx_scan_noalloc_status(vx_stream stream);
 
 /* ------------------------------------------------------------------ sort --
  * Stable LSD radix sort ("onesweep": one all-pass digit histogram, then one
- * partition kernel per 8-bit digit with decoupled look-back), in place.
+ * partition kernel per digit with decoupled look-back), in place.  The digit
+ * is 8 bits wide unless the "sort.radix_bits" tuning knob narrows it (6 or
+ * 7 bits; keys that would then take more than 8 passes keep 8-bit digits).
  * Only the low key_bits bits of each key order the output (key_bits in
  * [1, 32] for u32 keys, [1, 64] for u64 keys), matching the KeyBits contract
  * of algo::cuda::sort::RadixSort (docs/cuda/sort.md "Configuration").

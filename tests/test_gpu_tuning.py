@@ -39,22 +39,23 @@ def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
     vals = np.arange(n, dtype=np.uint32)
     ek, ev = oracle.stable_sort_pairs(keys, vals, key_bits)
     knob = "sort.items_u32" if key_bytes == 4 else "sort.items_u64"
-    for items, early, ballots in itertools.product(vx.tuning_options(knob),
-                                                   vx.tuning_options("sort.early_counts"),
-                                                   vx.tuning_options("sort.rank_ballots")):
+    for items, early, ballots, radix in itertools.product(
+            vx.tuning_options(knob), vx.tuning_options("sort.early_counts"),
+            vx.tuning_options("sort.rank_ballots"), vx.tuning_options("sort.radix_bits")):
         vx.set_tuning(knob, items)
         vx.set_tuning("sort.early_counts", early)
         vx.set_tuning("sort.rank_ballots", ballots)
+        vx.set_tuning("sort.radix_bits", radix)
         # offset 1: the arrays start one element into a buffer (not 16-byte aligned)
         kbuf = to_dev(np.concatenate([np.zeros(offset, dt), keys]), cuda)
         vbuf = to_dev(np.concatenate([np.zeros(offset, np.uint32), vals]), cuda)
         dk, dv = kbuf[offset:], vbuf[offset:]
         vx.sort_pairs(dk, dv, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots)
-        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early, ballots)
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, radix)
+        assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev), (items, early, ballots, radix)
         dk = to_dev(keys.copy(), cuda)
         vx.sort_pairs(dk, None, key_bits)
-        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, "keys only")
+        assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, radix, "keys only")
 
 
 def rand_prims(rng, n, world, rmax):

@@ -3,10 +3,11 @@ rejection of unknown knobs and disallowed values.  Host-only calls, no GPU."""
 import voxel_b200 as vx
 
 EXPECTED = {"sort.items_u32": 16, "sort.items_u64": 10, "sort.early_counts": 0, "sort.rank_ballots": 0,
-            "edit.big_item": 16, "edit.blocks_per_sm": 32,
+            "edit.big_item": 32, "edit.blocks_per_sm": 32,
             "edit.leafparent_blocks": 5, "serve.blocks_per_sm": 4,
             "edit.leafparent_lanes": 4, "edit.small_max_prims": 256,
-            "edit.small_blocks_per_sm": 1, "edit.small_max_voxels": 16384}
+            "edit.small_blocks_per_sm": 1, "edit.small_max_voxels": 16384,
+            "sort.radix_bits": 8}
 
 
 def test_knobs_and_defaults():

@@ -6,11 +6,12 @@ Times every allowed value of each knob on a representative workload on the
 current GPU and writes the fastest settings to voxel_b200/tuning/<device>.json,
 which the library applies when it is first loaded on that kind of device:
 
-  * sort.items_u32 / sort.items_u64 / sort.early_counts / sort.rank_ballots:
-    radix-sort partition tile size (items per thread, hence blocks per SM),
-    whether a tile publishes its digit counts before or after ranking, and
-    whether keys are ranked with per-bit ballots or a shared-memory atomic
-    OR per digit; timed on 2^26
+  * sort.items_u32 / sort.items_u64 / sort.early_counts / sort.rank_ballots /
+    sort.radix_bits: radix-sort partition tile size (items per thread, hence
+    blocks per SM), whether a tile publishes its digit counts before or after
+    ranking, whether keys are ranked with per-bit ballots or a shared-memory
+    atomic OR per digit, and the digit width (6, 7 or 8 bits: 6, 5 or 4
+    passes over 32-bit keys); timed on 2^26
     u32 and 2^25 60-bit u64 key/value pairs;
   * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks /
     edit.leafparent_lanes: the primitive-list length above which a work item
@@ -81,40 +82,44 @@ def tune_sort(n32: int, n64: int, reps: int, log) -> tuple[dict, dict]:
         restore()
         vx.sort_pairs(k, v, bits, ws)
         ref_k, ref_v = k.clone(), v.clone()
-        for items, early, ballots in itertools.product(
+        for items, early, ballots, radix in itertools.product(
                 vx.tuning_options(knob), vx.tuning_options("sort.early_counts"),
-                vx.tuning_options("sort.rank_ballots")):
+                vx.tuning_options("sort.rank_ballots"), vx.tuning_options("sort.radix_bits")):
             vx.set_tuning(knob, items)
             vx.set_tuning("sort.early_counts", early)
             vx.set_tuning("sort.rank_ballots", ballots)
+            vx.set_tuning("sort.radix_bits", radix)
             restore()
             vx.sort_pairs(k, v, bits, ws)
             same = bool(torch.equal(k, ref_k) and torch.equal(v, ref_v))
             ms = _time(lambda: vx.sort_pairs(k, v, bits, ws), reps, restore) if same else None
-            times[(label, items, early, ballots)] = ms
-            log(f"  sort {label} items={items} early={early} ballots={ballots}: "
+            times[(label, items, early, ballots, radix)] = ms
+            log(f"  sort {label} items={items} early={early} ballots={ballots} radix={radix}: "
                 + (f"{ms:.3f} ms" if same else "DIFFERENT OUTPUT (not used)"))
     vx.reset_tuning()
-    # early / ballots are shared by both key widths: pick the pair with the
-    # least total time (each width at its best items); then items per width.
+    # early / ballots / digit width are shared by both key widths: pick the
+    # triple with the least total time (each width at its best items); then
+    # items per width.
     best: dict = {}
     score = {}
-    for early, ballots in itertools.product(vx.tuning_options("sort.early_counts"),
-                                            vx.tuning_options("sort.rank_ballots")):
+    for early, ballots, radix in itertools.product(vx.tuning_options("sort.early_counts"),
+                                                   vx.tuning_options("sort.rank_ballots"),
+                                                   vx.tuning_options("sort.radix_bits")):
         tot = 0.0
         for label, (_, _, knob) in cases.items():
-            cand = [times[(label, i, early, ballots)] for i in vx.tuning_options(knob)]
+            cand = [times[(label, i, early, ballots, radix)] for i in vx.tuning_options(knob)]
             cand = [c for c in cand if c is not None]
             tot = tot + min(cand) if cand else float("inf")
-        score[(early, ballots)] = tot
-    early, ballots = min(score, key=score.get)
+        score[(early, ballots, radix)] = tot
+    early, ballots, radix = min(score, key=score.get)
     best["sort.early_counts"], best["sort.rank_ballots"] = early, ballots
+    best["sort.radix_bits"] = radix
     for label, (_, _, knob) in cases.items():
-        opts = {i: times[(label, i, early, ballots)] for i in vx.tuning_options(knob)}
+        opts = {i: times[(label, i, early, ballots, radix)] for i in vx.tuning_options(knob)}
         opts = {i: t for i, t in opts.items() if t is not None}
         best[knob] = min(opts, key=opts.get)
-    return best, {f"{l} items={i} early={e} ballots={b}": t
-                  for (l, i, e, b), t in times.items()}
+    return best, {f"{l} items={i} early={e} ballots={b} radix={r}": t
+                  for (l, i, e, b, r), t in times.items()}
 
 
 def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int,
@@ -234,11 +239,13 @@ def main(argv=None) -> dict:
         sort_best, sort_t = tune_sort(1 << 26, 1 << 25, 5, log)
         edit_best, edit_t = tune_edit(12, 64, 16384, 5, log, 1 << 27, 16 << 30)
         serve_best, serve_t = tune_serve(11, 32, 400, 9, log, 1 << 27, 8 << 30)
+    vx.reset_tuning()
+    untuned = vx.tuning()  # knobs no sweep here times keep their defaults
     result = {
         "device": dev,
         "quick": bool(args.quick),
         "seconds": round(time.time() - t0, 1),
-        "knobs": {**sort_best, **edit_best, **serve_best},
+        "knobs": {**untuned, **sort_best, **edit_best, **serve_best},
         "timings_ms": {"sort": sort_t, "edit": edit_t, "serve": serve_t},
     }
     out = args.out or str(tuning_file(dev))

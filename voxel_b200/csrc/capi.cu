@@ -178,7 +178,7 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.items_u64", 10, {8, 10}, 2},
     {"sort.early_counts", 0, {0, 1}, 2},
     {"sort.rank_ballots", 0, {0, 1}, 2},
-    {"edit.big_item", 16, {16, 32, 64, 128, 256, 512}, 6},
+    {"edit.big_item", 32, {16, 32, 64, 128, 256, 512}, 6},
     {"edit.blocks_per_sm", 32, {2, 4, 8, 16, 32}, 5},
     {"edit.leafparent_blocks", 5, {4, 5, 6}, 3},
     {"serve.blocks_per_sm", 4, {2, 4, 8, 16, 32}, 5},
@@ -186,9 +186,10 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"edit.small_max_prims", 256, {0, 64, 256, 1024, 4096}, 5},
     {"edit.small_blocks_per_sm", 1, {1, 2, 4}, 3},
     {"edit.small_max_voxels", 16384, {0, 4096, 16384, 65536}, 4},
+    {"sort.radix_bits", 8, {6, 7, 8}, 3},
 };
-std::atomic<int64_t> g_values[kKnobCount] = {{16}, {10}, {0}, {0}, {16}, {32}, {5}, {4}, {4},
-                                             {256}, {1}, {16384}};
+std::atomic<int64_t> g_values[kKnobCount] = {{16}, {10}, {0}, {0}, {32}, {32}, {5}, {4}, {4},
+                                             {256}, {1}, {16384}, {8}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

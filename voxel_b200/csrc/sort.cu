@@ -29,7 +29,8 @@
 
 namespace vx::sort {
 
-constexpr uint32_t kRadixBits = 8;
+constexpr uint32_t kRadixBits = 8;    // the widest digit (256 counters per table)
+constexpr uint32_t kMinRadixBits = 6; // the narrowest the "sort.radix_bits" knob offers
 constexpr uint32_t kBins = 1u << kRadixBits;
 constexpr uint32_t kBlock = 256;
 constexpr uint32_t kWarps = kBlock / kWarp;
@@ -60,8 +61,21 @@ template <class K> inline uint32_t max_tiles(uint32_t count) {
   return ceil_div(count, kBlock * Shape<K>::kSmall);
 }
 
-inline uint32_t pass_count(uint32_t key_bits) {
-  return (key_bits + kRadixBits - 1) / kRadixBits;
+inline uint32_t pass_count(uint32_t key_bits, uint32_t radix_bits = kRadixBits) {
+  return (key_bits + radix_bits - 1) / radix_bits;
+}
+
+// The digit width of a sort: the "sort.radix_bits" knob (6 to 8 bits; the
+// tables of 256 digit counters hold any of them), or 8 when the narrower
+// digit would take more than kMaxPasses passes (64-bit keys).  Digits wider
+// than 8 bits are not offered: the decoupled look-back keeps a record per
+// digit and tile, 2^width per tile, and 2048-digit tables leave no shared
+// memory for per-warp ranking.
+inline uint32_t radix_bits_for(uint32_t key_bits) {
+  const uint32_t r = static_cast<uint32_t>(tune::get(tune::kSortRadixBits));
+  return r >= kMinRadixBits && r <= kRadixBits && pass_count(key_bits, r) <= kMaxPasses
+             ? r
+             : kRadixBits;
 }
 
 template <class K>
@@ -418,7 +432,8 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
   if (keys == nullptr && count != 0) return VX_ERR_INVALID_VALUE;
   if (count > kMaxCount) return VX_ERR_INVALID_VALUE;
   if (count <= 1) return VX_OK;
-  const uint32_t passes = pass_count(key_bits);
+  const uint32_t radix = radix_bits_for(key_bits);
+  const uint32_t passes = pass_count(key_bits, radix);
   if (workspace == nullptr || ws_bytes < workspace_bytes<K>(count, passes))
     return VX_ERR_INVALID_VALUE;
   const Layout l = carve<K>(workspace, count, passes);
@@ -426,10 +441,8 @@ vx_status sort_pairs(K *keys, uint32_t *values, uint32_t count,
 
   PassInfo info{};
   for (uint32_t p = 0; p < passes; ++p) {
-    info.shift[p] = p * kRadixBits;
-    const uint32_t bits = key_bits - p * kRadixBits < kRadixBits
-                              ? key_bits - p * kRadixBits
-                              : kRadixBits;
+    info.shift[p] = p * radix;
+    const uint32_t bits = key_bits - p * radix < radix ? key_bits - p * radix : radix;
     info.mask[p] = (1u << bits) - 1u;
   }
   const uint32_t hist_blocks =
@@ -649,7 +662,9 @@ size_t vx_sort_workspace_size(uint32_t count, uint32_t key_bytes) {
   if (count <= 1) return 0;
   if (key_bytes == 8)
     return vx::sort::workspace_bytes<uint64_t>(count, vx::sort::kMaxPasses);
-  return vx::sort::workspace_bytes<uint32_t>(count, 4);
+  // passes of 32-bit keys at the narrowest digit
+  return vx::sort::workspace_bytes<uint32_t>(count,
+                                             vx::sort::pass_count(32, vx::sort::kMinRadixBits));
 }
 
 vx_status vx_sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t count,

@@ -20,6 +20,7 @@ enum Id : uint32_t {
   kEditSmallMaxPrims, // batches of at most this many primitives run as one cooperative kernel
   kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
   kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
+  kSortRadixBits,   // radix digit width in bits: 6, 7 or 8 (passes = key bits / width)
   kKnobCount
 };
 
