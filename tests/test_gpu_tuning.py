@@ -58,6 +58,32 @@ def test_sort_variants_match_oracle(cuda, key_bytes, key_bits, n, offset):
         assert np.array_equal(dk.cpu().numpy().view(dt), ek), (items, early, ballots, radix, "keys only")
 
 
+@pytest.mark.parametrize("n", [1, 1023, 1024, 1025, 2048 * 5 + 3, 4096 * 3, 1_000_003])
+def test_scan_tile_shapes_match_oracle(cuda, n):
+    """Every prefix-sum tile shape: u32 exclusive / inclusive (aligned and
+    4 bytes into a buffer) and u64 exclusive, against the oracle, with one
+    workspace reused across shapes (its size covers the smallest tile)."""
+    rng = np.random.default_rng(n + 5)
+    x32 = rng.integers(0, 2**32, n + 1, dtype=np.uint64).astype(np.uint32)
+    x64 = rng.integers(0, 2**63, n, dtype=np.uint64)
+    ws = torch.empty(vx.lib().vx_scan_workspace_size(n + 1), dtype=torch.uint8, device=cuda)
+    for kb in vx.tuning_options("scan.tile_kb"):
+        vx.set_tuning("scan.tile_kb", kb)
+        for off in (0, 1):
+            d = to_dev(x32, cuda)[off:off + n]
+            vx.exclusive_sum(d, ws)
+            assert np.array_equal(d.cpu().numpy().view(np.uint32),
+                                  oracle.exclusive_sum(x32[off:off + n])), (kb, off)
+            assert vx.workspace_status(ws) == 0
+            d = to_dev(x32, cuda)[off:off + n]
+            vx.inclusive_sum(d, ws)
+            assert np.array_equal(d.cpu().numpy().view(np.uint32),
+                                  np.cumsum(x32[off:off + n], dtype=np.uint32)), (kb, off, "inc")
+        d = to_dev(x64, cuda)
+        vx.exclusive_sum(d, ws)
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), oracle.exclusive_sum(x64)), (kb, "u64")
+
+
 def rand_prims(rng, n, world, rmax):
     p = np.zeros(n, oracle.PRIM_DTYPE)
     for i in range(n):

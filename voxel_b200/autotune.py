@@ -13,6 +13,8 @@ which the library applies when it is first loaded on that kind of device:
     atomic OR per digit, and the digit width (6, 7 or 8 bits: 6, 5 or 4
     passes over 32-bit keys); timed on 2^26
     u32 and 2^25 60-bit u64 key/value pairs;
+  * scan.tile_kb: the prefix sum's tile (32, 16 or 8 KB, with 6, 12 or 24
+    resident blocks per SM); timed on 2^28 u32;
   * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks /
     edit.leafparent_lanes: the primitive-list length above which a work item
     is expanded by a whole block, the grid of the edit pipelines' item
@@ -120,6 +122,31 @@ def tune_sort(n32: int, n64: int, reps: int, log) -> tuple[dict, dict]:
         best[knob] = min(opts, key=opts.get)
     return best, {f"{l} items={i} early={e} ballots={b} radix={r}": t
                   for (l, i, e, b, r), t in times.items()}
+
+
+def tune_scan(n: int, reps: int, log) -> tuple[dict, dict]:
+    """scan.tile_kb: exclusive sum of n u32 (inputs larger than L2), each
+    tile shape's output compared with the default shape's."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(13)
+    data0 = torch.randint(0, 1 << 20, (n,), dtype=torch.int32, device="cuda", generator=g)
+    ws = torch.empty(lib().vx_scan_workspace_size(n), dtype=torch.uint8, device="cuda")
+    d = data0.clone()
+    vx.reset_tuning()
+    vx.exclusive_sum(d, ws)
+    ref = d.clone()
+    times: dict = {}
+    for kb in vx.tuning_options("scan.tile_kb"):
+        vx.set_tuning("scan.tile_kb", kb)
+        d.copy_(data0)
+        vx.exclusive_sum(d, ws)
+        same = bool(torch.equal(d, ref))
+        ms = _time(lambda: vx.exclusive_sum(d, ws), reps, lambda: d.copy_(data0)) if same else None
+        times[f"tile_kb={kb}"] = ms
+        log(f"  scan u32 tile_kb={kb}: " + (f"{ms:.3f} ms" if same else "DIFFERENT OUTPUT (not used)"))
+    vx.reset_tuning()
+    valid = {int(k.split("=")[1]): t for k, t in times.items() if t is not None}
+    return {"scan.tile_kb": min(valid, key=valid.get)}, times
 
 
 def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int,
@@ -233,10 +260,12 @@ def main(argv=None) -> dict:
     t0 = time.time()
     if args.quick:
         sort_best, sort_t = tune_sort(1 << 20, 1 << 19, 2, log)
+        scan_best, scan_t = tune_scan(1 << 20, 2, log)
         edit_best, edit_t = tune_edit(6, 1, 256, 2, log, 1 << 18, 64 << 20)
         serve_best, serve_t = tune_serve(6, 1, 64, 2, log, 1 << 18, 64 << 20)
     else:
         sort_best, sort_t = tune_sort(1 << 26, 1 << 25, 5, log)
+        scan_best, scan_t = tune_scan(1 << 28, 5, log)
         edit_best, edit_t = tune_edit(12, 64, 16384, 5, log, 1 << 27, 16 << 30)
         serve_best, serve_t = tune_serve(11, 32, 400, 9, log, 1 << 27, 8 << 30)
     vx.reset_tuning()
@@ -245,8 +274,8 @@ def main(argv=None) -> dict:
         "device": dev,
         "quick": bool(args.quick),
         "seconds": round(time.time() - t0, 1),
-        "knobs": {**untuned, **sort_best, **edit_best, **serve_best},
-        "timings_ms": {"sort": sort_t, "edit": edit_t, "serve": serve_t},
+        "knobs": {**untuned, **sort_best, **scan_best, **edit_best, **serve_best},
+        "timings_ms": {"sort": sort_t, "scan": scan_t, "edit": edit_t, "serve": serve_t},
     }
     out = args.out or str(tuning_file(dev))
     from pathlib import Path

@@ -187,9 +187,10 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"edit.small_blocks_per_sm", 1, {1, 2, 4}, 3},
     {"edit.small_max_voxels", 16384, {0, 4096, 16384, 65536}, 4},
     {"sort.radix_bits", 8, {6, 7, 8}, 3},
+    {"scan.tile_kb", 32, {8, 16, 32}, 3},
 };
 std::atomic<int64_t> g_values[kKnobCount] = {{16}, {10}, {0}, {0}, {32}, {32}, {5}, {4}, {4},
-                                             {256}, {1}, {16384}, {8}};
+                                             {256}, {1}, {16384}, {8}, {32}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

@@ -2,6 +2,7 @@
 // small memset of the look-back records.  See scan.cuh for the design.
 #include "profile.cuh"
 #include "scan.cuh"
+#include "tuning.cuh"
 
 #include <cuda.h>
 
@@ -44,11 +45,10 @@ template <class T> typename RecordsFor<T>::type make_records(const ScanLayout &w
 // recomputes each thread's offset inside its warp (cheaper than holding it in
 // registers, which bound the resident blocks) and writes the prefix sums
 // straight to global memory.
-template <class T, bool Inclusive, bool Vectorised>
-__global__ void __launch_bounds__(TileShape<T>::kBlock, TileShape<T>::kMinBlocks)
+template <class T, bool Inclusive, bool Vectorised, class S = TileShape<T>>
+__global__ void __launch_bounds__(S::kBlock, S::kMinBlocks)
     scan_kernel(T *__restrict__ data, uint32_t count, ScanLayout ws,
                 typename RecordsFor<T>::type records) {
-  using S = TileShape<T>;
   constexpr uint32_t kTileBytes = S::kTile * sizeof(T);
   __shared__ __align__(128) T s_data[S::kTile];
   __shared__ uint64_t s_bar;
@@ -147,9 +147,36 @@ __global__ void __launch_bounds__(TileShape<T>::kBlock, TileShape<T>::kMinBlocks
   }
 }
 
-// Tiles for the element size that needs the most records (u64).
+// Tiles for the element size and tile shape that need the most records (u64
+// in the smallest, 8 KB, tile).
 uint32_t max_tiles(uint32_t count) {
-  return ceil_div(count, TileShape<uint64_t>::kTile) + 1;
+  return ceil_div(count, TileShape<uint64_t, 64, 24>::kTile) + 1;
+}
+
+template <class T, bool Inclusive, bool Vectorised, class S>
+void launch_shape(T *data, uint32_t count, const ScanLayout &ws,
+                  const typename RecordsFor<T>::type &records, cudaStream_t stream) {
+  const uint32_t tiles = ceil_div(count, S::kTile);
+  scan_kernel<T, Inclusive, Vectorised, S><<<tiles, S::kBlock, 0, stream>>>(data, count, ws,
+                                                                            records);
+}
+
+// Tile shape from the "scan.tile_kb" knob (32, 16 or 8 KB tiles).
+template <class T, bool Inclusive, bool Vectorised>
+void launch_tuned(T *data, uint32_t count, const ScanLayout &ws,
+                  const typename RecordsFor<T>::type &records, cudaStream_t stream) {
+  switch (tune::get(tune::kScanTileKb)) {
+  case 8:
+    launch_shape<T, Inclusive, Vectorised, TileShape<T, 64, 24>>(data, count, ws, records,
+                                                                 stream);
+    break;
+  case 16:
+    launch_shape<T, Inclusive, Vectorised, TileShape<T, 128, 12>>(data, count, ws, records,
+                                                                  stream);
+    break;
+  default:
+    launch_shape<T, Inclusive, Vectorised, TileShape<T>>(data, count, ws, records, stream);
+  }
 }
 
 } // namespace
@@ -188,23 +215,21 @@ vx_status scan_launch(T *data, uint32_t count, bool inclusive, void *workspace,
   if (count == 0) return VX_OK;
   if (workspace == nullptr || workspace_bytes < workspace_size(count))
     return VX_ERR_INVALID_VALUE;
-  using S = TileShape<T>;
   const ScanLayout ws = carve(workspace, count, sizeof(T));
   VX_TRY_CUDA(cudaMemsetAsync(workspace, 0, ws.clear_bytes, stream));
-  const uint32_t tiles = ceil_div(count, S::kTile);
   const bool vec = (reinterpret_cast<uintptr_t>(data) & 15u) == 0;
   const auto records = make_records<T>(ws);
   prof::Scope scope(sizeof(T) == 4 ? "scan_u32" : "scan_u64", stream);
   if (inclusive) {
     if (vec)
-      scan_kernel<T, true, true><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+      launch_tuned<T, true, true>(data, count, ws, records, stream);
     else
-      scan_kernel<T, true, false><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+      launch_tuned<T, true, false>(data, count, ws, records, stream);
   } else {
     if (vec)
-      scan_kernel<T, false, true><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+      launch_tuned<T, false, true>(data, count, ws, records, stream);
     else
-      scan_kernel<T, false, false><<<tiles, S::kBlock, 0, stream>>>(data, count, ws, records);
+      launch_tuned<T, false, false>(data, count, ws, records, stream);
   }
   return from_cuda(cudaGetLastError());
 }

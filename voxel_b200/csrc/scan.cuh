@@ -144,10 +144,14 @@ __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
 // on B200 (2^28 u32): 64 KB tiles x 3 per SM 0.63 ms, 128 KB x 1 0.72 ms,
 // 32 KB x 4 0.82 ms, this shape 0.61 ms; 512 threads x 4 rows held in
 // registers (2 per SM) 0.93 ms.
-template <class T> struct TileShape {
-  static constexpr uint32_t kBlock = 256;
+// The "scan.tile_kb" knob offers two smaller tiles of the same 8 rows with
+// more of them resident (16 KB: 128 threads, 12 blocks / SM; 8 KB: 64
+// threads, 24 blocks / SM): about as many bytes staged per SM, but a tile
+// that waits for its predecessors' aggregates holds less of it.
+template <class T, uint32_t Block = 256, uint32_t MinBlocks = 6> struct TileShape {
+  static constexpr uint32_t kBlock = Block;
   static constexpr uint32_t kRows = 8;
-  static constexpr uint32_t kMinBlocks = 6;
+  static constexpr uint32_t kMinBlocks = MinBlocks;
   static constexpr uint32_t kPerVec = 16 / sizeof(T);
   static constexpr uint32_t kTile = kBlock * kRows * kPerVec;
   static constexpr uint32_t kWarps = kBlock / kWarp;

@@ -21,6 +21,7 @@ enum Id : uint32_t {
   kEditSmallBlocksPerSm, // resident blocks per SM of that kernel
   kEditSmallMaxVoxels, // voxel lists / leaf commands of at most this length run that way
   kSortRadixBits,   // radix digit width in bits: 6, 7 or 8 (passes = key bits / width)
+  kScanTileKb,      // prefix-sum tile in KB: 32 (256 threads), 16 (128) or 8 (64)
   kKnobCount
 };
 
