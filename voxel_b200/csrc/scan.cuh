@@ -147,7 +147,10 @@ __device__ T warp_lookback(const Records &records, uint32_t tile, T aggregate,
 // The "scan.tile_kb" knob offers two smaller tiles of the same 8 rows with
 // more of them resident (16 KB: 128 threads, 12 blocks / SM; 8 KB: 64
 // threads, 24 blocks / SM): about as many bytes staged per SM, but a tile
-// that waits for its predecessors' aggregates holds less of it.
+// that waits for its predecessors' aggregates holds less of it.  On B200
+// they are slower (2^28 u32, median of 10: 32 KB 0.578 ms, 16 KB 0.598 ms,
+// 8 KB 0.672 ms; 2^27 u64: 0.755 / 0.815 / 0.924 ms): twice or four times
+// the tiles means as many more look-backs, each a round trip to L2.
 template <class T, uint32_t Block = 256, uint32_t MinBlocks = 6> struct TileShape {
   static constexpr uint32_t kBlock = Block;
   static constexpr uint32_t kRows = 8;
