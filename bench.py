@@ -1365,6 +1365,9 @@ def run_case(args):
     import torch
     import voxel_b200 as vx
     dev = torch.device("cuda:0")
+    for setting in args.tuning:  # NAME=VALUE launch-shape knobs for this case
+        name, _, value = setting.partition("=")
+        vx.set_tuning(name, int(value))
     n = args.elements
     ms = []
     if args.case == "dag_full":
@@ -1425,6 +1428,8 @@ def main():
                                        "slab", "cuckoo", "gather"],
                     default=None)
     ap.add_argument("--elements", type=int, default=1 << 24)
+    ap.add_argument("--tuning", action="append", default=[], metavar="NAME=VALUE",
+                    help="set a launch-shape knob for a --case run (repeatable)")
     ap.add_argument("--serve-seconds", type=float, default=SERVE_SECONDS,
                     help="length of the served arrival stream (0 skips serving)")
     args = ap.parse_args()

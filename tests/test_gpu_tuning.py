@@ -103,22 +103,28 @@ def test_edit_settings_match_oracle(cuda):
     # a long primitive list at the root exercises the block-per-item path
     t = oracle.terrain(seed=4, scale=1, caves=True)
     expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
-    for big, bps, lpb, lanes in [(16, 2, 4, 4), (64, 8, 5, 8), (512, 16, 6, 4), (32, 32, 4, 8),
-                                 (32, 32, 5, 4), (16, 32, 4, 2), (32, 16, 5, 2), (16, 8, 6, 2)]:
+    # pf: the leaf-parent and expansion prefetch knobs (bit 0 and bit 1)
+    for big, bps, lpb, lanes, pf in [(16, 2, 4, 4, 0), (64, 8, 5, 8, 0), (512, 16, 6, 4, 0),
+                                     (32, 32, 4, 8, 0), (32, 32, 5, 4, 0), (16, 32, 4, 2, 0),
+                                     (32, 16, 5, 2, 0), (16, 8, 6, 2, 0), (32, 32, 5, 4, 1),
+                                     (16, 2, 4, 4, 3), (64, 16, 6, 4, 1), (32, 32, 5, 8, 2),
+                                     (32, 32, 5, 4, 3), (16, 8, 4, 2, 2)]:
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)
         vx.set_tuning("edit.leafparent_lanes", lanes)
+        vx.set_tuning("edit.leafparent_prefetch", pf & 1)
+        vx.set_tuning("edit.expand_prefetch", pf >> 1)
         d = vx.HashDag(depth, 1 << 18, 64 << 20)
         d.build_terrain(4, 1, True)
         d.apply_primitives(vx.prims_to_device(prims, cuda))
         assert d.status() == 0
-        assert oracle.DagCanon(*d.canonical()) == expect.dag(), (big, bps, lpb, lanes)
+        assert oracle.DagCanon(*d.canonical()) == expect.dag(), (big, bps, lpb, lanes, pf)
         s = vx.Svo(depth, 1 << 18, 1 << 18, arena_bytes=64 << 20)
         s.build_terrain(4, 1, True)
         s.apply_primitives(vx.prims_to_device(prims, cuda))
         assert s.status() == 0
-        assert oracle.SvoCanon(*s.canonical()) == expect.svo(), (big, bps, lpb, lanes)
+        assert oracle.SvoCanon(*s.canonical()) == expect.svo(), (big, bps, lpb, lanes, pf)
 
 
 def test_quick_autotune_writes_settings(cuda, tmp_path):

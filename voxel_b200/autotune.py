@@ -16,10 +16,11 @@ which the library applies when it is first loaded on that kind of device:
   * scan.tile_kb: the prefix sum's tile (32, 16 or 8 KB, with 6, 12 or 24
     resident blocks per SM); timed on 2^28 u32;
   * edit.big_item / edit.blocks_per_sm / edit.leafparent_blocks /
-    edit.leafparent_lanes: the primitive-list length above which a work item
-    is expanded by a whole block, the grid of the edit pipelines' item
-    kernels, and the resident blocks and threads per item of the DAG
-    leaf-parent kernel; timed on the batched Hash
+    edit.leafparent_lanes / edit.leafparent_prefetch: the primitive-list
+    length above which a work item is expanded by a whole block, the grid of
+    the edit pipelines' item kernels, and the resident blocks, threads per
+    item and next-node prefetch of the DAG leaf-parent kernel; timed on the
+    batched Hash
     DAG edit of the benchmark (16384^3 cave terrain at scale 64, 16,384
     spheres of radius log-uniform in [1, 256], 60 % add).
 
@@ -169,11 +170,12 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
     ref = work.query(pts)
     times: dict = {}
 
-    def measure(big, bps, lpb, lanes):
+    def measure(big, bps, lpb, lanes, pf=0):
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)
         vx.set_tuning("edit.leafparent_lanes", lanes)
+        vx.set_tuning("edit.leafparent_prefetch", pf)
         work.copy_from(pristine)
         work.apply_primitives(prims)
         ok = work.status() == 0 and bool(torch.equal(work.query(pts), ref))
@@ -181,7 +183,8 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
                    lambda: work.copy_from(pristine)) if ok else None
         if ok and work.status() != 0:
             ms = None
-        key = f"big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb} leafparent_lanes={lanes}"
+        key = (f"big_item={big} blocks_per_sm={bps} leafparent_blocks={lpb} "
+               f"leafparent_lanes={lanes}" + (" leafparent_prefetch=1" if pf else ""))
         times[key] = ms
         log(f"  edit {key}: "
             + (f"{ms:.3f} ms" if ms is not None else "FAILED OR DIFFERENT (not used)"))
@@ -202,18 +205,23 @@ def tune_edit(depth: int, scale: int, count: int, reps: int, log, max_nodes: int
     fastest = min(stage1.values())
     near = [k for k, t in stage1.items() if t <= 1.02 * fastest]
     big, bps = min(near, key=lambda k: (k[1], stage1[k]))
-    # Stage 2: threads per item and resident blocks of the leaf-parent
-    # kernel at that setting.
+    # Stage 2: threads per item, resident blocks and next-node prefetch of
+    # the leaf-parent kernel at that setting (the prefetch form exists for 4
+    # threads per item).
     stage2 = {}
-    for lpb, lanes in itertools.product(vx.tuning_options("edit.leafparent_blocks"),
-                                        vx.tuning_options("edit.leafparent_lanes")):
-        ms = measure(big, bps, lpb, lanes)
+    for lpb, lanes, pf in itertools.product(vx.tuning_options("edit.leafparent_blocks"),
+                                            vx.tuning_options("edit.leafparent_lanes"),
+                                            vx.tuning_options("edit.leafparent_prefetch")):
+        if pf and lanes != 4:
+            continue
+        ms = measure(big, bps, lpb, lanes, pf)
         if ms is not None:
-            stage2[(lpb, lanes)] = ms
-    lpb, lanes = min(stage2, key=stage2.get)
+            stage2[(lpb, lanes, pf)] = ms
+    lpb, lanes, pf = min(stage2, key=stage2.get)
     vx.reset_tuning()
     return {"edit.big_item": big, "edit.blocks_per_sm": bps,
-            "edit.leafparent_blocks": lpb, "edit.leafparent_lanes": lanes}, times
+            "edit.leafparent_blocks": lpb, "edit.leafparent_lanes": lanes,
+            "edit.leafparent_prefetch": pf}, times
 
 
 def tune_serve(depth: int, scale: int, batch: int, reps: int, log, max_nodes: int,

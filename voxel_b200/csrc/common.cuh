@@ -70,6 +70,11 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t *p) {
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+// Bring the line holding p into L2 (a hint: no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
   uint64_t v;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");

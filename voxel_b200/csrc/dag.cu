@@ -276,6 +276,10 @@ struct DagTree {
   __device__ uint32_t child(uint32_t l, uint32_t ref, uint32_t c) const {
     return child_ref(t, l, ref, c);
   }
+  // Bring the node `ref` of inner level l into L2 (uniform refs hold none).
+  __device__ void prefetch(uint32_t l, uint32_t ref) const {
+    if (ref > kFullRef) prefetch_l2(t.pool[l] + (ref - 2u));
+  }
   // Superseded subtrees stay in the tables until vx_dag_compact.
   __device__ void replaced(uint32_t, uint32_t, uint32_t) const {}
   template <bool Terrain>
@@ -305,7 +309,12 @@ __device__ void finish_upwards(const Ctx &x, uint32_t parent, uint32_t l);
 
 // Climb: after storing an item's result, finish its ancestors (the single
 // cooperative kernel's bottom-up build, without level barriers).
-template <bool Terrain, uint32_t Lanes, bool Climb = false>
+// Prefetch (the knob "edit.leafparent_prefetch"): beside each item's record,
+// load the old ref of the group's next item, and once the current item's old
+// leaves are requested, prefetch that next old node into L2, so the next
+// iteration's first dependent read (node header and child refs) is an L2 hit
+// instead of a DRAM round trip.
+template <bool Terrain, uint32_t Lanes, bool Climb = false, bool Prefetch = false>
 __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
   static_assert(Lanes == 2 || Lanes == 4 || Lanes == 8, "2, 4 or 8 lanes per item");
   constexpr uint32_t kPer = 8 / Lanes; // leaves per lane
@@ -335,8 +344,11 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
 #pragma unroll
     for (uint32_t j = 0; j < kPer; ++j) result[j] = old_child[j] = kEmptyRef;
     Item it{};
+    uint32_t next_old = kEmptyRef; // Prefetch: the old ref of the group's next item
     if (have) {
       it = x.a.items[base + wi];
+      if (Prefetch && q == 0 && g + stride < total)
+        next_old = x.a.items[base + static_cast<uint32_t>((g + stride) / Lanes)].old;
       const Cell cell = unpack_cell(it.cell);
       // Independent loads side by side: the first chunk's pair index and the
       // old node, then its primitive and the old leaves (read speculatively:
@@ -363,6 +375,7 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
         mask[j] = 0;
         loaded[j] = touched[j] = false;
       }
+      if (Prefetch && next_old > kFullRef) prefetch_l2(x.t.pool[l] + (next_old - 2u));
       __syncwarp(gmask); // the group's previous item no longer reads s_pr
       s_pr[grp][q] = first;
       __syncwarp(gmask);
@@ -419,9 +432,9 @@ __device__ __forceinline__ void leafparent_body(Ctx x, Blocks blk) {
   }
 }
 
-template <bool Terrain, int MinBlocks, uint32_t Lanes>
+template <bool Terrain, int MinBlocks, uint32_t Lanes, bool Prefetch = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) leafparent_kernel(Ctx x) {
-  leafparent_body<Terrain, Lanes>(x, launch_blocks());
+  leafparent_body<Terrain, Lanes, false, Prefetch>(x, launch_blocks());
 }
 
 // The rebuilt ref of one item at inner level l from its children's results.
@@ -806,6 +819,8 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
       prof::Scope sc("dag_expand", s);
       if (terrain)
         expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(e, tree, l);
+      else if (tune::get(tune::kEditExpandPrefetch) != 0)
+        expand_prefetch_kernel<DagTree><<<grid, kBlock, 0, s>>>(e, tree, l);
       else
         expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(e, tree, l);
     }
@@ -829,8 +844,15 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
     const int64_t lb = tune::get(tune::kEditLeafparentBlocks);
     const int64_t lanes = tune::get(tune::kEditLeafparentLanes);
     const bool four = lanes == 4;
+    const bool prefetch = tune::get(tune::kEditLeafparentPrefetch) != 0;
     if (terrain)
       leafparent_kernel<true, 4, 8><<<grid, kBlock, 0, s>>>(x);
+    else if (four && prefetch && lb == 6)
+      leafparent_kernel<false, 6, 4, true><<<grid, kBlock, 0, s>>>(x);
+    else if (four && prefetch && lb == 5)
+      leafparent_kernel<false, 5, 4, true><<<grid, kBlock, 0, s>>>(x);
+    else if (four && prefetch)
+      leafparent_kernel<false, 4, 4, true><<<grid, kBlock, 0, s>>>(x);
     else if (lanes == 2 && lb == 6)
       leafparent_kernel<false, 6, 2><<<grid, kBlock, 0, s>>>(x);
     else if (lanes == 2 && lb == 5)
