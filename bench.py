@@ -62,10 +62,10 @@ DAG_MAX_NODES = 1 << 27
 DAG_ARENA = 16 << 30
 PLAIN_SAMPLE = 96         # spheres of the plain per-call sample (a prefix)
 # DRAM bytes per dag_leafparent work item: an ncu capture of the small case
-# (bench.py --case dag --elements 4096: dram__bytes_read 438.6 MB +
-# dram__bytes_write 216.5 MB) divided by that launch's 5,280,796 items; the
+# (bench.py --case dag --elements 4096: dram__bytes_read 441.5 MB +
+# dram__bytes_write 217.2 MB) divided by that launch's 5,280,796 items; the
 # roofline's `traffic` scales it by the full launch's items.
-LEAFPARENT_TRAFFIC_PER_ITEM = (438.6e6 + 216.5e6) / 5280796
+LEAFPARENT_TRAFFIC_PER_ITEM = (441.5e6 + 217.2e6) / 5280796
 SVO_C3_DEPTH = 10         # 4096^3
 SVO_C3_EDITS = 65536
 SERVE_DEPTH = 11          # 8192^3

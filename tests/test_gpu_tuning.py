@@ -103,18 +103,15 @@ def test_edit_settings_match_oracle(cuda):
     # a long primitive list at the root exercises the block-per-item path
     t = oracle.terrain(seed=4, scale=1, caves=True)
     expect = oracle.Grid(depth).terrain(t).apply_prims(prims)
-    # pf: the leaf-parent and expansion prefetch knobs (bit 0 and bit 1)
     for big, bps, lpb, lanes, pf in [(16, 2, 4, 4, 0), (64, 8, 5, 8, 0), (512, 16, 6, 4, 0),
                                      (32, 32, 4, 8, 0), (32, 32, 5, 4, 0), (16, 32, 4, 2, 0),
                                      (32, 16, 5, 2, 0), (16, 8, 6, 2, 0), (32, 32, 5, 4, 1),
-                                     (16, 2, 4, 4, 3), (64, 16, 6, 4, 1), (32, 32, 5, 8, 2),
-                                     (32, 32, 5, 4, 3), (16, 8, 4, 2, 2)]:
+                                     (16, 2, 4, 4, 1), (64, 16, 6, 4, 1), (32, 32, 5, 8, 1)]:
         vx.set_tuning("edit.big_item", big)
         vx.set_tuning("edit.blocks_per_sm", bps)
         vx.set_tuning("edit.leafparent_blocks", lpb)
         vx.set_tuning("edit.leafparent_lanes", lanes)
-        vx.set_tuning("edit.leafparent_prefetch", pf & 1)
-        vx.set_tuning("edit.expand_prefetch", pf >> 1)
+        vx.set_tuning("edit.leafparent_prefetch", pf)
         d = vx.HashDag(depth, 1 << 18, 64 << 20)
         d.build_terrain(4, 1, True)
         d.apply_primitives(vx.prims_to_device(prims, cuda))

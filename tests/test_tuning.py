@@ -8,8 +8,7 @@ EXPECTED = {"sort.items_u32": 16, "sort.items_u64": 10, "sort.early_counts": 0, 
             "edit.leafparent_lanes": 4, "edit.small_max_prims": 256,
             "edit.small_blocks_per_sm": 1, "edit.small_max_voxels": 16384,
             "sort.radix_bits": 8, "scan.tile_kb": 32,
-            "edit.leafparent_prefetch": 1,
-            "edit.expand_prefetch": 0}
+            "edit.leafparent_prefetch": 1}
 
 
 def test_knobs_and_defaults():

@@ -189,10 +189,9 @@ constexpr Knob kKnobs[kKnobCount] = {
     {"sort.radix_bits", 8, {6, 7, 8}, 3},
     {"scan.tile_kb", 32, {8, 16, 32}, 3},
     {"edit.leafparent_prefetch", 1, {0, 1}, 2},
-    {"edit.expand_prefetch", 0, {0, 1}, 2},
 };
 std::atomic<int64_t> g_values[kKnobCount] = {{16}, {10}, {0}, {0}, {32}, {32}, {5}, {4}, {4},
-                                             {256}, {1}, {16384}, {8}, {32}, {1}, {0}};
+                                             {256}, {1}, {16384}, {8}, {32}, {1}};
 
 int find(const char *name) {
   if (name == nullptr) return -1;

@@ -276,10 +276,6 @@ struct DagTree {
   __device__ uint32_t child(uint32_t l, uint32_t ref, uint32_t c) const {
     return child_ref(t, l, ref, c);
   }
-  // Bring the node `ref` of inner level l into L2 (uniform refs hold none).
-  __device__ void prefetch(uint32_t l, uint32_t ref) const {
-    if (ref > kFullRef) prefetch_l2(t.pool[l] + (ref - 2u));
-  }
   // Superseded subtrees stay in the tables until vx_dag_compact.
   __device__ void replaced(uint32_t, uint32_t, uint32_t) const {}
   template <bool Terrain>
@@ -819,8 +815,6 @@ vx_status run_pipeline(vx_dag *d, const vx_primitive *prims,
       prof::Scope sc("dag_expand", s);
       if (terrain)
         expand_kernel<DagTree, true><<<grid, kBlock, 0, s>>>(e, tree, l);
-      else if (tune::get(tune::kEditExpandPrefetch) != 0)
-        expand_prefetch_kernel<DagTree><<<grid, kBlock, 0, s>>>(e, tree, l);
       else
         expand_kernel<DagTree, false><<<grid, kBlock, 0, s>>>(e, tree, l);
     }

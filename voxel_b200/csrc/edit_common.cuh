@@ -457,11 +457,7 @@ __device__ __forceinline__ void plain_prep_fill(const PlainPrep &p, Blocks blk) 
 // entirely (which resets the count of partial ones before it) and counting the
 // partial ones after it; a second walk writes those to the child's list.
 // Output space for a block's 32 items is taken with one atomicAdd per counter.
-// Prefetch (the knob "edit.expand_prefetch", policies with prefetch()):
-// beside each item's record, load the old ref of the group's item in the
-// block's next tile and, once this item's old children are requested,
-// prefetch that old node into L2 (the next tile's first dependent read).
-template <class Policy, bool Terrain, bool Prefetch = false>
+template <class Policy, bool Terrain>
 __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, Blocks blk) {
   Header *h = x.hdr;
   // the level's counts load beside the status (one round trip, not two)
@@ -493,11 +489,6 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
     const bool have = wi < W;
     Item it{};
     if (have) it = x.a.items[base + wi];
-    uint32_t next_old = 0;
-    if constexpr (Prefetch) {
-      const uint64_t nwi = (tile + blk.count) * kGroups + group;
-      if (c == 0 && nwi < W) next_old = x.a.items[base + static_cast<uint32_t>(nwi)].old;
-    }
     // Long lists were listed for expand_big (one block per item) when the
     // item was emitted.
     const bool big = have && it.pcount > x.big_item;
@@ -509,9 +500,6 @@ __device__ __forceinline__ void expand_body(EditCtx x, Policy pol, uint32_t l, B
     // The child's previous content, read before the list walk so that the
     // two chains of loads overlap (unused when a primitive covers the child).
     const uint32_t old_child = have && !big ? pol.child(l, it.old, c) : 0u;
-    if constexpr (Prefetch) {
-      if (c == 0) pol.prefetch(l, next_old);
-    }
     int32_t last_full = -1;
     uint32_t cnt = 0;
     // Bit k: the list's k-th primitive cuts this child partially and comes
@@ -649,13 +637,6 @@ template <class Policy, bool Terrain>
 __global__ void __launch_bounds__(kBlock)
     expand_kernel(EditCtx x, Policy pol, uint32_t l) {
   expand_body<Policy, Terrain>(x, pol, l, launch_blocks());
-}
-
-// The prefetching form, held to the 64 registers the plain form gets.
-template <class Policy>
-__global__ void __launch_bounds__(kBlock, 4)
-    expand_prefetch_kernel(EditCtx x, Policy pol, uint32_t l) {
-  expand_body<Policy, false, true>(x, pol, l, launch_blocks());
 }
 
 // Expansion of the long-list items of level l: one block of Threads

@@ -23,7 +23,6 @@ enum Id : uint32_t {
   kSortRadixBits,   // radix digit width in bits: 6, 7 or 8 (passes = key bits / width)
   kScanTileKb,      // prefix-sum tile in KB: 32 (256 threads), 16 (128) or 8 (64)
   kEditLeafparentPrefetch, // DAG leaf-parent kernel prefetches the next item's old node: 0 or 1
-  kEditExpandPrefetch, // DAG expansion prefetches the next tile's old nodes: 0 or 1
   kKnobCount
 };
 
