@@ -175,6 +175,25 @@ def dist_setup():
     return ws, rank, local
 
 
+def max_over_ranks(ms: float, ws: int, device) -> float:
+    """The largest of every rank's `ms` (the job's time for a timed region
+    that all replicas run between the same barriers); `ms` itself on one
+    rank.  Every rank must call it at the same point."""
+    if ws <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, ws: int, job_ms: float) -> float:
+    """Whole-job throughput of ws replicas that each processed
+    units_per_rank in the region the slowest rank timed at job_ms."""
+    return ws * units_per_rank / (job_ms / 1e3)
+
+
 # ------------------------------------------------------------ workloads --
 
 def make_inputs(torch, device, seed_base=0):
@@ -311,11 +330,7 @@ def run_sweep(args, ws, rank, local, torch, vx, device):
     dropped = cuckoo.dropped()
     part_ms = _prof(lib, "sort_partition_u64")
 
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, ws, device)
 
     # correctness spot check of the timed outputs (cheap, device-side)
     scan, k32, v32, k64, v64 = bufs[warm]
@@ -334,7 +349,7 @@ def run_sweep(args, ws, rank, local, torch, vx, device):
 
     bytes_step = (N_SCAN * BYTES_SCAN + N_SORT * BYTES_SORT_U32 + N_SORT * BYTES_SORT_U64
                   + 2 * N_HASH * (BYTES_HASH_INSERT + BYTES_HASH_LOOKUP))
-    value = ws * bytes_step * steps / (total_ms / 1e3) / 1e9
+    value = job_rate(bytes_step * steps, ws, total_ms) / 1e9
     del bufs
     torch.cuda.empty_cache()
     # A library sort beside ours, for context: torch.sort (CUB radix sort),
@@ -478,12 +493,7 @@ def run_dag(args, ws, rank, local, torch, vx, device):
     # checked against the CPU oracle after the timed legs
     canon = work.canonical() if rank == 0 else None
     rays = run_raycast(torch, vx, device, work)
-    ms = sum(a.elapsed_time(b) for a, b in ev)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], device=device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), ws, device)
     es = work.stats()
     edited_nodes = [int(es.nodes_per_level[l]) - terrain_nodes[l] for l in range(DAG_DEPTH + 1)]
     items = [int(es.items_per_level[l]) for l in range(DAG_DEPTH)]
@@ -514,7 +524,8 @@ def run_dag(args, ws, rank, local, torch, vx, device):
         if st != 0:
             raise RuntimeError(f"e2e batched edit failed: status {st}")
         e2e_ms += a.elapsed_time(b)
-    e2e = {"value": round(voxels_batch * e_steps / (e2e_ms / 1e3), 1),
+    e2e_ms = max_over_ranks(e2e_ms, ws, device)  # whole job: the slowest replica
+    e2e = {"value": round(job_rate(voxels_batch * e_steps, ws, e2e_ms), 1),
            "unit": "voxels/s", "h2d_bytes_per_step": int(prims.numel() * 4),
            "d2h_bytes_per_step": 4, "ms_per_step": round(e2e_ms / e_steps, 3)}
     # The same batch replayed as a CUDA graph (one launch per edit).
