@@ -35,3 +35,16 @@ def test_status_strings_and_workspace_sizes_need_no_device():
     assert lib.vx_scan_workspace_size(1 << 20) > 0
     assert lib.vx_sort_workspace_size(1, 4) == 0
     assert lib.vx_sort_workspace_size(1 << 20, 8) > lib.vx_sort_workspace_size(1 << 20, 4)
+
+
+def test_scan_workspace_covers_the_smallest_tile():
+    """The scan workspace holds one look-back record per tile of the
+    smallest tile shape the "scan.tile_kb" knob offers (8 KB = 1024 u64
+    elements): a u64 record is an aggregate, an inclusive value and a state
+    word (20 B), plus the tile counter and status (8 B)."""
+    lib = voxel_b200.lib()
+    smallest_kb = min(voxel_b200.tuning_options("scan.tile_kb"))
+    per_tile = smallest_kb * 1024 // 8  # u64 elements per tile
+    for n in (1, 1023, 1024, 1025, 1 << 20, 5_000_011, 1 << 28):
+        tiles = -(-n // per_tile)
+        assert lib.vx_scan_workspace_size(n) >= 8 + 20 * tiles, n
